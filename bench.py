@@ -1,0 +1,541 @@
+"""Benchmark of the B200 PySPH particle-update path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dam_break|drop|lattice3d|batched]
+
+Default workload: the 2D dam break (320,000 fluid + 12,018 wall particles,
+dx = 0.0025, summation density + Tait + momentum with Monaghan viscosity +
+gravity, predictor-corrector with the CFL time step), FP32 pair sums with
+Kahan compensation and FP64 state.  One bench step = one predictor-corrector
+step (two rebins, two density+EOS passes, two force passes, two integrator
+stages), replayed from a captured CUDA graph.  Between timed steps the L2 is
+flushed by writing a 256 MiB buffer, outside the timed events.
+
+The JSON line reports pair-interactions/s (value), steps/s, the plain FP64
+GPU path on the same workload, the density error of the FP32C path against
+FP64, the roofline of the dominant kernel, a CPU baseline (the oracle port on
+this host) and an end-to-end figure through host buffers.
+
+--impl reference times the reference algorithm's CPU implementation (the
+C restatement in oracle/, OpenMP over all host cores) on a bounded sample of
+the same workload.  Under torchrun (N > 1) every rank advances its own
+independent replica (weak scaling) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("pair-interactions/s & steps/s, FP32-comp vs FP64 GPU at <=1e-5 rho "
+          "error; bwd/fwd ratio")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dam_break",
+                    choices=["dam_break", "drop", "lattice3d", "batched"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--pair-block", type=int, default=0)
+    ap.add_argument("--stencil", type=int, default=1)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ inputs
+def workload(name):
+    from pysph_b200 import workloads as W
+    from pysph_b200.engine import fluid_scheme
+    if name == "dam_break":
+        arrays, types, params = W.dam_break()
+        return dict(scenes=[(arrays, params)], scheme=fluid_scheme(2), dim=2,
+                    desc="2D dam break, dx=0.0025, 320,000 fluid + 12,018 wall, CFL dt")
+    if name == "drop":
+        arrays, types, params = W.elliptical_drop(dx=0.025)
+        return dict(scenes=[(arrays, dict(params, dt=1e-5))], scheme=fluid_scheme(1),
+                    dim=2, desc="2D elliptical drop, dx=0.025, 5,025 particles, dt=1e-5")
+    if name == "lattice3d":
+        arrays, types, params = W.lattice3d(n=128)
+        return dict(scenes=[(arrays, dict(params, dt=1e-6))], scheme=fluid_scheme(1),
+                    dim=3, desc="3D jittered 128^3 lattice (1,048,576), h=1.2dx")
+    if name == "batched":
+        scenes = W.batched_drops(num_scenes=256, seed=0)
+        return dict(scenes=[(a, dict(p, dt=1e-5)) for a, _, p in scenes],
+                    scheme=fluid_scheme(1), dim=2,
+                    desc="256 elliptical drops, N_s ~ U[1k,20k], dt=1e-5")
+    raise ValueError(name)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# bytes per particle each kernel must move at least once (FP32C, 2D),
+# counted from the fields it reads and writes at their stored widths
+def algorithmic_bytes(dim, f32):
+    if f32 and dim == 2:
+        return {"density": 16 + 4 + 4 + 16 + 16,         # geo, cell, tag, thermo r/w
+                "force": 16 + 8 + 16 + 4 + 4 + 12,       # geo, vel, thermo, cell, tag; a, dt_fac
+                "pc_stage": 8 * 8 + 4 + 8,               # x,y,u,v r/w + x0.. ; tag; a
+                "bin": 16 + 8 + 8 + 4 * 4 + 2 * 88 + 24}  # x,y; key,slot w/r; perm; gather 88 B r/w; records
+    if f32 and dim == 3:
+        return {"density": 16 + 4 + 4 + 4 + 16 + 16,
+                "force": 16 + 4 + 16 + 16 + 4 + 4 + 16,
+                "pc_stage": 12 * 8 + 4 + 12,
+                "bin": 24 + 8 + 8 + 16 + 2 * 128 + 40}
+    w = 8
+    return {"density": dim * w + 2 * w + 4 + 4 + 3 * w,
+            "force": 2 * dim * w + 2 * w + 3 * w + 4 + 4 + (dim + 1) * w,
+            "pc_stage": 4 * dim * w + 4 + dim * w,
+            "bin": dim * w + 8 + 8 + 16 + 2 * (4 * dim + 2) * w}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local):
+    import torch
+    from pysph_b200.engine import Engine
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = workload(args.workload)
+    lanes = args.lanes or (4 if wl["dim"] == 3 else 1)
+    pb = args.pair_block or 128
+    eng = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=args.precision,
+                 stencil=args.stencil, lanes=lanes, pair_block=pb, device=dev)
+    N = eng.N
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(max(args.warmup, 3)):
+        eng.pc_step()
+    torch.cuda.synchronize()
+    eng.check_status()
+
+    graph = None
+    if not args.no_graph:
+        try:
+            s = torch.cuda.Stream(dev)
+            s.wait_stream(stream)
+            with torch.cuda.stream(s):
+                eng.pc_step()   # warm the side stream
+            stream.wait_stream(s)
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                eng.pc_step()
+            torch.cuda.synchronize()
+            graph.replay()
+            torch.cuda.synchronize()
+            eng.check_status()
+        except Exception as ex:  # report, fall back to eager launches
+            print(f"graph capture failed: {ex}", file=sys.stderr)
+            graph = None
+
+    def step():
+        if graph is not None:
+            graph.replay()
+        else:
+            eng.pc_step()
+
+    # ---- timed region: K steps, L2 flushed between them
+    eng.reset_pair_counts()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = sum(starts[i].elapsed_time(ends[i]) for i in range(args.steps))
+    eng.check_status()
+    pairs_d, pairs_f = eng.pair_counts()
+    pairs = pairs_d + pairs_f
+    ms_max = max_over_ranks(ms, world)
+    pairs_all = sum_over_ranks(pairs, world)
+    value = pairs_all / (ms_max / 1e3)
+    steps_per_s = args.steps / (ms_max / 1e3)
+
+    # ---- per-kernel timing for the roofline (one rebin + one stage)
+    kern = kernel_times(eng, flush, stream)
+    byts = algorithmic_bytes(wl["dim"], eng.f32)
+    dominant = max(kern, key=lambda k: kern[k])
+    hbm, which = peaks()
+    ach = byts[dominant] * N / (kern[dominant] * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
+            "peak": hbm, "peak_kind": which, "unit": "GB/s",
+            "frac": round(ach / hbm, 4), "traffic": None,
+            "per_kernel_ms": {k: round(v, 5) for k, v in kern.items()},
+            "bytes_per_particle": byts}
+
+    out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32+kahan pair sums, fp64 state" if eng.f32 else "fp64",
+           "data": "synthetic",
+           "config": {"workload": args.workload, "description": wl["desc"],
+                      "particles": N, "precision": args.precision,
+                      "stencil": args.stencil, "lanes": lanes, "pair_block": pb,
+                      "cuda_graph": graph is not None,
+                      "l2": "flushed (256 MiB write) between timed steps",
+                      "parallelism": f"replicas x{world}"},
+           "steps_per_s": steps_per_s,
+           "pairs_per_step": pairs / args.steps,
+           "gpu_launches": launches_per_step(eng) * args.steps,
+           "roofline": roof, "clocks": clk.summary()}
+
+    if rank == 0:
+        if args.precision == "fp32c":
+            out["fp64_gpu"] = fp64_comparison(args, wl, eng, flush, stream, dev)
+        out["e2e"] = e2e(eng, wl, stream, dev, args)
+        if not args.no_cpu:
+            out["cpu_baseline"] = cpu_baseline(args)
+    del graph
+    return out
+
+
+def launches_per_step(eng):
+    # step_begin + 2 x (bin: grid, hash, 3 scan, scatter, cell sort, reorder
+    # [+ box reset/accum when the box is stale]) + 2 x (density, force, stage)
+    return 1 + 2 * 8 + 2 * 3
+
+
+def kernel_times(eng, flush, stream, reps=20):
+    import torch
+    res = {}
+
+    def timeit(fn):
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+
+    # bin twice per timing so the buffer parity is preserved
+    res["bin"] = timeit(lambda: (eng.bin(0), eng.bin(0))) / 2
+    res["density"] = timeit(lambda: eng.density())
+    res["force"] = timeit(lambda: eng.momentum())
+    res["pc_stage"] = timeit(lambda: (eng.pc_stage(0)))
+    torch.cuda.synchronize()
+    eng.check_status()
+    return res
+
+
+def fp64_comparison(args, wl, eng32, flush, stream, dev):
+    """The plain FP64 GPU path on the same workload and the FP32C density
+    error against it after one step from the same state."""
+    import torch
+    from pysph_b200.engine import Engine
+    e64 = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision="fp64",
+                 stencil=args.stencil, lanes=eng32.lanes, pair_block=eng32.pair_block,
+                 device=dev)
+    e32 = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision="fp32c",
+                 stencil=args.stencil, lanes=eng32.lanes, pair_block=eng32.pair_block,
+                 device=dev)
+    e64.pc_step()
+    e32.pc_step()
+    err = 0.0
+    for a in range(e64.A):
+        r64 = e64.get(a, "rho")
+        r32 = e32.get(a, "rho")
+        err = max(err, float(((r32 - r64).abs() / r64.abs()).max().item()))
+    del e32
+    for _ in range(3):
+        e64.pc_step()
+    k = max(10, args.steps // 4)
+    tot = 0.0
+    e64.reset_pair_counts()
+    for _ in range(k):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e64.pc_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    pd, pf = e64.pair_counts()
+    e64.check_status()
+    return {"steps_per_s": k / (tot / 1e3), "value": (pd + pf) / (tot / 1e3),
+            "unit": "pair-interactions/s", "steps": k, "cuda_graph": False,
+            "rho_rel_err_fp32c_vs_fp64": err}
+
+
+def e2e(eng, wl, stream, dev, args):
+    """Through the public engine API with host buffers: every step uploads
+    the fluid state (x, y, u, v) from pinned host memory, advances one PC
+    step and reads back x, y, u, v, rho, p into pinned host memory."""
+    import torch
+    a = 0
+    n = eng.user_n[a]
+    ins = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in ("x", "y", "u", "v")}
+    outs = {k: torch.empty(n, dtype=torch.float64).pin_memory()
+            for k in ("x", "y", "u", "v", "rho", "p")}
+    for k in ins:
+        ins[k].copy_(eng.get(a, k).cpu())
+    dev_in = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ins}
+    k_steps = max(10, args.steps // 4)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(k_steps):
+        for k in ins:
+            dev_in[k].copy_(ins[k], non_blocking=True)
+            eng.exchange_in(a, k, dev_in[k])
+        eng.invalidate_box()
+        eng.pc_step()
+        for k in outs:
+            outs[k].copy_(eng.get(a, k), non_blocking=True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    pairs_step = None
+    return {"value": k_steps / (ms / 1e3), "unit": "steps/s",
+            "h2d_bytes_per_step": 8 * n * len(ins),
+            "d2h_bytes_per_step": 8 * n * len(outs), "steps": k_steps,
+            "note": "state uploaded and results read back every step"}
+
+
+def oracle_systems(name, threads):
+    """The workload's scenes as oracle systems (CPU legs only)."""
+    from oracle import OracleArray, OracleSystem
+    wl = workload(name)
+    sc = wl["scheme"]
+    systems = []
+    for arrays, p in wl["scenes"]:
+        oarrs = [OracleArray(f"a{i}", **{k: np.array(v, np.float64, copy=True)
+                                         for k, v in a.items()})
+                 for i, a in enumerate(arrays)]
+        systems.append((OracleSystem(
+            oarrs, dim=wl["dim"], rho_src=sc.rho_src, tait_on=sc.tait_on,
+            mom_src=sc.mom_src, step_on=sc.step_on, c0=p["c0"], rho0=p["rho0"],
+            gamma=p.get("gamma", 7.0), alpha=p["alpha"], beta=p["beta"],
+            eta=p.get("eta", 0.1), gravity=tuple(p.get("gravity", (0, 0, 0))),
+            nthreads=threads), p))
+    return wl, systems
+
+
+def oracle_step(osys, p):
+    if p.get("cfl", 0) > 0:
+        dt = osys.cfl_time_step(p["cfl"], p["c0"], p["dt_initial"])
+    else:
+        dt = p.get("dt", 1e-5)
+    osys.pc_step(dt)
+
+
+def oracle_run(name, steps, warmup, threads, max_scenes=None):
+    """Time `steps` PC steps of the oracle port after `warmup` steps."""
+    wl, systems = oracle_systems(name, threads)
+    if max_scenes:
+        systems = systems[:max_scenes]
+    for _ in range(warmup):
+        for osys, p in systems:
+            oracle_step(osys, p)
+    p0 = sum(o.pairs for o, _ in systems)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for osys, p in systems:
+            oracle_step(osys, p)
+    dt = time.perf_counter() - t0
+    pairs = sum(o.pairs for o, _ in systems) - p0
+    n = sum(sum(a.n for a in o.arrays) for o, _ in systems)
+    return {"value": pairs / dt, "ms_per_step": 1e3 * dt / steps,
+            "steps_per_s": steps / dt, "particles": n, "desc": wl["desc"]}
+
+
+def cpu_baseline(args):
+    """The oracle port (C, 1 thread) on a bounded sample of the workload:
+    a few full steps (about 10-20 s of CPU work)."""
+    steps = {"dam_break": 16, "drop": 100, "lattice3d": 1, "batched": 2}[args.workload]
+    scenes = 16 if args.workload == "batched" else None
+    r = oracle_run(args.workload, steps, 1, threads=1, max_scenes=scenes)
+    sample = f"{steps} PC steps of {r['desc']}"
+    if scenes:
+        sample += f" (first {scenes} scenes)"
+    return {"value": r["value"], "unit": "pair-interactions/s", "cores": 1,
+            "kind": "port", "sample": sample, "steps_per_s": r["steps_per_s"],
+            "cpu": cpu_model()}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    ncores = os.cpu_count() or 1
+    scenes = 32 if args.workload == "batched" else None
+    r = oracle_run(args.workload, args.steps, args.warmup, threads=ncores,
+                   max_scenes=scenes)
+    sample = f"{args.steps} PC steps of {r['desc']}"
+    if scenes:
+        sample += f" (first {scenes} scenes)"
+    res = {"value": r["value"], "ms_per_step": r["ms_per_step"], "sample": sample}
+    out = {"metric": METRIC, "impl": "reference", "value": res["value"],
+           "unit": "pair-interactions/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp64", "data": "synthetic",
+           "config": {"workload": args.workload, "sample": res["sample"]},
+           "cpu_baseline": {"value": res["value"], "unit": "pair-interactions/s",
+                            "cores": ncores, "kind": "port", "sample": res["sample"]},
+           "e2e": {"value": res["value"], "unit": "pair-interactions/s",
+                   "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return out
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if rank == 0:
+            print(json.dumps(out))
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    out = run_ours(args, rank, world, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,286 @@
+/*
+ * sphb.h -- C ABI of the B200 (sm_100a) PySPH particle-update engine.
+ *
+ * Plain C: device pointers, sizes, a CUDA stream passed as void*, int status.
+ * The library never allocates device memory: the caller owns every buffer,
+ * including the scratch workspace whose size sphb_workspace_layout reports.
+ * Calls are stream-ordered and asynchronous; concurrent use on different
+ * streams is safe when the engines (and so their buffers) are distinct.
+ *
+ * Each entry point names the reference interface it replaces (paths in the
+ * PySPH project, S/ = source/pysph/).  The reference binds its particle path
+ * through OpenCL kernel signatures assembled by SPHFunction.set_cl_kernel_args
+ * (S/sph/sph_func.pyx:295-351) plus the locator arguments of
+ * RadixSortNeighborLocator (S/base/locator.py:576-600); here each of those
+ * kernels is one entry point over an engine descriptor instead.
+ *
+ * Particle storage ("engine order"): all particles of all scenes in one SoA
+ * set, grouped in segments (scene s, array a) at fixed offsets
+ * seg_offset[s*A + a], and sorted by cell inside each segment after every
+ * sphb_bin.  idx[k] maps engine position k back to the particle's index in
+ * its ParticleArray.
+ */
+#ifndef SPHB_H
+#define SPHB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHB_MAX_ARRAYS 4
+#define SPHB_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SPHB_API __attribute__((visibility("default")))
+#else
+#define SPHB_API
+#endif
+
+/* return codes of every entry point */
+enum {
+    SPHB_OK = 0,
+    SPHB_ERR_ARG = -1,          /* bad argument (NULL, size, mode) */
+    SPHB_ERR_WORKSPACE = -2,    /* a buffer is smaller than required */
+    SPHB_ERR_CUDA = -3,         /* a launch failed (sphb_last_cuda_error) */
+    SPHB_ERR_UNSUPPORTED = -4   /* dim / precision / stencil not built */
+};
+
+/* device status word bits (sphb_engine.work.status); kernels OR them in */
+enum {
+    SPHB_ST_GRID_OVERFLOW = 1u << 0,  /* cells needed > cell_capacity */
+    SPHB_ST_NONFINITE_POS = 1u << 1,  /* NaN/Inf position met while binning */
+    SPHB_ST_OUT_OF_GRID = 1u << 2,    /* a particle fell outside its scene grid */
+    SPHB_ST_NONFINITE_RHO = 1u << 3,  /* NaN/Inf density or pressure */
+    SPHB_ST_NONFINITE_ACC = 1u << 4,  /* NaN/Inf acceleration */
+    SPHB_ST_BAD_INDEX = 1u << 5,      /* an index failed its bounds check */
+    SPHB_ST_NBR_CAPACITY = 1u << 6    /* neighbour list output too small */
+};
+
+enum { SPHB_FP64 = 0, SPHB_FP32C = 1 };   /* plain FP64 / FP32 + Kahan */
+
+/* Engine-wide configuration. */
+typedef struct {
+    int32_t dim;            /* 2 or 3 */
+    int32_t precision;      /* SPHB_FP64 or SPHB_FP32C */
+    int32_t num_scenes;     /* S >= 1 */
+    int32_t num_arrays;     /* A, arrays per scene, 1..SPHB_MAX_ARRAYS */
+    int32_t stencil;        /* R: cell size = support / R; 1 or 2 */
+    int32_t lanes;          /* lanes per dest particle in pair kernels: 1,2,4,8 */
+    int32_t pair_block;     /* threads per block of the pair kernels */
+    int32_t num_particles;  /* total over all segments */
+    int32_t cell_capacity;  /* cell table capacity (all scenes, all arrays) */
+    int32_t pad0;
+    /* the scheme, per array index (identical for every scene):
+     * SPHRho sources, MomentumEquation sources (bitmasks over arrays),
+     * TaitEquation dests and integrated arrays (bitmasks) */
+    uint32_t rho_src[SPHB_MAX_ARRAYS];
+    uint32_t mom_src[SPHB_MAX_ARRAYS];
+    uint32_t tait_on;
+    uint32_t step_on;
+} sphb_config;
+
+/* Per-scene constants, written by the host once. */
+typedef struct {
+    double cell_size;       /* radius_scale * max h / stencil */
+    double radius_scale;    /* kernel support in units of h (2, cubic spline) */
+    double h_min;           /* min h over the integrated arrays (CFL) */
+    double c0, rho0, gamma, B;   /* TaitEquation, B = c0*c0*rho0/gamma */
+    double alpha, beta, eta;     /* MomentumEquation */
+    double g[3];                 /* GravityForce */
+    double cfl, dt_initial;      /* ViscousAndForceBasedTimeStep */
+    double static_lo[3];    /* bounds of the particles the integrator never */
+    double static_hi[3];    /*   moves (+inf / -inf when there are none) */
+    int32_t use_cfl;        /* 1: dt from the CFL rule, 0: dt kept as set */
+    int32_t pad0;
+} sphb_scene;
+
+/* Per-scene state, written by the kernels (host may seed dt, t, count). */
+typedef struct {
+    int32_t lo[3];          /* global cell coordinates of local cell (0,0,0) */
+    int32_t n[3];           /* grid dimensions (n[2] == 1 in 2D) */
+    int32_t cell_base;      /* first cell key of the scene */
+    int32_t ncells;         /* cells per array of this scene */
+    unsigned long long box[6];  /* order-encoded min xyz, max xyz (next bin) */
+    double dt;              /* time step used by the next integrator stage */
+    double t;               /* simulated time */
+    long long count;        /* completed steps */
+    unsigned long long max_dtfac;  /* bits of max dt_fac (double, >= 0) */
+    unsigned long long max_acc2;   /* bits of max |a|^2 (double, >= 0) */
+} sphb_scene_state;
+
+/* Contiguous particle range inside one segment; launch unit of every
+ * particle kernel. */
+typedef struct {
+    int32_t seg;            /* s * A + a */
+    int32_t begin, end;     /* engine positions [begin, end) */
+    int32_t pad0;
+} sphb_tile;
+
+/* Double-buffered particle state (engine order, FP64 masters). */
+typedef struct {
+    double *x, *y, *z, *u, *v, *w;      /* z, w unused (may be NULL) in 2D */
+    double *x0, *y0, *z0, *u0, *v0, *w0;
+    double *m, *h;
+    int32_t *idx;           /* index inside the particle's ParticleArray */
+    int32_t *tag;           /* 0 == LocalReal (S/base/particle_array.pxd:20) */
+} sphb_buffers;
+
+/* Fields recomputed every stage, in the current engine order.  Element type
+ * T is double for SPHB_FP64, float for SPHB_FP32C. */
+typedef struct {
+    void *rho, *p, *cs;     /* T[N] (FP64 only; FP32C keeps them in thermo) */
+    void *au, *av, *aw;     /* T[N]  _a_u_1, _a_v_1, _a_w_1 */
+    void *dt_fac;           /* T[N]  MomentumEquation dt_fac */
+    void *geo;              /* FP32C float4[N]: 2D {xr,yr,h,m}, 3D {xr,yr,zr,h} */
+    void *mass;             /* FP32C 3D float[N]: m */
+    void *vel;              /* FP32C: 2D float2 {u,v}, 3D float4 {u,v,w,0} */
+    void *thermo;           /* FP32C float4[N]: {rho, p, cs, p/rho^2} */
+    int32_t *cell;          /* local cell index of each particle */
+} sphb_fields;
+
+/* Scratch; carve it from one buffer with sphb_workspace_layout. */
+typedef struct {
+    int32_t *count;         /* [cell_capacity], zero between bins */
+    int32_t *start;         /* [cell_capacity + 1] */
+    int32_t *key;           /* [N] */
+    int32_t *slot;          /* [N] */
+    int32_t *perm;          /* [N] */
+    int32_t *bsum;          /* [scan blocks + 1] */
+    int32_t *meta;          /* [8]  meta[0] = cells in use (all scenes) */
+    unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
+    unsigned long long *pairs;  /* [4]  pairs evaluated: density, force, -, - */
+} sphb_work;
+
+/* Everything the kernels see.  Tables are device pointers. */
+typedef struct {
+    sphb_config cfg;
+    const int32_t *seg_offset;      /* [S*A + 1] */
+    const sphb_scene *scene;        /* [S] */
+    sphb_scene_state *sstate;       /* [S] */
+    const sphb_tile *tiles;         /* elementwise tiles (256 particles) */
+    const sphb_tile *pair_tiles;    /* pair-kernel tiles (pair_block/lanes) */
+    int32_t num_tiles;
+    int32_t num_pair_tiles;
+    sphb_buffers buf[2];
+    sphb_fields f;
+    sphb_work work;
+} sphb_engine;
+
+/* ---- host-side helpers (no device work) ---------------------------- */
+
+SPHB_API int sphb_abi_version(void);
+
+/* Number of tiles of at most tile_size particles covering the segments
+ * seg_offset[0..nseg]; writes them to `tiles` (host memory) when non-NULL. */
+SPHB_API int sphb_make_tiles(const int32_t *seg_offset_host, int32_t nseg,
+                    int32_t tile_size, sphb_tile *tiles, int32_t *num_tiles);
+
+/* Byte offsets of the sphb_work members inside one workspace buffer
+ * (offsets[0..8] in member order, 256-byte aligned) and its total size.
+ * Replaces the buffer sizing of RadixSortManager._setup_buffers
+ * (S/base/domain_manager.py:840-899). */
+SPHB_API int sphb_workspace_layout(const sphb_config *cfg, size_t offsets[9],
+                          size_t *total_bytes);
+
+/* Last CUDA error string seen by this thread ("" when none). */
+SPHB_API const char *sphb_last_cuda_error(void);
+
+/* ---- device entry points ------------------------------------------ */
+
+/* Bounding box of every particle of every scene into sstate[].box; run it
+ * after the host writes positions.  Replaces DomainManager._find_bounds
+ * (S/base/domain_manager.py:94-131). */
+SPHB_API int sphb_box_init(const sphb_engine *e, int cur, void *stream);
+
+/* Rebin: grid per scene from the accumulated box, cell key per particle,
+ * counting sort (stable by engine position), per-cell start table, and the
+ * gather of buf[cur] into buf[cur^1] plus the FP32 pair records.  Replaces
+ * CellManager.update/_rebin_particles (S/base/cell.pyx:943-986, :1179-1300),
+ * RadixSortManager._cl_update (S/base/domain_manager.py:901-972) and the
+ * `bin` / `compute_cell_counts` kernels (S/base/radix_sort.cl:31-108).
+ * flags: SPHB_BIN_MOVE_INITIAL carries x0..w0 too; SPHB_BIN_BOX first
+ * recomputes every scene box from all particles (needed whenever no
+ * sphb_pc_stage accumulated it since the last bin).  The grid setup resets
+ * each scene's box to its static bounds and its dt_fac / |a| maxima. */
+#define SPHB_BIN_MOVE_INITIAL 1
+#define SPHB_BIN_BOX 2
+SPHB_API int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream);
+
+/* Neighbour lists of every particle of the dest arrays in dest_mask among
+ * the source arrays in src_mask, FP64 predicate r^2 < (radius_scale*h_dest)^2
+ * on the master positions (FixedDestNbrParticleLocator._update_cache,
+ * S/base/nnps.pyx:596-621).  counts[k] (engine order) always; when
+ * nbr_offsets != NULL (exclusive prefix of counts, host computed) the engine
+ * positions of the neighbours are written to nbr_index[nbr_offsets[k]..]. */
+SPHB_API int sphb_neighbors(const sphb_engine *e, int cur, uint32_t dest_mask,
+                   uint32_t src_mask, int32_t *counts,
+                   const int64_t *nbr_offsets, int32_t *nbr_index,
+                   int64_t nbr_capacity, void *stream);
+
+/* Global integer cell coordinates floor(x / cell_size) of every particle
+ * (int32[3*N], engine order); find_cell_id (S/base/cell.pyx:63-84). */
+SPHB_API int sphb_cell_coords(const sphb_engine *e, int cur, int32_t *out, void *stream);
+
+/* Summation density, optionally followed by the Tait EOS, over the dest
+ * arrays in dest_mask.  Sources per dest array come from cfg.rho_src.
+ * with_eos: p, cs from Tait for dest arrays in cfg.tait_on.  SPHRho
+ * (S/sph/funcs/density_funcs.pyx:37-73, .clt:3-53) + TaitEquation
+ * (S/sph/funcs/eos_funcs.pyx:88-129, .clt:36-65). */
+SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
+                 int with_eos, void *stream);
+
+/* Tait EOS alone on the dest arrays in dest_mask (rho already set). */
+SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *stream);
+
+/* MomentumEquation (pressure gradient + Monaghan artificial viscosity,
+ * dt_fac) over the dest arrays in dest_mask with sources cfg.mom_src,
+ * then GravityForce when with_gravity; writes au/av/aw and dt_fac and the
+ * per-scene max dt_fac and |a|^2.  S/sph/funcs/pressure_funcs.pyx:246-391,
+ * .clt:69-157; S/sph/funcs/external_force.pyx:13-62.
+ * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV). */
+SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
+                  int with_gravity, int mode, void *stream);
+
+/* Predictor-corrector stage on the integrated arrays (cfg.step_on):
+ * stage 0 = predict (save X0, X = X0 + dt/2 F), stage 1 = correct and
+ * final (X = 2 (X0 + dt/2 F) - X0), which also advances t and count.
+ * Accumulates the scene boxes for the next sphb_bin.  PositionStepping
+ * (S/sph/funcs/position_funcs.pyx:10-56) supplies F_x = u.
+ * PredictorCorrectorIntegrator.integrate (S/solver/integrator.py:646-683),
+ * step (:340-367), final_step (:632-644); integrator.cl step_array /
+ * pc_final_step (S/solver/integrator.cl:1-24). */
+SPHB_API int sphb_pc_stage(const sphb_engine *e, int cur, int stage, void *stream);
+
+/* Per-step prologue of Solver.solve (S/solver/solver.py:546-566): for
+ * every scene count += 1, then, for scenes with use_cfl, dt from
+ * ViscousAndForceBasedTimeStep.compute_time_step
+ * (S/solver/time_step_functions.py:8-57, Integrator.get_max_acceleration
+ * S/solver/integrator.py:369-412) using the max dt_fac and |a| of the last
+ * sphb_momentum; then t += dt. */
+SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
+
+/* Gather (dir 0: user order -> engine order) or scatter (dir 1: engine ->
+ * user order) one FP64 property of the particles in array `array`:
+ * engine[k] <-> user[seg-local idx[k]], for every scene's segment of that
+ * array, with user arrays concatenated over scenes (user_offset[s]).
+ * `field` names the engine field: 0..5 x..w, 6..11 x0..w0, 12 m, 13 h,
+ * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac. Fields 14..20 are
+ * scatter-only. */
+SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
+                  int dir, double *user, const int32_t *user_offset,
+                  void *stream);
+
+/* Same for the int32 tag field. */
+SPHB_API int sphb_exchange_tag(const sphb_engine *e, int cur, int array, int dir,
+                      int32_t *user, const int32_t *user_offset, void *stream);
+
+/* Write identity idx (0..n-1 inside each segment) into buf[cur].idx. */
+SPHB_API int sphb_init_index(const sphb_engine *e, int cur, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHB_H */

@@ -1,0 +1,707 @@
+/*
+ * sph_oracle.c -- CPU restatement of PySPH's FP64 particle-update path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path in
+ * pysph_b200/csrc and the timed CPU baseline of bench.py.  Nothing in the
+ * product imports, links or calls it.
+ *
+ * Each routine restates the reference algorithm it cites (paths relative to
+ * the reference project, S/ = source/pysph/), including the operand order of
+ * every floating-point expression and the order in which neighbours are
+ * visited, so that its FP64 results reproduce the reference's own Cython
+ * results bit for bit (pinned by tests/golden fixtures made by the reference
+ * itself).  Build with -ffp-contract=off: the reference is compiled for
+ * x86-64 without FMA contraction.
+ *
+ *   cubic spline W, grad W ........ S/base/kernels.pyx:349-454 (h_dim :59-66)
+ *   cell id = floor(x / cs) ........ S/base/cell.pyx:44-84
+ *   cell size = scale * max h ...... S/base/cell.pyx:911-941
+ *   stencil order (x, y, z) ........ S/base/cell.pyx:95-118, :996-1032
+ *   neighbour predicate, self last . S/base/nnps.pyx:271-356, :525-621
+ *   SPHRho ......................... S/sph/funcs/density_funcs.pyx:37-73,
+ *                                    S/sph/sph_func.pyx:513-531
+ *   TaitEquation ................... S/sph/funcs/eos_funcs.pyx:88-129
+ *   MomentumEquation ............... S/sph/funcs/pressure_funcs.pyx:246-391
+ *   SPHPressureGradient ............ S/sph/funcs/pressure_funcs.pyx:62-161
+ *   GravityForce, PositionStepping . S/sph/funcs/external_force.pyx:13-62,
+ *                                    S/sph/funcs/position_funcs.pyx:10-56
+ *   SPHFunction.eval (+= / tag) .... S/sph/sph_func.pyx:208-227
+ *   SPHCalc.sph resets ............. S/sph/sph_calc.pyx:307-331, :431-440
+ *   PredictorCorrector ............. S/solver/integrator.py:262-367, :614-683
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_MAX_ARRAYS 4
+#define ORC_PI 3.141592653589793
+
+typedef struct {
+    int64_t n;
+    double *x, *y, *z, *u, *v, *w, *m, *h, *rho, *p, *cs;
+    double *au, *av, *aw;      /* _a_u_1, _a_v_1, _a_w_1 */
+    double *ax, *ay, *az;      /* _a_x_1, _a_y_1, _a_z_1 (PositionStepping) */
+    double *dt_fac;
+    double *x0, *y0, *z0, *u0, *v0, *w0;
+    int64_t *tag;              /* 0 == LocalReal */
+} orc_array;
+
+typedef struct {
+    int32_t dim;
+    int32_t narrays;
+    double radius_scale;       /* kernel support in units of h: 2 */
+    double cell_scale;         /* cell size = cell_scale * max h: 2 */
+    uint32_t rho_src[ORC_MAX_ARRAYS];  /* SPHRho sources per dest (bitmask) */
+    uint32_t tait_on;                  /* TaitEquation dests (bitmask) */
+    uint32_t mom_src[ORC_MAX_ARRAYS];  /* MomentumEquation sources per dest */
+    uint32_t step_on;                  /* arrays stepped by the integrator */
+    double c0, rho0, gamma_eos;
+    double alpha, beta, gamma_av, eta;
+    double gx, gy, gz;
+    int32_t nthreads;
+    int32_t pad_;
+    orc_array a[ORC_MAX_ARRAYS];
+    int64_t pairs;             /* pair interactions evaluated by orc_eval */
+} orc_system;
+
+typedef struct {
+    double cell_size;
+    int32_t g0[3];
+    int32_t gn[3];
+    int64_t ncells;
+    int64_t *cstart[ORC_MAX_ARRAYS];   /* ncells + 1 */
+    int32_t *cidx[ORC_MAX_ARRAYS];     /* particle indices sorted by cell */
+    int64_t *off[ORC_MAX_ARRAYS][ORC_MAX_ARRAYS];
+    int32_t *idx[ORC_MAX_ARRAYS][ORC_MAX_ARRAYS];
+    int64_t nn[ORC_MAX_ARRAYS];        /* dest sizes the lists were built for */
+} orc_nnps;
+
+/* ------------------------------------------------------------------ */
+/* cubic spline (S/base/kernels.pyx:349-454)                          */
+/* ------------------------------------------------------------------ */
+static double kfac_unit(int dim)
+{
+    /* _fac(1.0), S/base/kernels.pyx:441-447 */
+    double h = 1.0;
+    if (dim == 1) return (2. / 3.) / h;
+    if (dim == 2) return 10 / (7 * ORC_PI) / (h * h);
+    return 1. / ORC_PI / (h * h * h);
+}
+
+static double h_dim(double h, int dim)
+{
+    if (dim == 1) return 1 / h;
+    if (dim == 2) return 1 / (h * h);
+    return 1 / (h * h * h);
+}
+
+/* CubicSplineKernel.function(pa, pb, h) */
+static double cs_function(double pax, double pay, double paz,
+                          double pbx, double pby, double pbz,
+                          double h, int dim, double kfac)
+{
+    double rab = sqrt((pax - pbx) * (pax - pbx) + (pay - pby) * (pay - pby) +
+                      (paz - pbz) * (paz - pbz));
+    double q = rab / h;
+    double val;
+    double fac = h_dim(h, dim) * kfac;
+    if (q > 2.0)
+        val = 0.0;
+    else if (q > 1.0)
+        val = 0.25 * (2 - q) * (2 - q) * (2 - q);
+    else
+        val = 1 - 1.5 * (q * q) * (1 - 0.5 * q);
+    return val * fac;
+}
+
+/* CubicSplineKernel.gradient(pa, pb, h) */
+static void cs_gradient(double pax, double pay, double paz,
+                        double pbx, double pby, double pbz,
+                        double h, int dim, double kfac, double *g)
+{
+    double rab = sqrt((pax - pbx) * (pax - pbx) + (pay - pby) * (pay - pby) +
+                      (paz - pbz) * (paz - pbz));
+    double q = rab / h;
+    double val = 0.0;
+    double fac = h_dim(h, dim) * kfac;
+    double rx = pax - pbx, ry = pay - pby, rz = paz - pbz;
+    if (q > 2.0) {
+    } else if (q >= 1.0) {
+        val = -0.75 * (2 - q) * (2 - q) / (h * rab);
+    } else if (q > 1e-14) {
+        val = 3.0 * (0.75 * q - 1) / (h * h);
+    }
+    g[0] = rx * (val * fac);
+    g[1] = ry * (val * fac);
+    g[2] = rz * (val * fac);
+}
+
+double orc_kernel_w(double dx, double dy, double dz, double h, int dim)
+{
+    return cs_function(dx, dy, dz, 0.0, 0.0, 0.0, h, dim, kfac_unit(dim));
+}
+
+void orc_kernel_grad(double dx, double dy, double dz, double h, int dim,
+                     double *g)
+{
+    cs_gradient(dx, dy, dz, 0.0, 0.0, 0.0, h, dim, kfac_unit(dim), g);
+}
+
+/* ------------------------------------------------------------------ */
+/* binning (S/base/cell.pyx:44-84, :911-941, :1229-1300)              */
+/* ------------------------------------------------------------------ */
+static inline int real_to_int(double real_val, double step)
+{
+    return (int)floor(real_val / step);
+}
+
+void orc_cell_ids(int64_t n, const double *x, const double *y,
+                  const double *z, double cell_size, int32_t *out)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        out[3 * i + 0] = real_to_int(x[i], cell_size);
+        out[3 * i + 1] = real_to_int(y[i], cell_size);
+        out[3 * i + 2] = real_to_int(z[i], cell_size);
+    }
+}
+
+orc_nnps *orc_nnps_new(void)
+{
+    return (orc_nnps *)calloc(1, sizeof(orc_nnps));
+}
+
+static void nnps_clear(orc_nnps *c)
+{
+    for (int a = 0; a < ORC_MAX_ARRAYS; ++a) {
+        free(c->cstart[a]);
+        free(c->cidx[a]);
+        c->cstart[a] = NULL;
+        c->cidx[a] = NULL;
+        for (int b = 0; b < ORC_MAX_ARRAYS; ++b) {
+            free(c->off[a][b]);
+            free(c->idx[a][b]);
+            c->off[a][b] = NULL;
+            c->idx[a][b] = NULL;
+        }
+    }
+}
+
+void orc_nnps_free(orc_nnps *c)
+{
+    if (!c) return;
+    nnps_clear(c);
+    free(c);
+}
+
+double orc_cell_size(const orc_nnps *c) { return c->cell_size; }
+
+void orc_grid(const orc_nnps *c, int32_t *g0, int32_t *gn)
+{
+    for (int d = 0; d < 3; ++d) {
+        g0[d] = c->g0[d];
+        gn[d] = c->gn[d];
+    }
+}
+
+/* CellManager.compute_cell_size: cell_size = radius_scale * max_h over all
+ * binned arrays; 0 -> 1 (S/base/cell.pyx:911-941). */
+static double compute_cell_size(const orc_system *s)
+{
+    double max_h = -INFINITY;
+    int any = 0;
+    for (int a = 0; a < s->narrays; ++a)
+        for (int64_t i = 0; i < s->a[a].n; ++i) {
+            if (!any || s->a[a].h[i] > max_h) max_h = s->a[a].h[i];
+            any = 1;
+        }
+    if (!any) max_h = 0.0;
+    double cs = s->cell_scale * max_h;
+    if (cs == 0.0) cs = 1.0;
+    return cs;
+}
+
+static int bin_all(const orc_system *s, orc_nnps *c)
+{
+    double cs = c->cell_size;
+    int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX};
+    int32_t hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    int any = 0;
+    for (int a = 0; a < s->narrays; ++a) {
+        const orc_array *A = &s->a[a];
+        for (int64_t i = 0; i < A->n; ++i) {
+            int32_t id[3] = {real_to_int(A->x[i], cs), real_to_int(A->y[i], cs),
+                             real_to_int(A->z[i], cs)};
+            for (int d = 0; d < 3; ++d) {
+                if (id[d] < lo[d]) lo[d] = id[d];
+                if (id[d] > hi[d]) hi[d] = id[d];
+            }
+            any = 1;
+        }
+    }
+    if (!any) {
+        for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = 0; }
+    }
+    int64_t ncells = 1;
+    for (int d = 0; d < 3; ++d) {
+        c->g0[d] = lo[d];
+        c->gn[d] = hi[d] - lo[d] + 1;
+        ncells *= c->gn[d];
+    }
+    if (ncells > ((int64_t)1 << 28)) return -2;
+    c->ncells = ncells;
+    for (int a = 0; a < s->narrays; ++a) {
+        const orc_array *A = &s->a[a];
+        int64_t *start = (int64_t *)calloc((size_t)ncells + 1, sizeof(int64_t));
+        int32_t *idx = (int32_t *)malloc(sizeof(int32_t) * (size_t)(A->n > 0 ? A->n : 1));
+        int64_t *key = (int64_t *)malloc(sizeof(int64_t) * (size_t)(A->n > 0 ? A->n : 1));
+        if (!start || !idx || !key) { free(start); free(idx); free(key); return -3; }
+        for (int64_t i = 0; i < A->n; ++i) {
+            int64_t ix = real_to_int(A->x[i], cs) - lo[0];
+            int64_t iy = real_to_int(A->y[i], cs) - lo[1];
+            int64_t iz = real_to_int(A->z[i], cs) - lo[2];
+            key[i] = (ix * c->gn[1] + iy) * c->gn[2] + iz;
+            start[key[i] + 1]++;
+        }
+        for (int64_t k = 0; k < ncells; ++k) start[k + 1] += start[k];
+        int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * (size_t)ncells);
+        if (!cur) { free(start); free(idx); free(key); return -3; }
+        memcpy(cur, start, sizeof(int64_t) * (size_t)ncells);
+        /* ascending particle index inside each cell, as _insert_particles
+         * appends indices in order (S/base/cell.pyx:1272-1291) */
+        for (int64_t i = 0; i < A->n; ++i) idx[cur[key[i]]++] = (int32_t)i;
+        free(cur);
+        free(key);
+        c->cstart[a] = start;
+        c->cidx[a] = idx;
+    }
+    return 0;
+}
+
+/* One dest particle's neighbours in source array `sa`, in the reference
+ * order: stencil cells x-major, then y, then z (construct_immediate_neighbor_
+ * list), ascending index inside a cell, strict d2 < (scale*h)^2, then self
+ * swapped to the last slot when source is dest (S/base/nnps.pyx:612-619).
+ * Returns the count; writes up to `cap` indices when out != NULL. */
+static int64_t query(const orc_system *s, const orc_nnps *c, int da, int sa,
+                     int64_t i, int32_t *out)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    double cs = c->cell_size;
+    double px = D->x[i], py = D->y[i], pz = D->z[i];
+    double radius = D->h[i] * s->radius_scale;
+    double radius2 = radius * radius;
+    int dist = (int)ceil(radius / cs);
+    int32_t cx = real_to_int(px, cs), cy = real_to_int(py, cs),
+            cz = real_to_int(pz, cs);
+    int64_t cnt = 0;
+    for (int di = -dist; di <= dist; ++di) {
+        int64_t ix = (int64_t)cx + di - c->g0[0];
+        if (ix < 0 || ix >= c->gn[0]) continue;
+        for (int dj = -dist; dj <= dist; ++dj) {
+            int64_t iy = (int64_t)cy + dj - c->g0[1];
+            if (iy < 0 || iy >= c->gn[1]) continue;
+            for (int dk = -dist; dk <= dist; ++dk) {
+                int64_t iz = (int64_t)cz + dk - c->g0[2];
+                if (iz < 0 || iz >= c->gn[2]) continue;
+                int64_t key = (ix * c->gn[1] + iy) * c->gn[2] + iz;
+                for (int64_t k = c->cstart[sa][key]; k < c->cstart[sa][key + 1]; ++k) {
+                    int32_t j = c->cidx[sa][k];
+                    double sx = S->x[j], sy = S->y[j], sz = S->z[j];
+                    double d2 = (sx - px) * (sx - px) + (sy - py) * (sy - py) +
+                                (sz - pz) * (sz - pz);
+                    if (d2 < radius2) {
+                        if (out) out[cnt] = j;
+                        cnt++;
+                    }
+                }
+            }
+        }
+    }
+    if (out && da == sa) {
+        for (int64_t j = 0; j < cnt - 1; ++j) {
+            if (out[j] == (int32_t)i) {
+                out[j] = out[cnt - 1];
+                out[cnt - 1] = (int32_t)i;
+                break;
+            }
+        }
+    }
+    return cnt;
+}
+
+static int build_lists(const orc_system *s, orc_nnps *c, int da, int sa)
+{
+    int64_t n = s->a[da].n;
+    int64_t *off = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    if (!off) return -3;
+    off[0] = 0;
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < n; ++i) off[i + 1] = query(s, c, da, sa, i, NULL);
+    for (int64_t i = 0; i < n; ++i) off[i + 1] += off[i];
+    int32_t *idx = (int32_t *)malloc(sizeof(int32_t) * (size_t)(off[n] > 0 ? off[n] : 1));
+    if (!idx) { free(off); return -3; }
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < n; ++i) query(s, c, da, sa, i, idx + off[i]);
+    c->off[da][sa] = off;
+    c->idx[da][sa] = idx;
+    c->nn[da] = n;
+    return 0;
+}
+
+static void set_threads(const orc_system *s)
+{
+#ifdef _OPENMP
+    if (s->nthreads > 0) omp_set_num_threads(s->nthreads);
+#else
+    (void)s;
+#endif
+}
+
+/* Particles.update(): recompute the cell size, rebin every array and rebuild
+ * the cached neighbour lists of every (dest, source) pair in pair_mask
+ * (bit dest*4 + source). */
+int orc_update(const orc_system *s, orc_nnps *c, uint32_t pair_mask)
+{
+    set_threads(s);
+    nnps_clear(c);
+    c->cell_size = compute_cell_size(s);
+    int rc = bin_all(s, c);
+    if (rc) return rc;
+    for (int da = 0; da < s->narrays; ++da)
+        for (int sa = 0; sa < s->narrays; ++sa)
+            if (pair_mask & (1u << (da * 4 + sa))) {
+                rc = build_lists(s, c, da, sa);
+                if (rc) return rc;
+            }
+    return 0;
+}
+
+int64_t orc_nbr_total(const orc_nnps *c, int da, int sa)
+{
+    if (!c->off[da][sa]) return -1;
+    return c->off[da][sa][c->nn[da]];
+}
+
+int orc_nbr_copy(const orc_nnps *c, int da, int sa, int64_t *off, int32_t *idx)
+{
+    if (!c->off[da][sa]) return -1;
+    int64_t n = c->nn[da];
+    memcpy(off, c->off[da][sa], sizeof(int64_t) * (size_t)(n + 1));
+    memcpy(idx, c->idx[da][sa], sizeof(int32_t) * (size_t)c->off[da][sa][n]);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* SPH functions, function-level semantics of SPHFunction.eval:        */
+/* out[i] += result for LocalReal dests, out[i] = 0 otherwise.          */
+/* ------------------------------------------------------------------ */
+int orc_sph_rho(const orc_system *s, const orc_nnps *c, int da, int sa,
+                double *out1)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kfac_unit(dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = 0; continue; }
+        double nr = 0.0;
+        double ha = D->h[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double hb = S->h[j];
+            double hab = 0.5 * (ha + hb);
+            double w = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j],
+                                   S->z[j], hab, dim, kfac);
+            nr += w * S->m[j];
+        }
+        out1[i] += nr;
+    }
+    return 0;
+}
+
+int orc_tait(const orc_system *s, int da, double co, double ro, double gamma,
+             double *out1, double *out2)
+{
+    const orc_array *D = &s->a[da];
+    double B = co * co * ro / gamma;
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = 0; out2[i] = 0; continue; }
+        double rhoa = D->rho[i];
+        double ratio = rhoa / ro;
+        double gamma2 = 0.5 * (gamma - 1.0);
+        double tmp = pow(ratio, gamma);
+        out1[i] += (tmp - 1.0) * B;
+        out2[i] += pow(ratio, gamma2) * co;
+    }
+    return 0;
+}
+
+int orc_momentum(const orc_system *s, const orc_nnps *c, int da, int sa,
+                 double alpha, double beta, double eta, double *out1,
+                 double *out2, double *out3, double *dt_fac)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kfac_unit(dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = out2[i] = out3[i] = 0; continue; }
+        double nr0 = 0.0, nr1 = 0.0, nr2 = 0.0;
+        double ha = D->h[i];
+        double ca = D->cs[i];
+        double Pa = D->p[i];
+        double rhoa = D->rho[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double hb = S->h[j];
+            double hab = 0.5 * (ha + hb);
+            double cb = S->cs[j];
+            double rx = D->x[i] - S->x[j];
+            double ry = D->y[i] - S->y[j];
+            double rz = D->z[i] - S->z[j];
+            double vx = D->u[i] - S->u[j];
+            double vy = D->v[i] - S->v[j];
+            double vz = D->w[i] - S->w[j];
+            double dot = vx * rx + vy * ry + vz * rz;
+            double rab2 = rx * rx + ry * ry + rz * rz;
+            double dtf = fabs(hab * dot / (rab2 + eta * eta * hab * hab));
+            dt_fac[i] = dt_fac[i] > dtf ? dt_fac[i] : dtf;
+            double Pb = S->p[j];
+            double rhob = S->rho[j];
+            double mb = S->m[j];
+            double rhoa2 = 1.0 / (rhoa * rhoa);
+            double rhob2 = 1.0 / (rhob * rhob);
+            double tmp = Pa * rhoa2 + Pb * rhob2;
+            double piab = 0;
+            if (dot < 0) {
+                double cab = 0.5 * (ca + cb);
+                double rhoab = 0.5 * (rhoa + rhob);
+                double mu = hab * dot;
+                mu /= (rab2 + eta * eta * hab * hab);
+                piab = -alpha * cab * mu + beta * mu * mu;
+                piab /= rhoab;
+            }
+            tmp += piab;
+            tmp *= -mb;
+            double g[3];
+            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                        hab, dim, kfac, g);
+            nr0 += tmp * g[0];
+            nr1 += tmp * g[1];
+            nr2 += tmp * g[2];
+        }
+        out1[i] += nr0;
+        out2[i] += nr1;
+        out3[i] += nr2;
+    }
+    return 0;
+}
+
+int orc_pgrad(const orc_system *s, const orc_nnps *c, int da, int sa,
+              double *out1, double *out2, double *out3)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kfac_unit(dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = out2[i] = out3[i] = 0; continue; }
+        double nr0 = 0.0, nr1 = 0.0, nr2 = 0.0;
+        double ha = D->h[i];
+        double pa = D->p[i];
+        double rhoa = D->rho[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double mb = S->m[j];
+            double rhob = S->rho[j];
+            double pb = S->p[j];
+            double hb = S->h[j];
+            double h = 0.5 * (ha + hb);
+            double rhoa2 = 1.0 / (rhoa * rhoa);
+            double rhob2 = 1.0 / (rhob * rhob);
+            double temp = -mb * (pa * rhoa2 + pb * rhob2);
+            double artificial_stress = 0.0;
+            temp = temp + artificial_stress;
+            double g[3];
+            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                        h, dim, kfac, g);
+            nr0 += temp * g[0];
+            nr1 += temp * g[1];
+            nr2 += temp * g[2];
+        }
+        out1[i] += nr0;
+        out2[i] += nr1;
+        out3[i] += nr2;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* the pinned scheme: SPHRho -> Tait -> MomentumEquation -> Gravity ->  */
+/* PositionStepping, evaluated as Integrator.eval does                  */
+/* ------------------------------------------------------------------ */
+static uint32_t pair_mask_of(const orc_system *s)
+{
+    uint32_t mask = 0;
+    for (int d = 0; d < s->narrays; ++d)
+        for (int a = 0; a < s->narrays; ++a)
+            if ((s->rho_src[d] | s->mom_src[d]) & (1u << a))
+                mask |= 1u << (d * 4 + a);
+    return mask;
+}
+
+uint32_t orc_scheme_pairs(const orc_system *s) { return pair_mask_of(s); }
+
+int orc_eval(orc_system *s, const orc_nnps *c)
+{
+    int rc;
+    /* SPHRho: non-integrating calc resets rho, _tmpy, _tmpz then adds each
+     * source in array order */
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->rho_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) D->rho[i] = 0.0;
+        for (int a = 0; a < s->narrays; ++a)
+            if (s->rho_src[d] & (1u << a)) {
+                rc = orc_sph_rho(s, c, d, a, D->rho);
+                if (rc) return rc;
+                s->pairs += c->off[d][a][D->n];
+            }
+    }
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->tait_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) { D->p[i] = 0.0; D->cs[i] = 0.0; }
+        orc_tait(s, d, s->c0, s->rho0, s->gamma_eos, D->p, D->cs);
+    }
+    /* accelerations were reset by reset_accelerations; dt_fac by to_reset */
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->mom_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) D->dt_fac[i] = 0.0;
+        for (int a = 0; a < s->narrays; ++a)
+            if (s->mom_src[d] & (1u << a)) {
+                rc = orc_momentum(s, c, d, a, s->alpha, s->beta, s->eta, D->au,
+                                  D->av, D->aw, D->dt_fac);
+                if (rc) return rc;
+                s->pairs += c->off[d][a][D->n];
+            }
+    }
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->step_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) {
+            if (D->tag[i] != 0) {
+                D->au[i] = D->av[i] = D->aw[i] = 0;
+                D->ax[i] = D->ay[i] = D->az[i] = 0;
+                continue;
+            }
+            D->au[i] += s->gx;
+            D->av[i] += s->gy;
+            D->aw[i] += s->gz;
+            D->ax[i] = D->u[i];
+            D->ay[i] = D->v[i];
+            D->az[i] = D->w[i];
+        }
+    }
+    return 0;
+}
+
+static void reset_acc(const orc_system *s)
+{
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->step_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) {
+            D->au[i] = D->av[i] = D->aw[i] = 0.0;
+            D->ax[i] = D->ay[i] = D->az[i] = 0.0;
+        }
+    }
+}
+
+/* Integrator.step: prop = initial + step_arr * dt (numpy, no FMA) */
+static void half_step(const orc_system *s, double dt)
+{
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->step_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) {
+            double t;
+            t = D->ax[i] * dt; D->x[i] = D->x0[i] + t;
+            t = D->ay[i] * dt; D->y[i] = D->y0[i] + t;
+            t = D->au[i] * dt; D->u[i] = D->u0[i] + t;
+            t = D->av[i] * dt; D->v[i] = D->v0[i] + t;
+            if (s->dim == 3) {
+                t = D->az[i] * dt; D->z[i] = D->z0[i] + t;
+                t = D->aw[i] * dt; D->w[i] = D->w0[i] + t;
+            }
+        }
+    }
+}
+
+/* One PredictorCorrectorIntegrator.integrate(dt) preceded by the
+ * particles.update() of Solver.solve (S/solver/solver.py:546-566). */
+int orc_pc_step(orc_system *s, orc_nnps *c, double dt)
+{
+    uint32_t pm = pair_mask_of(s);
+    int rc = orc_update(s, c, pm);
+    if (rc) return rc;
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->step_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        memcpy(D->x0, D->x, sizeof(double) * (size_t)D->n);
+        memcpy(D->y0, D->y, sizeof(double) * (size_t)D->n);
+        memcpy(D->u0, D->u, sizeof(double) * (size_t)D->n);
+        memcpy(D->v0, D->v, sizeof(double) * (size_t)D->n);
+        if (s->dim == 3) {
+            memcpy(D->z0, D->z, sizeof(double) * (size_t)D->n);
+            memcpy(D->w0, D->w, sizeof(double) * (size_t)D->n);
+        }
+    }
+    double half = dt / 2;
+    reset_acc(s);
+    rc = orc_eval(s, c);
+    if (rc) return rc;
+    half_step(s, half);
+    rc = orc_update(s, c, pm);
+    if (rc) return rc;
+    reset_acc(s);
+    rc = orc_eval(s, c);
+    if (rc) return rc;
+    half_step(s, half);
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!(s->step_on & (1u << d))) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) {
+            D->x[i] = 2 * D->x[i] - D->x0[i];
+            D->y[i] = 2 * D->y[i] - D->y0[i];
+            D->u[i] = 2 * D->u[i] - D->u0[i];
+            D->v[i] = 2 * D->v[i] - D->v0[i];
+            if (s->dim == 3) {
+                D->z[i] = 2 * D->z[i] - D->z0[i];
+                D->w[i] = 2 * D->w[i] - D->w0[i];
+            }
+        }
+    }
+    return 0;
+}

@@ -1,0 +1,168 @@
+"""ctypes binding of libsphb.so (include/sphb.h).
+
+The structures below mirror the C ABI field by field; tests/test_abi.py
+checks their sizes and offsets against the header compiled by gcc.  Loading
+fails loudly when the library is missing: there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsphb.so")
+
+MAX_ARRAYS = 4
+FP64, FP32C = 0, 1
+BIN_MOVE_INITIAL, BIN_BOX = 1, 2
+
+OK = 0
+ERRORS = {-1: "bad argument", -2: "workspace too small", -3: "CUDA launch failed",
+          -4: "unsupported configuration"}
+
+ST_GRID_OVERFLOW = 1 << 0
+ST_NONFINITE_POS = 1 << 1
+ST_OUT_OF_GRID = 1 << 2
+ST_NONFINITE_RHO = 1 << 3
+ST_NONFINITE_ACC = 1 << 4
+ST_BAD_INDEX = 1 << 5
+ST_NBR_CAPACITY = 1 << 6
+STATUS_NAMES = {
+    ST_GRID_OVERFLOW: "cell grid larger than cell_capacity",
+    ST_NONFINITE_POS: "non-finite particle position",
+    ST_OUT_OF_GRID: "particle outside its scene grid",
+    ST_NONFINITE_RHO: "non-finite density or pressure",
+    ST_NONFINITE_ACC: "non-finite acceleration",
+    ST_BAD_INDEX: "index failed a bounds check",
+    ST_NBR_CAPACITY: "neighbour list output too small",
+}
+
+# engine field ids of sphb_exchange
+FIELDS = {"x": 0, "y": 1, "z": 2, "u": 3, "v": 4, "w": 5,
+          "_x0": 6, "_y0": 7, "_z0": 8, "_u0": 9, "_v0": 10, "_w0": 11,
+          "m": 12, "h": 13, "rho": 14, "p": 15, "cs": 16,
+          "_a_u_1": 17, "_a_v_1": 18, "_a_w_1": 19, "dt_fac": 20}
+
+i32, u32, f64, vp = ctypes.c_int32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p
+u64, i64 = ctypes.c_uint64, ctypes.c_int64
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("dim", i32), ("precision", i32), ("num_scenes", i32),
+                ("num_arrays", i32), ("stencil", i32), ("lanes", i32),
+                ("pair_block", i32), ("num_particles", i32),
+                ("cell_capacity", i32), ("pad0", i32),
+                ("rho_src", u32 * MAX_ARRAYS), ("mom_src", u32 * MAX_ARRAYS),
+                ("tait_on", u32), ("step_on", u32)]
+
+
+class Scene(ctypes.Structure):
+    _fields_ = [("cell_size", f64), ("radius_scale", f64), ("h_min", f64),
+                ("c0", f64), ("rho0", f64), ("gamma", f64), ("B", f64),
+                ("alpha", f64), ("beta", f64), ("eta", f64), ("g", f64 * 3),
+                ("cfl", f64), ("dt_initial", f64), ("static_lo", f64 * 3),
+                ("static_hi", f64 * 3), ("use_cfl", i32), ("pad0", i32)]
+
+
+class SceneState(ctypes.Structure):
+    _fields_ = [("lo", i32 * 3), ("n", i32 * 3), ("cell_base", i32),
+                ("ncells", i32), ("box", u64 * 6), ("dt", f64), ("t", f64),
+                ("count", i64), ("max_dtfac", u64), ("max_acc2", u64)]
+
+
+class Tile(ctypes.Structure):
+    _fields_ = [("seg", i32), ("begin", i32), ("end", i32), ("pad0", i32)]
+
+
+BUFFER_FIELDS = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0",
+                 "w0", "m", "h", "idx", "tag")
+
+
+class Buffers(ctypes.Structure):
+    _fields_ = [(n, vp) for n in BUFFER_FIELDS]
+
+
+FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
+               "vel", "thermo", "cell")
+
+
+class Fields(ctypes.Structure):
+    _fields_ = [(n, vp) for n in FIELD_NAMES]
+
+
+WORK_NAMES = ("count", "start", "key", "slot", "perm", "bsum", "meta",
+              "status", "pairs")
+
+
+class Work(ctypes.Structure):
+    _fields_ = [(n, vp) for n in WORK_NAMES]
+
+
+class EngineDesc(ctypes.Structure):
+    _fields_ = [("cfg", Config), ("seg_offset", vp), ("scene", vp),
+                ("sstate", vp), ("tiles", vp), ("pair_tiles", vp),
+                ("num_tiles", i32), ("num_pair_tiles", i32),
+                ("buf", Buffers * 2), ("f", Fields), ("work", Work)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libsphb.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m pysph_b200.build` "
+            "(the CUDA engine has no fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    E = ctypes.POINTER(EngineDesc)
+    sig = {
+        "sphb_abi_version": (i32, []),
+        "sphb_last_cuda_error": (ctypes.c_char_p, []),
+        "sphb_make_tiles": (i32, [vp, i32, i32, vp, ctypes.POINTER(i32)]),
+        "sphb_workspace_layout": (i32, [ctypes.POINTER(Config),
+                                        ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_size_t)]),
+        "sphb_box_init": (i32, [E, i32, vp]),
+        "sphb_bin": (i32, [E, i32, i32, vp]),
+        "sphb_neighbors": (i32, [E, i32, u32, u32, vp, vp, vp, i64, vp]),
+        "sphb_cell_coords": (i32, [E, i32, vp, vp]),
+        "sphb_density": (i32, [E, i32, u32, i32, vp]),
+        "sphb_tait": (i32, [E, i32, u32, vp]),
+        "sphb_momentum": (i32, [E, i32, u32, i32, i32, vp]),
+        "sphb_pc_stage": (i32, [E, i32, i32, vp]),
+        "sphb_step_begin": (i32, [E, vp]),
+        "sphb_exchange": (i32, [E, i32, i32, i32, i32, vp, vp, vp]),
+        "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
+        "sphb_init_index": (i32, [E, i32, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    if L.sphb_abi_version() != 1:
+        raise RuntimeError("libsphb.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
+            "sphb_workspace_layout", "sphb_box_init", "sphb_bin",
+            "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
+            "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
+            "sphb_exchange", "sphb_exchange_tag", "sphb_init_index")
+
+
+def check(rc: int, what: str):
+    if rc != OK:
+        msg = ERRORS.get(rc, f"error {rc}")
+        if rc == -3:
+            msg += ": " + lib().sphb_last_cuda_error().decode()
+        raise RuntimeError(f"{what} failed: {msg}")
+
+
+def status_message(bits: int) -> str:
+    return ", ".join(v for k, v in STATUS_NAMES.items() if bits & k)

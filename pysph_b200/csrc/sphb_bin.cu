@@ -1,0 +1,489 @@
+// sphb_bin.cu -- cell binning for the particle engine (sm_100a).
+//
+// One rebin = scene boxes -> per-scene grids -> cell key per particle ->
+// counting sort (histogram, two-level scan, scatter, per-cell sort that makes
+// the order stable by engine position) -> gather of the particle state into
+// the other buffer in cell order, plus the FP32 pair records.
+//
+// The reference bins with a Python dict of cells keyed by floor(x / cs)
+// (CellManager._insert_particles, S/base/cell.pyx:1229-1300); its OpenCL
+// manager hashes to a flattened cell id and radix-sorts the keys
+// (RadixSortManager._cl_update, S/base/domain_manager.py:901-972;
+// bin / compute_cell_counts, S/base/radix_sort.cl:31-108).  Here the keys are
+// bounded by the grid, so a counting sort replaces the radix sort and the
+// state itself is permuted so every later kernel reads it coalesced.
+
+#include "sphb_common.cuh"
+
+namespace sphb {
+
+// ---------------------------------------------------------------- boxes --
+__global__ void k_box_reset(const __grid_constant__ sphb_engine e)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= e.cfg.num_scenes) return;
+    for (int d = 0; d < 3; ++d) {
+        e.sstate[s].box[d] = enc_double(INFINITY);
+        e.sstate[s].box[3 + d] = enc_double(-INFINITY);
+    }
+}
+
+__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_box_accum(const __grid_constant__ sphb_engine e, int cur)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int s = t.seg / e.cfg.num_arrays;
+    const int k = t.begin + threadIdx.x;
+    const sphb_buffers &B = e.buf[cur];
+    const int dim = e.cfg.dim;
+    double p[3] = {0.0, 0.0, 0.0};
+    bool ok = false;
+    if (k < t.end) {
+        p[0] = B.x[k];
+        p[1] = B.y[k];
+        if (dim == 3) p[2] = B.z[k];
+        ok = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
+    }
+    for (int d = 0; d < dim; ++d) {
+        double lo = block_reduce(ok ? p[d] : INFINITY, OpMin(), (double)INFINITY);
+        if (threadIdx.x == 0 && lo < INFINITY)
+            atomicMin(&e.sstate[s].box[d], enc_double(lo));
+        double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
+        if (threadIdx.x == 0 && hi > -INFINITY)
+            atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
+    }
+}
+
+// ----------------------------------------------------------- grid setup --
+// One block.  Grid of scene s: cells floor(lo/cs)-R .. floor(hi/cs)+R per
+// axis (R padding cells, so every stencil row of every particle exists);
+// exclusive prefix of A*ncells over scenes gives the scene key bases.
+__global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sphb_engine e)
+{
+    __shared__ long long sh[1024];
+    __shared__ long long s_carry;
+    const int S = e.cfg.num_scenes, A = e.cfg.num_arrays, R = e.cfg.stencil;
+    const int dim = e.cfg.dim;
+    const long long cap = e.cfg.cell_capacity;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < S; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        long long need = 0;
+        int lo[3] = {0, 0, 0}, n[3] = {1, 1, 1};
+        bool bad = false;
+        if (s < S) {
+            const sphb_scene &sc = e.scene[s];
+            sphb_scene_state &st = e.sstate[s];
+            const double cs = sc.cell_size;
+            for (int d = 0; d < dim; ++d) {
+                double blo = dec_double(st.box[d]);
+                double bhi = dec_double(st.box[3 + d]);
+                if (!(blo <= bhi)) { blo = 0.0; bhi = 0.0; }
+                const double flo = floor(blo / cs), fhi = floor(bhi / cs);
+                if (!(fabs(flo) < 1.0e9) || !(fabs(fhi) < 1.0e9) ||
+                    !(fhi - flo < 1.0e8)) {
+                    bad = true;
+                    lo[d] = 0;
+                    n[d] = 1;
+                } else {
+                    lo[d] = (int)flo - R;
+                    n[d] = (int)(fhi - flo) + 1 + 2 * R;
+                }
+            }
+            need = (long long)A * n[0] * n[1] * n[2];
+            if (bad || need > cap) { bad = true; need = 0; }
+        }
+        sh[threadIdx.x] = need;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+            long long v = (int)threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += v;
+            __syncthreads();
+        }
+        const long long incl = sh[threadIdx.x];
+        const long long total = sh[blockDim.x - 1];
+        if (s < S) {
+            sphb_scene_state &st = e.sstate[s];
+            const sphb_scene &sc = e.scene[s];
+            const long long cb = s_carry + incl - need;
+            if (bad || cb + need > cap) {
+                flag(e, SPHB_ST_GRID_OVERFLOW);
+                for (int d = 0; d < 3; ++d) { st.lo[d] = 0; st.n[d] = 1; }
+                st.cell_base = 0;
+                st.ncells = 0;
+            } else {
+                for (int d = 0; d < 3; ++d) { st.lo[d] = lo[d]; st.n[d] = n[d]; }
+                st.cell_base = (int)cb;
+                st.ncells = n[0] * n[1] * n[2];
+            }
+            for (int d = 0; d < 3; ++d) {
+                st.box[d] = enc_double(sc.static_lo[d]);
+                st.box[3 + d] = enc_double(sc.static_hi[d]);
+            }
+            st.max_dtfac = 0ull;
+            st.max_acc2 = 0ull;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        long long used = s_carry;
+        if (used > cap) {
+            flag(e, SPHB_ST_GRID_OVERFLOW);
+            used = 0;
+        }
+        e.work.meta[0] = (int)used;
+    }
+}
+
+// ----------------------------------------------------------------- hash --
+__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_hash(const __grid_constant__ sphb_engine e, int cur)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A, a = t.seg - s * A;
+    const sphb_scene_state &st = e.sstate[s];
+    const double cs = e.scene[s].cell_size;
+    const sphb_buffers &B = e.buf[cur];
+    const int dim = e.cfg.dim;
+    double p[3] = {B.x[k], B.y[k], dim == 3 ? B.z[k] : 0.0};
+    int c[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) {
+        if (!isfinite(p[d])) {
+            flag(e, SPHB_ST_NONFINITE_POS);
+            e.work.key[k] = -1;
+            return;
+        }
+        // floor(x / cs) exactly as find_cell_id (S/base/cell.pyx:44-84)
+        const double f = floor(p[d] / cs) - (double)st.lo[d];
+        if (!(f >= 0.0) || !(f < (double)st.n[d])) {
+            flag(e, SPHB_ST_OUT_OF_GRID);
+            e.work.key[k] = -1;
+            return;
+        }
+        c[d] = (int)f;
+    }
+    const int local = (c[2] * st.n[1] + c[1]) * st.n[0] + c[0];
+    const long long key = (long long)st.cell_base + (long long)a * st.ncells + local;
+    if (local >= st.ncells || key >= (long long)e.work.meta[0]) {
+        flag(e, SPHB_ST_OUT_OF_GRID);
+        e.work.key[k] = -1;
+        return;
+    }
+    e.work.slot[k] = atomicAdd(&e.work.count[key], 1);
+    e.work.key[k] = (int)key;
+}
+
+// ----------------------------------------------------------------- scan --
+__device__ __forceinline__ int block_excl_scan_int(int v, int &total)
+{
+    __shared__ int wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    total = wsum[(blockDim.x >> 5) - 1];
+    const int before = warp > 0 ? wsum[warp - 1] : 0;
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_reduce(const __grid_constant__ sphb_engine e)
+{
+    const int T = e.work.meta[0];
+    const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
+    int sum = 0;
+    if (base < T) {
+#pragma unroll
+        for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
+            const long long c = base + (long long)i * SPHB_SCAN_THREADS + threadIdx.x;
+            if (c < T) sum += e.work.count[c];
+        }
+    }
+    int total;
+    block_excl_scan_int(sum, total);
+    if (threadIdx.x == 0) e.work.bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_top(const __grid_constant__ sphb_engine e, int nb)
+{
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < nb ? e.work.bsum[i] : 0;
+        int total;
+        const int ex = block_excl_scan_int(v, total);
+        const int carry = s_carry;
+        if (i < nb) e.work.bsum[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) e.work.bsum[nb] = s_carry;
+}
+
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_apply(const __grid_constant__ sphb_engine e)
+{
+    const int T = e.work.meta[0];
+    const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
+    if (T == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) e.work.start[0] = 0;
+        return;
+    }
+    if (base >= T) return;
+    const long long c0 = base + (long long)threadIdx.x * SPHB_SCAN_ITEMS;
+    int v[SPHB_SCAN_ITEMS];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
+        v[i] = (c0 + i < T) ? e.work.count[c0 + i] : 0;
+        sum += v[i];
+    }
+    int total;
+    int run = block_excl_scan_int(sum, total) + e.work.bsum[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
+        const long long c = c0 + i;
+        if (c < T) {
+            e.work.start[c] = run;
+            e.work.count[c] = 0;  // ready for the next bin
+            run += v[i];
+            if (c == T - 1) e.work.start[T] = run;
+        }
+    }
+}
+
+// -------------------------------------------------------------- scatter --
+__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_scatter(const __grid_constant__ sphb_engine e)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int key = e.work.key[k];
+    if (key < 0) return;
+    const int pos = e.work.start[key] + e.work.slot[k];
+    if (pos < 0 || pos >= e.cfg.num_particles) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        return;
+    }
+    e.work.perm[pos] = k;
+}
+
+// The particle holding slot 0 of its cell sorts the cell's perm entries, so
+// the order inside a cell is by previous engine position (deterministic).
+__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_cell_sort(const __grid_constant__ sphb_engine e)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int key = e.work.key[k];
+    if (key < 0 || e.work.slot[k] != 0) return;
+    const int b = e.work.start[key], en = e.work.start[key + 1];
+    const int len = en - b;
+    if (len <= 1) return;
+    if (b < 0 || en > e.cfg.num_particles) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        return;
+    }
+    int *p = e.work.perm + b;
+    if (len <= 32) {
+        int v[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i < len) v[i] = p[i];
+        for (int i = 1; i < len; ++i) {
+            const int x = v[i];
+            int j = i - 1;
+            while (j >= 0 && v[j] > x) {
+                v[j + 1] = v[j];
+                --j;
+            }
+            v[j + 1] = x;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i < len) p[i] = v[i];
+    } else {
+        // shell sort (Ciura gaps) in place for crowded cells
+        const int gaps[8] = {701, 301, 132, 57, 23, 10, 4, 1};
+        for (int g = 0; g < 8; ++g) {
+            const int gap = gaps[g];
+            for (int i = gap; i < len; ++i) {
+                const int x = p[i];
+                int j = i;
+                while (j >= gap && p[j - gap] > x) {
+                    p[j] = p[j - gap];
+                    j -= gap;
+                }
+                p[j] = x;
+            }
+        }
+    }
+}
+
+// -------------------------------------------------------------- reorder --
+template <int DIM, bool F32>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A, a = t.seg - s * A;
+    const int seg_lo = e.seg_offset[t.seg], seg_hi = e.seg_offset[t.seg + 1];
+    int p = e.work.perm[k];
+    if (p < seg_lo || p >= seg_hi) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        p = k;
+    }
+    const sphb_buffers &S = e.buf[cur];
+    const sphb_buffers &D = e.buf[cur ^ 1];
+    const double x = S.x[p], y = S.y[p];
+    const double u = S.u[p], v = S.v[p];
+    const double m = S.m[p], h = S.h[p];
+    D.x[k] = x;
+    D.y[k] = y;
+    D.u[k] = u;
+    D.v[k] = v;
+    D.m[k] = m;
+    D.h[k] = h;
+    D.idx[k] = S.idx[p];
+    D.tag[k] = S.tag[p];
+    double z = 0.0, w = 0.0;
+    if (DIM == 3) {
+        z = S.z[p];
+        w = S.w[p];
+        D.z[k] = z;
+        D.w[k] = w;
+    }
+    if (move_initial) {
+        D.x0[k] = S.x0[p];
+        D.y0[k] = S.y0[p];
+        D.u0[k] = S.u0[p];
+        D.v0[k] = S.v0[p];
+        if (DIM == 3) {
+            D.z0[k] = S.z0[p];
+            D.w0[k] = S.w0[p];
+        }
+    }
+    const sphb_scene_state &st = e.sstate[s];
+    const int key = e.work.key[p];
+    int local = key - st.cell_base - a * st.ncells;
+    if (key < 0 || local < 0 || local >= st.ncells) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        local = 0;
+    }
+    e.f.cell[k] = local;
+    if (F32) {
+        const double cs = e.scene[s].cell_size;
+        int cx, cy, cz;
+        cell_coords(local, st.n, cx, cy, cz);
+        // position relative to the origin of the particle's own cell
+        const float xr = (float)(x - (double)(st.lo[0] + cx) * cs);
+        const float yr = (float)(y - (double)(st.lo[1] + cy) * cs);
+        if (DIM == 2) {
+            ((float4 *)e.f.geo)[k] = make_float4(xr, yr, (float)h, (float)m);
+            ((float2 *)e.f.vel)[k] = make_float2((float)u, (float)v);
+        } else {
+            const float zr = (float)(z - (double)(st.lo[2] + cz) * cs);
+            ((float4 *)e.f.geo)[k] = make_float4(xr, yr, zr, (float)h);
+            ((float *)e.f.mass)[k] = (float)m;
+            ((float4 *)e.f.vel)[k] = make_float4((float)u, (float)v, (float)w, 0.f);
+        }
+    }
+}
+
+// --------------------------------------------------------- entry points --
+static int check_engine(const sphb_engine *e, int cur)
+{
+    if (!e || (cur != 0 && cur != 1)) return SPHB_ERR_ARG;
+    const sphb_config &c = e->cfg;
+    if (c.dim != 2 && c.dim != 3) return SPHB_ERR_UNSUPPORTED;
+    if (c.precision != SPHB_FP64 && c.precision != SPHB_FP32C) return SPHB_ERR_UNSUPPORTED;
+    if (c.stencil < 1 || c.stencil > SPHB_MAX_STENCIL) return SPHB_ERR_UNSUPPORTED;
+    if (c.num_scenes < 1 || c.num_arrays < 1 || c.num_arrays > SPHB_MAX_ARRAYS)
+        return SPHB_ERR_ARG;
+    if (c.num_particles < 0 || c.cell_capacity < 1) return SPHB_ERR_ARG;
+    if (!e->tiles || e->num_tiles < 0 || !e->seg_offset || !e->scene || !e->sstate)
+        return SPHB_ERR_ARG;
+    return SPHB_OK;
+}
+
+int check_engine_public(const sphb_engine *e, int cur) { return check_engine(e, cur); }
+
+int bin_scan_blocks(const sphb_config &c)
+{
+    return (int)((c.cell_capacity + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK);
+}
+
+}  // namespace sphb
+
+using namespace sphb;
+
+extern "C" int sphb_box_init(const sphb_engine *e, int cur, void *stream)
+{
+    int rc = check_engine(e, cur);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_box_reset<<<(e->cfg.num_scenes + 127) / 128, 128, 0, st>>>(*e);
+    if (e->num_tiles > 0)
+        k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    return launch_status("sphb_box_init");
+}
+
+extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
+{
+    int rc = check_engine(e, cur);
+    if (rc) return rc;
+    const sphb_config &c = e->cfg;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (flags & SPHB_BIN_BOX) {
+        k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e);
+        if (e->num_tiles > 0)
+            k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    }
+    k_grid_setup<<<1, 1024, 0, st>>>(*e);
+    const int nt = e->num_tiles;
+    if (nt > 0) k_hash<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    const int nb = bin_scan_blocks(c);
+    k_scan_reduce<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e);
+    k_scan_top<<<1, SPHB_SCAN_THREADS, 0, st>>>(*e, nb);
+    k_scan_apply<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e);
+    if (nt > 0) {
+        k_scatter<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e);
+        k_cell_sort<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e);
+        const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
+        if (c.dim == 2 && c.precision == SPHB_FP32C)
+            k_reorder<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+        else if (c.dim == 2)
+            k_reorder<2, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+        else if (c.precision == SPHB_FP32C)
+            k_reorder<3, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+        else
+            k_reorder<3, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+    }
+    return launch_status("sphb_bin");
+}

@@ -1,0 +1,147 @@
+// sphb_common.cuh -- device helpers shared by the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "sphb.h"
+
+#define SPHB_ELEM_TILE 256          // particles per elementwise tile / block
+#define SPHB_SCAN_THREADS 1024
+#define SPHB_SCAN_ITEMS 4
+#define SPHB_SCAN_CHUNK (SPHB_SCAN_THREADS * SPHB_SCAN_ITEMS)
+#define SPHB_MAX_STENCIL 2
+
+namespace sphb {
+
+// Records the failure of the last launch for sphb_last_cuda_error.
+int launch_status(const char *what);
+
+__device__ __forceinline__ void flag(const sphb_engine &e, unsigned bits)
+{
+    atomicOr(e.work.status, bits);
+}
+
+// Monotone map double -> uint64 so atomicMin/atomicMax order doubles.
+__host__ __device__ __forceinline__ unsigned long long enc_double(double v)
+{
+    unsigned long long b;
+#ifdef __CUDA_ARCH__
+    b = (unsigned long long)__double_as_longlong(v);
+#else
+    memcpy(&b, &v, sizeof(b));
+#endif
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__host__ __device__ __forceinline__ double dec_double(unsigned long long e)
+{
+    unsigned long long b = (e & 0x8000000000000000ull)
+                               ? (e & 0x7fffffffffffffffull)
+                               : ~e;
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double v;
+    memcpy(&v, &b, sizeof(v));
+    return v;
+#endif
+}
+
+// Non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr,
+                                                  double v)
+{
+    if (!(v >= 0.0)) return;
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// Local cell index -> (cx, cy, cz) within the scene grid.
+__device__ __forceinline__ void cell_coords(int c, const int *n, int &cx,
+                                            int &cy, int &cz)
+{
+    cx = c % n[0];
+    int r = c / n[0];
+    cy = r % n[1];
+    cz = r / n[1];
+}
+
+// Block-wide reductions (blockDim.x multiple of 32, <= 1024).
+template <typename T, typename Op>
+__device__ __forceinline__ T block_reduce(T v, Op op, T identity)
+{
+    __shared__ T red_smem[32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) red_smem[warp] = v;
+    __syncthreads();
+    const unsigned nw = blockDim.x >> 5;
+    v = (threadIdx.x < nw) ? red_smem[threadIdx.x] : identity;
+    if (warp == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;  // valid in thread 0
+}
+
+struct OpMin {
+    __device__ __forceinline__ double operator()(double a, double b) const
+    {
+        return fmin(a, b);
+    }
+};
+struct OpMax {
+    __device__ __forceinline__ double operator()(double a, double b) const
+    {
+        return fmax(a, b);
+    }
+};
+struct OpAddU64 {
+    __device__ __forceinline__ unsigned long long
+    operator()(unsigned long long a, unsigned long long b) const
+    {
+        return a + b;
+    }
+};
+
+// Kahan-compensated FP32 accumulator: the running value is sum - c.
+struct Kahan {
+    float sum, c;
+    __device__ __forceinline__ Kahan() : sum(0.f), c(0.f) {}
+    __device__ __forceinline__ void add(float term)
+    {
+        float y = term - c;
+        float t = sum + y;
+        c = (t - sum) - y;
+        sum = t;
+    }
+    // Merge another partial sum (two-sum of the heads, compensations added).
+    __device__ __forceinline__ void merge(float osum, float oc)
+    {
+        float t = sum + osum;
+        float bp = t - sum;
+        float err = (sum - (t - bp)) + (osum - bp);
+        sum = t;
+        c = c + oc - err;
+    }
+    __device__ __forceinline__ double value() const
+    {
+        return (double)sum - (double)c;
+    }
+};
+
+// Cubic-spline normalisation at h = 1 (CubicSplineKernel._fac(1.0),
+// S/base/kernels.pyx:441-447).
+template <int DIM>
+__host__ __device__ __forceinline__ double kfac_unit()
+{
+    return DIM == 2 ? 10.0 / (7.0 * 3.141592653589793)
+                    : 1.0 / 3.141592653589793;
+}
+
+}  // namespace sphb

@@ -1,0 +1,335 @@
+// sphb_density.cu -- summation density + Tait EOS, the stand-alone Tait
+// kernel, neighbour-list emission and cell coordinates (sm_100a).
+//
+// SPHRho (S/sph/funcs/density_funcs.pyx:37-73; OpenCL S/sph/funcs/
+// density_funcs.clt:3-53): rho_a = sum_b m_b W(r_ab, (h_a + h_b)/2) over the
+// neighbours r_ab^2 < (2 h_a)^2 of every source array, self included.
+// TaitEquation (S/sph/funcs/eos_funcs.pyx:88-129): p = B((rho/rho0)^gamma-1),
+// cs = c0 (rho/rho0)^((gamma-1)/2), fused as the epilogue of the density
+// pass.  Non-LocalReal dests get 0 (S/sph/sph_func.pyx:220-227).
+//
+// FP32C: pair geometry in FP32 from cell-relative positions, the sum in FP32
+// with Kahan compensation, the EOS in FP64.  FP64: the reference's
+// arithmetic, with its exact neighbour predicate.
+
+#include "sphb_pairs.cuh"
+
+namespace sphb {
+
+int check_engine_public(const sphb_engine *e, int cur);
+
+template <int DIM, bool F32, int LANES, int R>
+__global__ void __launch_bounds__(512)
+k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int with_eos)
+{
+    const sphb_tile tl = e.pair_tiles[blockIdx.x];
+    const int A = e.cfg.num_arrays;
+    const int s = tl.seg / A, a = tl.seg - s * A;
+    const uint32_t src = e.cfg.rho_src[a];
+    if (!((dest_mask >> a) & 1u) || src == 0u) return;  // block-uniform
+    const int lane = threadIdx.x & (LANES - 1);
+    const int k = tl.begin + (int)(threadIdx.x / LANES);
+    const bool active = k < tl.end;
+    const sphb_scene_state &st = e.sstate[s];
+    const int n[3] = {st.n[0], st.n[1], st.n[2]};
+    const int cell_base = st.cell_base, ncells = st.ncells;
+    const sphb_scene &sc = e.scene[s];
+    const int *__restrict__ start = e.work.start;
+    unsigned long long np = 0;
+    double rho = 0.0;
+
+    if constexpr (F32) {
+        Kahan acc;
+        if (active) {
+            const float4 *__restrict__ geo = (const float4 *)e.f.geo;
+            const float *__restrict__ mass = (const float *)e.f.mass;
+            const float4 gk = geo[k];
+            const float csf = (float)sc.cell_size;
+            const float xk = gk.x, yk = gk.y, zk = DIM == 3 ? gk.z : 0.f;
+            const float hk = DIM == 3 ? gk.w : gk.z;
+            const float rad = hk * (float)sc.radius_scale;
+            const float rad2 = rad * rad;
+            int cx, cy, cz;
+            cell_coords(e.f.cell[k], n, cx, cy, cz);
+            for_each_candidate<DIM, R, LANES>(
+                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
+                e.cfg.num_particles, e.work.status,
+                [&](int j, int o, int dy, int dz) {
+                    const float4 gj = __ldg(geo + j);
+                    const float dx = (xk - gj.x) - (float)o * csf;
+                    const float ddy = (yk - gj.y) - (float)dy * csf;
+                    float r2 = dx * dx + ddy * ddy;
+                    if (DIM == 3) {
+                        const float ddz = (zk - gj.z) - (float)dz * csf;
+                        r2 += ddz * ddz;
+                    }
+                    if (r2 < rad2) {
+                        const float hj = DIM == 3 ? gj.w : gj.z;
+                        const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
+                        acc.add(mj * w_cubic_f<DIM>(r2, 0.5f * (hk + hj)));
+                        ++np;
+                    }
+                });
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) {
+            const float os = __shfl_xor_sync(0xffffffffu, acc.sum, o);
+            const float oc = __shfl_xor_sync(0xffffffffu, acc.c, o);
+            acc.merge(os, oc);
+        }
+        rho = acc.value();
+    } else {
+        double sum = 0.0;
+        if (active) {
+            const sphb_buffers &B = e.buf[cur];
+            const double xk = B.x[k], yk = B.y[k], zk = DIM == 3 ? B.z[k] : 0.0;
+            const double hk = B.h[k];
+            const double rad = hk * sc.radius_scale;
+            const double rad2 = __dmul_rn(rad, rad);
+            int cx, cy, cz;
+            cell_coords(e.f.cell[k], n, cx, cy, cz);
+            for_each_candidate<DIM, R, LANES>(
+                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
+                e.cfg.num_particles, e.work.status,
+                [&](int j, int, int, int) {
+                    const double dx = xk - __ldg(B.x + j);
+                    const double dy = yk - __ldg(B.y + j);
+                    const double dz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
+                    const double d2 = dist2_ref<DIM>(dx, dy, dz);
+                    if (d2 < rad2) {
+                        const double hab = 0.5 * (hk + __ldg(B.h + j));
+                        sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
+                        ++np;
+                    }
+                });
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        rho = sum;
+    }
+
+    if (active && lane == 0) {
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (!real) rho = 0.0;
+        const bool eos = with_eos && ((e.cfg.tait_on >> a) & 1u);
+        double p = 0.0, c = 0.0;
+        if (eos && real) {
+            const double ratio = rho / sc.rho0;
+            p = (pow(ratio, sc.gamma) - 1.0) * sc.B;
+            c = pow(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
+        }
+        if constexpr (F32) {
+            float4 *th = (float4 *)e.f.thermo;
+            float4 t = th[k];
+            t.x = (float)rho;
+            if (eos) {
+                t.y = (float)p;
+                t.z = (float)c;
+            }
+            t.w = t.x != 0.f ? t.y / (t.x * t.x) : 0.f;
+            th[k] = t;
+            if (!isfinite(t.x) || !isfinite(t.y)) flag(e, SPHB_ST_NONFINITE_RHO);
+        } else {
+            ((double *)e.f.rho)[k] = rho;
+            if (eos) {
+                ((double *)e.f.p)[k] = p;
+                ((double *)e.f.cs)[k] = c;
+            }
+            if (!isfinite(rho) || !isfinite(p)) flag(e, SPHB_ST_NONFINITE_RHO);
+        }
+    }
+    const unsigned long long tot = block_reduce(np, OpAddU64(), 0ull);
+    if (threadIdx.x == 0 && tot) atomicAdd(&e.work.pairs[0], tot);
+}
+
+// Tait alone (rho given).
+template <bool F32>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A, a = t.seg - s * A;
+    if (!((dest_mask >> a) & 1u)) return;
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const sphb_scene &sc = e.scene[s];
+    const bool real = e.buf[cur].tag[k] == 0;
+    double rho;
+    if constexpr (F32) rho = ((const float4 *)e.f.thermo)[k].x;
+    else rho = ((const double *)e.f.rho)[k];
+    double p = 0.0, c = 0.0;
+    if (real) {
+        const double ratio = rho / sc.rho0;
+        p = (pow(ratio, sc.gamma) - 1.0) * sc.B;
+        c = pow(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
+    }
+    if constexpr (F32) {
+        float4 *th = (float4 *)e.f.thermo;
+        float4 v = th[k];
+        v.y = (float)p;
+        v.z = (float)c;
+        v.w = v.x != 0.f ? v.y / (v.x * v.x) : 0.f;
+        th[k] = v;
+    } else {
+        ((double *)e.f.p)[k] = p;
+        ((double *)e.f.cs)[k] = c;
+    }
+}
+
+// Neighbour lists with the reference's exact FP64 predicate.
+template <int DIM, int R>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_neighbors(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, uint32_t src_mask,
+            int *counts, const long long *offs, int *out, long long cap)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A, a = t.seg - s * A;
+    if (!((dest_mask >> a) & 1u)) return;
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const sphb_scene_state &st = e.sstate[s];
+    const int n[3] = {st.n[0], st.n[1], st.n[2]};
+    const sphb_buffers &B = e.buf[cur];
+    const double xk = B.x[k], yk = B.y[k], zk = DIM == 3 ? B.z[k] : 0.0;
+    const double rad = B.h[k] * e.scene[s].radius_scale;
+    const double rad2 = __dmul_rn(rad, rad);
+    int cx, cy, cz;
+    cell_coords(e.f.cell[k], n, cx, cy, cz);
+    int cnt = 0;
+    const long long base = offs ? offs[k] : 0;
+    for_each_candidate<DIM, R, 1>(
+        e.work.start, A, src_mask, st.cell_base, st.ncells, n, cx, cy, cz, 0,
+        e.cfg.num_particles, e.work.status,
+        [&](int j, int, int, int) {
+            const double dx = B.x[j] - xk;
+            const double dy = B.y[j] - yk;
+            const double dz = DIM == 3 ? B.z[j] - zk : 0.0;
+            if (dist2_ref<DIM>(dx, dy, dz) < rad2) {
+                if (offs) {
+                    const long long pos = base + cnt;
+                    if (pos < cap) out[pos] = j;
+                    else flag(e, SPHB_ST_NBR_CAPACITY);
+                }
+                ++cnt;
+            }
+        });
+    counts[k] = cnt;
+}
+
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_cell_coords(const __grid_constant__ sphb_engine e, int *out)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int s = t.seg / e.cfg.num_arrays;
+    const sphb_scene_state &st = e.sstate[s];
+    int cx, cy, cz;
+    cell_coords(e.f.cell[k], st.n, cx, cy, cz);
+    out[3 * k + 0] = st.lo[0] + cx;
+    out[3 * k + 1] = st.lo[1] + cy;
+    out[3 * k + 2] = e.cfg.dim == 3 ? st.lo[2] + cz : 0;
+}
+
+template <int DIM, bool F32>
+static void launch_density(const sphb_engine &e, int cur, uint32_t dm, int eos,
+                           cudaStream_t st)
+{
+    const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
+#define SPHB_L(LV, RV) k_density<DIM, F32, LV, RV><<<g, b, 0, st>>>(e, cur, dm, eos)
+    switch (e.cfg.lanes * 10 + e.cfg.stencil) {
+    case 11: SPHB_L(1, 1); break;
+    case 12: SPHB_L(1, 2); break;
+    case 21: SPHB_L(2, 1); break;
+    case 22: SPHB_L(2, 2); break;
+    case 41: SPHB_L(4, 1); break;
+    case 42: SPHB_L(4, 2); break;
+    case 81: SPHB_L(8, 1); break;
+    case 82: SPHB_L(8, 2); break;
+    }
+#undef SPHB_L
+}
+
+int check_pair_cfg(const sphb_engine *e)
+{
+    const sphb_config &c = e->cfg;
+    if (c.lanes != 1 && c.lanes != 2 && c.lanes != 4 && c.lanes != 8) return SPHB_ERR_UNSUPPORTED;
+    if (c.pair_block < 32 || c.pair_block > 512 || (c.pair_block & 31)) return SPHB_ERR_ARG;
+    if (!e->pair_tiles || e->num_pair_tiles < 0) return SPHB_ERR_ARG;
+    if (!e->work.start || !e->f.cell) return SPHB_ERR_ARG;
+    return SPHB_OK;
+}
+
+}  // namespace sphb
+
+using namespace sphb;
+
+extern "C" int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
+                            int with_eos, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if ((rc = check_pair_cfg(e))) return rc;
+    if (e->num_pair_tiles == 0) return SPHB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const sphb_config &c = e->cfg;
+    if (c.precision == SPHB_FP32C) {
+        if (!e->f.geo || !e->f.thermo || (c.dim == 3 && !e->f.mass)) return SPHB_ERR_ARG;
+        if (c.dim == 2) launch_density<2, true>(*e, cur, dest_mask, with_eos, st);
+        else launch_density<3, true>(*e, cur, dest_mask, with_eos, st);
+    } else {
+        if (!e->f.rho || !e->f.p || !e->f.cs) return SPHB_ERR_ARG;
+        if (c.dim == 2) launch_density<2, false>(*e, cur, dest_mask, with_eos, st);
+        else launch_density<3, false>(*e, cur, dest_mask, with_eos, st);
+    }
+    return launch_status("sphb_density");
+}
+
+extern "C" int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if (e->num_tiles == 0) return SPHB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (e->cfg.precision == SPHB_FP32C)
+        k_tait<true><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask);
+    else
+        k_tait<false><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask);
+    return launch_status("sphb_tait");
+}
+
+extern "C" int sphb_neighbors(const sphb_engine *e, int cur, uint32_t dest_mask,
+                              uint32_t src_mask, int32_t *counts,
+                              const int64_t *nbr_offsets, int32_t *nbr_index,
+                              int64_t nbr_capacity, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if (!counts || (nbr_offsets && !nbr_index) || !e->work.start || !e->f.cell)
+        return SPHB_ERR_ARG;
+    if (e->num_tiles == 0) return SPHB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long *offs = (const long long *)nbr_offsets;
+    const int nt = e->num_tiles;
+    const int key = e->cfg.dim * 10 + e->cfg.stencil;
+    switch (key) {
+    case 21: k_neighbors<2, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, src_mask, counts, offs, nbr_index, nbr_capacity); break;
+    case 22: k_neighbors<2, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, src_mask, counts, offs, nbr_index, nbr_capacity); break;
+    case 31: k_neighbors<3, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, src_mask, counts, offs, nbr_index, nbr_capacity); break;
+    case 32: k_neighbors<3, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, src_mask, counts, offs, nbr_index, nbr_capacity); break;
+    default: return SPHB_ERR_UNSUPPORTED;
+    }
+    return launch_status("sphb_neighbors");
+}
+
+extern "C" int sphb_cell_coords(const sphb_engine *e, int cur, int32_t *out, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if (!out || !e->f.cell) return SPHB_ERR_ARG;
+    if (e->num_tiles == 0) return SPHB_OK;
+    k_cell_coords<<<e->num_tiles, SPHB_ELEM_TILE, 0, (cudaStream_t)stream>>>(*e, out);
+    return launch_status("sphb_cell_coords");
+}

@@ -1,0 +1,284 @@
+// sphb_force.cu -- MomentumEquation / SPHPressureGradient + GravityForce
+// (sm_100a).
+//
+// MomentumEquation.eval_nbr (S/sph/funcs/pressure_funcs.pyx:246-391; OpenCL
+// pressure_funcs.clt:69-157), per neighbour b of dest a:
+//   dot = v_ab . r_ab,  dt_fac_a = max |h_ab dot / (r_ab^2 + eta^2 h_ab^2)|
+//   tmp = P_a/rho_a^2 + P_b/rho_b^2 (+ Pi_ab when dot < 0,
+//         Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab, mu = h_ab dot /
+//         (r_ab^2 + eta^2 h_ab^2))
+//   a_a += -m_b tmp grad W(r_ab, h_ab)
+// SPHPressureGradient (:62-161) is the same without Pi and dt_fac.
+// GravityForce (S/sph/funcs/external_force.pyx:13-62) adds g afterwards.
+// Per scene the kernel also keeps max dt_fac and max |a|^2 for the CFL rule.
+
+#include "sphb_pairs.cuh"
+
+namespace sphb {
+
+int check_engine_public(const sphb_engine *e, int cur);
+int check_pair_cfg(const sphb_engine *e);
+
+template <int DIM, bool F32, int LANES, int R>
+__global__ void __launch_bounds__(512)
+k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
+        int with_gravity, int mode)
+{
+    const sphb_tile tl = e.pair_tiles[blockIdx.x];
+    const int A = e.cfg.num_arrays;
+    const int s = tl.seg / A, a = tl.seg - s * A;
+    const uint32_t src = e.cfg.mom_src[a];
+    if (!((dest_mask >> a) & 1u) || src == 0u) return;  // block-uniform
+    const int lane = threadIdx.x & (LANES - 1);
+    const int k = tl.begin + (int)(threadIdx.x / LANES);
+    const bool active = k < tl.end;
+    const sphb_scene_state &st = e.sstate[s];
+    const int n[3] = {st.n[0], st.n[1], st.n[2]};
+    const int cell_base = st.cell_base, ncells = st.ncells;
+    const sphb_scene &sc = e.scene[s];
+    const int *__restrict__ start = e.work.start;
+    const bool visc = mode == 0;
+    unsigned long long np = 0;
+    double acc[3] = {0.0, 0.0, 0.0};
+    double dtf = 0.0;
+
+    if constexpr (F32) {
+        Kahan ax, ay, az;
+        float dtmax = 0.f;
+        if (active) {
+            const float4 *__restrict__ geo = (const float4 *)e.f.geo;
+            const float *__restrict__ mass = (const float *)e.f.mass;
+            const float4 *__restrict__ th = (const float4 *)e.f.thermo;
+            const float csf = (float)sc.cell_size;
+            const float4 gk = geo[k];
+            const float4 tk = th[k];
+            float uk, vk, wk = 0.f;
+            if (DIM == 2) {
+                const float2 vv = ((const float2 *)e.f.vel)[k];
+                uk = vv.x;
+                vk = vv.y;
+            } else {
+                const float4 vv = ((const float4 *)e.f.vel)[k];
+                uk = vv.x;
+                vk = vv.y;
+                wk = vv.z;
+            }
+            const float xk = gk.x, yk = gk.y, zk = DIM == 3 ? gk.z : 0.f;
+            const float hk = DIM == 3 ? gk.w : gk.z;
+            const float rad = hk * (float)sc.radius_scale;
+            const float rad2 = rad * rad;
+            const float alpha = (float)sc.alpha, beta = (float)sc.beta;
+            const float eta2 = (float)(sc.eta * sc.eta);
+            int cx, cy, cz;
+            cell_coords(e.f.cell[k], n, cx, cy, cz);
+            for_each_candidate<DIM, R, LANES>(
+                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
+                e.cfg.num_particles, e.work.status,
+                [&](int j, int o, int dy, int dz) {
+                    const float4 gj = __ldg(geo + j);
+                    const float rx = (xk - gj.x) - (float)o * csf;
+                    const float ry = (yk - gj.y) - (float)dy * csf;
+                    float rz = 0.f;
+                    float r2 = rx * rx + ry * ry;
+                    if (DIM == 3) {
+                        rz = (zk - gj.z) - (float)dz * csf;
+                        r2 += rz * rz;
+                    }
+                    if (!(r2 < rad2)) return;
+                    ++np;
+                    const float hj = DIM == 3 ? gj.w : gj.z;
+                    const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
+                    const float hab = 0.5f * (hk + hj);
+                    const float4 tj = __ldg(th + j);
+                    float tmp = tk.w + tj.w;
+                    if (visc) {
+                        float vx, vy, vz = 0.f;
+                        if (DIM == 2) {
+                            const float2 vv = __ldg((const float2 *)e.f.vel + j);
+                            vx = uk - vv.x;
+                            vy = vk - vv.y;
+                        } else {
+                            const float4 vv = __ldg((const float4 *)e.f.vel + j);
+                            vx = uk - vv.x;
+                            vy = vk - vv.y;
+                            vz = wk - vv.z;
+                        }
+                        float dot = vx * rx + vy * ry;
+                        if (DIM == 3) dot += vz * rz;
+                        const float mu = __fdividef(hab * dot, r2 + eta2 * hab * hab);
+                        dtmax = fmaxf(dtmax, fabsf(mu));
+                        if (dot < 0.f) {
+                            const float cab = 0.5f * (tk.z + tj.z);
+                            const float rhoab = 0.5f * (tk.x + tj.x);
+                            tmp += __fdividef(-alpha * cab * mu + beta * mu * mu, rhoab);
+                        }
+                    }
+                    const float f = -mj * tmp * gw_cubic_f<DIM>(r2, hab);
+                    ax.add(f * rx);
+                    ay.add(f * ry);
+                    if (DIM == 3) az.add(f * rz);
+                });
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) {
+            ax.merge(__shfl_xor_sync(0xffffffffu, ax.sum, o), __shfl_xor_sync(0xffffffffu, ax.c, o));
+            ay.merge(__shfl_xor_sync(0xffffffffu, ay.sum, o), __shfl_xor_sync(0xffffffffu, ay.c, o));
+            if (DIM == 3)
+                az.merge(__shfl_xor_sync(0xffffffffu, az.sum, o), __shfl_xor_sync(0xffffffffu, az.c, o));
+            dtmax = fmaxf(dtmax, __shfl_xor_sync(0xffffffffu, dtmax, o));
+        }
+        acc[0] = ax.value();
+        acc[1] = ay.value();
+        acc[2] = az.value();
+        dtf = dtmax;
+    } else {
+        if (active) {
+            const sphb_buffers &B = e.buf[cur];
+            const double *__restrict__ rho = (const double *)e.f.rho;
+            const double *__restrict__ pr = (const double *)e.f.p;
+            const double *__restrict__ csnd = (const double *)e.f.cs;
+            const double xk = B.x[k], yk = B.y[k], zk = DIM == 3 ? B.z[k] : 0.0;
+            const double uk = B.u[k], vk = B.v[k], wk = DIM == 3 ? B.w[k] : 0.0;
+            const double hk = B.h[k];
+            const double rhoa = rho[k], Pa = pr[k], ca = csnd[k];
+            const double rhoa2 = 1.0 / (rhoa * rhoa);
+            const double rad = hk * sc.radius_scale;
+            const double rad2 = __dmul_rn(rad, rad);
+            const double alpha = sc.alpha, beta = sc.beta, eta = sc.eta;
+            int cx, cy, cz;
+            cell_coords(e.f.cell[k], n, cx, cy, cz);
+            for_each_candidate<DIM, R, LANES>(
+                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
+                e.cfg.num_particles, e.work.status,
+                [&](int j, int, int, int) {
+                    const double rx = xk - __ldg(B.x + j);
+                    const double ry = yk - __ldg(B.y + j);
+                    const double rz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
+                    const double rab2 = dist2_ref<DIM>(rx, ry, rz);
+                    if (!(rab2 < rad2)) return;
+                    ++np;
+                    const double hab = 0.5 * (hk + __ldg(B.h + j));
+                    const double rhob = __ldg(rho + j), Pb = __ldg(pr + j);
+                    const double mb = __ldg(B.m + j);
+                    double tmp = Pa * rhoa2 + Pb * (1.0 / (rhob * rhob));
+                    if (visc) {
+                        const double vx = uk - __ldg(B.u + j);
+                        const double vy = vk - __ldg(B.v + j);
+                        const double vz = DIM == 3 ? wk - __ldg(B.w + j) : 0.0;
+                        double dot = vx * rx + vy * ry;
+                        if (DIM == 3) dot += vz * rz;
+                        const double den = rab2 + eta * eta * hab * hab;
+                        dtf = fmax(dtf, fabs(hab * dot / den));
+                        if (dot < 0) {
+                            const double cab = 0.5 * (ca + __ldg(csnd + j));
+                            const double rhoab = 0.5 * (rhoa + rhob);
+                            double mu = hab * dot;
+                            mu /= den;
+                            double piab = -alpha * cab * mu + beta * mu * mu;
+                            piab /= rhoab;
+                            tmp += piab;
+                        }
+                    }
+                    tmp *= -mb;
+                    const double gw = gw_cubic_d<DIM>(sqrt(rab2), hab);
+                    acc[0] += tmp * (rx * gw);
+                    acc[1] += tmp * (ry * gw);
+                    if (DIM == 3) acc[2] += tmp * (rz * gw);
+                });
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) {
+            acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o);
+            acc[1] += __shfl_xor_sync(0xffffffffu, acc[1], o);
+            if (DIM == 3) acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], o);
+            dtf = fmax(dtf, __shfl_xor_sync(0xffffffffu, dtf, o));
+        }
+    }
+
+    double a2 = 0.0, dtf_out = 0.0;
+    if (active && lane == 0) {
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (real) {
+            if (with_gravity) {
+                acc[0] += sc.g[0];
+                acc[1] += sc.g[1];
+                if (DIM == 3) acc[2] += sc.g[2];
+            }
+            dtf_out = visc ? dtf : 0.0;
+        } else {
+            acc[0] = acc[1] = acc[2] = 0.0;
+        }
+        if (F32) {
+            const float fx = (float)acc[0], fy = (float)acc[1], fz = (float)acc[2];
+            ((float *)e.f.au)[k] = fx;
+            ((float *)e.f.av)[k] = fy;
+            if (DIM == 3) ((float *)e.f.aw)[k] = fz;
+            if (visc) ((float *)e.f.dt_fac)[k] = (float)dtf_out;
+            a2 = (double)fx * fx + (double)fy * fy + (double)fz * fz;
+        } else {
+            ((double *)e.f.au)[k] = acc[0];
+            ((double *)e.f.av)[k] = acc[1];
+            if (DIM == 3) ((double *)e.f.aw)[k] = acc[2];
+            if (visc) ((double *)e.f.dt_fac)[k] = dtf_out;
+            a2 = acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2];
+        }
+        if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
+    }
+    const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
+    const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
+    const unsigned long long tot = block_reduce(np, OpAddU64(), 0ull);
+    if (threadIdx.x == 0) {
+        sphb_scene_state &sw = e.sstate[s];
+        atomic_max_nonneg(&sw.max_dtfac, bdt);
+        atomic_max_nonneg(&sw.max_acc2, ba2);
+        if (tot) atomicAdd(&e.work.pairs[1], tot);
+    }
+}
+
+template <int DIM, bool F32>
+static void launch_force(const sphb_engine &e, int cur, uint32_t dm, int grav,
+                         int mode, cudaStream_t st)
+{
+    const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
+#define SPHB_L(LV, RV) k_force<DIM, F32, LV, RV><<<g, b, 0, st>>>(e, cur, dm, grav, mode)
+    switch (e.cfg.lanes * 10 + e.cfg.stencil) {
+    case 11: SPHB_L(1, 1); break;
+    case 12: SPHB_L(1, 2); break;
+    case 21: SPHB_L(2, 1); break;
+    case 22: SPHB_L(2, 2); break;
+    case 41: SPHB_L(4, 1); break;
+    case 42: SPHB_L(4, 2); break;
+    case 81: SPHB_L(8, 1); break;
+    case 82: SPHB_L(8, 2); break;
+    }
+#undef SPHB_L
+}
+
+}  // namespace sphb
+
+using namespace sphb;
+
+extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
+                             int with_gravity, int mode, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if ((rc = check_pair_cfg(e))) return rc;
+    if (mode != 0 && mode != 1) return SPHB_ERR_ARG;
+    if (!e->f.au || !e->f.av || (e->cfg.dim == 3 && !e->f.aw)) return SPHB_ERR_ARG;
+    if (mode == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
+    if (e->num_pair_tiles == 0) return SPHB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const sphb_config &c = e->cfg;
+    if (c.precision == SPHB_FP32C) {
+        if (!e->f.geo || !e->f.thermo || !e->f.vel || (c.dim == 3 && !e->f.mass))
+            return SPHB_ERR_ARG;
+        if (c.dim == 2) launch_force<2, true>(*e, cur, dest_mask, with_gravity, mode, st);
+        else launch_force<3, true>(*e, cur, dest_mask, with_gravity, mode, st);
+    } else {
+        if (!e->f.rho || !e->f.p || !e->f.cs) return SPHB_ERR_ARG;
+        if (c.dim == 2) launch_force<2, false>(*e, cur, dest_mask, with_gravity, mode, st);
+        else launch_force<3, false>(*e, cur, dest_mask, with_gravity, mode, st);
+    }
+    return launch_status("sphb_momentum");
+}

@@ -1,0 +1,151 @@
+// sphb_pairs.cuh -- neighbour traversal and the cubic spline for the pair
+// kernels.
+//
+// Cells are keyed row-major with x fastest, so the 2R+1 cells of one stencil
+// row (cx-R .. cx+R at fixed y, z) hold one contiguous particle range
+// [start[row-R], start[row+R+1]).  A dest particle visits (2R+1)^(DIM-1) such
+// ranges instead of (2R+1)^DIM cells; the 2R inner boundaries tell which
+// cell (x offset o) a candidate sits in, which the FP32 path needs because
+// its positions are stored relative to their own cell origin.
+
+#pragma once
+
+#include "sphb_common.cuh"
+
+namespace sphb {
+
+// A dest cell must lie at least R cells inside its grid (the grid is padded
+// by R cells), so every stencil row exists.  Anything else means the binning
+// state is corrupt (the status word says why); the particle is skipped.
+template <int DIM, int R>
+__device__ __forceinline__ bool dest_cell_ok(int cx, int cy, int cz, const int *n)
+{
+    bool ok = cx >= R && cx < n[0] - R && cy >= R && cy < n[1] - R;
+    if (DIM == 3) ok = ok && cz >= R && cz < n[2] - R;
+    return ok;
+}
+
+// Visits every candidate j of the stencil rows; returns false (visiting
+// nothing more) if a row range falls outside [0, num_particles).
+template <int DIM, int R, int LANES, typename F>
+__device__ __forceinline__ bool for_each_candidate(
+    const int *__restrict__ start, int num_arrays, uint32_t src_mask,
+    int cell_base, int ncells, const int *n, int cx, int cy, int cz, int lane,
+    int num_particles, unsigned *status, F &&f)
+{
+    if (!dest_cell_ok<DIM, R>(cx, cy, cz, n)) {
+        atomicOr(status, (unsigned)SPHB_ST_BAD_INDEX);
+        return false;
+    }
+    for (int b = 0; b < num_arrays; ++b) {
+        if (!((src_mask >> b) & 1u)) continue;
+        const int base = cell_base + b * ncells;
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -R : 0); dz <= (DIM == 3 ? R : 0); ++dz) {
+#pragma unroll 1
+            for (int dy = -R; dy <= R; ++dy) {
+                const int row = base + ((cz + dz) * n[1] + (cy + dy)) * n[0] + cx;
+                int bd[2 * R + 2];
+#pragma unroll
+                for (int i = 0; i < 2 * R + 2; ++i) bd[i] = __ldg(start + row - R + i);
+                if (bd[0] < 0 || bd[2 * R + 1] > num_particles || bd[0] > bd[2 * R + 1]) {
+                    atomicOr(status, (unsigned)SPHB_ST_BAD_INDEX);
+                    return false;
+                }
+                for (int j = bd[0] + lane; j < bd[2 * R + 1]; j += LANES) {
+                    int o = -R;
+#pragma unroll
+                    for (int i = 1; i <= 2 * R; ++i) o += (j >= bd[i]) ? 1 : 0;
+                    f(j, o, dy, dz);
+                }
+            }
+        }
+    }
+    return true;
+}
+
+// Cubic spline W(r, h) in FP32 (CubicSplineKernel.function,
+// S/base/kernels.pyx:355-378): fac * {1 - 1.5 q^2 (1 - q/2); (2-q)^3 / 4; 0}.
+template <int DIM>
+__device__ __forceinline__ float w_cubic_f(float r2, float hab)
+{
+    const float ih = __fdividef(1.0f, hab);
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    const float q = r * ih;
+    float val;
+    if (q > 2.0f) {
+        val = 0.0f;
+    } else if (q > 1.0f) {
+        const float t = 2.0f - q;
+        val = 0.25f * t * t * t;
+    } else {
+        val = 1.0f - 1.5f * (q * q) * (1.0f - 0.5f * q);
+    }
+    float fac = (float)kfac_unit<DIM>() * ih * ih;
+    if (DIM == 3) fac *= ih;
+    return val * fac;
+}
+
+// dW/dr / r, so grad W = (x_a - x_b) * gw (CubicSplineKernel.gradient,
+// S/base/kernels.pyx:380-417), FP32.
+template <int DIM>
+__device__ __forceinline__ float gw_cubic_f(float r2, float hab)
+{
+    const float ih = __fdividef(1.0f, hab);
+    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+    const float q = r2 * ir * ih;
+    float val = 0.0f;
+    if (q > 2.0f) {
+    } else if (q >= 1.0f) {
+        const float t = 2.0f - q;
+        val = -0.75f * t * t * ih * ir;
+    } else if (q > 1e-14f) {
+        val = 3.0f * (0.75f * q - 1.0f) * ih * ih;
+    }
+    float fac = (float)kfac_unit<DIM>() * ih * ih;
+    if (DIM == 3) fac *= ih;
+    return val * fac;
+}
+
+// FP64 versions with the reference's operations.
+template <int DIM>
+__device__ __forceinline__ double w_cubic_d(double rab, double h)
+{
+    const double q = rab / h;
+    double val;
+    const double fac = (DIM == 2 ? 1.0 / (h * h) : 1.0 / (h * h * h)) * kfac_unit<DIM>();
+    if (q > 2.0)
+        val = 0.0;
+    else if (q > 1.0)
+        val = 0.25 * (2 - q) * (2 - q) * (2 - q);
+    else
+        val = 1 - 1.5 * (q * q) * (1 - 0.5 * q);
+    return val * fac;
+}
+
+template <int DIM>
+__device__ __forceinline__ double gw_cubic_d(double rab, double h)
+{
+    const double q = rab / h;
+    double val = 0.0;
+    const double fac = (DIM == 2 ? 1.0 / (h * h) : 1.0 / (h * h * h)) * kfac_unit<DIM>();
+    if (q > 2.0) {
+    } else if (q >= 1.0) {
+        val = -0.75 * (2 - q) * (2 - q) / (h * rab);
+    } else if (q > 1e-14) {
+        val = 3.0 * (0.75 * q - 1) / (h * h);
+    }
+    return val * fac;
+}
+
+// Squared distance with the reference's rounding (no FMA contraction):
+// cPoint_distance2 (S/base/point.pxd:35-37).
+template <int DIM>
+__device__ __forceinline__ double dist2_ref(double dx, double dy, double dz)
+{
+    double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    if (DIM == 3) d2 = __dadd_rn(d2, __dmul_rn(dz, dz));
+    return d2;
+}
+
+}  // namespace sphb

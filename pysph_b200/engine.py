@@ -1,0 +1,558 @@
+"""Engine: the device state of a batch of independent scenes and the calls
+that advance it through libsphb.so.
+
+A scene is a list of particle arrays (e.g. [fluid, wall]) with its own
+physical parameters; every scene of an engine has the same array roles, and
+the scheme (which arrays are SPHRho / Tait / MomentumEquation destinations,
+which are their sources, which are integrated) is shared.  All scenes live
+in one SoA set ("engine order"), sorted by cell inside each (scene, array)
+segment, and every stage is one launch over all scenes.
+
+torch provides the device memory and the stream; all arithmetic runs in
+the sm_100a kernels of libsphb.so.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+ELEM_TILE = 256
+MASTER = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0", "w0",
+          "m", "h")
+USER_PROPS = ("x", "y", "z", "u", "v", "w", "m", "h")
+
+
+@dataclass
+class SceneParams:
+    """Per-scene constants of the pinned scheme (defaults: the reference's
+    own defaults for TaitEquation and MomentumEquation)."""
+    c0: float = 1.0
+    rho0: float = 1000.0
+    gamma: float = 7.0
+    alpha: float = 1.0
+    beta: float = 1.0
+    eta: float = 0.1
+    gravity: tuple = (0.0, 0.0, 0.0)
+    dt: float = 1e-4
+    cfl: float = 0.0            # > 0: ViscousAndForceBasedTimeStep
+    dt_initial: float = 1e-4     # solver.dt, used by the CFL rule at step 1
+    radius_scale: float = 2.0    # cubic-spline support / h
+
+    @staticmethod
+    def from_dict(d: dict) -> "SceneParams":
+        keys = SceneParams.__dataclass_fields__.keys()
+        return SceneParams(**{k: v for k, v in d.items() if k in keys})
+
+
+@dataclass
+class Scheme:
+    """Which array indices take part in which operation."""
+    rho_src: dict = field(default_factory=dict)   # dest -> [sources]
+    mom_src: dict = field(default_factory=dict)   # dest -> [sources]
+    tait_on: tuple = ()
+    step_on: tuple = ()
+
+    def masks(self):
+        rho = [0] * nat.MAX_ARRAYS
+        mom = [0] * nat.MAX_ARRAYS
+        for d, s in self.rho_src.items():
+            rho[d] = sum(1 << a for a in s)
+        for d, s in self.mom_src.items():
+            mom[d] = sum(1 << a for a in s)
+        tait = sum(1 << a for a in self.tait_on)
+        step = sum(1 << a for a in self.step_on)
+        return rho, mom, tait, step
+
+    @property
+    def rho_dests(self) -> int:
+        return sum(1 << d for d, s in self.rho_src.items() if s)
+
+    @property
+    def mom_dests(self) -> int:
+        return sum(1 << d for d, s in self.mom_src.items() if s)
+
+
+def fluid_scheme(num_arrays: int = 1) -> Scheme:
+    """Array 0 is the fluid; arrays 1.. are fixed walls.  SPHRho and Tait on
+    every array from every array; MomentumEquation on the fluid from every
+    array; only the fluid is integrated."""
+    all_ = list(range(num_arrays))
+    return Scheme(rho_src={a: all_ for a in all_}, mom_src={0: all_},
+                  tait_on=tuple(all_), step_on=(0,))
+
+
+class Engine:
+    """Batch of scenes on one GPU.
+
+    scenes: list of (arrays, params) where arrays is a list of dicts of
+    numpy/torch FP64 properties (x, y, z, u, v, w, m, h, rho, p, cs, tag)
+    and params a SceneParams or dict."""
+
+    def __init__(self, scenes, scheme: Scheme, dim: int = 2,
+                 precision: str = "fp32c", stencil: int = 1, lanes: int = 1,
+                 pair_block: int = 128, cell_capacity: int | None = None,
+                 grid_growth: float = 2.0, device=None):
+        if dim not in (2, 3):
+            raise ValueError("dim must be 2 or 3")
+        if precision not in ("fp64", "fp32c"):
+            raise ValueError("precision must be 'fp64' or 'fp32c'")
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("the engine runs on CUDA devices only")
+        self.L = nat.lib()
+        self.dim = dim
+        self.precision = precision
+        self.f32 = precision == "fp32c"
+        self.scheme = scheme
+        self.S = len(scenes)
+        self.A = len(scenes[0][0])
+        if self.S < 1 or not 1 <= self.A <= nat.MAX_ARRAYS:
+            raise ValueError("need >= 1 scene and 1..4 arrays per scene")
+        self.params = [p if isinstance(p, SceneParams) else SceneParams.from_dict(p)
+                       for _, p in scenes]
+        sizes = np.zeros((self.S, self.A), np.int64)
+        for s, (arrays, _) in enumerate(scenes):
+            if len(arrays) != self.A:
+                raise ValueError("every scene needs the same number of arrays")
+            for a, arr in enumerate(arrays):
+                sizes[s, a] = len(arr["x"])
+        self.sizes = sizes
+        seg = np.zeros(self.S * self.A + 1, np.int64)
+        seg[1:] = np.cumsum(sizes.ravel())
+        if seg[-1] >= 2 ** 31 - 1:
+            raise ValueError("too many particles for int32 indexing")
+        self.N = int(seg[-1])
+        self.seg_offset_host = seg.astype(np.int32)
+        # user-side layout: per array, scenes concatenated
+        self.user_offset_host = [np.concatenate([[0], np.cumsum(sizes[:, a])[:-1]]).astype(np.int32)
+                                 for a in range(self.A)]
+        self.user_n = [int(sizes[:, a].sum()) for a in range(self.A)]
+        self._stencil = stencil
+        self._host_scene_tables(scenes)
+        if cell_capacity is None:
+            cell_capacity = self._estimate_capacity(grid_growth)
+        self.cell_capacity = int(cell_capacity)
+        self._alloc(lanes, pair_block)
+        self._upload(scenes)
+
+    # ------------------------------------------------------------------ setup
+    def _host_scene_tables(self, scenes):
+        dim = self.dim
+        step = set(self.scheme.step_on)
+        sc = (nat.Scene * self.S)()
+        self._extent = []
+        for s, (arrays, _) in enumerate(scenes):
+            p = self.params[s]
+            hs = [np.asarray(_np(arr["h"]), np.float64) for arr in arrays]
+            max_h = max(float(h.max()) if len(h) else 0.0 for h in hs)
+            if max_h <= 0:
+                max_h = 0.5  # the reference's "cell size 0 -> 1"
+            cs = p.radius_scale * max_h / self._stencil
+            step_h = [h for a, h in enumerate(hs) if a in step and len(h)]
+            h_min = min(float(h.min()) for h in step_h) if step_h else max_h
+            lo = np.full(3, np.inf)
+            hi = np.full(3, -np.inf)
+            alo = np.full(3, np.inf)
+            ahi = np.full(3, -np.inf)
+            for a, arr in enumerate(arrays):
+                if len(arr["x"]) == 0:
+                    continue
+                pts = [np.asarray(_np(arr[c]), np.float64) for c in "xyz"[:dim]]
+                for d in range(dim):
+                    alo[d] = min(alo[d], pts[d].min())
+                    ahi[d] = max(ahi[d], pts[d].max())
+                    if a not in step:
+                        lo[d] = min(lo[d], pts[d].min())
+                        hi[d] = max(hi[d], pts[d].max())
+            self._extent.append((alo, ahi, cs))
+            t = sc[s]
+            t.cell_size = cs
+            t.radius_scale = p.radius_scale
+            t.h_min = h_min
+            t.c0, t.rho0, t.gamma = p.c0, p.rho0, p.gamma
+            t.B = p.c0 * p.c0 * p.rho0 / p.gamma
+            t.alpha, t.beta, t.eta = p.alpha, p.beta, p.eta
+            for d in range(3):
+                t.g[d] = float(p.gravity[d]) if d < len(p.gravity) else 0.0
+                t.static_lo[d] = lo[d]
+                t.static_hi[d] = hi[d]
+            t.cfl = p.cfl
+            t.dt_initial = p.dt_initial
+            t.use_cfl = 1 if p.cfl > 0 else 0
+        self._scene_host = sc
+
+    def _estimate_capacity(self, growth: float) -> int:
+        R = self._stencil
+        total = 0
+        for alo, ahi, cs in self._extent:
+            n = 1
+            for d in range(self.dim):
+                span = (ahi[d] - alo[d]) if np.isfinite(ahi[d]) else 0.0
+                cells = math.floor(span / cs) + 2
+                n *= int(math.ceil(cells * growth)) + 2 * R + 2
+            total += self.A * n
+        return max(total, 1024)
+
+    def _alloc(self, lanes, pair_block):
+        dev, N, dim = self.device, self.N, self.dim
+        f64 = dict(dtype=torch.float64, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.seg_offset = torch.from_numpy(self.seg_offset_host).to(dev)
+        self.user_offset = [torch.from_numpy(u).to(dev) for u in self.user_offset_host]
+        self.scene_dev = _struct_to_device(self._scene_host, dev)
+        st = (nat.SceneState * self.S)()
+        for s in range(self.S):
+            st[s].dt = self.params[s].dt
+        self.sstate_dev = _struct_to_device(st, dev)
+        # buffers
+        self.bufs = []
+        for _ in range(2):
+            b = {}
+            for name in MASTER:
+                if dim == 2 and name in ("z", "w", "z0", "w0"):
+                    b[name] = None
+                else:
+                    b[name] = torch.zeros(N, **f64)
+            b["idx"] = torch.zeros(N, **i32)
+            b["tag"] = torch.zeros(N, **i32)
+            self.bufs.append(b)
+        f = {}
+        if self.f32:
+            f32 = dict(dtype=torch.float32, device=dev)
+            f["rho"] = f["p"] = f["cs"] = None
+            f["au"] = torch.zeros(N, **f32)
+            f["av"] = torch.zeros(N, **f32)
+            f["aw"] = torch.zeros(N, **f32) if dim == 3 else None
+            f["dt_fac"] = torch.zeros(N, **f32)
+            f["geo"] = torch.zeros(N, 4, **f32)
+            f["mass"] = torch.zeros(N, **f32) if dim == 3 else None
+            f["vel"] = torch.zeros(N, 2 if dim == 2 else 4, **f32)
+            f["thermo"] = torch.zeros(N, 4, **f32)
+        else:
+            for n in ("rho", "p", "cs", "au", "av", "dt_fac"):
+                f[n] = torch.zeros(N, **f64)
+            f["aw"] = torch.zeros(N, **f64) if dim == 3 else None
+            f["geo"] = f["mass"] = f["vel"] = f["thermo"] = None
+        f["cell"] = torch.zeros(N, **i32)
+        self.fields = f
+        # scratch
+        cfg = self._config(lanes, pair_block)
+        offs = (ctypes.c_size_t * 9)()
+        total = ctypes.c_size_t()
+        nat.check(self.L.sphb_workspace_layout(ctypes.byref(cfg), offs,
+                                               ctypes.byref(total)),
+                  "sphb_workspace_layout")
+        self.work_buf = torch.zeros(total.value, dtype=torch.uint8, device=dev)
+        self.work_offsets = list(offs)
+        self.tiles = self._make_tiles(ELEM_TILE)
+        self.set_launch(lanes, pair_block)
+
+    def _config(self, lanes, pair_block):
+        cfg = nat.Config()
+        cfg.dim = self.dim
+        cfg.precision = nat.FP32C if self.f32 else nat.FP64
+        cfg.num_scenes = self.S
+        cfg.num_arrays = self.A
+        cfg.stencil = self._stencil
+        cfg.lanes = lanes
+        cfg.pair_block = pair_block
+        cfg.num_particles = self.N
+        cfg.cell_capacity = self.cell_capacity
+        rho, mom, tait, step = self.scheme.masks()
+        for a in range(nat.MAX_ARRAYS):
+            cfg.rho_src[a] = rho[a]
+            cfg.mom_src[a] = mom[a]
+        cfg.tait_on = tait
+        cfg.step_on = step
+        return cfg
+
+    def _make_tiles(self, tile_size):
+        n = ctypes.c_int32()
+        seg = self.seg_offset_host
+        nseg = len(seg) - 1
+        nat.check(self.L.sphb_make_tiles(seg.ctypes.data, nseg, tile_size, None,
+                                         ctypes.byref(n)), "sphb_make_tiles")
+        arr = (nat.Tile * max(n.value, 1))()
+        nat.check(self.L.sphb_make_tiles(seg.ctypes.data, nseg, tile_size,
+                                         ctypes.addressof(arr), ctypes.byref(n)),
+                  "sphb_make_tiles")
+        return _struct_to_device(arr, self.device), n.value
+
+    def set_launch(self, lanes: int, pair_block: int):
+        """Pair-kernel launch shape: lanes per dest particle and block size."""
+        if lanes not in (1, 2, 4, 8) or pair_block % 32 or not 32 <= pair_block <= 512:
+            raise ValueError("bad pair-kernel launch shape")
+        self.lanes, self.pair_block = lanes, pair_block
+        self.pair_tiles = self._make_tiles(pair_block // lanes)
+        self._build_desc()
+
+    def _build_desc(self):
+        d = nat.EngineDesc()
+        d.cfg = self._config(self.lanes, self.pair_block)
+        d.seg_offset = self.seg_offset.data_ptr()
+        d.scene = self.scene_dev.data_ptr()
+        d.sstate = self.sstate_dev.data_ptr()
+        d.tiles = self.tiles[0].data_ptr()
+        d.num_tiles = self.tiles[1]
+        d.pair_tiles = self.pair_tiles[0].data_ptr()
+        d.num_pair_tiles = self.pair_tiles[1]
+        for i in range(2):
+            for name in nat.BUFFER_FIELDS:
+                t = self.bufs[i][name]
+                setattr(d.buf[i], name, t.data_ptr() if t is not None else None)
+        for name in nat.FIELD_NAMES:
+            t = self.fields[name]
+            setattr(d.f, name, t.data_ptr() if t is not None else None)
+        base = self.work_buf.data_ptr()
+        for name, off in zip(nat.WORK_NAMES, self.work_offsets):
+            setattr(d.work, name, base + off)
+        self.desc = d
+        self._pdesc = ctypes.byref(d)
+        self.cur = getattr(self, "cur", 0)
+
+    def _upload(self, scenes):
+        """Copy the user arrays in, set identity indices, then bin."""
+        self.cur = 0
+        self._box_valid = False
+        self.call("sphb_init_index", 0)
+        user = self._user_tensors(scenes)
+        for a in range(self.A):
+            for name in USER_PROPS:
+                if self.dim == 2 and name in ("z", "w"):
+                    continue
+                self.exchange_in(a, name, user[a][name])
+            self.exchange_tag(a, user[a]["tag"], 0)
+        self.bin(0)
+        for a in range(self.A):
+            for name in ("rho", "p", "cs"):
+                self.exchange_in(a, name, user[a][name])
+
+    def _user_tensors(self, scenes):
+        out = []
+        for a in range(self.A):
+            d = {}
+            for name in USER_PROPS + ("rho", "p", "cs"):
+                parts = []
+                for arrays, _ in scenes:
+                    arr = arrays[a]
+                    n = len(arr["x"])
+                    v = arr.get(name)
+                    if v is None:
+                        v = {"m": 1.0, "h": 1.0, "rho": 1.0}.get(name, 0.0)
+                    parts.append(torch.as_tensor(_np_b(v, n), dtype=torch.float64))
+                d[name] = torch.cat(parts).to(self.device)
+            tags = []
+            for arrays, _ in scenes:
+                arr = arrays[a]
+                n = len(arr["x"])
+                v = arr.get("tag", 0)
+                tags.append(torch.as_tensor(_np_b(v, n), dtype=torch.int32))
+            d["tag"] = torch.cat(tags).to(self.device)
+            out.append(d)
+        return out
+
+    # ------------------------------------------------------------ low level
+    @property
+    def stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def call(self, name, *args):
+        fn = getattr(self.L, name)
+        if name == "sphb_step_begin":
+            rc = fn(self._pdesc, self.stream)
+        else:
+            rc = fn(self._pdesc, *args, self.stream)
+        nat.check(rc, name)
+
+    def bin(self, flags: int = 0):
+        if not self._box_valid:
+            flags |= nat.BIN_BOX
+        self.call("sphb_bin", self.cur, flags)
+        self.cur ^= 1
+        self._box_valid = False   # until a pc_stage accumulates it again
+
+    def invalidate_box(self):
+        """Positions were changed outside the integrator: the next bin
+        recomputes every scene box from all particles."""
+        self._box_valid = False
+
+    def density(self, dest_mask=None, eos=True):
+        if dest_mask is None:
+            dest_mask = self.scheme.rho_dests
+        self.call("sphb_density", self.cur, dest_mask, 1 if eos else 0)
+
+    def tait(self, dest_mask=None):
+        if dest_mask is None:
+            dest_mask = sum(1 << a for a in self.scheme.tait_on)
+        self.call("sphb_tait", self.cur, dest_mask)
+
+    def momentum(self, dest_mask=None, gravity=True, mode=0):
+        if dest_mask is None:
+            dest_mask = self.scheme.mom_dests
+        self.call("sphb_momentum", self.cur, dest_mask, 1 if gravity else 0, mode)
+
+    def pc_stage(self, stage: int):
+        self.call("sphb_pc_stage", self.cur, stage)
+        self._box_valid = True
+
+    def step_begin(self):
+        self.call("sphb_step_begin")
+
+    def eval_stage(self):
+        """Integrator.eval of the pinned scheme at the current positions."""
+        self.density()
+        self.momentum()
+
+    def pc_step(self):
+        """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
+        preceded by the Solver's per-step prologue (count, dt)."""
+        self.step_begin()
+        self.bin(0)
+        self.eval_stage()
+        self.pc_stage(0)
+        self.bin(nat.BIN_MOVE_INITIAL)
+        self.eval_stage()
+        self.pc_stage(1)
+
+    # ---------------------------------------------------------- host sync
+    def status(self) -> int:
+        off = self.work_offsets[nat.WORK_NAMES.index("status")]
+        return int(self.work_buf[off:off + 4].view(torch.int32).item())
+
+    def clear_status(self):
+        off = self.work_offsets[nat.WORK_NAMES.index("status")]
+        self.work_buf[off:off + 4].zero_()
+
+    def check_status(self):
+        st = self.status()
+        if st:
+            raise RuntimeError("engine status: " + nat.status_message(st))
+
+    def pair_counts(self):
+        off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
+        v = self.work_buf[off:off + 32].view(torch.int64).tolist()
+        return v[0], v[1]
+
+    def reset_pair_counts(self):
+        off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
+        self.work_buf[off:off + 32].zero_()
+
+    def scene_state(self):
+        raw = self.sstate_dev.cpu().numpy().tobytes()
+        arr = (nat.SceneState * self.S).from_buffer_copy(raw)
+        return [arr[s] for s in range(self.S)]
+
+    def set_dt(self, dt):
+        st = (nat.SceneState * self.S).from_buffer_copy(self.sstate_dev.cpu().numpy().tobytes())
+        dts = dt if isinstance(dt, (list, tuple, np.ndarray)) else [dt] * self.S
+        for s in range(self.S):
+            st[s].dt = float(dts[s])
+        self.sstate_dev.copy_(_struct_to_device(st, self.device))
+
+    # --------------------------------------------------------- exchange
+    def exchange_in(self, array: int, name: str, values: torch.Tensor):
+        """User-order FP64 values (scenes concatenated) -> engine."""
+        v = values.to(device=self.device, dtype=torch.float64).contiguous()
+        if v.numel() != self.user_n[array]:
+            raise ValueError("size mismatch")
+        self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 0,
+                  v.data_ptr(), self.user_offset[array].data_ptr())
+        self._keep = v  # keep alive until the stream passes it
+
+    def exchange_out(self, array: int, name: str, out: torch.Tensor | None = None):
+        """Engine -> user-order FP64 tensor (scenes concatenated)."""
+        if out is None:
+            out = torch.empty(self.user_n[array], dtype=torch.float64, device=self.device)
+        self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 1,
+                  out.data_ptr(), self.user_offset[array].data_ptr())
+        return out
+
+    def exchange_tag(self, array: int, values: torch.Tensor, direction: int):
+        v = values.to(device=self.device, dtype=torch.int32).contiguous()
+        self.call("sphb_exchange_tag", self.cur, array, direction, v.data_ptr(),
+                  self.user_offset[array].data_ptr())
+        return v
+
+    def get(self, array: int, name: str, scene: int | None = None):
+        out = self.exchange_out(array, name)
+        if scene is None:
+            return out
+        o = int(self.user_offset_host[array][scene])
+        return out[o:o + int(self.sizes[scene, array])]
+
+    # ------------------------------------------------------- inspection
+    def neighbors(self, dest_array: int, src_mask: int, scene: int = 0):
+        """Neighbour pairs of scene `scene`, dest array `dest_array`, with the
+        FP64 reference predicate: numpy arrays (dest user index, source array,
+        source user index), lexicographically sorted."""
+        dev = self.device
+        counts = torch.zeros(self.N, dtype=torch.int32, device=dev)
+        dm = 1 << dest_array
+        self.call("sphb_neighbors", self.cur, dm, src_mask, counts.data_ptr(),
+                  None, None, 0)
+        c64 = counts.to(torch.int64)
+        offs = torch.cumsum(c64, 0) - c64
+        total = int(c64.sum().item())
+        out = torch.zeros(max(total, 1), dtype=torch.int32, device=dev)
+        self.call("sphb_neighbors", self.cur, dm, src_mask, counts.data_ptr(),
+                  offs.data_ptr(), out.data_ptr(), total)
+        self.check_status()
+        idx = self.bufs[self.cur]["idx"].cpu().numpy()
+        counts = counts.cpu().numpy()
+        out = out[:total].cpu().numpy()
+        seg = self.seg_offset_host
+        k = np.repeat(np.arange(self.N), counts)
+        seg_of = np.searchsorted(seg, np.arange(self.N), side="right") - 1
+        keep = seg_of[k] == scene * self.A + dest_array
+        k = k[keep]
+        j = out[keep]
+        sj = seg_of[j]
+        d_user = idx[k]
+        s_arr = sj % self.A
+        j_user = idx[j]
+        order = np.lexsort((j_user, s_arr, d_user))
+        return d_user[order], s_arr[order], j_user[order]
+
+    def cell_coords(self, scene: int = 0, array: int = 0):
+        """Global integer cell coordinates floor(x / cell_size) per user
+        particle of (scene, array)."""
+        out = torch.zeros(self.N * 3, dtype=torch.int32, device=self.device)
+        self.call("sphb_cell_coords", self.cur, out.data_ptr())
+        out = out.view(self.N, 3).cpu().numpy()
+        g = scene * self.A + array
+        b, e = self.seg_offset_host[g], self.seg_offset_host[g + 1]
+        idx = self.bufs[self.cur]["idx"][b:e].cpu().numpy()
+        res = np.empty((e - b, 3), np.int32)
+        res[idx] = out[b:e]
+        return res
+
+    def cell_size(self, scene: int = 0) -> float:
+        return self._scene_host[scene].cell_size
+
+
+def _canon(name: str) -> str:
+    return {"x0": "_x0", "y0": "_y0", "z0": "_z0", "u0": "_u0", "v0": "_v0",
+            "w0": "_w0", "au": "_a_u_1", "av": "_a_v_1", "aw": "_a_w_1"}.get(name, name)
+
+
+def _np(v):
+    if isinstance(v, torch.Tensor):
+        return v.detach().cpu().numpy()
+    return v
+
+
+def _np_b(v, n):
+    v = _np(v)
+    return np.ascontiguousarray(np.broadcast_to(np.asarray(v), (n,)))
+
+
+def _struct_to_device(cstruct, device):
+    raw = ctypes.string_at(ctypes.addressof(cstruct), ctypes.sizeof(cstruct))
+    t = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+    return t.to(device)

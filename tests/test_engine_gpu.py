@@ -1,0 +1,239 @@
+"""Parity of the sm_100a engine (through the C ABI) with the oracle.
+
+Integer work is compared bit for bit: cell coordinates floor(x / cs) and
+neighbour sets (sorted index lists) against the reference algorithm.
+Floating point: FP64 against the oracle to 1e-12 (densities) / 1e-10
+(accelerations, relative to the largest); FP32C (FP32 pair sums with Kahan
+compensation) to 1e-5 relative density error, the accuracy bar of the FP32
+path, and 1e-4 for accelerations relative to the largest.
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import (oracle_from, oracle_density_eos, oracle_momentum, rel_err,
+                     pairs_from_oracle)
+from pysph_b200 import workloads as W
+from pysph_b200.engine import Engine, fluid_scheme, SceneParams
+from pysph_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+RHO_TOL = {"fp64": 1e-12, "fp32c": 1e-5}
+ACC_TOL = {"fp64": 1e-10, "fp32c": 1e-4}
+
+
+def drop(dx=0.025):
+    arrays, types, params = W.elliptical_drop(dx=dx)
+    return arrays, params, fluid_scheme(1), 2
+
+
+def small_dam(dx=0.02):
+    arrays, types, params = W.dam_break(dx=dx)
+    return arrays, params, fluid_scheme(2), 2
+
+
+def lattice(n=20):
+    arrays, types, params = W.lattice3d(n=n)
+    return arrays, params, fluid_scheme(1), 3
+
+
+CASES = {"drop": drop, "dam": small_dam, "lattice3d": lattice}
+
+
+def engine_for(case, precision, **kw):
+    arrays, params, scheme, dim = CASES[case]()
+    eng = Engine([(arrays, params)], scheme, dim=dim, precision=precision, **kw)
+    return eng, arrays, params, scheme, dim
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_cell_coords_bit_exact(case):
+    eng, arrays, params, scheme, dim = engine_for(case, "fp64")
+    cs = eng.cell_size()
+    # CellManager cell size = 2 * max h over all arrays (S/base/cell.pyx:911-941)
+    max_h = max(float(np.max(a["h"])) for a in arrays)
+    assert cs == 2.0 * max_h
+    import oracle
+    for a, arr in enumerate(arrays):
+        got = eng.cell_coords(0, a)
+        ref = oracle.cell_ids(arr["x"], arr["y"], arr["z"], cs)
+        if dim == 2:
+            ref[:, 2] = 0
+        np.testing.assert_array_equal(got, ref)
+    eng.check_status()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("stencil", [1, 2])
+def test_neighbor_sets_bit_exact(case, stencil):
+    eng, arrays, params, scheme, dim = engine_for(case, "fp64", stencil=stencil)
+    osys = oracle_from(arrays, params, scheme, dim)
+    A = len(arrays)
+    osys.update_pairs([(d, s) for d in range(A) for s in range(A)])
+    for d in range(A):
+        for s in range(A):
+            di, sa, sj = eng.neighbors(d, 1 << s)
+            assert np.all(sa == s)
+            odi, osj = pairs_from_oracle(osys, d, s)
+            np.testing.assert_array_equal(di, odi)
+            np.testing.assert_array_equal(sj, osj)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("lanes", [1, 4])
+def test_density_eos(case, precision, lanes):
+    eng, arrays, params, scheme, dim = engine_for(case, precision, lanes=lanes)
+    osys = oracle_from(arrays, params, scheme, dim)
+    osys.update()
+    oracle_density_eos(osys, scheme)
+    eng.density()
+    eng.check_status()
+    for a in range(len(arrays)):
+        rho = eng.get(a, "rho").cpu().numpy()
+        ref = osys.arrays[a].rho
+        err = np.max(np.abs(rho - ref) / np.abs(ref))
+        assert err <= RHO_TOL[precision], (a, err)
+        p = eng.get(a, "p").cpu().numpy()
+        B = params["c0"] ** 2 * params["rho0"] / params["gamma"]
+        assert rel_err(p, osys.arrays[a].p, scale=B) <= 10 * RHO_TOL[precision]
+    npairs, _ = eng.pair_counts()
+    total = sum(len(osys.neighbors(d, s)[1]) for d, srcs in scheme.rho_src.items()
+                for s in srcs)
+    if precision == "fp64":
+        assert npairs == total
+    else:
+        assert abs(npairs - total) <= max(2, total * 1e-5)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("lanes", [1, 8])
+def test_momentum(case, precision, lanes):
+    eng, arrays, params, scheme, dim = engine_for(case, precision, lanes=lanes)
+    osys = oracle_from(arrays, params, scheme, dim)
+    osys.update()
+    oracle_density_eos(osys, scheme)
+    oracle_momentum(osys, scheme)
+    eng.density()
+    eng.momentum()
+    eng.check_status()
+    for d in scheme.mom_src:
+        O = osys.arrays[d]
+        names = ("au", "av", "aw")[:dim]
+        refs = [O.au, O.av, O.aw][:dim]
+        scale = max(np.max(np.abs(r)) for r in refs)
+        for nm, ref in zip(names, refs):
+            got = eng.get(d, nm).cpu().numpy()
+            assert rel_err(got, ref, scale) <= ACC_TOL[precision], nm
+        dtf = eng.get(d, "dt_fac").cpu().numpy()
+        assert rel_err(dtf, O.dt_fac) <= ACC_TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_drop_trajectory(precision):
+    arrays, params, scheme, dim = drop()
+    params = dict(params, dt=1e-5)
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision)
+    osys = oracle_from(arrays, params, scheme, dim)
+    for _ in range(10):
+        eng.pc_step()
+        osys.pc_step(1e-5)
+    eng.check_status()
+    O = osys.arrays[0]
+    x = eng.get(0, "x").cpu().numpy()
+    y = eng.get(0, "y").cpu().numpy()
+    u = eng.get(0, "u").cpu().numpy()
+    tol_x = 1e-13 if precision == "fp64" else 1e-9
+    assert np.max(np.abs(x - O.x)) <= tol_x
+    assert np.max(np.abs(y - O.y)) <= tol_x
+    assert rel_err(u, O.u) <= (1e-12 if precision == "fp64" else 1e-7)
+    rho = eng.get(0, "rho").cpu().numpy()
+    assert np.max(np.abs(rho - O.rho) / O.rho) <= RHO_TOL[precision]
+    st = eng.scene_state()[0]
+    assert st.count == 10
+    assert st.t == pytest.approx(1e-4)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dam_break_cfl(precision):
+    arrays, params, scheme, dim = small_dam()
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision)
+    osys = oracle_from(arrays, params, scheme, dim)
+    dts = []
+    for _ in range(6):
+        dt = osys.cfl_time_step(params["cfl"], params["c0"], params["dt_initial"])
+        osys.pc_step(dt)
+        dts.append(dt)
+        eng.pc_step()
+        st = eng.scene_state()[0]
+        if precision == "fp64":
+            assert st.dt == pytest.approx(dt, rel=1e-12)
+        else:
+            assert st.dt == pytest.approx(dt, rel=1e-5)
+    eng.check_status()
+    O = osys.arrays[0]
+    for nm in ("x", "y"):
+        got = eng.get(0, nm).cpu().numpy()
+        assert np.max(np.abs(got - getattr(O, nm))) <= (1e-12 if precision == "fp64" else 1e-9)
+    rho = eng.get(1, "rho").cpu().numpy()
+    assert np.max(np.abs(rho - osys.arrays[1].rho) / osys.arrays[1].rho) <= RHO_TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_batched_scenes_match_single(precision):
+    scenes = W.batched_drops(num_scenes=5, seed=1, n_lo=300, n_hi=1500)
+    specs = [(arrs, dict(p, dt=1e-5)) for arrs, _, p in scenes]
+    eng = Engine(specs, fluid_scheme(1), dim=2, precision=precision, lanes=4)
+    for _ in range(4):
+        eng.pc_step()
+    eng.check_status()
+    for s, (arrs, p) in enumerate(specs):
+        osys = oracle_from(arrs, p, fluid_scheme(1), 2)
+        for _ in range(4):
+            osys.pc_step(1e-5)
+        x = eng.get(0, "x", scene=s).cpu().numpy()
+        rho = eng.get(0, "rho", scene=s).cpu().numpy()
+        assert np.max(np.abs(x - osys.arrays[0].x)) <= (1e-13 if precision == "fp64" else 1e-9)
+        assert np.max(np.abs(rho - osys.arrays[0].rho) / osys.arrays[0].rho) <= RHO_TOL[precision]
+
+
+def test_free_fall_closed_form():
+    n = 6
+    arr = dict(x=np.arange(n) * 10.0, y=np.zeros(n), z=np.zeros(n),
+               u=np.linspace(-1, 1, n), v=np.zeros(n), w=np.zeros(n),
+               m=np.ones(n), h=np.full(n, 0.1), rho=np.ones(n), p=np.zeros(n),
+               cs=np.ones(n))
+    params = dict(c0=1.0, rho0=1.0, alpha=0.1, beta=0.0, gravity=(0.0, -9.81, 0.0),
+                  dt=1e-3)
+    eng = Engine([([arr], params)], fluid_scheme(1), dim=2, precision="fp64")
+    for _ in range(100):
+        eng.pc_step()
+    t = 0.1
+    np.testing.assert_allclose(eng.get(0, "x").cpu().numpy(), arr["x"] + arr["u"] * t,
+                               rtol=0, atol=1e-12)
+    np.testing.assert_allclose(eng.get(0, "y").cpu().numpy(), -0.5 * 9.81 * t * t, rtol=1e-10)
+
+
+def test_nonfinite_position_reported_not_faulted():
+    """A NaN position planted on the host is caught by the binning bounds
+    checks and reported through the status word; nothing is written out of
+    bounds and the context stays usable."""
+    arrays, params, scheme, dim = drop(dx=0.1)
+    arrays[0]["x"] = arrays[0]["x"].copy()
+    arrays[0]["x"][3] = np.nan
+    eng = Engine([(arrays, params)], scheme, dim=2, precision="fp64")
+    st = eng.status()
+    assert st & nat.ST_NONFINITE_POS
+    eng.clear_status()
+    assert eng.status() == 0
+    torch.cuda.synchronize()
+
+
+def test_grid_overflow_reported():
+    arrays, params, scheme, dim = drop(dx=0.1)
+    eng = Engine([(arrays, params)], scheme, dim=2, precision="fp64",
+                 cell_capacity=16)
+    assert eng.status() & nat.ST_GRID_OVERFLOW
+    torch.cuda.synchronize()
