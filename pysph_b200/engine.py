@@ -549,7 +549,7 @@ def _np(v):
 
 def _np_b(v, n):
     v = _np(v)
-    return np.ascontiguousarray(np.broadcast_to(np.asarray(v), (n,)))
+    return np.array(np.broadcast_to(np.asarray(v), (n,)))
 
 
 def _struct_to_device(cstruct, device):
