@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="only the timed steps (no FP64 leg, e2e, per-kernel timing)")
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--pair-block", type=int, default=0)
     ap.add_argument("--stencil", type=int, default=1)
@@ -111,6 +113,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, timeout=3.0):
+        """Block until nvidia-smi has produced a sample (it needs ~0.2 s to
+        start), so the samples cover the timed region that follows."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -213,6 +222,8 @@ def run_ours(args, rank, world, local):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    # clocks are sampled from the warm-up through the end of the timed region
+    clk = ClockSampler(local).__enter__()
     for _ in range(max(args.warmup, 3)):
         eng.pc_step()
     torch.cuda.synchronize()
@@ -252,13 +263,14 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.zero_()
-            starts[i].record(stream)
-            step()
-            ends[i].record(stream)
-        torch.cuda.synchronize()
+    clk.wait_first()
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    clk.__exit__(None, None, None)
     if world > 1:
         dist.barrier()
     ms = sum(starts[i].elapsed_time(ends[i]) for i in range(args.steps))
@@ -269,6 +281,14 @@ def run_ours(args, rank, world, local):
     pairs_all = sum_over_ranks(pairs, world)
     value = pairs_all / (ms_max / 1e3)
     steps_per_s = args.steps / (ms_max / 1e3)
+
+    if args.no_extras:
+        out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
+               "n_gpus": world, "steps": args.steps, "ms_per_step": ms_max / args.steps,
+               "steps_per_s": steps_per_s, "config": {"workload": args.workload},
+               "clocks": clk.summary()}
+        del graph
+        return out
 
     # ---- per-kernel timing for the roofline (one rebin + one stage)
     kern = kernel_times(eng, flush, stream)

@@ -21,10 +21,16 @@ pytestmark = pytest.mark.gpu
 
 RHO_TOL = {"fp64": 1e-12, "fp32c": 1e-5}
 ACC_TOL = {"fp64": 1e-10, "fp32c": 1e-4}
-# trajectories over a few steps, absolute position error (domains of size
-# 1-4): FP64 to round-off; FP32C accelerations carry ~1e-7 relative error,
-# which moves particles by ~1e-10 per step
-POS_TOL = {"fp64": 1e-12, "fp32c": 1e-8}
+# trajectories over <= 10 steps: position error in units of the particle
+# spacing dx, max|x - x_ref| / dx.  FP64 to round-off; FP32C accelerations
+# carry ~1e-7..1e-6 relative error (the Tait EOS amplifies a density error
+# by 7 B / rho0), which moves particles by ~1e-9 of a unit per step.
+TRAJ_TOL = {"fp64": 1e-10, "fp32c": 2e-6}
+
+
+def traj_err(got, ref, h):
+    dx = float(np.max(h)) / 1.3
+    return float(np.max(np.abs(got - ref)) / dx)
 
 
 def drop(dx=0.025):
@@ -149,10 +155,9 @@ def test_drop_trajectory(precision):
     x = eng.get(0, "x").cpu().numpy()
     y = eng.get(0, "y").cpu().numpy()
     u = eng.get(0, "u").cpu().numpy()
-    tol_x = POS_TOL[precision]
-    assert np.max(np.abs(x - O.x)) <= tol_x
-    assert np.max(np.abs(y - O.y)) <= tol_x
-    assert rel_err(u, O.u) <= (1e-12 if precision == "fp64" else 1e-7)
+    assert traj_err(x, O.x, arrays[0]["h"]) <= TRAJ_TOL[precision]
+    assert traj_err(y, O.y, arrays[0]["h"]) <= TRAJ_TOL[precision]
+    assert rel_err(u, O.u) <= (1e-12 if precision == "fp64" else 1e-6)
     rho = eng.get(0, "rho").cpu().numpy()
     assert np.max(np.abs(rho - O.rho) / O.rho) <= RHO_TOL[precision]
     st = eng.scene_state()[0]
@@ -180,7 +185,7 @@ def test_dam_break_cfl(precision):
     O = osys.arrays[0]
     for nm in ("x", "y"):
         got = eng.get(0, nm).cpu().numpy()
-        assert np.max(np.abs(got - getattr(O, nm))) <= POS_TOL[precision]
+        assert traj_err(got, getattr(O, nm), arrays[0]["h"]) <= TRAJ_TOL[precision]
     rho = eng.get(1, "rho").cpu().numpy()
     assert np.max(np.abs(rho - osys.arrays[1].rho) / osys.arrays[1].rho) <= RHO_TOL[precision]
 
@@ -199,7 +204,7 @@ def test_batched_scenes_match_single(precision):
             osys.pc_step(1e-5)
         x = eng.get(0, "x", scene=s).cpu().numpy()
         rho = eng.get(0, "rho", scene=s).cpu().numpy()
-        assert np.max(np.abs(x - osys.arrays[0].x)) <= POS_TOL[precision]
+        assert traj_err(x, osys.arrays[0].x, arrs[0]["h"]) <= TRAJ_TOL[precision]
         assert np.max(np.abs(rho - osys.arrays[0].rho) / osys.arrays[0].rho) <= RHO_TOL[precision]
 
 
