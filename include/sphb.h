@@ -280,6 +280,38 @@ SPHB_API int sphb_exchange_tag(const sphb_engine *e, int cur, int array, int dir
 /* Write identity idx (0..n-1 inside each segment) into buf[cur].idx. */
 SPHB_API int sphb_init_index(const sphb_engine *e, int cur, void *stream);
 
+/* ---- neighbour counts without caller scratch ------------------------ */
+
+/* Largest particle set sphb_neighbor_counts_static accepts. */
+#define SPHB_STATIC_MAX_PARTICLES (1 << 18)
+
+/* Neighbour count of every particle of one particle set: counts[i] = number
+ * of j (self included) with |x_i - x_j|^2 < (radius_scale * h_i)^2, the FP64
+ * predicate of sphb_neighbors; -1 for a particle with a non-finite position.
+ * x, y, z (z may be NULL when dim == 2), h and counts are device arrays of n
+ * elements in the caller's order.
+ *
+ * It has no counterpart in the reference.  It exists for callers that cannot
+ * call cudaMalloc -- a host application whose own memory manager owns all
+ * device memory and gives this library only the particle arrays, or code on
+ * a latency-critical path where cudaMalloc's implicit device-wide
+ * synchronisation is not acceptable -- and so cannot provide the workspace
+ * the engine entry points take.  Its scratch is one file-scope device array
+ * inside the library of about 7 MiB (cell tables for up to 2^19 cells plus
+ * three int32 arrays of SPHB_STATIC_MAX_PARTICLES), which every GPU that
+ * loads the library holds until the process exits.  n above
+ * SPHB_STATIC_MAX_PARTICLES returns SPHB_ERR_WORKSPACE; the cell size grows
+ * past radius_scale * max h when a grid would need more than 2^19 cells.
+ * The call allocates nothing (no cudaMalloc, cudaFree or allocating library
+ * routine).  Its first call on a device looks up the scratch array's device
+ * address with that device current; make that first call before any stream
+ * capture.  All calls share the one array, which keeps the last call's
+ * contents, so calls that overlap on the GPU race: serialise them. */
+SPHB_API int sphb_neighbor_counts_static(int32_t n, int32_t dim, const double *x,
+                                         const double *y, const double *z,
+                                         const double *h, double radius_scale,
+                                         int32_t *counts, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -138,6 +138,7 @@ def lib():
         "sphb_exchange": (i32, [E, i32, i32, i32, i32, vp, vp, vp]),
         "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
         "sphb_init_index": (i32, [E, i32, vp]),
+        "sphb_neighbor_counts_static": (i32, [i32, i32, vp, vp, vp, vp, f64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -153,7 +154,10 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_workspace_layout", "sphb_box_init", "sphb_bin",
             "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
-            "sphb_exchange", "sphb_exchange_tag", "sphb_init_index")
+            "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
+            "sphb_neighbor_counts_static")
+
+STATIC_MAX_PARTICLES = 1 << 18
 
 
 def check(rc: int, what: str):

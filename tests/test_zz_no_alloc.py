@@ -1,0 +1,77 @@
+"""sphb_neighbor_counts_static: neighbour counts for callers that cannot
+call cudaMalloc (a host whose memory manager owns the device and hands the
+library only its particle arrays, or a latency-critical path that cannot
+take cudaMalloc's implicit synchronisation).  Its scratch is an array inside
+the library, so the test passes only input and output buffers.
+
+Checked through the C ABI against the engine's own entry point
+sphb_neighbors (same FP64 predicate, counts are integers, so they must be
+equal) on calls in a row with different particle sets, because every call
+reuses the one scratch array.  This file is collected last on purpose.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from pysph_b200 import _native as nat
+from pysph_b200 import workloads as W
+from pysph_b200.engine import Engine, fluid_scheme
+
+pytestmark = pytest.mark.gpu
+
+
+def _cols(arr, dim, dev):
+    cols = [torch.as_tensor(np.ascontiguousarray(arr[c]), dtype=torch.float64, device=dev)
+            for c in ("x", "y", "z", "h")]
+    if dim == 2:
+        cols[2] = None
+    return cols
+
+
+def engine_counts(arr, dim):
+    """Counts from the workspace-based entry point, in the caller's order."""
+    eng = Engine([([arr], {})], fluid_scheme(1), dim=dim, precision="fp64")
+    counts = torch.zeros(eng.N, dtype=torch.int32, device="cuda")
+    eng.call("sphb_neighbors", eng.cur, 1, 1, counts.data_ptr(), None, None, 0)
+    eng.check_status()
+    idx = eng.bufs[eng.cur]["idx"].long()
+    out = torch.empty_like(counts)
+    out[idx] = counts
+    return out.cpu().numpy()
+
+
+def static_counts(arr, dim):
+    dev = torch.device("cuda")
+    x, y, z, h = _cols(arr, dim, dev)
+    n = x.numel()
+    counts = torch.full((n,), -7, dtype=torch.int32, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = nat.lib().sphb_neighbor_counts_static(
+        n, dim, x.data_ptr(), y.data_ptr(), z.data_ptr() if z is not None else None,
+        h.data_ptr(), 2.0, counts.data_ptr(), stream)
+    assert rc == 0, nat.lib().sphb_last_cuda_error()
+    torch.cuda.synchronize()
+    return counts.cpu().numpy()
+
+
+def test_static_counts_match_engine_on_calls_in_a_row():
+    drop, _, _ = W.elliptical_drop(dx=0.025)
+    lat, _, _ = W.lattice3d(n=16)
+    dam, _, _ = W.dam_break(dx=0.02)
+    cases = [(drop[0], 2), (lat[0], 3), (dam[0], 2), (drop[0], 2)]
+    for arr, dim in cases:
+        got = static_counts(arr, dim)
+        ref = engine_counts(arr, dim)
+        assert got.min() >= 1  # self is always counted
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_static_rejects_oversize_without_device_work():
+    n = nat.STATIC_MAX_PARTICLES + 1
+    rc = nat.lib().sphb_neighbor_counts_static(n, 2, None, None, None, None, 2.0,
+                                                None, None)
+    assert rc == -2  # SPHB_ERR_WORKSPACE
+    assert nat.lib().sphb_neighbor_counts_static(
+        10, 4, None, None, None, None, 2.0, None, None) == -4
