@@ -57,7 +57,8 @@ def parse():
                     help="only the timed steps (no FP64 leg, e2e, per-kernel timing)")
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--pair-block", type=int, default=0)
-    ap.add_argument("--stencil", type=int, default=1)
+    ap.add_argument("--stencil", type=int, default=0,
+                    help="fix the cell size (support / R); default: autotuned")
     return ap.parse_args()
 
 
@@ -214,10 +215,18 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wl = workload(args.workload)
-    lanes = args.lanes or (4 if wl["dim"] == 3 else 1)
-    pb = args.pair_block or 128
+    tune = None
+    if args.lanes or args.pair_block or args.stencil:
+        lanes = args.lanes or (4 if wl["dim"] == 3 else 1)
+        pb = args.pair_block or 128
+        stencil = args.stencil or 1
+    else:
+        from pysph_b200.autotune import autotune
+        tune = autotune(wl["scenes"], wl["scheme"], wl["dim"], args.precision, device=dev)
+        lanes, pb, stencil = tune["lanes"], tune["pair_block"], tune["stencil"]
+    args.stencil = stencil
     eng = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=args.precision,
-                 stencil=args.stencil, lanes=lanes, pair_block=pb, device=dev)
+                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev)
     N = eng.N
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -315,6 +324,8 @@ def run_ours(args, rank, world, local):
                       "l2": "flushed (256 MiB write) between timed steps",
                       "parallelism": f"replicas x{world}"},
            "steps_per_s": steps_per_s,
+           "autotune": ({"chosen": {k: tune[k] for k in ("stencil", "lanes", "pair_block")},
+                         "table": tune["table"]} if tune else None),
            "pairs_per_step": pairs / args.steps,
            "gpu_launches": launches_per_step(eng) * args.steps,
            "roofline": roof, "clocks": clk.summary()}

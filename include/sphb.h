@@ -93,7 +93,8 @@ typedef struct {
     double cfl, dt_initial;      /* ViscousAndForceBasedTimeStep */
     double static_lo[3];    /* bounds of the particles the integrator never */
     double static_hi[3];    /*   moves (+inf / -inf when there are none) */
-    int32_t use_cfl;        /* 1: dt from the CFL rule, 0: dt kept as set */
+    int32_t use_cfl;        /* 0: dt kept as set; 1: viscous + force CFL rule;
+                               2: viscous rule only (ViscousTimeStep) */
     int32_t pad0;
 } sphb_scene;
 
@@ -276,6 +277,11 @@ SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
 /* Same for the int32 tag field. */
 SPHB_API int sphb_exchange_tag(const sphb_engine *e, int cur, int array, int dir,
                       int32_t *user, const int32_t *user_offset, void *stream);
+
+/* Time step of the next sphb_pc_stage for every scene without use_cfl: the
+ * dt argument of PredictorCorrectorIntegrator.integrate(dt)
+ * (S/solver/integrator.py:646). */
+SPHB_API int sphb_set_dt(const sphb_engine *e, double dt, void *stream);
 
 /* Write identity idx (0..n-1 inside each segment) into buf[cur].idx. */
 SPHB_API int sphb_init_index(const sphb_engine *e, int cur, void *stream);

@@ -138,6 +138,7 @@ def lib():
         "sphb_exchange": (i32, [E, i32, i32, i32, i32, vp, vp, vp]),
         "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
         "sphb_init_index": (i32, [E, i32, vp]),
+        "sphb_set_dt": (i32, [E, f64, vp]),
         "sphb_neighbor_counts_static": (i32, [i32, i32, vp, vp, vp, vp, f64, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -155,7 +156,7 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
             "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
-            "sphb_neighbor_counts_static")
+            "sphb_set_dt", "sphb_neighbor_counts_static")
 
 STATIC_MAX_PARTICLES = 1 << 18
 

@@ -1,0 +1,91 @@
+"""Launch-shape autotuner for the pair kernels.
+
+For a workload it times whole predictor-corrector steps for every candidate
+of cell size (stencil R: cell = support / R), lanes per dest particle and
+threads per block, and returns the fastest.  Results are cached per
+(dim, precision, particle-count bucket, scene-count bucket), in memory and,
+when PYSPH_B200_TUNE_CACHE names a file, in that JSON file.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import torch
+
+from .engine import Engine
+
+LANES = (1, 2, 4, 8)
+BLOCKS = (64, 128, 256)
+STENCILS = (1, 2)
+
+_cache: dict = {}
+
+
+def _key(dim, precision, n, scenes):
+    return f"{dim}d-{precision}-n{int(math.log2(max(n, 1)))}-s{int(math.log2(max(scenes, 1)))}"
+
+
+def _load():
+    path = os.environ.get("PYSPH_B200_TUNE_CACHE")
+    if path and os.path.exists(path):
+        try:
+            with open(path) as f:
+                _cache.update(json.load(f))
+        except (OSError, ValueError):
+            pass
+
+
+def _store():
+    path = os.environ.get("PYSPH_B200_TUNE_CACHE")
+    if path:
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(_cache, f, indent=1)
+        os.replace(tmp, path)
+
+
+def time_steps(eng: Engine, steps: int = 4, warm: int = 2) -> float:
+    """Milliseconds per PC step (CUDA events on the current stream)."""
+    for _ in range(warm):
+        eng.pc_step()
+    stream = torch.cuda.current_stream(eng.device)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        eng.pc_step()
+    b.record(stream)
+    torch.cuda.synchronize(eng.device)
+    return a.elapsed_time(b) / steps
+
+
+def autotune(scenes, scheme, dim, precision="fp32c", device=None, stencils=STENCILS,
+             lanes=LANES, blocks=BLOCKS, steps=4, force=False):
+    """Best {"stencil", "lanes", "pair_block", "ms_per_step"} plus the table of
+    every candidate timed."""
+    _load()
+    n = sum(len(a["x"]) for arrays, _ in scenes for a in arrays)
+    key = _key(dim, precision, n, len(scenes))
+    if not force and key in _cache:
+        return _cache[key]
+    table = []
+    for R in stencils:
+        eng = Engine(scenes, scheme, dim=dim, precision=precision, stencil=R,
+                     device=device)
+        for L in lanes:
+            for B in blocks:
+                if B % L or B // L < 8:
+                    continue
+                eng.set_launch(L, B)
+                ms = time_steps(eng, steps)
+                eng.check_status()
+                table.append({"stencil": R, "lanes": L, "pair_block": B,
+                              "ms_per_step": ms})
+        del eng
+    best = min(table, key=lambda r: r["ms_per_step"])
+    res = dict(best, key=key, table=table)
+    _cache[key] = res
+    _store()
+    return res

@@ -1,9 +1,10 @@
 // sphb_bin.cu -- cell binning for the particle engine (sm_100a).
 //
 // One rebin = scene boxes -> per-scene grids -> cell key per particle ->
-// counting sort (histogram, two-level scan, scatter, per-cell sort that makes
-// the order stable by engine position) -> gather of the particle state into
-// the other buffer in cell order, plus the FP32 pair records.
+// counting sort (histogram, two-level scan, scatter) -> gather of the
+// particle state into the other buffer in cell order, ranking the members of
+// each cell by previous engine position so the order is deterministic, plus
+// the FP32 pair records.
 //
 // The reference bins with a Python dict of cells keyed by floor(x / cs)
 // (CellManager._insert_particles, S/base/cell.pyx:1229-1300); its OpenCL
@@ -291,73 +292,38 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_scatter(const __grid_constan
     e.work.perm[pos] = k;
 }
 
-// The particle holding slot 0 of its cell sorts the cell's perm entries, so
-// the order inside a cell is by previous engine position (deterministic).
-__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_cell_sort(const __grid_constant__ sphb_engine e)
-{
-    const sphb_tile t = e.tiles[blockIdx.x];
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
-    const int key = e.work.key[k];
-    if (key < 0 || e.work.slot[k] != 0) return;
-    const int b = e.work.start[key], en = e.work.start[key + 1];
-    const int len = en - b;
-    if (len <= 1) return;
-    if (b < 0 || en > e.cfg.num_particles) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        return;
-    }
-    int *p = e.work.perm + b;
-    if (len <= 32) {
-        int v[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i < len) v[i] = p[i];
-        for (int i = 1; i < len; ++i) {
-            const int x = v[i];
-            int j = i - 1;
-            while (j >= 0 && v[j] > x) {
-                v[j + 1] = v[j];
-                --j;
-            }
-            v[j + 1] = x;
-        }
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i < len) p[i] = v[i];
-    } else {
-        // shell sort (Ciura gaps) in place for crowded cells
-        const int gaps[8] = {701, 301, 132, 57, 23, 10, 4, 1};
-        for (int g = 0; g < 8; ++g) {
-            const int gap = gaps[g];
-            for (int i = gap; i < len; ++i) {
-                const int x = p[i];
-                int j = i;
-                while (j >= gap && p[j - gap] > x) {
-                    p[j] = p[j - gap];
-                    j -= gap;
-                }
-                p[j] = x;
-            }
-        }
-    }
-}
-
 // -------------------------------------------------------------- reorder --
+// Thread k takes particle p = perm[k] (the scatter put it somewhere inside
+// its cell's range [b, e)), ranks it among the cell's members by previous
+// engine position, and writes it to b + rank: the order inside a cell is
+// deterministic whatever order the atomics handed out the slots.
 template <int DIM, bool F32>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
 {
     const sphb_tile t = e.tiles[blockIdx.x];
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
+    const int kk = t.begin + threadIdx.x;
+    if (kk >= t.end) return;
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;
     const int seg_lo = e.seg_offset[t.seg], seg_hi = e.seg_offset[t.seg + 1];
-    int p = e.work.perm[k];
+    const int p = e.work.perm[kk];
     if (p < seg_lo || p >= seg_hi) {
         flag(e, SPHB_ST_BAD_INDEX);
-        p = k;
+        return;
+    }
+    int k = kk;
+    {
+        const int key = e.work.key[p];
+        const int b = key >= 0 ? e.work.start[key] : -1;
+        const int en = key >= 0 ? e.work.start[key + 1] : -1;
+        if (b < seg_lo || en > seg_hi || kk < b || kk >= en) {
+            flag(e, SPHB_ST_BAD_INDEX);
+            return;
+        }
+        int rank = 0;
+        for (int i = b; i < en; ++i) rank += (e.work.perm[i] < p) ? 1 : 0;
+        k = b + rank;
     }
     const sphb_buffers &S = e.buf[cur];
     const sphb_buffers &D = e.buf[cur ^ 1];
@@ -474,7 +440,6 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
     k_scan_apply<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e);
     if (nt > 0) {
         k_scatter<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e);
-        k_cell_sort<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e);
         const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
         if (c.dim == 2 && c.precision == SPHB_FP32C)
             k_reorder<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);

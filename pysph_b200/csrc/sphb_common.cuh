@@ -89,6 +89,14 @@ __device__ __forceinline__ T block_reduce(T v, Op op, T identity)
     return v;  // valid in thread 0
 }
 
+template <typename T, typename Op>
+__device__ __forceinline__ T warp_reduce(T v, Op op)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;  // valid in every lane
+}
+
 struct OpMin {
     __device__ __forceinline__ double operator()(double a, double b) const
     {

@@ -138,8 +138,9 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             if (!isfinite(rho) || !isfinite(p)) flag(e, SPHB_ST_NONFINITE_RHO);
         }
     }
-    const unsigned long long tot = block_reduce(np, OpAddU64(), 0ull);
-    if (threadIdx.x == 0 && tot) atomicAdd(&e.work.pairs[0], tot);
+    // warp-level, so warps that finish early leave without a block barrier
+    const unsigned long long tot = warp_reduce(np, OpAddU64());
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&e.work.pairs[0], tot);
 }
 
 // Tait alone (rho given).

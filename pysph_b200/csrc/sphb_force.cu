@@ -224,10 +224,11 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         }
         if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
     }
-    const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
-    const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
-    const unsigned long long tot = block_reduce(np, OpAddU64(), 0ull);
-    if (threadIdx.x == 0) {
+    // warp-level, so warps that finish early leave without a block barrier
+    const double bdt = warp_reduce(dtf_out, OpMax());
+    const double ba2 = warp_reduce(isfinite(a2) ? a2 : 0.0, OpMax());
+    const unsigned long long tot = warp_reduce(np, OpAddU64());
+    if ((threadIdx.x & 31) == 0) {
         sphb_scene_state &sw = e.sstate[s];
         atomic_max_nonneg(&sw.max_dtfac, bdt);
         atomic_max_nonneg(&sw.max_acc2, ba2);

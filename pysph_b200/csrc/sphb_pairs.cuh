@@ -52,11 +52,18 @@ __device__ __forceinline__ bool for_each_candidate(
                     atomicOr(status, (unsigned)SPHB_ST_BAD_INDEX);
                     return false;
                 }
-                for (int j = bd[0] + lane; j < bd[2 * R + 1]; j += LANES) {
-                    int o = -R;
+                if (LANES == 1) {
+                    // one loop per cell: the x offset is loop-invariant
 #pragma unroll
-                    for (int i = 1; i <= 2 * R; ++i) o += (j >= bd[i]) ? 1 : 0;
-                    f(j, o, dy, dz);
+                    for (int c = 0; c <= 2 * R; ++c)
+                        for (int j = bd[c]; j < bd[c + 1]; ++j) f(j, c - R, dy, dz);
+                } else {
+                    for (int j = bd[0] + lane; j < bd[2 * R + 1]; j += LANES) {
+                        int o = -R;
+#pragma unroll
+                        for (int i = 1; i <= 2 * R; ++i) o += (j >= bd[i]) ? 1 : 0;
+                        f(j, o, dy, dz);
+                    }
                 }
             }
         }

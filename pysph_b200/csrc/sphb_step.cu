@@ -116,13 +116,23 @@ __global__ void k_step_begin(const __grid_constant__ sphb_engine e)
         // ViscousTimeStep: min(cfl * h / (co + max dt_fac))
         const double dv = __ddiv_rn(__dmul_rn(sc.cfl, sc.h_min), __dadd_rn(sc.c0, dtfac));
         dt = dv < dt ? dv : dt;
-        // force criterion: cfl * min(sqrt(h / fmax)); fmax = solver.dt at count 1
-        const double fmax = st.count == 1 ? sc.dt_initial : sqrt(acc2);
-        const double df = __dmul_rn(sc.cfl, sqrt(__ddiv_rn(sc.h_min, fmax)));
-        dt = dt < df ? dt : df;
+        // force criterion (use_cfl == 1): cfl * min(sqrt(h / fmax)), with
+        // fmax = solver.dt at count 1; use_cfl == 2 is ViscousTimeStep alone
+        if (sc.use_cfl == 1) {
+            const double fmax = st.count == 1 ? sc.dt_initial : sqrt(acc2);
+            const double df = __dmul_rn(sc.cfl, sqrt(__ddiv_rn(sc.h_min, fmax)));
+            dt = dt < df ? dt : df;
+        }
         st.dt = dt;
     }
     st.t += st.dt;
+}
+
+__global__ void k_set_dt(const __grid_constant__ sphb_engine e, double dt)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= e.cfg.num_scenes || e.scene[s].use_cfl) return;
+    e.sstate[s].dt = dt;
 }
 
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
@@ -310,6 +320,15 @@ extern "C" int sphb_step_begin(const sphb_engine *e, void *stream)
     if (rc) return rc;
     k_step_begin<<<(e->cfg.num_scenes + 127) / 128, 128, 0, (cudaStream_t)stream>>>(*e);
     return launch_status("sphb_step_begin");
+}
+
+extern "C" int sphb_set_dt(const sphb_engine *e, double dt, void *stream)
+{
+    int rc = check_engine_public(e, 0);
+    if (rc) return rc;
+    if (!(dt > 0.0) || !isfinite(dt)) return SPHB_ERR_ARG;
+    k_set_dt<<<(e->cfg.num_scenes + 127) / 128, 128, 0, (cudaStream_t)stream>>>(*e, dt);
+    return launch_status("sphb_set_dt");
 }
 
 extern "C" int sphb_init_index(const sphb_engine *e, int cur, void *stream)

@@ -13,6 +13,7 @@ the sm_100a kernels of libsphb.so.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import math
 from dataclasses import dataclass, field
@@ -43,6 +44,7 @@ class SceneParams:
     cfl: float = 0.0            # > 0: ViscousAndForceBasedTimeStep
     dt_initial: float = 1e-4     # solver.dt, used by the CFL rule at step 1
     radius_scale: float = 2.0    # cubic-spline support / h
+    cfl_force: bool = True       # CFL rule with the force criterion too
 
     @staticmethod
     def from_dict(d: dict) -> "SceneParams":
@@ -134,6 +136,8 @@ class Engine:
                                  for a in range(self.A)]
         self.user_n = [int(sizes[:, a].sum()) for a in range(self.A)]
         self._stencil = stencil
+        self.force_mode = 0        # 0 MomentumEquation, 1 SPHPressureGradient
+        self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
         if cell_capacity is None:
             cell_capacity = self._estimate_capacity(grid_growth)
@@ -184,7 +188,7 @@ class Engine:
                 t.static_hi[d] = hi[d]
             t.cfl = p.cfl
             t.dt_initial = p.dt_initial
-            t.use_cfl = 1 if p.cfl > 0 else 0
+            t.use_cfl = (1 if p.cfl_force else 2) if p.cfl > 0 else 0
         self._scene_host = sc
 
     def _estimate_capacity(self, growth: float) -> int:
@@ -377,6 +381,58 @@ class Engine:
         self.cur ^= 1
         self._box_valid = False   # until a pc_stage accumulates it again
 
+    @contextlib.contextmanager
+    def masks(self, rho_src=None, mom_src=None, tait_on=None, step_on=None):
+        """Temporarily replace the scheme masks the kernels see (dest array
+        -> source bitmask), for evaluating one calc at a time."""
+        cfg = self.desc.cfg
+        saved = (list(cfg.rho_src), list(cfg.mom_src), cfg.tait_on, cfg.step_on)
+        try:
+            for a, m in (rho_src or {}).items():
+                cfg.rho_src[a] = m
+            for a, m in (mom_src or {}).items():
+                cfg.mom_src[a] = m
+            if tait_on is not None:
+                cfg.tait_on = tait_on
+            if step_on is not None:
+                cfg.step_on = step_on
+            yield
+        finally:
+            for a in range(nat.MAX_ARRAYS):
+                cfg.rho_src[a] = saved[0][a]
+                cfg.mom_src[a] = saved[1][a]
+            cfg.tait_on, cfg.step_on = saved[2], saved[3]
+
+    def update_params(self, scene=None, **kw):
+        """Change scene constants (c0, rho0, gamma, alpha, beta, eta, gravity,
+        cfl, dt_initial) and re-upload the scene table when they differ."""
+        scenes = range(self.S) if scene is None else [scene]
+        changed = False
+        for s in scenes:
+            p = self.params[s]
+            for k, v in kw.items():
+                if getattr(p, k) != v:
+                    setattr(p, k, v)
+                    changed = True
+        if not changed:
+            return
+        for s in scenes:
+            p = self.params[s]
+            t = self._scene_host[s]
+            t.c0, t.rho0, t.gamma = p.c0, p.rho0, p.gamma
+            t.B = p.c0 * p.c0 * p.rho0 / p.gamma
+            t.alpha, t.beta, t.eta = p.alpha, p.beta, p.eta
+            for d in range(3):
+                t.g[d] = float(p.gravity[d]) if d < len(p.gravity) else 0.0
+            t.cfl, t.dt_initial = p.cfl, p.dt_initial
+            t.use_cfl = (1 if p.cfl_force else 2) if p.cfl > 0 else 0
+        self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
+
+    def set_dt_async(self, dt: float):
+        """dt of the next stages for every scene without the CFL rule, set by
+        a kernel (no host round trip)."""
+        nat.check(self.L.sphb_set_dt(self._pdesc, float(dt), self.stream), "sphb_set_dt")
+
     def invalidate_box(self):
         """Positions were changed outside the integrator: the next bin
         recomputes every scene box from all particles."""
@@ -405,9 +461,13 @@ class Engine:
         self.call("sphb_step_begin")
 
     def eval_stage(self):
-        """Integrator.eval of the pinned scheme at the current positions."""
+        """Integrator.eval of the pinned scheme at the current positions:
+        SPHRho + Tait (fused), Tait on arrays without SPHRho, then
+        MomentumEquation (or SPHPressureGradient) + GravityForce."""
         self.density()
-        self.momentum()
+        if self.tait_only_mask:
+            self.tait(self.tait_only_mask)
+        self.momentum(mode=self.force_mode)
 
     def pc_step(self):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,

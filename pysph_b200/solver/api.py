@@ -1,0 +1,14 @@
+"""`import pysph_b200.solver.api as solver` -- operations, integrators,
+time-step functions and the Solver of the particle-update path."""
+from .integrator import (Integrator, PredictorCorrectorIntegrator, EulerIntegrator,
+                         fused_plan)
+from .solver import Solver
+from .sph_equation import SPHOperation, SPHIntegration
+from .time_step_functions import (TimeStep, ViscousTimeStep,
+                                  ViscousAndForceBasedTimeStep, VelocityBasedTimeStep)
+
+HAS_CL = False
+
+__all__ = ["Integrator", "PredictorCorrectorIntegrator", "EulerIntegrator", "Solver",
+           "SPHOperation", "SPHIntegration", "TimeStep", "ViscousTimeStep",
+           "ViscousAndForceBasedTimeStep", "VelocityBasedTimeStep", "fused_plan"]

@@ -1,0 +1,159 @@
+"""Solver: operations -> calcs -> integrator, and the time loop
+(S/solver/solver.py:60-590).
+
+solve() runs the reference's loop: t += dt, count += 1, update the
+particles, choose dt, integrate.  With the fused engine path and a
+viscous / force-based time-step function, dt is chosen on the GPU by the
+same rule (sphb_step_begin) and read back once per step together with the
+simulated time, which the loop needs to know when to stop.
+"""
+from __future__ import annotations
+
+import logging
+
+from ..base.kernels import CubicSplineKernel
+from ..base.particle_types import ParticleType
+from ..sph.sph_func import PositionStepping
+from .integrator import PredictorCorrectorIntegrator
+from .sph_equation import SPHIntegration, SPHOperation
+from .time_step_functions import TimeStep
+
+logger = logging.getLogger(__name__)
+
+Fluids = ParticleType.Fluid
+
+
+class Solver:
+    def __init__(self, dim, integrator_type=PredictorCorrectorIntegrator,
+                 kernel=None, **kwargs):
+        self.dim = dim
+        self.integrator_type = integrator_type
+        self.kernel = kernel or CubicSplineKernel(dim=dim)
+        self.operation_dict = {}
+        self.order = []
+        self.t = 0.0
+        self.tf = 1.0
+        self.dt = 1e-3
+        self.count = 0
+        self.pfreq = 100
+        self.time_step_function = TimeStep()
+        self.pre_step_functions = []
+        self.post_step_functions = []
+        self.execute_commands = None
+        self.command_interval = 1
+        self.print_properties = ["x", "u", "m", "h", "p", "e", "rho"]
+        self.particles = None
+        self.integrator = None
+        self.with_cl = False
+        self.output_directory = "."
+        self.detailed_output = False
+        self.dt_history = []
+
+    # ------------------------------------------------------------ set-up
+    def add_operation(self, operation, before=False, id=None):
+        if operation.id in self.operation_dict:
+            raise RuntimeError(f"operation {operation.id!r} exists")
+        self.operation_dict[operation.id] = operation
+        if id is None:
+            self.order.append(operation.id)
+        else:
+            i = self.order.index(id)
+            self.order.insert(i if before else i + 1, operation.id)
+
+    def replace_operation(self, id, new_operation):
+        i = self.order.index(id)
+        self.operation_dict.pop(id)
+        self.order[i] = new_operation.id
+        self.operation_dict[new_operation.id] = new_operation
+
+    def remove_operation(self, id):
+        self.order.remove(id)
+        self.operation_dict.pop(id)
+
+    def add_operation_step(self, types, xsph=False, eps=0.5):
+        """Position stepping dx/dt = v on `types` (S/solver/solver.py:186-220)."""
+        if xsph:
+            raise NotImplementedError("XSPH correction is not part of this build")
+        updates = ["x", "y", "z"][:self.dim]
+        self.add_operation(SPHIntegration(PositionStepping.withargs(), on_types=types,
+                                          updates=updates, id="step"))
+
+    def add_operation_xsph(self, eps, hks=False):
+        raise NotImplementedError("XSPH correction is not part of this build")
+
+    def set_final_time(self, tf):
+        self.tf = tf
+
+    def set_time_step(self, dt):
+        self.dt = dt
+
+    def set_print_freq(self, n):
+        self.pfreq = n
+
+    def set_output_fname(self, fname):
+        self.fname = fname
+
+    def set_output_printing_level(self, detailed_output):
+        self.detailed_output = detailed_output
+
+    def set_output_directory(self, path):
+        self.output_directory = path
+
+    def set_command_handler(self, callable, command_interval=1):
+        self.execute_commands = callable
+        self.command_interval = command_interval
+
+    def setup(self, particles=None):
+        """Build the calcs of every operation, in order, and the integrator."""
+        self.particles = particles
+        particles.kernel = self.kernel
+        calcs = []
+        for oid in self.order:
+            op = self.operation_dict[oid]
+            calcs.extend(op.get_calcs(particles, self.kernel))
+        self.integrator = self.integrator_type(particles, calcs)
+        self.integrator.setup_integrator()
+
+    # -------------------------------------------------------------- loop
+    def _device_rule(self):
+        rule = getattr(self.time_step_function, "device_rule", None)
+        return rule if (rule and self.integrator.plan is not None) else None
+
+    def solve(self, show_progress=False):
+        dt = self.dt
+        self.integrator.time = self.t
+        rule = self._device_rule()
+        if rule:
+            f = self.time_step_function
+            s = self.integrator._fused_session()
+            s.engine.update_params(cfl=float(f.cfl), c0=s.engine.params[0].c0,
+                                   dt_initial=float(self.dt),
+                                   cfl_force=(rule == "viscous+force"))
+            self.integrator.plan.params = s.engine.params[0]
+        while self.t < self.tf:
+            self.t += dt
+            self.count += 1
+            self.particles.update()
+            for func in self.pre_step_functions:
+                func.eval(self)
+            if rule:
+                self.integrator.integrate(0.0, device_dt=True)
+                st = self.integrator.particles.session().engine.scene_state()[0]
+                dt = st.dt
+                self.integrator.time += dt
+            else:
+                dt = self.time_step_function.compute_time_step(self)
+                self.integrator.integrate(dt)
+                self.integrator.time += dt
+            self.dt_history.append(dt)
+            for array in self.particles.arrays:
+                array.set_time(self.t)
+            for func in self.post_step_functions:
+                func.eval(self)
+            if self.execute_commands is not None and self.count % self.command_interval == 0:
+                self.execute_commands(self)
+        if rule:
+            self.particles.session().check()
+
+    def get_options(self, opt_parser):
+        pass

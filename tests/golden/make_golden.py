@@ -1,0 +1,228 @@
+"""Write the golden fixtures of tests/golden from the reference itself.
+
+    python tests/golden/build_reference.py      # patched build in _work/refbuild
+    python tests/golden/make_golden.py          # writes tests/golden/*.npz
+
+Every fixture is computed by the reference's own FP64 Cython path, through
+its own API: get_particle_array, Particles (CellManager + NNPSManager),
+SPHCalc / SPHOperation / SPHIntegration, PredictorCorrectorIntegrator and
+ViscousAndForceBasedTimeStep, with the solver loop's order of calls
+(S/solver/solver.py:546-566).  Inputs come from pysph_b200.workloads
+(seeded, synthetic).  Fixtures:
+
+  square.npz      the 4-particle unit square of the reference's function
+                  tests: SPHRho, TaitEquation, SPHPressureGradient and
+                  MomentumEquation outputs
+  drop.npz        elliptical drop, dx = 0.025 (5,025 particles): neighbour
+                  lists in the reference's order, the first stage's rho, p,
+                  cs, accelerations and dt_fac, and the state after 1 and 10
+                  predictor-corrector steps of dt = 1e-5
+  lattice3d.npz   3D jittered 16^3 lattice (h = 1.2 dx): neighbour lists,
+                  SPHRho and SPHPressureGradient
+  dam.npz         dam break at dx = 0.05 with walls: 5 steps with the CFL
+                  time step (the dt sequence and the final state)
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from pysph_b200 import workloads as W  # noqa: E402
+
+PROPS = ("x", "y", "z", "u", "v", "w", "m", "h", "rho", "p", "cs")
+
+
+def ref_modules(build_dir):
+    sys.path.insert(0, build_dir)
+    import pysph.base.particle_array as PA
+    import pysph.base.particles as P
+    import pysph.base.kernels as K
+    import pysph.sph.sph_calc as C
+    import pysph.sph.funcs.density_funcs as D
+    import pysph.sph.funcs.eos_funcs as E
+    import pysph.sph.funcs.pressure_funcs as PF
+    import pysph.sph.funcs.position_funcs as POS
+    import pysph.sph.funcs.external_force as EF
+    import pysph.solver.sph_equation as EQ
+    import pysph.solver.integrator as I
+    import pysph.solver.time_step_functions as T
+    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T)
+
+
+def make_array(R, props, name, ptype):
+    d = {k: np.asarray(props[k], np.float64).copy() for k in PROPS if k in props}
+    return R["PA"].get_particle_array(name=name, type=ptype, **d)
+
+
+def lists_of(R, particles, src, dst):
+    loc = particles.nnps_manager.get_neighbor_particle_locator(src, dst, 2.0)
+    n = dst.get_number_of_particles()
+    out = [np.asarray(loc.py_get_nearest_particles(i).get_npy_array(), np.int32).copy()
+           for i in range(n)]
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum([len(a) for a in out])
+    return off, np.concatenate(out) if out else np.zeros(0, np.int32)
+
+
+def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim):
+    EQ, D, E, PF, POS, EF = R["EQ"], R["D"], R["E"], R["PF"], R["POS"], R["EF"]
+    types = list(range(ntypes))
+    vel = ["u", "v", "w"][:dim]
+    pos = ["x", "y", "z"][:dim]
+    ops = [EQ.SPHOperation(D.SPHRho.withargs(), on_types=types, from_types=types,
+                           updates=["rho"], id="sd"),
+           EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
+                           updates=["p", "cs"], id="eos"),
+           EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta),
+                             on_types=[0], from_types=types, updates=vel, id="mom")]
+    if gy:
+        ops.append(EQ.SPHIntegration(EF.GravityForce.withargs(gy=gy), on_types=[0],
+                                     updates=vel, id="grav"))
+    ops.append(EQ.SPHIntegration(POS.PositionStepping.withargs(), on_types=[0],
+                                 updates=pos, id="step"))
+    return ops
+
+
+def build_sim(R, arrays, types, params, dim):
+    pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
+    particles = R["P"].Particles(pas)
+    kernel = R["K"].CubicSplineKernel(dim=dim)
+    ops = scheme_ops(R, len(pas), params["c0"], params["rho0"], params["alpha"],
+                     params["beta"], params["eta"], params["gravity"][1], dim)
+    calcs = []
+    for op in ops:
+        calcs.extend(op.get_calcs(particles, kernel))
+    integ = R["I"].PredictorCorrectorIntegrator(particles, calcs)
+    integ.setup_integrator()
+    return pas, particles, integ
+
+
+def state(pas, names=("x", "y", "u", "v", "rho", "p", "cs")):
+    return {f"{n}_{i}": np.asarray(pa.get(n), np.float64).copy()
+            for i, pa in enumerate(pas) for n in names}
+
+
+def square(R):
+    x = np.array([0, 0, 1, 1], np.float64)
+    y = np.array([0, 1, 1, 0], np.float64)
+    out = {}
+    kernel = R["K"].CubicSplineKernel(dim=2)
+    for fname, fac, outs in (
+            ("rho", lambda pa: R["D"].SPHRho.withargs().get_func(pa, pa), 1),
+            ("tait", lambda pa: R["E"].TaitEquation.withargs(gamma=7.0).get_func(pa, pa), 2),
+            ("pgrad", lambda pa: R["PF"].SPHPressureGradient.withargs().get_func(pa, pa), 3),
+            ("mom", lambda pa: R["PF"].MomentumEquation.withargs(
+                alpha=1.0, beta=1.0, gamma=1.4, eta=0.1).get_func(pa, pa), 3)):
+        pa = R["PA"].get_particle_array(name="test", x=x.copy(), y=y.copy(), z=np.zeros(4),
+                                        m=np.ones(4), u=np.array([1, 0, 0, -1.0]),
+                                        p=np.array([0, 0, 1, 1.0]),
+                                        cs=np.array([1.0, 2.0, 0.5, 1.5]),
+                                        rho=np.array([1000.0, 1001.5, 998.0, 1010.0])
+                                        if fname == "tait" else np.ones(4))
+        particles = R["P"].Particles([pa])
+        calc = R["C"].SPHCalc(particles, [pa], pa, kernel, [fac(pa)], ["rho"])
+        calc.sph()
+        for k, n in enumerate(("_tmpx", "_tmpy", "_tmpz")[:outs]):
+            out[f"{fname}_{k}"] = np.asarray(pa.get(n), np.float64).copy()
+    return out
+
+
+def drop(R):
+    arrays, types, params = W.elliptical_drop(dx=0.025)
+    pas, particles, integ = build_sim(R, arrays, types, params, 2)
+    out = {f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS}
+    off, idx = lists_of(R, particles, pas[0], pas[0])
+    out["nbr_off"], out["nbr_idx"] = off, idx
+    out["cell_size"] = particles.cell_manager.cell_size
+    # the first stage: Integrator.eval at t = 0
+    integ.save_initial_arrays()
+    integ.reset_accelerations(step=1)
+    integ.eval()
+    out.update({f"stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                for n in ("rho", "p", "cs", "_a_u_1", "_a_v_1", "dt_fac")})
+    pas, particles, integ = build_sim(R, arrays, types, params, 2)
+    for step in range(10):
+        particles.update()
+        integ.integrate(1e-5)
+        if step == 0:
+            out.update({f"step1_{k}": v for k, v in state(pas).items()})
+    out.update({f"step10_{k}": v for k, v in state(pas).items()})
+    return out
+
+
+def lattice(R):
+    arrays, types, params = W.lattice3d(n=16)
+    a = arrays[0]
+    pa = make_array(R, a, "lat", 0)
+    particles = R["P"].Particles([pa])
+    kernel = R["K"].CubicSplineKernel(dim=3)
+    out = {f"in_{k}": np.asarray(a[k]) for k in PROPS}
+    off, idx = lists_of(R, particles, pa, pa)
+    out["nbr_off"], out["nbr_idx"] = off, idx
+    out["cell_size"] = particles.cell_manager.cell_size
+    calc = R["C"].SPHCalc(particles, [pa], pa, kernel,
+                          [R["D"].SPHRho.withargs().get_func(pa, pa)], ["rho"])
+    calc.sph("_tmpx")
+    out["rho_sum"] = np.asarray(pa.get("_tmpx"), np.float64).copy()
+    calc = R["C"].SPHCalc(particles, [pa], pa, kernel,
+                          [R["PF"].SPHPressureGradient.withargs().get_func(pa, pa)],
+                          ["u", "v", "w"], integrates=True)
+    for n in ("_tmpx", "_tmpy", "_tmpz"):
+        pa.get(n)[:] = 0
+    calc.sph("_tmpx", "_tmpy", "_tmpz")
+    for k, n in enumerate(("_tmpx", "_tmpy", "_tmpz")):
+        out[f"pgrad_{k}"] = np.asarray(pa.get(n), np.float64).copy()
+    return out
+
+
+class _SolverView:
+    """What the time-step functions read from a Solver."""
+
+    def __init__(self, integrator, dt, dim):
+        self.integrator = integrator
+        self.dt = dt
+        self.dim = dim
+        self.count = 0
+
+
+def dam(R):
+    arrays, types, params = W.dam_break(dx=0.05)
+    pas, particles, integ = build_sim(R, arrays, types, params, 2)
+    out = {f"in{i}_{k}": np.asarray(arrays[i][k]) for i in range(2) for k in PROPS}
+    tsf = R["T"].ViscousAndForceBasedTimeStep(cfl=params["cfl"], co=params["c0"],
+                                              particles=particles)
+    sv = _SolverView(integ, params["dt_initial"], 2)
+    dts = []
+    for _ in range(5):
+        sv.count += 1
+        particles.update()
+        dt = tsf.compute_time_step(sv)
+        integ.integrate(dt)
+        dts.append(dt)
+    out["dts"] = np.asarray(dts)
+    out.update({f"step5_{k}": v for k, v in state(pas).items()})
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--build", default=os.path.join(ROOT, "_work", "refbuild"))
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    R = ref_modules(a.build)
+    for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam)):
+        data = fn(R)
+        path = os.path.join(a.out, f"{name}.npz")
+        np.savez_compressed(path, **data)
+        print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main()

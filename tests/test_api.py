@@ -1,0 +1,134 @@
+"""Host-side logic of the reference-shaped API (no device work): particle
+array defaults and properties, operation -> calc grouping, and recognition
+of the fused particle-update scheme."""
+import numpy as np
+import pytest
+import torch
+
+import pysph_b200.base.api as base
+import pysph_b200.sph.api as sph
+import pysph_b200.solver.api as solver
+
+Fluid, Solid = base.Fluid, base.Solid
+
+
+def arrays(device="cpu"):
+    x = np.linspace(0, 1, 11)
+    f = base.get_particle_array(name="fluid", type=Fluid, x=x, y=x * 0, h=np.full(11, 0.2),
+                                device=device)
+    w = base.get_particle_array(name="wall", type=Solid, x=x, y=x * 0 - 0.1,
+                                h=np.full(11, 0.2), device=device)
+    return f, w
+
+
+def test_get_particle_array_defaults():
+    # S/base/particle_array.pyx:1428-1470
+    pa = base.get_particle_array(x=[0.0, 1.0, 2.0], name="a", device="cpu", cl_precision="double")
+    assert pa.name == "a" and pa.particle_type == Fluid
+    assert pa.get_number_of_particles() == 3
+    for name, v in {"m": 1.0, "h": 1.0, "rho": 1.0, "p": 0.0, "cs": 0.0, "u": 0.0}.items():
+        assert torch.all(pa.get(name) == v)
+    assert pa.get("idx").tolist() == [0, 1, 2]
+    assert pa.get("tag").dtype == torch.int64 and int(pa.get("tag").sum()) == 0
+    assert pa.num_real_particles == 3
+    pa.set(u=np.array([1.0, 2.0, 3.0]))
+    assert pa.u.tolist() == [1.0, 2.0, 3.0]
+    x, u = pa.get("x", "u")
+    assert x.tolist() == [0.0, 1.0, 2.0]
+    pa.add_property({"name": "dt_fac"})
+    assert pa.has_array("dt_fac")
+    pa.copy_over_properties({"u": "_tmpx"})
+    assert pa._tmpx.tolist() == [1.0, 2.0, 3.0]
+    pa.set_to_zero(["_tmpx"])
+    assert float(pa._tmpx.abs().sum()) == 0
+    pa.remove_particles([1])
+    assert pa.get_number_of_particles() == 2 and pa.u.tolist() == [1.0, 3.0]
+    with pytest.raises(AssertionError):
+        base.get_particle_array(x=[0.0], type=99)
+
+
+def test_operation_grouping():
+    # S/solver/sph_equation.py:101-228: one calc per dest, one func per source
+    f, w = arrays()
+    particles = base.Particles([f, w])
+    k = base.CubicSplineKernel(dim=2)
+    op = solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid, Solid],
+                             from_types=[Fluid, Solid], updates=["rho"], id="sd")
+    calcs = op.get_calcs(particles, k)
+    assert [c.dest.name for c in calcs] == ["fluid", "wall"]
+    assert [[s.name for s in c.sources] for c in calcs] == [["fluid", "wall"]] * 2
+    assert calcs[0].id == "sd_fluid"
+    mom = solver.SPHIntegration(sph.MomentumEquation.withargs(alpha=0.1, beta=0.0),
+                                on_types=[Fluid], from_types=[Fluid, Solid],
+                                updates=["u", "v"], id="mom")
+    mc = mom.get_calcs(particles, k)
+    assert len(mc) == 1 and mc[0].integrates and mc[0].to_reset == ["dt_fac"]
+    assert f.has_array("dt_fac")
+    with pytest.raises(ValueError):
+        solver.SPHOperation(sph.TaitEquation.withargs(), on_types=[Fluid],
+                            from_types=[Fluid], updates=["p", "cs"], id="eos").get_calcs(particles, k)
+
+
+def dam_solver(order=("sd", "eos", "mom", "grav", "step"), gravity=True):
+    f, w = arrays()
+    particles = base.Particles([f, w])
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+    ops = {
+        "sd": solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid, Solid],
+                                  from_types=[Fluid, Solid], updates=["rho"], id="sd"),
+        "eos": solver.SPHOperation(sph.TaitEquation.withargs(co=62.6, ro=1000.0),
+                                   on_types=[Fluid, Solid], updates=["p", "cs"], id="eos"),
+        "mom": solver.SPHIntegration(sph.MomentumEquation.withargs(alpha=0.1, beta=0.0),
+                                     on_types=[Fluid], from_types=[Fluid, Solid],
+                                     updates=["u", "v"], id="mom"),
+        "grav": solver.SPHIntegration(sph.GravityForce.withargs(gy=-9.81),
+                                      on_types=[Fluid], updates=["u", "v"], id="grav"),
+    }
+    for oid in order:
+        if oid == "step":
+            s.add_operation_step([Fluid])
+        elif oid != "grav" or gravity:
+            s.add_operation(ops[oid])
+    s.setup(particles)
+    return s
+
+
+def test_fused_plan_recognised():
+    s = dam_solver()
+    plan = s.integrator.plan
+    assert plan is not None
+    assert plan.scheme.rho_src == {0: [0, 1], 1: [0, 1]}
+    assert plan.scheme.mom_src == {0: [0, 1]}
+    assert plan.scheme.tait_on == (0, 1) and plan.scheme.step_on == (0,)
+    assert plan.params.c0 == 62.6 and plan.params.rho0 == 1000.0
+    assert plan.params.alpha == 0.1 and plan.params.beta == 0.0
+    assert plan.params.gravity == (0.0, -9.81, 0.0)
+    # initial-value and acceleration properties (S/solver/integrator.py:212-260)
+    f = s.particles.arrays[0]
+    for name in ("_u0", "_v0", "_x0", "_y0", "_a_u_1", "_a_v_1", "_a_x_1", "_a_y_1"):
+        assert f.has_array(name)
+
+
+def test_fused_plan_rejects_other_orders():
+    # Tait before SPHRho reads the old density: not the fused scheme
+    assert dam_solver(order=("eos", "sd", "mom", "grav", "step")).integrator.plan is None
+    assert dam_solver(gravity=False).integrator.plan.params.gravity == (0.0, 0.0, 0.0)
+
+
+def test_unsupported_features_fail_loudly():
+    f, w = arrays()
+    with pytest.raises(NotImplementedError):
+        base.Particles([f], variable_h=True)
+    with pytest.raises(NotImplementedError):
+        sph.MomentumEquation(f, f, deltap=0.1)
+    with pytest.raises(NotImplementedError):
+        solver.Solver(dim=2).add_operation_xsph(eps=0.5)
+
+
+def test_kernel_host_formulas():
+    k = base.CubicSplineKernel(dim=2)
+    assert k.radius() == 2.0
+    assert k.py_fac(0.01) == pytest.approx(10 / (7 * np.pi) / 1e-4)
+    g = base.Point()
+    k.py_gradient(base.Point(0.5, 0, 0), base.Point(0, 0, 0), 1.0, g)
+    assert g.x < 0 and g.y == 0
