@@ -286,6 +286,34 @@ SPHB_API int sphb_set_dt(const sphb_engine *e, double dt, void *stream);
 /* Write identity idx (0..n-1 inside each segment) into buf[cur].idx. */
 SPHB_API int sphb_init_index(const sphb_engine *e, int cur, void *stream);
 
+/* Copy one FP64 per-particle array of array index `array` between the
+ * caller's order (dir 0: user -> engine_buf; dir 1: engine_buf -> user)
+ * and the engine order of buf[cur]; like sphb_exchange for arbitrary
+ * buffers (adjoint vectors, ...). */
+SPHB_API int sphb_permute(const sphb_engine *e, int cur, int array, int dir, double *user,
+                          double *engine_buf, const int32_t *user_offset, void *stream);
+
+/* ---- adjoint of the particle update ---------------------------------
+ * The reference has no gradients; these are the reverse-mode kernels of the
+ * differentiable rollout (FP64 engines only).  Vectors are SoA [dim][N] in
+ * engine order.  Each needs the forward quantities of the stage (positions,
+ * velocities, rho, p, cs from sphb_density) and its bin. */
+
+/* Given lam_a, the adjoint of the MomentumEquation acceleration of the dest
+ * arrays in dest_mask: lam_x += (da/dx)^T lam_a, lam_v += (da/dv)^T lam_a;
+ * lam_rho, lam_p, lam_c = (da/drho, dp, dcs)^T lam_a. */
+SPHB_API int sphb_force_vjp(const sphb_engine *e, int cur, uint32_t dest_mask,
+                            const double *lam_a, double *lam_x, double *lam_v,
+                            double *lam_rho, double *lam_p, double *lam_c, void *stream);
+
+/* lam_rho += lam_p dp/drho + lam_c dcs/drho through the Tait EOS. */
+SPHB_API int sphb_eos_vjp(const sphb_engine *e, int cur, double *lam_rho,
+                          const double *lam_p, const double *lam_c, void *stream);
+
+/* lam_x += (drho/dx)^T lam_rho through summation density. */
+SPHB_API int sphb_density_vjp(const sphb_engine *e, int cur, uint32_t dest_mask,
+                              const double *lam_rho, double *lam_x, void *stream);
+
 /* ---- neighbour counts without caller scratch ------------------------ */
 
 /* Largest particle set sphb_neighbor_counts_static accepts. */

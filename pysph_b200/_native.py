@@ -139,6 +139,10 @@ def lib():
         "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
         "sphb_init_index": (i32, [E, i32, vp]),
         "sphb_set_dt": (i32, [E, f64, vp]),
+        "sphb_permute": (i32, [E, i32, i32, i32, vp, vp, vp, vp]),
+        "sphb_force_vjp": (i32, [E, i32, u32, vp, vp, vp, vp, vp, vp, vp]),
+        "sphb_eos_vjp": (i32, [E, i32, vp, vp, vp, vp]),
+        "sphb_density_vjp": (i32, [E, i32, u32, vp, vp, vp]),
         "sphb_neighbor_counts_static": (i32, [i32, i32, vp, vp, vp, vp, f64, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -156,7 +160,8 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
             "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
-            "sphb_set_dt", "sphb_neighbor_counts_static")
+            "sphb_set_dt", "sphb_permute", "sphb_force_vjp", "sphb_eos_vjp",
+            "sphb_density_vjp", "sphb_neighbor_counts_static")
 
 STATIC_MAX_PARTICLES = 1 << 18
 
