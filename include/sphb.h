@@ -140,7 +140,20 @@ typedef struct {
     void *vel;              /* FP32C: 2D float2 {u,v}, 3D float4 {u,v,w,0} */
     void *thermo;           /* FP32C float4[N]: {rho, p, cs, p/rho^2} */
     int32_t *cell;          /* local cell index of each particle */
+    /* Neighbour lists of the last sphb_density pass (optional, may be
+     * NULL): uint32 [list_cap][N] slot-major, entry = j | cell offsets
+     * (SPHB_NBR_* packing), and int32 [lanes][N] entries per lane (-1 when
+     * a lane overflowed its list_cap / lanes slots). */
+    uint32_t *nbr;
+    int32_t *nbr_cnt;
+    int32_t list_cap;       /* slots per particle, 0 = no lists */
+    int32_t pad0;
 } sphb_fields;
+
+/* List entry packing: particle index in the low bits, each cell offset
+ * (-2..2) + 2 in 3 bits above it.  2D: 26 index bits; 3D: 23. */
+#define SPHB_NBR_IDX_BITS_2D 26
+#define SPHB_NBR_IDX_BITS_3D 23
 
 /* Scratch; carve it from one buffer with sphb_workspace_layout. */
 typedef struct {
@@ -205,7 +218,7 @@ SPHB_API int sphb_box_init(const sphb_engine *e, int cur, void *stream);
  * flags: SPHB_BIN_MOVE_INITIAL carries x0..w0 too; SPHB_BIN_BOX first
  * recomputes every scene box from all particles (needed whenever no
  * sphb_pc_stage accumulated it since the last bin).  The grid setup resets
- * each scene's box to its static bounds and its dt_fac / |a| maxima. */
+ * each scene's box to its static bounds. */
 #define SPHB_BIN_MOVE_INITIAL 1
 #define SPHB_BIN_BOX 2
 SPHB_API int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream);
@@ -229,7 +242,10 @@ SPHB_API int sphb_cell_coords(const sphb_engine *e, int cur, int32_t *out, void 
  * arrays in dest_mask.  Sources per dest array come from cfg.rho_src.
  * with_eos: p, cs from Tait for dest arrays in cfg.tait_on.  SPHRho
  * (S/sph/funcs/density_funcs.pyx:37-73, .clt:3-53) + TaitEquation
- * (S/sph/funcs/eos_funcs.pyx:88-129, .clt:36-65). */
+ * (S/sph/funcs/eos_funcs.pyx:88-129, .clt:36-65).  When f.list_cap > 0 the
+ * pass also records every dest particle's neighbour list (the reference
+ * caches one list per particle for all calcs of a stage,
+ * FixedDestNbrParticleLocator._update_cache, S/base/nnps.pyx:596-621). */
 SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
                  int with_eos, void *stream);
 
@@ -241,13 +257,17 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
  * then GravityForce when with_gravity; writes au/av/aw and dt_fac and the
  * per-scene max dt_fac and |a|^2.  S/sph/funcs/pressure_funcs.pyx:246-391,
  * .clt:69-157; S/sph/funcs/external_force.pyx:13-62.
- * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV). */
+ * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV).
+ * mode | SPHB_FORCE_USE_LIST: iterate the lists of the last sphb_density
+ * pass (same bin, same sources) instead of searching cells. */
+#define SPHB_FORCE_USE_LIST 16
 SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
                   int with_gravity, int mode, void *stream);
 
 /* Predictor-corrector stage on the integrated arrays (cfg.step_on):
  * stage 0 = predict (save X0, X = X0 + dt/2 F), stage 1 = correct and
- * final (X = 2 (X0 + dt/2 F) - X0), which also advances t and count.
+ * final (X = 2 (X0 + dt/2 F) - X0).  Stage 0 also clears the per-scene
+ * dt_fac / |a| maxima, so sphb_step_begin sees the corrector's pass only.
  * Accumulates the scene boxes for the next sphb_bin.  PositionStepping
  * (S/sph/funcs/position_funcs.pyx:10-56) supplies F_x = u.
  * PredictorCorrectorIntegrator.integrate (S/solver/integrator.py:646-683),

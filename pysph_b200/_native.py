@@ -83,11 +83,12 @@ class Buffers(ctypes.Structure):
 
 
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
-               "vel", "thermo", "cell")
+               "vel", "thermo", "cell", "nbr", "nbr_cnt")
+FORCE_USE_LIST = 16
 
 
 class Fields(ctypes.Structure):
-    _fields_ = [(n, vp) for n in FIELD_NAMES]
+    _fields_ = [(n, vp) for n in FIELD_NAMES] + [("list_cap", i32), ("pad0", i32)]
 
 
 WORK_NAMES = ("count", "start", "key", "slot", "perm", "bsum", "meta",

@@ -304,9 +304,10 @@ class Particles:
         return self._session
 
     def update(self, cache_neighbors=False):
-        """Positions may have moved: the next engine use rebins."""
-        if self._session is not None:
-            self._session.need_bin = True
+        """Particles.update (S/base/particles.py:184-215).  Positions the
+        engine moved are rebinned by the engine itself at the start of every
+        stage, and positions set through ParticleArray.set are tracked; only
+        in-place tensor edits need ParticleArray.set_dirty(True)."""
         for f in self.misc_prop_update_functions:
             f.eval()
 

@@ -122,8 +122,6 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
                 st.box[d] = enc_double(sc.static_lo[d]);
                 st.box[3 + d] = enc_double(sc.static_hi[d]);
             }
-            st.max_dtfac = 0ull;
-            st.max_acc2 = 0ull;
         }
         __syncthreads();
         if (threadIdx.x == 0) s_carry += total;

@@ -37,6 +37,18 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     const int *__restrict__ start = e.work.start;
     unsigned long long np = 0;
     double rho = 0.0;
+    // neighbour list of this lane: slots lane, lane + LANES, ... of k
+    const int N = e.cfg.num_particles;
+    uint32_t *__restrict__ nbr = e.f.list_cap > 0 ? e.f.nbr : nullptr;
+    const int cap_lane = e.f.list_cap / LANES;
+    int cnt = 0;
+    auto record = [&](int j, int o, int dy, int dz) {
+        if (nbr) {
+            if (cnt < cap_lane)
+                nbr[(size_t)(lane + LANES * cnt) * N + k] = nbr_pack<DIM>(j, o, dy, dz);
+            ++cnt;
+        }
+    };
 
     if constexpr (F32) {
         Kahan acc;
@@ -68,6 +80,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                         const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
                         acc.add(mj * w_cubic_f<DIM>(r2, 0.5f * (hk + hj)));
                         ++np;
+                        record(j, o, dy, dz);
                     }
                 });
         }
@@ -91,7 +104,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             for_each_candidate<DIM, R, LANES>(
                 start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
                 e.cfg.num_particles, e.work.status,
-                [&](int j, int, int, int) {
+                [&](int j, int o, int oy, int oz) {
                     const double dx = xk - __ldg(B.x + j);
                     const double dy = yk - __ldg(B.y + j);
                     const double dz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
@@ -100,6 +113,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                         const double hab = 0.5 * (hk + __ldg(B.h + j));
                         sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
                         ++np;
+                        record(j, o, oy, oz);
                     }
                 });
         }
@@ -108,6 +122,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
         rho = sum;
     }
 
+    if (active && nbr) e.f.nbr_cnt[(size_t)lane * N + k] = cnt <= cap_lane ? cnt : -1;
     if (active && lane == 0) {
         const bool real = e.buf[cur].tag[k] == 0;
         if (!real) rho = 0.0;

@@ -37,7 +37,10 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
     const int cell_base = st.cell_base, ncells = st.ncells;
     const sphb_scene &sc = e.scene[s];
     const int *__restrict__ start = e.work.start;
-    const bool visc = mode == 0;
+    const bool visc = (mode & 15) == 0;
+    // reuse the density pass's lists when they were built from the same sources
+    const bool use_list = (mode & SPHB_FORCE_USE_LIST) && e.f.list_cap > 0 && e.f.nbr &&
+                          e.f.nbr_cnt && e.cfg.rho_src[a] == e.cfg.mom_src[a];
     unsigned long long np = 0;
     double acc[3] = {0.0, 0.0, 0.0};
     double dtf = 0.0;
@@ -71,9 +74,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             const float eta2 = (float)(sc.eta * sc.eta);
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
-            for_each_candidate<DIM, R, LANES>(
-                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
-                e.cfg.num_particles, e.work.status,
+            traverse<DIM, R, LANES>(
+                e, use_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
                 [&](int j, int o, int dy, int dz) {
                     const float4 gj = __ldg(geo + j);
                     const float rx = (xk - gj.x) - (float)o * csf;
@@ -147,9 +149,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             const double alpha = sc.alpha, beta = sc.beta, eta = sc.eta;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
-            for_each_candidate<DIM, R, LANES>(
-                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
-                e.cfg.num_particles, e.work.status,
+            traverse<DIM, R, LANES>(
+                e, use_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
                 [&](int j, int, int, int) {
                     const double rx = xk - __ldg(B.x + j);
                     const double ry = yk - __ldg(B.y + j);
@@ -265,9 +266,10 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
     if ((rc = check_pair_cfg(e))) return rc;
-    if (mode != 0 && mode != 1) return SPHB_ERR_ARG;
+    if ((mode & ~SPHB_FORCE_USE_LIST) != 0 && (mode & ~SPHB_FORCE_USE_LIST) != 1)
+        return SPHB_ERR_ARG;
     if (!e->f.au || !e->f.av || (e->cfg.dim == 3 && !e->f.aw)) return SPHB_ERR_ARG;
-    if (mode == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
+    if ((mode & 15) == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
     if (e->num_pair_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const sphb_config &c = e->cfg;

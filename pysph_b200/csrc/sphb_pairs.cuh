@@ -71,6 +71,59 @@ __device__ __forceinline__ bool for_each_candidate(
     return true;
 }
 
+// Neighbour-list entries: index plus the candidate's cell offsets.
+template <int DIM>
+__device__ __forceinline__ uint32_t nbr_pack(int j, int o, int dy, int dz)
+{
+    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
+    uint32_t v = (uint32_t)j | ((uint32_t)(o + 2) << B) | ((uint32_t)(dy + 2) << (B + 3));
+    if constexpr (DIM == 3) v |= (uint32_t)(dz + 2) << (B + 6);
+    return v;
+}
+
+template <int DIM>
+__device__ __forceinline__ void nbr_unpack(uint32_t v, int &j, int &o, int &dy, int &dz)
+{
+    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
+    j = (int)(v & ((1u << B) - 1u));
+    o = (int)((v >> B) & 7u) - 2;
+    dy = (int)((v >> (B + 3)) & 7u) - 2;
+    dz = DIM == 3 ? (int)((v >> (B + 6)) & 7u) - 2 : 0;
+}
+
+// The pairs of dest k: its list from the last density pass when use_list
+// and every lane's list is complete, else the cell search.
+template <int DIM, int R, int LANES, typename F>
+__device__ __forceinline__ void traverse(const sphb_engine &e, bool use_list, int k, int lane,
+                                         const int *__restrict__ start, int num_arrays,
+                                         uint32_t src_mask, int cell_base, int ncells,
+                                         const int *n, int cx, int cy, int cz, F &&f)
+{
+    const int N = e.cfg.num_particles;
+    if (use_list) {
+        bool ok = true;
+        int mine = 0;
+#pragma unroll
+        for (int l = 0; l < LANES; ++l) {
+            const int c = __ldg(e.f.nbr_cnt + (size_t)l * N + k);
+            ok = ok && c >= 0;
+            if (l == lane) mine = c;
+        }
+        if (ok) {
+            const uint32_t *__restrict__ nbr = e.f.nbr;
+            for (int c = 0; c < mine; ++c) {
+                int j, o, dy, dz;
+                nbr_unpack<DIM>(__ldg(nbr + (size_t)(lane + LANES * c) * N + k), j, o, dy, dz);
+                if (j < N) f(j, o, dy, dz);
+                else atomicOr(e.work.status, (unsigned)SPHB_ST_BAD_INDEX);
+            }
+            return;
+        }
+    }
+    for_each_candidate<DIM, R, LANES>(start, num_arrays, src_mask, cell_base, ncells, n, cx, cy,
+                                      cz, lane, N, e.work.status, f);
+}
+
 // Cubic spline W(r, h) in FP32 (CubicSplineKernel.function,
 // S/base/kernels.pyx:355-378): fac * {1 - 1.5 q^2 (1 - q/2); (2-q)^3 / 4; 0}.
 template <int DIM>

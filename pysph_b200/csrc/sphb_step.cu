@@ -44,6 +44,15 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;
+    if (stage == 0 && blockIdx.x == 0) {
+        // the CFL rule reads the maxima of the corrector's force pass only
+        // (dt_fac is reset per calc, S/sph/sph_calc.pyx:324): clear what the
+        // predictor's pass accumulated
+        for (int q = threadIdx.x; q < e.cfg.num_scenes; q += blockDim.x) {
+            e.sstate[q].max_dtfac = 0ull;
+            e.sstate[q].max_acc2 = 0ull;
+        }
+    }
     if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
     const int k = t.begin + threadIdx.x;
     const bool active = k < t.end;

@@ -99,7 +99,7 @@ class Engine:
     def __init__(self, scenes, scheme: Scheme, dim: int = 2,
                  precision: str = "fp32c", stencil: int = 1, lanes: int = 1,
                  pair_block: int = 128, cell_capacity: int | None = None,
-                 grid_growth: float = 2.0, device=None):
+                 grid_growth: float = 2.0, device=None, use_lists: bool = True):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -136,7 +136,8 @@ class Engine:
                                  for a in range(self.A)]
         self.user_n = [int(sizes[:, a].sum()) for a in range(self.A)]
         self._stencil = stencil
-        self.force_mode = 0        # 0 MomentumEquation, 1 SPHPressureGradient
+        self.use_lists = use_lists
+        self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
         if cell_capacity is None:
@@ -244,6 +245,14 @@ class Engine:
             f["aw"] = torch.zeros(N, **f64) if dim == 3 else None
             f["geo"] = f["mass"] = f["vel"] = f["thermo"] = None
         f["cell"] = torch.zeros(N, **i32)
+        # per-stage neighbour lists (density pass writes, force pass reads)
+        idx_bits = 26 if dim == 2 else 23
+        self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
+        if self.list_cap:
+            f["nbr"] = torch.zeros(self.list_cap * N, **i32)
+            f["nbr_cnt"] = torch.zeros(8 * N, **i32)
+        else:
+            f["nbr"] = f["nbr_cnt"] = None
         self.fields = f
         # scratch
         cfg = self._config(lanes, pair_block)
@@ -313,6 +322,7 @@ class Engine:
         for name in nat.FIELD_NAMES:
             t = self.fields[name]
             setattr(d.f, name, t.data_ptr() if t is not None else None)
+        d.f.list_cap = self.list_cap
         base = self.work_buf.data_ptr()
         for name, off in zip(nat.WORK_NAMES, self.work_offsets):
             setattr(d.work, name, base + off)
@@ -467,7 +477,7 @@ class Engine:
         self.density()
         if self.tait_only_mask:
             self.tait(self.tait_only_mask)
-        self.momentum(mode=self.force_mode)
+        self.momentum(mode=self.force_mode | (nat.FORCE_USE_LIST if self.list_cap else 0))
 
     def pc_step(self):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
