@@ -168,44 +168,66 @@ def dist_info():
     return rank, world, local
 
 
-def max_over_ranks(v, world):
+def reduce_over_ranks(v, world, op="max", device="cuda"):
+    """Max or sum of a host scalar over the ranks (no-op on one rank); the
+    only collective of the benchmark -- the replicas share no data."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(v, world):
+    return reduce_over_ranks(v, world, "max")
 
 
 def sum_over_ranks(v, world):
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return reduce_over_ranks(v, world, "sum")
+
+
+def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
+    """Whole-job figures of independent replicas: the time is the slowest
+    rank's, the work is every rank's."""
+    ms = reduce_over_ranks(ms_per_rank, world, "max", device)
+    pairs = reduce_over_ranks(pairs_per_rank, world, "sum", device)
+    return {"ms": ms, "pairs": pairs, "value": pairs / (ms / 1e3),
+            "steps_per_s": steps / (ms / 1e3)}
 
 
 # bytes per particle each kernel must move at least once (FP32C, 2D),
 # counted from the fields it reads and writes at their stored widths
 def algorithmic_bytes(dim, f32):
+    """Bytes per particle each phase must move once, at the stored widths
+    (neighbour re-reads and the neighbour lists, which are scratch, are not
+    counted)."""
     if f32 and dim == 2:
-        return {"density": 16 + 4 + 4 + 16 + 16,         # geo, cell, tag, thermo r/w
-                "force": 16 + 8 + 16 + 4 + 4 + 12,       # geo, vel, thermo, cell, tag; a, dt_fac
-                "pc_stage": 8 * 8 + 4 + 8,               # x,y,u,v r/w + x0.. ; tag; a
-                "bin": 16 + 8 + 8 + 4 * 4 + 2 * 88 + 24}  # x,y; key,slot w/r; perm; gather 88 B r/w; records
-    if f32 and dim == 3:
-        return {"density": 16 + 4 + 4 + 4 + 16 + 16,
-                "force": 16 + 4 + 16 + 16 + 4 + 4 + 16,
-                "pc_stage": 12 * 8 + 4 + 12,
-                "bin": 24 + 8 + 8 + 16 + 2 * 128 + 40}
-    w = 8
-    return {"density": dim * w + 2 * w + 4 + 4 + 3 * w,
-            "force": 2 * dim * w + 2 * w + 3 * w + 4 + 4 + (dim + 1) * w,
-            "pc_stage": 4 * dim * w + 4 + dim * w,
-            "bin": dim * w + 8 + 8 + 16 + 2 * (4 * dim + 2) * w}
+        d = {"density": 16 + 4 + 4 + 16 + 16,           # geo, cell, tag; thermo r/w
+             "force": 16 + 8 + 16 + 4 + 4 + 12,         # geo, vel, thermo, cell, tag; a, dt_fac
+             "pc_stage": 8 * 8 + 4 + 8,                 # x,y,u,v r/w + x0.. ; tag; a
+             # hash x,y 16, key/slot w+r 16, perm w+r 8, key 4; gather
+             # x,y,u,v,m,h,idx,tag 56 r + 56 w; cell 4, geo 16, vel 8 w
+             "bin": 16 + 16 + 8 + 4 + 56 + 56 + 4 + 16 + 8,
+             "refresh": 32 + 4 + 16 + 16 + 8}           # x,y,u,v, cell, geo r/w, vel w
+    elif f32 and dim == 3:
+        d = {"density": 16 + 4 + 4 + 4 + 16 + 16,
+             "force": 16 + 4 + 16 + 16 + 4 + 4 + 16,
+             "pc_stage": 12 * 8 + 4 + 12,
+             "bin": 24 + 16 + 8 + 4 + 72 + 72 + 4 + 16 + 4 + 16,
+             "refresh": 48 + 4 + 16 + 16 + 16}
+    else:
+        w = 8
+        d = {"density": dim * w + 2 * w + 4 + 4 + 3 * w,
+             "force": 2 * dim * w + 2 * w + 3 * w + 4 + 4 + (dim + 1) * w,
+             "pc_stage": 4 * dim * w + 4 + dim * w,
+             "bin": dim * w + 16 + 8 + 4 + 2 * (2 * dim * w + 2 * w + 8) + 4,
+             "refresh": 0}
+    d["density_list"] = d["density"]
+    d["density2"] = d["density"]
+    d["bin_mid"] = d["bin"] + (32 if dim == 2 else 48) * 2
+    return d
 
 
 # ------------------------------------------------------------------ our arm
@@ -286,10 +308,8 @@ def run_ours(args, rank, world, local):
     eng.check_status()
     pairs_d, pairs_f = eng.pair_counts()
     pairs = pairs_d + pairs_f
-    ms_max = max_over_ranks(ms, world)
-    pairs_all = sum_over_ranks(pairs, world)
-    value = pairs_all / (ms_max / 1e3)
-    steps_per_s = args.steps / (ms_max / 1e3)
+    job = replica_result(ms, pairs, args.steps, world)
+    ms_max, value, steps_per_s = job["ms"], job["value"], job["steps_per_s"]
 
     if args.no_extras:
         out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
@@ -302,7 +322,7 @@ def run_ours(args, rank, world, local):
     # ---- per-kernel timing for the roofline (one rebin + one stage)
     kern = kernel_times(eng, flush, stream)
     byts = algorithmic_bytes(wl["dim"], eng.f32)
-    dominant = max(kern, key=lambda k: kern[k])
+    dominant = max((k for k in kern if k in byts), key=lambda k: kern[k])
     hbm, which = peaks()
     ach = byts[dominant] * N / (kern[dominant] * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
@@ -334,10 +354,136 @@ def run_ours(args, rank, world, local):
         if args.precision == "fp32c":
             out["fp64_gpu"] = fp64_comparison(args, wl, eng, flush, stream, dev)
         out["e2e"] = e2e(eng, wl, stream, dev, args)
+        if args.workload == "dam_break":
+            out["adjoint"] = adjoint_measure(dev, stream)
+            out["other_configs"] = other_configs(dev, flush, stream)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(args)
     del graph
     return out
+
+
+def timed_steps(eng, steps, flush, stream, graph=True):
+    """ms per PC step of an engine (CUDA graph replay, L2 flushed between
+    steps, events around each step) and pair-interactions per step."""
+    import torch
+    for _ in range(3):
+        eng.pc_step()
+    g = None
+    if graph:
+        s = torch.cuda.Stream(eng.device)
+        s.wait_stream(stream)
+        with torch.cuda.stream(s):
+            eng.pc_step()
+        stream.wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            eng.pc_step()
+        torch.cuda.synchronize()
+    eng.reset_pair_counts()
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        if g is not None:
+            g.replay()
+        else:
+            eng.pc_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    eng.check_status()
+    pd, pf = eng.pair_counts()
+    del g
+    return tot / steps, (pd + pf) / steps
+
+
+def other_configs(dev, flush, stream):
+    """The other workloads, briefly: elliptical drop (5,025), the 3D
+    128^3 lattice (one evaluation), 256 batched drops, each FP32C and FP64."""
+    import torch
+    from pysph_b200.engine import Engine
+    out = {}
+    for name, steps in (("drop", 50), ("batched", 10)):
+        wl = workload(name)
+        for prec in ("fp32c", "fp64"):
+            eng = Engine(wl["scenes"], wl["scheme"], dim=2, precision=prec, lanes=2,
+                         pair_block=128, stencil=2, device=dev)
+            ms, pairs = timed_steps(eng, steps, flush, stream)
+            out[f"{name}_{prec}"] = {"particles": eng.N, "scenes": eng.S,
+                                     "ms_per_step": ms, "steps_per_s": 1e3 / ms,
+                                     "pair_interactions_per_s": pairs / (ms / 1e3)}
+            del eng
+            torch.cuda.empty_cache()
+    wl = workload("lattice3d")
+    for prec in ("fp32c", "fp64"):
+        eng = Engine(wl["scenes"], wl["scheme"], dim=3, precision=prec, lanes=4,
+                     pair_block=128, stencil=1, device=dev)
+        # one evaluation: rebin + SPHRho + SPHPressureGradient
+        def one():
+            eng.bin(0)
+            eng.density(eos=False)
+            eng.momentum(gravity=False, mode=1 | (16 if eng.list_cap else 0))
+        for _ in range(3):
+            one()
+        eng.reset_pair_counts()
+        tot = 0.0
+        for _ in range(5):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one()
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        eng.check_status()
+        pd, pf = eng.pair_counts()
+        ms = tot / 5
+        out[f"lattice3d_{prec}"] = {"particles": eng.N, "ms_per_evaluation": ms,
+                                    "pair_interactions_per_s": (pd + pf) / 5 / (ms / 1e3)}
+        del eng
+        torch.cuda.empty_cache()
+    return out
+
+
+def adjoint_measure(dev, stream):
+    """Differentiable rollout: elliptical drop, 50k particles (dx = 0.0079),
+    200 steps of dt = 2e-6, checkpoints every 20, FP32C forward, FP64
+    adjoint; times forward and backward with CUDA events."""
+    import torch
+    from pysph_b200 import workloads as W
+    from pysph_b200.adjoint import Rollout
+    from pysph_b200.engine import fluid_scheme
+    arrays, _, params = W.elliptical_drop(dx=0.0079)
+    tarr, _, _ = W.elliptical_drop(dx=0.0079, vel_scale=110.0)
+    a = arrays[0]
+    n = len(a["x"])
+    v0 = torch.tensor(np.stack([a["u"], a["v"]]), dtype=torch.float64, device=dev)
+    vt = torch.tensor(np.stack([tarr[0]["u"], tarr[0]["v"]]), dtype=torch.float64, device=dev)
+    xt = Rollout(tarr, params, fluid_scheme(1), 2, 2e-6, 200, precision="fp32c",
+                 device=dev).forward({0: vt})[0][0]
+    r = Rollout(arrays, params, fluid_scheme(1), 2, 2e-6, 200, checkpoint_every=20,
+                precision="fp32c", device=dev)
+    r.forward({0: v0})  # warm
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    xf = r.forward({0: v0})[0][0]
+    ev[1].record(stream)
+    lam = {0: (2.0 * (xf - xt) / n, torch.zeros_like(xf))}
+    g = r.backward(lam)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    fwd = ev[0].elapsed_time(ev[1])
+    bwd = ev[1].elapsed_time(ev[2])
+    return {"workload": "elliptical drop 50k (dx=0.0079), 200 steps dt=2e-6, "
+                        "checkpoints every 20, FP32C forward, FP64 adjoint",
+            "particles": n, "fwd_ms": fwd, "bwd_ms": bwd, "bwd_fwd_ratio": bwd / fwd,
+            "grad_norm": float(torch.linalg.norm(g[0][1]))}
 
 
 def launches_per_step(eng):
@@ -347,30 +493,53 @@ def launches_per_step(eng):
 
 
 def kernel_times(eng, flush, stream, reps=20):
+    """Milliseconds of each phase of a real step (events between the
+    launches of eager steps, L2 flushed before every step).  Phases of the
+    step-list pipeline: bin (7 launches), density (stage 1, records the
+    lists), force, pc_stage, refresh, density_list (stage 2, from the
+    lists); the force and pc_stage figures average both stages."""
     import torch
-    res = {}
-
-    def timeit(fn):
-        tot = 0.0
-        for _ in range(reps):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fn()
-            b.record(stream)
-            torch.cuda.synchronize()
-            tot += a.elapsed_time(b)
-        return tot / reps
-
-    # bin twice per timing so the buffer parity is preserved
-    res["bin"] = timeit(lambda: (eng.bin(0), eng.bin(0))) / 2
-    res["density"] = timeit(lambda: eng.density())
-    res["force"] = timeit(lambda: eng.momentum())
-    res["pc_stage"] = timeit(lambda: (eng.pc_stage(0)))
-    torch.cuda.synchronize()
+    from pysph_b200 import _native as nat
+    names = ["step_begin", "bin", "density", "force1", "pc0", "mid", "density2",
+             "force2", "pc1"]
+    acc = {n: 0.0 for n in names}
+    for _ in range(reps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+        ev[0].record(stream)
+        eng.step_begin()
+        ev[1].record(stream)
+        eng.bin(0)
+        ev[2].record(stream)
+        eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, nat.DENSITY_EOS)
+        ev[3].record(stream)
+        eng.momentum(mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0))
+        ev[4].record(stream)
+        eng.pc_stage(0)
+        ev[5].record(stream)
+        if eng.step_lists:
+            eng.call("sphb_refresh", eng.cur)
+        else:
+            eng.bin(nat.BIN_MOVE_INITIAL)
+        ev[6].record(stream)
+        flags = nat.DENSITY_EOS | (nat.DENSITY_USE_LIST if eng.step_lists else 0)
+        eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, flags)
+        ev[7].record(stream)
+        eng.momentum(mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0))
+        ev[8].record(stream)
+        eng.pc_stage(1)
+        ev[9].record(stream)
+        torch.cuda.synchronize()
+        for i, n in enumerate(names):
+            acc[n] += ev[i].elapsed_time(ev[i + 1])
     eng.check_status()
-    return res
+    t = {n: v / reps for n, v in acc.items()}
+    return {"bin": t["bin"], "density": t["density"],
+            "force": 0.5 * (t["force1"] + t["force2"]),
+            "pc_stage": 0.5 * (t["pc0"] + t["pc1"]),
+            ("refresh" if eng.step_lists else "bin_mid"): t["mid"],
+            "density_list" if eng.step_lists else "density2": t["density2"],
+            "step_begin": t["step_begin"]}
 
 
 def fp64_comparison(args, wl, eng32, flush, stream, dev):

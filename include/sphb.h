@@ -56,7 +56,9 @@ enum {
     SPHB_ST_NONFINITE_RHO = 1u << 3,  /* NaN/Inf density or pressure */
     SPHB_ST_NONFINITE_ACC = 1u << 4,  /* NaN/Inf acceleration */
     SPHB_ST_BAD_INDEX = 1u << 5,      /* an index failed its bounds check */
-    SPHB_ST_NBR_CAPACITY = 1u << 6    /* neighbour list output too small */
+    SPHB_ST_NBR_CAPACITY = 1u << 6,   /* neighbour list output too small */
+    SPHB_ST_SKIN = 1u << 7            /* a step moved particles further than
+                                         the list skin the cell size allows */
 };
 
 enum { SPHB_FP64 = 0, SPHB_FP32C = 1 };   /* plain FP64 / FP32 + Kahan */
@@ -96,6 +98,9 @@ typedef struct {
     int32_t use_cfl;        /* 0: dt kept as set; 1: viscous + force CFL rule;
                                2: viscous rule only (ViscousTimeStep) */
     int32_t pad0;
+    double skin_max;        /* largest motion skin the cell size allows for
+                               lists reused across a step (0: lists serve
+                               one stage only) */
 } sphb_scene;
 
 /* Per-scene state, written by the kernels (host may seed dt, t, count). */
@@ -110,6 +115,8 @@ typedef struct {
     long long count;        /* completed steps */
     unsigned long long max_dtfac;  /* bits of max dt_fac (double, >= 0) */
     unsigned long long max_acc2;   /* bits of max |a|^2 (double, >= 0) */
+    unsigned long long max_v2;     /* bits of max |v|^2 of the integrated
+                                      particles at the start of a step */
 } sphb_scene_state;
 
 /* Contiguous particle range inside one segment; launch unit of every
@@ -248,6 +255,21 @@ SPHB_API int sphb_cell_coords(const sphb_engine *e, int cur, int32_t *out, void 
  * FixedDestNbrParticleLocator._update_cache, S/base/nnps.pyx:596-621). */
 SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
                  int with_eos, void *stream);
+/* with_eos bits: SPHB_DENSITY_EOS applies Tait; SPHB_DENSITY_USE_LIST sums
+ * over the lists recorded by an earlier pass of the same step instead of
+ * searching cells (see sphb_refresh).  A list records every pair within
+ * (radius_scale h + dt |v|max)(1 + 1e-5) of the positions it was built at:
+ * the predictor moves each particle by dt/2 v, so the list holds every
+ * neighbour of the mid-step positions; each pass still applies the exact
+ * predicate. */
+#define SPHB_DENSITY_EOS 1
+#define SPHB_DENSITY_USE_LIST 2
+
+/* Refresh the FP32 pair records (positions relative to each particle's
+ * cell of the last bin, velocities) from the FP64 state after
+ * sphb_pc_stage(0), instead of a full rebin: the mid-step stage then runs
+ * on the lists of the step's first stage.  No-op for SPHB_FP64. */
+SPHB_API int sphb_refresh(const sphb_engine *e, int cur, void *stream);
 
 /* Tait EOS alone on the dest arrays in dest_mask (rho already set). */
 SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *stream);

@@ -27,7 +27,9 @@ ST_NONFINITE_RHO = 1 << 3
 ST_NONFINITE_ACC = 1 << 4
 ST_BAD_INDEX = 1 << 5
 ST_NBR_CAPACITY = 1 << 6
+ST_SKIN = 1 << 7
 STATUS_NAMES = {
+    ST_SKIN: "a step moved particles further than the list skin allows",
     ST_GRID_OVERFLOW: "cell grid larger than cell_capacity",
     ST_NONFINITE_POS: "non-finite particle position",
     ST_OUT_OF_GRID: "particle outside its scene grid",
@@ -61,13 +63,14 @@ class Scene(ctypes.Structure):
                 ("c0", f64), ("rho0", f64), ("gamma", f64), ("B", f64),
                 ("alpha", f64), ("beta", f64), ("eta", f64), ("g", f64 * 3),
                 ("cfl", f64), ("dt_initial", f64), ("static_lo", f64 * 3),
-                ("static_hi", f64 * 3), ("use_cfl", i32), ("pad0", i32)]
+                ("static_hi", f64 * 3), ("use_cfl", i32), ("pad0", i32),
+                ("skin_max", f64)]
 
 
 class SceneState(ctypes.Structure):
     _fields_ = [("lo", i32 * 3), ("n", i32 * 3), ("cell_base", i32),
                 ("ncells", i32), ("box", u64 * 6), ("dt", f64), ("t", f64),
-                ("count", i64), ("max_dtfac", u64), ("max_acc2", u64)]
+                ("count", i64), ("max_dtfac", u64), ("max_acc2", u64), ("max_v2", u64)]
 
 
 class Tile(ctypes.Structure):
@@ -85,6 +88,8 @@ class Buffers(ctypes.Structure):
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
                "vel", "thermo", "cell", "nbr", "nbr_cnt")
 FORCE_USE_LIST = 16
+DENSITY_EOS = 1
+DENSITY_USE_LIST = 2
 
 
 class Fields(ctypes.Structure):
@@ -140,6 +145,7 @@ def lib():
         "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
         "sphb_init_index": (i32, [E, i32, vp]),
         "sphb_set_dt": (i32, [E, f64, vp]),
+        "sphb_refresh": (i32, [E, i32, vp]),
         "sphb_permute": (i32, [E, i32, i32, i32, vp, vp, vp, vp]),
         "sphb_force_vjp": (i32, [E, i32, u32, vp, vp, vp, vp, vp, vp, vp]),
         "sphb_eos_vjp": (i32, [E, i32, vp, vp, vp, vp]),
@@ -161,7 +167,7 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
             "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
-            "sphb_set_dt", "sphb_permute", "sphb_force_vjp", "sphb_eos_vjp",
+            "sphb_set_dt", "sphb_refresh", "sphb_permute", "sphb_force_vjp", "sphb_eos_vjp",
             "sphb_density_vjp", "sphb_neighbor_counts_static")
 
 STATIC_MAX_PARTICLES = 1 << 18

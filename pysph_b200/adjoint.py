@@ -90,7 +90,11 @@ class Rollout:
         for n in range(self.steps):
             eng.pc_step()
             if (n + 1) % self.k == 0 and n + 1 < self.steps:
-                self.checkpoints.append(self._clone(self.get_state()))
+                ck = self._clone(self.get_state())
+                self.checkpoints.append(ck)
+                # restart from the checkpoint exactly as backward() will, so
+                # the recomputed segment is bit-identical to this one
+                self.set_state(ck)
         eng.check_status()
         return self.get_state()
 
@@ -112,15 +116,9 @@ class Rollout:
         out = []
         for _ in range(nsteps):
             s0 = self.get_state()
-            eng.step_begin()
-            eng.bin(0)
-            eng.eval_stage()
-            eng.pc_stage(0)
-            sh = self.get_state()
-            eng.bin(nat.BIN_MOVE_INITIAL)
-            eng.eval_stage()
-            eng.pc_stage(1)
-            out.append((s0, sh))
+            half = {}
+            eng.pc_step(on_half=lambda: half.__setitem__("sh", self.get_state()))
+            out.append((s0, half["sh"]))
         return out
 
     # ---------------------------------------------------------------- VJP

@@ -3,8 +3,8 @@
 // One rebin = scene boxes -> per-scene grids -> cell key per particle ->
 // counting sort (histogram, two-level scan, scatter) -> gather of the
 // particle state into the other buffer in cell order, ranking the members of
-// each cell by previous engine position so the order is deterministic, plus
-// the FP32 pair records.
+// each cell by particle index so the order is canonical, plus the FP32 pair
+// records.
 //
 // The reference bins with a Python dict of cells keyed by floor(x / cs)
 // (CellManager._insert_particles, S/base/cell.pyx:1229-1300); its OpenCL
@@ -27,6 +27,7 @@ __global__ void k_box_reset(const __grid_constant__ sphb_engine e)
         e.sstate[s].box[d] = enc_double(INFINITY);
         e.sstate[s].box[3 + d] = enc_double(-INFINITY);
     }
+    e.sstate[s].max_v2 = 0ull;
 }
 
 __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_box_accum(const __grid_constant__ sphb_engine e, int cur)
@@ -51,6 +52,53 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_box_accum(const __grid_const
         double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
         if (threadIdx.x == 0 && hi > -INFINITY)
             atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
+    }
+    // largest speed of the integrated particles: the motion skin of a step
+    const int a = t.seg - s * e.cfg.num_arrays;
+    double v2 = 0.0;
+    if (k < t.end && ((e.cfg.step_on >> a) & 1u)) {
+        v2 = B.u[k] * B.u[k] + B.v[k] * B.v[k];
+        if (dim == 3) v2 += B.w[k] * B.w[k];
+        if (!isfinite(v2)) v2 = 0.0;
+    }
+    const double bv = block_reduce(v2, OpMax(), 0.0);
+    if (threadIdx.x == 0) atomic_max_nonneg(&e.sstate[s].max_v2, bv);
+}
+
+// FP32 pair records from the FP64 state without reordering: positions
+// relative to the origin of each particle's cell of the last bin (still
+// within a skin of that cell), velocities.
+template <int DIM>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_refresh(const __grid_constant__ sphb_engine e, int cur)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A;
+    const sphb_scene_state &st = e.sstate[s];
+    const double cs = e.scene[s].cell_size;
+    const sphb_buffers &B = e.buf[cur];
+    int local = e.f.cell[k];
+    if (local < 0 || local >= st.ncells) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        local = 0;
+    }
+    int cx, cy, cz;
+    cell_coords(local, st.n, cx, cy, cz);
+    const float xr = (float)(B.x[k] - (double)(st.lo[0] + cx) * cs);
+    const float yr = (float)(B.y[k] - (double)(st.lo[1] + cy) * cs);
+    float4 *geo = (float4 *)e.f.geo;
+    if (DIM == 2) {
+        const float4 g = geo[k];
+        geo[k] = make_float4(xr, yr, g.z, g.w);
+        ((float2 *)e.f.vel)[k] = make_float2((float)B.u[k], (float)B.v[k]);
+    } else {
+        const float zr = (float)(B.z[k] - (double)(st.lo[2] + cz) * cs);
+        const float4 g = geo[k];
+        geo[k] = make_float4(xr, yr, zr, g.w);
+        ((float4 *)e.f.vel)[k] = make_float4((float)B.u[k], (float)B.v[k], (float)B.w[k], 0.f);
     }
 }
 
@@ -292,9 +340,10 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_scatter(const __grid_constan
 
 // -------------------------------------------------------------- reorder --
 // Thread k takes particle p = perm[k] (the scatter put it somewhere inside
-// its cell's range [b, e)), ranks it among the cell's members by previous
-// engine position, and writes it to b + rank: the order inside a cell is
-// deterministic whatever order the atomics handed out the slots.
+// its cell's range [b, e)), ranks it among the cell's members by their index
+// in the particle array, and writes it to b + rank: the order inside a cell
+// is canonical whatever order the atomics handed out the slots, and it does
+// not depend on the order the particles had before.
 template <int DIM, bool F32>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
@@ -319,8 +368,12 @@ k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
             flag(e, SPHB_ST_BAD_INDEX);
             return;
         }
+        // canonical order inside a cell: by the particle's index in its
+        // array, so the order depends on the positions alone
+        const int *__restrict__ sidx = e.buf[cur].idx;
+        const int me = sidx[p];
         int rank = 0;
-        for (int i = b; i < en; ++i) rank += (e.work.perm[i] < p) ? 1 : 0;
+        for (int i = b; i < en; ++i) rank += (sidx[e.work.perm[i]] < me) ? 1 : 0;
         k = b + rank;
     }
     const sphb_buffers &S = e.buf[cur];
@@ -416,6 +469,18 @@ extern "C" int sphb_box_init(const sphb_engine *e, int cur, void *stream)
     if (e->num_tiles > 0)
         k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
     return launch_status("sphb_box_init");
+}
+
+extern "C" int sphb_refresh(const sphb_engine *e, int cur, void *stream)
+{
+    int rc = check_engine(e, cur);
+    if (rc) return rc;
+    if (e->cfg.precision != SPHB_FP32C || e->num_tiles == 0) return SPHB_OK;
+    if (!e->f.geo || !e->f.vel || !e->f.cell) return SPHB_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (e->cfg.dim == 2) k_refresh<2><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    else k_refresh<3><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    return launch_status("sphb_refresh");
 }
 
 extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)

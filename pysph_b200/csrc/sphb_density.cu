@@ -20,8 +20,10 @@ int check_engine_public(const sphb_engine *e, int cur);
 
 template <int DIM, bool F32, int LANES, int R>
 __global__ void __launch_bounds__(512)
-k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int with_eos)
+k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
+    const int with_eos = flags & SPHB_DENSITY_EOS;
+    const bool from_list = (flags & SPHB_DENSITY_USE_LIST) && e.f.list_cap > 0;
     const sphb_tile tl = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = tl.seg / A, a = tl.seg - s * A;
@@ -37,10 +39,19 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     const int *__restrict__ start = e.work.start;
     unsigned long long np = 0;
     double rho = 0.0;
-    // neighbour list of this lane: slots lane, lane + LANES, ... of k
+    // neighbour list of this lane: slots lane, lane + LANES, ... of k,
+    // recorded with the motion skin dt |v|max unless this pass reads them
     const int N = e.cfg.num_particles;
-    uint32_t *__restrict__ nbr = e.f.list_cap > 0 ? e.f.nbr : nullptr;
+    uint32_t *__restrict__ nbr = (e.f.list_cap > 0 && !from_list) ? e.f.nbr : nullptr;
     const int cap_lane = e.f.list_cap / LANES;
+    double skin = 0.0;
+    if (nbr && sc.skin_max > 0.0) {
+        skin = st.dt * sqrt(__longlong_as_double((long long)st.max_v2));
+        if (skin > sc.skin_max) {
+            if (threadIdx.x == 0) flag(e, SPHB_ST_SKIN);
+            skin = sc.skin_max;
+        }
+    }
     int cnt = 0;
     auto record = [&](int j, int o, int dy, int dz) {
         if (nbr) {
@@ -61,11 +72,12 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const float hk = DIM == 3 ? gk.w : gk.z;
             const float rad = hk * (float)sc.radius_scale;
             const float rad2 = rad * rad;
+            const float radl = (float)((hk * sc.radius_scale + skin) * (1.0 + 1e-5));
+            const float radl2 = nbr ? radl * radl : rad2;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
-            for_each_candidate<DIM, R, LANES>(
-                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
-                e.cfg.num_particles, e.work.status,
+            traverse<DIM, R, LANES>(
+                e, from_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
                 [&](int j, int o, int dy, int dz) {
                     const float4 gj = __ldg(geo + j);
                     const float dx = (xk - gj.x) - (float)o * csf;
@@ -75,12 +87,14 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                         const float ddz = (zk - gj.z) - (float)dz * csf;
                         r2 += ddz * ddz;
                     }
-                    if (r2 < rad2) {
-                        const float hj = DIM == 3 ? gj.w : gj.z;
-                        const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
-                        acc.add(mj * w_cubic_f<DIM>(r2, 0.5f * (hk + hj)));
-                        ++np;
+                    if (r2 < radl2) {
                         record(j, o, dy, dz);
+                        if (r2 < rad2) {
+                            const float hj = DIM == 3 ? gj.w : gj.z;
+                            const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
+                            acc.add(mj * w_cubic_f<DIM>(r2, 0.5f * (hk + hj)));
+                            ++np;
+                        }
                     }
                 });
         }
@@ -99,21 +113,24 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const double hk = B.h[k];
             const double rad = hk * sc.radius_scale;
             const double rad2 = __dmul_rn(rad, rad);
+            const double radl = (rad + skin) * (1.0 + 1e-5);
+            const double radl2 = nbr ? radl * radl : rad2;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
-            for_each_candidate<DIM, R, LANES>(
-                start, A, src, cell_base, ncells, n, cx, cy, cz, lane,
-                e.cfg.num_particles, e.work.status,
+            traverse<DIM, R, LANES>(
+                e, from_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
                 [&](int j, int o, int oy, int oz) {
                     const double dx = xk - __ldg(B.x + j);
                     const double dy = yk - __ldg(B.y + j);
                     const double dz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
                     const double d2 = dist2_ref<DIM>(dx, dy, dz);
-                    if (d2 < rad2) {
-                        const double hab = 0.5 * (hk + __ldg(B.h + j));
-                        sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
-                        ++np;
+                    if (d2 < radl2) {
                         record(j, o, oy, oz);
+                        if (d2 < rad2) {
+                            const double hab = 0.5 * (hk + __ldg(B.h + j));
+                            sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
+                            ++np;
+                        }
                     }
                 });
         }

@@ -51,6 +51,7 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         for (int q = threadIdx.x; q < e.cfg.num_scenes; q += blockDim.x) {
             e.sstate[q].max_dtfac = 0ull;
             e.sstate[q].max_acc2 = 0ull;
+            e.sstate[q].max_v2 = 0ull;   // the corrector stage records the next step's
         }
     }
     if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
@@ -59,6 +60,7 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const sphb_buffers &B = e.buf[cur];
     const double dt2 = e.sstate[s].dt / 2;
     double p[3] = {0.0, 0.0, 0.0};
+    double vsq = 0.0;   // |v|^2 after the corrector: the next step's skin
     if (active) {
         const bool real = B.tag[k] == 0;
         double f[3] = {0.0, 0.0, 0.0};
@@ -94,8 +96,10 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
                 const double vh = axpy_rn(v0, f[d], dt2);
                 const double xn = __dadd_rn(2 * xh, -x0);
                 X[d][k] = xn;
-                V[d][k] = __dadd_rn(2 * vh, -v0);
+                const double vn = __dadd_rn(2 * vh, -v0);
+                V[d][k] = vn;
                 p[d] = xn;
+                vsq += vn * vn;
             }
         }
     }
@@ -107,6 +111,10 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         const double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
         if (threadIdx.x == 0 && hi > -INFINITY)
             atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
+    }
+    if (stage == 1) {
+        const double bv = block_reduce(isfinite(vsq) ? vsq : 0.0, OpMax(), 0.0);
+        if (threadIdx.x == 0) atomic_max_nonneg(&e.sstate[s].max_v2, bv);
     }
 }
 

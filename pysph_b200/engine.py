@@ -24,6 +24,7 @@ import torch
 from . import _native as nat
 
 ELEM_TILE = 256
+SKIN_MARGIN = 0.05
 MASTER = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0", "w0",
           "m", "h")
 USER_PROPS = ("x", "y", "z", "u", "v", "w", "m", "h")
@@ -99,7 +100,8 @@ class Engine:
     def __init__(self, scenes, scheme: Scheme, dim: int = 2,
                  precision: str = "fp32c", stencil: int = 1, lanes: int = 1,
                  pair_block: int = 128, cell_capacity: int | None = None,
-                 grid_growth: float = 2.0, device=None, use_lists: bool = True):
+                 grid_growth: float = 2.0, device=None, use_lists: bool = True,
+                 step_lists: bool = True):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -137,6 +139,11 @@ class Engine:
         self.user_n = [int(sizes[:, a].sum()) for a in range(self.A)]
         self._stencil = stencil
         self.use_lists = use_lists
+        # one list per step (the mid-step stage refreshes records instead of
+        # rebinning): cells 5% larger than the support leave room for the
+        # motion skin; off, the cell size is exactly the reference's
+        self.step_lists = bool(use_lists and step_lists)
+        self.skin_margin = SKIN_MARGIN if self.step_lists else 0.0
         self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
@@ -158,7 +165,7 @@ class Engine:
             max_h = max(float(h.max()) if len(h) else 0.0 for h in hs)
             if max_h <= 0:
                 max_h = 0.5  # the reference's "cell size 0 -> 1"
-            cs = p.radius_scale * max_h / self._stencil
+            cs = p.radius_scale * max_h * (1.0 + self.skin_margin) / self._stencil
             step_h = [h for a, h in enumerate(hs) if a in step and len(h)]
             h_min = min(float(h.min()) for h in step_h) if step_h else max_h
             lo = np.full(3, np.inf)
@@ -178,6 +185,9 @@ class Engine:
             self._extent.append((alo, ahi, cs))
             t = sc[s]
             t.cell_size = cs
+            # list radius (support + skin)(1 + 1e-5) must stay within R cells
+            t.skin_max = (p.radius_scale * max_h * (self.skin_margin - 1e-4)
+                          if self.skin_margin else 0.0)
             t.radius_scale = p.radius_scale
             t.h_min = h_min
             t.c0, t.rho0, t.gamma = p.c0, p.rho0, p.gamma
@@ -470,24 +480,34 @@ class Engine:
     def step_begin(self):
         self.call("sphb_step_begin")
 
-    def eval_stage(self):
+    def eval_stage(self, from_list=False):
         """Integrator.eval of the pinned scheme at the current positions:
         SPHRho + Tait (fused), Tait on arrays without SPHRho, then
-        MomentumEquation (or SPHPressureGradient) + GravityForce."""
-        self.density()
+        MomentumEquation (or SPHPressureGradient) + GravityForce.  The
+        density pass records the neighbour lists the force pass reads, or
+        with from_list reads the lists of the step's first stage."""
+        flags = nat.DENSITY_EOS | (nat.DENSITY_USE_LIST if from_list else 0)
+        self.call("sphb_density", self.cur, self.scheme.rho_dests, flags)
         if self.tait_only_mask:
             self.tait(self.tait_only_mask)
         self.momentum(mode=self.force_mode | (nat.FORCE_USE_LIST if self.list_cap else 0))
 
-    def pc_step(self):
+    def pc_step(self, on_half=None):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
-        preceded by the Solver's per-step prologue (count, dt)."""
+        preceded by the Solver's per-step prologue (count, dt).  on_half,
+        when given, is called after the predictor stage."""
         self.step_begin()
         self.bin(0)
         self.eval_stage()
         self.pc_stage(0)
-        self.bin(nat.BIN_MOVE_INITIAL)
-        self.eval_stage()
+        if on_half is not None:
+            on_half()
+        if self.step_lists:
+            self.call("sphb_refresh", self.cur)
+            self.eval_stage(from_list=True)
+        else:
+            self.bin(nat.BIN_MOVE_INITIAL)
+            self.eval_stage()
         self.pc_stage(1)
 
     # ---------------------------------------------------------- host sync
@@ -534,6 +554,9 @@ class Engine:
         self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 0,
                   v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it
+        if name in ("x", "y", "z", "u", "v", "w"):
+            # the next bin recomputes the boxes and the step's motion skin
+            self._box_valid = False
 
     def exchange_out(self, array: int, name: str, out: torch.Tensor | None = None):
         """Engine -> user-order FP64 tensor (scenes concatenated)."""

@@ -59,7 +59,8 @@ def engine_for(case, precision, **kw):
 
 @pytest.mark.parametrize("case", list(CASES))
 def test_cell_coords_bit_exact(case):
-    eng, arrays, params, scheme, dim = engine_for(case, "fp64")
+    # step_lists=False: the cell size is exactly the reference's 2 * max h
+    eng, arrays, params, scheme, dim = engine_for(case, "fp64", step_lists=False)
     cs = eng.cell_size()
     # CellManager cell size = 2 * max h over all arrays (S/base/cell.pyx:911-941)
     max_h = max(float(np.max(a["h"])) for a in arrays)

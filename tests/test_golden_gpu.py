@@ -39,7 +39,8 @@ def sorted_pairs(off, idx):
 def test_neighbour_sets_and_cells(name, dim):
     g = load(name)
     arr = arrays(g, ["in_"])
-    eng = Engine([(arr, DROP)], fluid_scheme(1), dim=dim, precision="fp64")
+    eng = Engine([(arr, DROP)], fluid_scheme(1), dim=dim, precision="fp64",
+                 step_lists=False)
     assert eng.cell_size() == float(g["cell_size"])
     di, _, sj = eng.neighbors(0, 1)
     rdi, rsj = sorted_pairs(g["nbr_off"], g["nbr_idx"])
