@@ -202,31 +202,29 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 def algorithmic_bytes(dim, f32):
     """Bytes per particle each phase must move once, at the stored widths
     (neighbour re-reads and the neighbour lists, which are scratch, are not
-    counted)."""
+    counted).  pc_stage includes the FP32 record refresh and the anchor
+    read of the displacement check; bin is one full rebin."""
     if f32 and dim == 2:
         d = {"density": 16 + 4 + 4 + 16 + 16,           # geo, cell, tag; thermo r/w
              "force": 16 + 8 + 16 + 4 + 4 + 12,         # geo, vel, thermo, cell, tag; a, dt_fac
-             "pc_stage": 8 * 8 + 4 + 8,                 # x,y,u,v r/w + x0.. ; tag; a
+             # x,y,u,v r/w, x0..v0, tag, a; cell, geo.xy w, vel w, anchor r
+             "pc_stage": 8 * 8 + 4 + 8 + 4 + 8 + 8 + 8,
              # hash x,y 16, key/slot w+r 16, perm w+r 8, key 4; gather
-             # x,y,u,v,m,h,idx,tag 56 r + 56 w; cell 4, geo 16, vel 8 w
-             "bin": 16 + 16 + 8 + 4 + 56 + 56 + 4 + 16 + 8,
-             "refresh": 32 + 4 + 16 + 16 + 8}           # x,y,u,v, cell, geo r/w, vel w
+             # x,y,u,v,m,h,idx,tag 56 r + 56 w; cell 4, geo 16, vel 8,
+             # anchor 8 w; copy back 56 r + 56 w
+             "bin": 16 + 16 + 8 + 4 + 56 + 56 + 4 + 16 + 8 + 8 + 56 + 56}
     elif f32 and dim == 3:
         d = {"density": 16 + 4 + 4 + 4 + 16 + 16,
              "force": 16 + 4 + 16 + 16 + 4 + 4 + 16,
-             "pc_stage": 12 * 8 + 4 + 12,
-             "bin": 24 + 16 + 8 + 4 + 72 + 72 + 4 + 16 + 4 + 16,
-             "refresh": 48 + 4 + 16 + 16 + 16}
+             "pc_stage": 12 * 8 + 4 + 12 + 4 + 8 + 16 + 16 + 16,
+             "bin": 24 + 16 + 8 + 4 + 72 + 72 + 4 + 16 + 4 + 16 + 16 + 72 + 72}
     else:
         w = 8
         d = {"density": dim * w + 2 * w + 4 + 4 + 3 * w,
              "force": 2 * dim * w + 2 * w + 3 * w + 4 + 4 + (dim + 1) * w,
-             "pc_stage": 4 * dim * w + 4 + dim * w,
-             "bin": dim * w + 16 + 8 + 4 + 2 * (2 * dim * w + 2 * w + 8) + 4,
-             "refresh": 0}
-    d["density_list"] = d["density"]
-    d["density2"] = d["density"]
-    d["bin_mid"] = d["bin"] + (32 if dim == 2 else 48) * 2
+             "pc_stage": 4 * dim * w + 4 + dim * w + 4 + (8 if dim == 2 else 16),
+             "bin": (dim * w + 16 + 8 + 4 + 2 * (2 * dim * w + 2 * w + 8) + 4
+                     + (8 if dim == 2 else 16) + 2 * (2 * dim * w + 2 * w + 8))}
     return d
 
 
@@ -319,12 +317,16 @@ def run_ours(args, rank, world, local):
         del graph
         return out
 
-    # ---- per-kernel timing for the roofline (one rebin + one stage)
+    # ---- per-phase timing for the roofline
     kern = kernel_times(eng, flush, stream)
     byts = algorithmic_bytes(wl["dim"], eng.f32)
-    dominant = max((k for k in kern if k in byts), key=lambda k: kern[k])
+    # a full rebin for "bin" (its per-stage average includes the kept lists)
+    per_launch = {"density": kern["density"], "force": kern["force"],
+                  "pc_stage": kern["pc_stage"], "bin": kern["rebin_ms"]}
+    dominant = max(per_launch, key=lambda k: per_launch[k] * (
+        kern["rebins_per_stage"] if k == "bin" else 1.0))
     hbm, which = peaks()
-    ach = byts[dominant] * N / (kern[dominant] * 1e-3) / 1e9
+    ach = byts[dominant] * N / (per_launch[dominant] * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
             "peak": hbm, "peak_kind": which, "unit": "GB/s",
             "frac": round(ach / hbm, 4), "traffic": None,
@@ -487,59 +489,67 @@ def adjoint_measure(dev, stream):
 
 
 def launches_per_step(eng):
-    # step_begin + 2 x (bin: grid, hash, 3 scan, scatter, cell sort, reorder
-    # [+ box reset/accum when the box is stale]) + 2 x (density, force, stage)
-    return 1 + 2 * 8 + 2 * 3
+    """Kernels launched per PC step (every launch counts, including the
+    rebin kernels that return at once when the device keeps the lists)."""
+    # per rebin: [decide] + grid, hash, 3 scan, scatter, reorder [+ copy back]
+    rebin = 7 + (2 if eng.step_lists else 0)
+    return 1 + 2 * rebin + 2 * 3 + (2 if eng.tait_only_mask else 0)
 
 
-def kernel_times(eng, flush, stream, reps=20):
-    """Milliseconds of each phase of a real step (events between the
-    launches of eager steps, L2 flushed before every step).  Phases of the
-    step-list pipeline: bin (7 launches), density (stage 1, records the
-    lists), force, pc_stage, refresh, density_list (stage 2, from the
-    lists); the force and pc_stage figures average both stages."""
+def kernel_times(eng, flush, stream, reps=40):
+    """Milliseconds of each phase of real steps (eager launches, events
+    around each phase, L2 flushed before every step), averaged per stage,
+    with the device's rebin decisions counted: bin (decision + rebin when
+    taken), density (records the lists after a rebin, reads them
+    otherwise), force (from the lists), pc_stage."""
     import torch
     from pysph_b200 import _native as nat
-    names = ["step_begin", "bin", "density", "force1", "pc0", "mid", "density2",
-             "force2", "pc1"]
-    acc = {n: 0.0 for n in names}
-    for _ in range(reps):
+    phases = ["step_begin", "bin0", "density0", "force0", "pc0",
+              "bin1", "density1", "force1", "pc1"]
+    acc = {n: 0.0 for n in phases}
+    reuse = nat.BIN_IF_NEEDED if eng.step_lists else 0
+    moff = eng.work_offsets[nat.WORK_NAMES.index("meta")]
+    meta1 = eng.work_buf[moff + 4:moff + 8].view(torch.int32)
+    took = torch.zeros(reps, 2, dtype=torch.int32, device=eng.device)
+    rebin_ms = [0.0, 0.0]
+    for r in range(reps):
         flush.zero_()
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
-        ev[0].record(stream)
-        eng.step_begin()
-        ev[1].record(stream)
-        eng.bin(0)
-        ev[2].record(stream)
-        eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, nat.DENSITY_EOS)
-        ev[3].record(stream)
-        eng.momentum(mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0))
-        ev[4].record(stream)
-        eng.pc_stage(0)
-        ev[5].record(stream)
-        if eng.step_lists:
-            eng.call("sphb_refresh", eng.cur)
-        else:
-            eng.bin(nat.BIN_MOVE_INITIAL)
-        ev[6].record(stream)
-        flags = nat.DENSITY_EOS | (nat.DENSITY_USE_LIST if eng.step_lists else 0)
-        eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, flags)
-        ev[7].record(stream)
-        eng.momentum(mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0))
-        ev[8].record(stream)
-        eng.pc_stage(1)
-        ev[9].record(stream)
+        ev = {n: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for n in phases}
+
+        def run(n, fn):
+            ev[n][0].record(stream)
+            fn()
+            ev[n][1].record(stream)
+        run("step_begin", eng.step_begin)
+        for st in (0, 1):
+            flags = reuse | (nat.BIN_MOVE_INITIAL if st else 0)
+            run(f"bin{st}", lambda: eng.bin(flags))
+            took[r, st].copy_(meta1[0])
+            dflags = nat.DENSITY_EOS | (nat.DENSITY_LIST_IF_VALID if eng.step_lists else 0)
+            run(f"density{st}",
+                lambda: eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, dflags))
+            run(f"force{st}", lambda: eng.momentum(
+                mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0)))
+            run(f"pc{st}", lambda: eng.pc_stage(st))
         torch.cuda.synchronize()
-        for i, n in enumerate(names):
-            acc[n] += ev[i].elapsed_time(ev[i + 1])
+        tk = took[r].tolist()
+        for n in phases:
+            acc[n] += ev[n][0].elapsed_time(ev[n][1])
+        for st in (0, 1):
+            if tk[st] or not eng.step_lists:
+                rebin_ms[0] += ev[f"bin{st}"][0].elapsed_time(ev[f"bin{st}"][1])
+                rebin_ms[1] += 1
     eng.check_status()
     t = {n: v / reps for n, v in acc.items()}
-    return {"bin": t["bin"], "density": t["density"],
-            "force": 0.5 * (t["force1"] + t["force2"]),
+    rebins = int(took.sum().item()) if eng.step_lists else 2 * reps
+    return {"bin": 0.5 * (t["bin0"] + t["bin1"]),
+            "density": 0.5 * (t["density0"] + t["density1"]),
+            "force": 0.5 * (t["force0"] + t["force1"]),
             "pc_stage": 0.5 * (t["pc0"] + t["pc1"]),
-            ("refresh" if eng.step_lists else "bin_mid"): t["mid"],
-            "density_list" if eng.step_lists else "density2": t["density2"],
-            "step_begin": t["step_begin"]}
+            "step_begin": t["step_begin"],
+            "rebin_ms": rebin_ms[0] / max(rebin_ms[1], 1),
+            "rebins_per_stage": rebins / (2.0 * reps)}
 
 
 def fp64_comparison(args, wl, eng32, flush, stream, dev):

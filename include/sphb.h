@@ -56,9 +56,7 @@ enum {
     SPHB_ST_NONFINITE_RHO = 1u << 3,  /* NaN/Inf density or pressure */
     SPHB_ST_NONFINITE_ACC = 1u << 4,  /* NaN/Inf acceleration */
     SPHB_ST_BAD_INDEX = 1u << 5,      /* an index failed its bounds check */
-    SPHB_ST_NBR_CAPACITY = 1u << 6,   /* neighbour list output too small */
-    SPHB_ST_SKIN = 1u << 7            /* a step moved particles further than
-                                         the list skin the cell size allows */
+    SPHB_ST_NBR_CAPACITY = 1u << 6    /* neighbour list output too small */
 };
 
 enum { SPHB_FP64 = 0, SPHB_FP32C = 1 };   /* plain FP64 / FP32 + Kahan */
@@ -98,9 +96,11 @@ typedef struct {
     int32_t use_cfl;        /* 0: dt kept as set; 1: viscous + force CFL rule;
                                2: viscous rule only (ViscousTimeStep) */
     int32_t pad0;
-    double skin_max;        /* largest motion skin the cell size allows for
-                               lists reused across a step (0: lists serve
-                               one stage only) */
+    double skin_max;        /* list skin: lists hold every pair within
+                               (radius_scale h + skin_max)(1 + 1e-5) and
+                               stay valid while no particle has moved
+                               skin_max / 2 from where it was binned
+                               (0: lists serve one stage only) */
 } sphb_scene;
 
 /* Per-scene state, written by the kernels (host may seed dt, t, count). */
@@ -115,8 +115,10 @@ typedef struct {
     long long count;        /* completed steps */
     unsigned long long max_dtfac;  /* bits of max dt_fac (double, >= 0) */
     unsigned long long max_acc2;   /* bits of max |a|^2 (double, >= 0) */
-    unsigned long long max_v2;     /* bits of max |v|^2 of the integrated
-                                      particles at the start of a step */
+    unsigned long long max_disp2;  /* bits of max |x - x_bin|^2 over the
+                                      particles, from the last
+                                      sphb_pc_stage (x_bin: position at the
+                                      last rebin) */
 } sphb_scene_state;
 
 /* Contiguous particle range inside one segment; launch unit of every
@@ -153,6 +155,11 @@ typedef struct {
      * a lane overflowed its list_cap / lanes slots). */
     uint32_t *nbr;
     int32_t *nbr_cnt;
+    /* Optional (NULL: no list reuse across stages): FP32 position of every
+     * particle at its last rebin, relative to the origin of its cell; 2D
+     * float2, 3D float4 {x, y, z, 0}.  sphb_pc_stage measures how far the
+     * particles have moved from it. */
+    void *anchor;
     int32_t list_cap;       /* slots per particle, 0 = no lists */
     int32_t pad0;
 } sphb_fields;
@@ -170,7 +177,13 @@ typedef struct {
     int32_t *slot;          /* [N] */
     int32_t *perm;          /* [N] */
     int32_t *bsum;          /* [scan blocks + 1] */
-    int32_t *meta;          /* [8]  meta[0] = cells in use (all scenes) */
+    int32_t *meta;          /* [8]  meta[0] = cells in use (all scenes);
+                               meta[1] = 1 when the last rebin decision
+                               rebinned; meta[2] = 1 when it kept the lists
+                               (cleared by anything that moves particles);
+                               meta[3] = 2 while the positions are those of
+                               the last rebin; meta[4] = 1 when the lists
+                               were recorded with the skin at them */
     unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
     unsigned long long *pairs;  /* [4]  pairs evaluated: density, force, -, - */
 } sphb_work;
@@ -228,6 +241,20 @@ SPHB_API int sphb_box_init(const sphb_engine *e, int cur, void *stream);
  * each scene's box to its static bounds. */
 #define SPHB_BIN_MOVE_INITIAL 1
 #define SPHB_BIN_BOX 2
+/* SPHB_BIN_IF_NEEDED (needs f.anchor): the device decides whether to
+ * rebin.  It does not while the particles are where the last rebin put them
+ * (work.meta[3] == 2); otherwise it rebins unless the lists were recorded
+ * with the skin right after the last rebin (work.meta[4]) and no particle
+ * has moved skin_max / 2 since (max_disp2 of the last sphb_pc_stage).  The
+ * decision goes to work.meta[1] and [2].  A rebin then
+ * gathers into buf[cur ^ 1] and copies the result back into buf[cur], so
+ * the state stays in buf[cur] whatever the decision: the caller does not
+ * flip cur, and one captured graph serves every step.  Between rebins the
+ * lists, the cell tables and the cell of each particle stay those of the
+ * last rebin; they remain complete because no pair can close from beyond
+ * support + skin while every particle stays within skin / 2 of its binned
+ * position.  Without the flag, sphb_bin always rebins into buf[cur ^ 1]. */
+#define SPHB_BIN_IF_NEEDED 4
 SPHB_API int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream);
 
 /* Neighbour lists of every particle of the dest arrays in dest_mask among
@@ -256,19 +283,23 @@ SPHB_API int sphb_cell_coords(const sphb_engine *e, int cur, int32_t *out, void 
 SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
                  int with_eos, void *stream);
 /* with_eos bits: SPHB_DENSITY_EOS applies Tait; SPHB_DENSITY_USE_LIST sums
- * over the lists recorded by an earlier pass of the same step instead of
- * searching cells (see sphb_refresh).  A list records every pair within
- * (radius_scale h + dt |v|max)(1 + 1e-5) of the positions it was built at:
- * the predictor moves each particle by dt/2 v, so the list holds every
- * neighbour of the mid-step positions; each pass still applies the exact
- * predicate. */
+ * over the lists of an earlier pass instead of searching cells (the caller
+ * vouches that they are complete).  SPHB_DENSITY_LIST_IF_VALID is the list
+ * reuse of the integrator: it reads the lists when the last
+ * SPHB_BIN_IF_NEEDED kept them and nothing moved the particles since, and
+ * otherwise searches cells and records lists with the skin
+ * (radius_scale h + skin_max)(1 + 1e-5), which become reusable when
+ * recorded right after a rebin.  A pass that records without it uses no
+ * skin and withdraws the lists from reuse.  Every pass applies
+ * the exact predicate r^2 < (radius_scale h)^2 to what it visits. */
 #define SPHB_DENSITY_EOS 1
 #define SPHB_DENSITY_USE_LIST 2
+#define SPHB_DENSITY_LIST_IF_VALID 4
 
 /* Refresh the FP32 pair records (positions relative to each particle's
- * cell of the last bin, velocities) from the FP64 state after
- * sphb_pc_stage(0), instead of a full rebin: the mid-step stage then runs
- * on the lists of the step's first stage.  No-op for SPHB_FP64. */
+ * cell of the last bin, velocities) from the FP64 state without rebinning.
+ * sphb_pc_stage refreshes them itself; this is for state written by other
+ * means.  No-op for SPHB_FP64. */
 SPHB_API int sphb_refresh(const sphb_engine *e, int cur, void *stream);
 
 /* Tait EOS alone on the dest arrays in dest_mask (rho already set). */
@@ -290,7 +321,9 @@ SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
  * stage 0 = predict (save X0, X = X0 + dt/2 F), stage 1 = correct and
  * final (X = 2 (X0 + dt/2 F) - X0).  Stage 0 also clears the per-scene
  * dt_fac / |a| maxima, so sphb_step_begin sees the corrector's pass only.
- * Accumulates the scene boxes for the next sphb_bin.  PositionStepping
+ * Accumulates the scene boxes for the next sphb_bin, refreshes the FP32
+ * pair records of the moved particles and, with f.anchor, accumulates
+ * max_disp2 (cleared by the next SPHB_BIN_IF_NEEDED decision).  PositionStepping
  * (S/sph/funcs/position_funcs.pyx:10-56) supplies F_x = u.
  * PredictorCorrectorIntegrator.integrate (S/solver/integrator.py:646-683),
  * step (:340-367), final_step (:632-644); integrator.cl step_array /
@@ -311,7 +344,9 @@ SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
  * array, with user arrays concatenated over scenes (user_offset[s]).
  * `field` names the engine field: 0..5 x..w, 6..11 x0..w0, 12 m, 13 h,
  * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac. Fields 14..20 are
- * scatter-only. */
+ * scatter-only.  Gathering x..w, m or h marks the lists invalid
+ * (work.meta[2] = 0): the next SPHB_BIN_IF_NEEDED rebins, which also
+ * rebuilds the FP32 pair records from the new state. */
 SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
                   int dir, double *user, const int32_t *user_offset,
                   void *stream);

@@ -27,9 +27,9 @@ ST_NONFINITE_RHO = 1 << 3
 ST_NONFINITE_ACC = 1 << 4
 ST_BAD_INDEX = 1 << 5
 ST_NBR_CAPACITY = 1 << 6
-ST_SKIN = 1 << 7
+BIN_IF_NEEDED = 4
+DENSITY_LIST_IF_VALID = 4
 STATUS_NAMES = {
-    ST_SKIN: "a step moved particles further than the list skin allows",
     ST_GRID_OVERFLOW: "cell grid larger than cell_capacity",
     ST_NONFINITE_POS: "non-finite particle position",
     ST_OUT_OF_GRID: "particle outside its scene grid",
@@ -70,7 +70,7 @@ class Scene(ctypes.Structure):
 class SceneState(ctypes.Structure):
     _fields_ = [("lo", i32 * 3), ("n", i32 * 3), ("cell_base", i32),
                 ("ncells", i32), ("box", u64 * 6), ("dt", f64), ("t", f64),
-                ("count", i64), ("max_dtfac", u64), ("max_acc2", u64), ("max_v2", u64)]
+                ("count", i64), ("max_dtfac", u64), ("max_acc2", u64), ("max_disp2", u64)]
 
 
 class Tile(ctypes.Structure):
@@ -86,7 +86,7 @@ class Buffers(ctypes.Structure):
 
 
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
-               "vel", "thermo", "cell", "nbr", "nbr_cnt")
+               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor")
 FORCE_USE_LIST = 16
 DENSITY_EOS = 1
 DENSITY_USE_LIST = 2

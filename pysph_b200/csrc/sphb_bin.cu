@@ -4,7 +4,11 @@
 // counting sort (histogram, two-level scan, scatter) -> gather of the
 // particle state into the other buffer in cell order, ranking the members of
 // each cell by particle index so the order is canonical, plus the FP32 pair
-// records.
+// records and the anchors (binned positions).  With SPHB_BIN_IF_NEEDED a
+// one-block kernel first decides on the device whether the lists still
+// cover every pair (no particle has moved skin/2 from its anchor); when they
+// do, every later kernel of the rebin returns at once, and when they do not,
+// the gathered state is copied back so it stays in buf[cur].
 //
 // The reference bins with a Python dict of cells keyed by floor(x / cs)
 // (CellManager._insert_particles, S/base/cell.pyx:1229-1300); its OpenCL
@@ -19,19 +23,54 @@
 namespace sphb {
 
 // ---------------------------------------------------------------- boxes --
-__global__ void k_box_reset(const __grid_constant__ sphb_engine e)
+// work.meta[1] == 0 after a decision to keep the lists: the rebin is off
+__device__ __forceinline__ bool skip_rebin(const sphb_engine &e, int gated)
 {
+    return gated && *(volatile int *)&e.work.meta[1] == 0;
+}
+
+// One block.  No rebin while the particles sit where the last rebin put
+// them (work.meta[3] == 2); otherwise rebin unless the lists were recorded
+// with the skin at those positions (work.meta[4]) and no particle of any
+// scene has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding
+// of the displacement) from its anchor.  max_disp2 restarts either way.
+__global__ void k_bin_decide(const __grid_constant__ sphb_engine e)
+{
+    __shared__ int s_far;
+    if (threadIdx.x == 0) s_far = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) {
+        sphb_scene_state &st = e.sstate[s];
+        const double d2 = __longlong_as_double((long long)st.max_disp2);
+        const double lim = 0.5 * e.scene[s].skin_max * (1.0 - 1e-4);
+        if (!(d2 < lim * lim)) s_far = 1;
+        st.max_disp2 = 0ull;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool at_anchor = e.work.meta[3] == 2;
+        const bool lists = e.work.meta[4] == 1;
+        const bool keep = at_anchor || (lists && !s_far);
+        e.work.meta[1] = keep ? 0 : 1;
+        e.work.meta[2] = (keep && lists) ? 1 : 0;
+    }
+}
+
+__global__ void k_box_reset(const __grid_constant__ sphb_engine e, int gated)
+{
+    if (skip_rebin(e, gated)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= e.cfg.num_scenes) return;
     for (int d = 0; d < 3; ++d) {
         e.sstate[s].box[d] = enc_double(INFINITY);
         e.sstate[s].box[3 + d] = enc_double(-INFINITY);
     }
-    e.sstate[s].max_v2 = 0ull;
 }
 
-__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_box_accum(const __grid_constant__ sphb_engine e, int cur)
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_box_accum(const __grid_constant__ sphb_engine e, int cur, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const sphb_tile t = e.tiles[blockIdx.x];
     const int s = t.seg / e.cfg.num_arrays;
     const int k = t.begin + threadIdx.x;
@@ -53,16 +92,6 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_box_accum(const __grid_const
         if (threadIdx.x == 0 && hi > -INFINITY)
             atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
     }
-    // largest speed of the integrated particles: the motion skin of a step
-    const int a = t.seg - s * e.cfg.num_arrays;
-    double v2 = 0.0;
-    if (k < t.end && ((e.cfg.step_on >> a) & 1u)) {
-        v2 = B.u[k] * B.u[k] + B.v[k] * B.v[k];
-        if (dim == 3) v2 += B.w[k] * B.w[k];
-        if (!isfinite(v2)) v2 = 0.0;
-    }
-    const double bv = block_reduce(v2, OpMax(), 0.0);
-    if (threadIdx.x == 0) atomic_max_nonneg(&e.sstate[s].max_v2, bv);
 }
 
 // FP32 pair records from the FP64 state without reordering: positions
@@ -106,8 +135,9 @@ k_refresh(const __grid_constant__ sphb_engine e, int cur)
 // One block.  Grid of scene s: cells floor(lo/cs)-R .. floor(hi/cs)+R per
 // axis (R padding cells, so every stencil row of every particle exists);
 // exclusive prefix of A*ncells over scenes gives the scene key bases.
-__global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sphb_engine e)
+__global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sphb_engine e, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     __shared__ long long sh[1024];
     __shared__ long long s_carry;
     const int S = e.cfg.num_scenes, A = e.cfg.num_arrays, R = e.cfg.stencil;
@@ -170,6 +200,7 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
                 st.box[d] = enc_double(sc.static_lo[d]);
                 st.box[3 + d] = enc_double(sc.static_hi[d]);
             }
+            st.max_disp2 = 0ull;   // the anchors are the new positions
         }
         __syncthreads();
         if (threadIdx.x == 0) s_carry += total;
@@ -182,12 +213,20 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
             used = 0;
         }
         e.work.meta[0] = (int)used;
+        // new order: the lists must be recorded again before they are
+        // reused; the positions are the anchors
+        e.work.meta[1] = 1;
+        e.work.meta[2] = 0;
+        e.work.meta[3] = 2;
+        e.work.meta[4] = 0;
     }
 }
 
 // ----------------------------------------------------------------- hash --
-__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_hash(const __grid_constant__ sphb_engine e, int cur)
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_hash(const __grid_constant__ sphb_engine e, int cur, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
@@ -255,8 +294,10 @@ __device__ __forceinline__ int block_excl_scan_int(int v, int &total)
     return before + x - v;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_reduce(const __grid_constant__ sphb_engine e)
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
+k_scan_reduce(const __grid_constant__ sphb_engine e, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const int T = e.work.meta[0];
     const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
     int sum = 0;
@@ -272,8 +313,10 @@ __global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_reduce(const __grid_
     if (threadIdx.x == 0) e.work.bsum[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_top(const __grid_constant__ sphb_engine e, int nb)
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
+k_scan_top(const __grid_constant__ sphb_engine e, int nb, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     __shared__ int s_carry;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
@@ -291,8 +334,10 @@ __global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_top(const __grid_con
     if (threadIdx.x == 0) e.work.bsum[nb] = s_carry;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_apply(const __grid_constant__ sphb_engine e)
+__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
+k_scan_apply(const __grid_constant__ sphb_engine e, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const int T = e.work.meta[0];
     const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
     if (T == 0) {
@@ -323,8 +368,10 @@ __global__ void __launch_bounds__(SPHB_SCAN_THREADS) k_scan_apply(const __grid_c
 }
 
 // -------------------------------------------------------------- scatter --
-__global__ void __launch_bounds__(SPHB_ELEM_TILE) k_scatter(const __grid_constant__ sphb_engine e)
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_scatter(const __grid_constant__ sphb_engine e, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
@@ -346,8 +393,9 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE) k_scatter(const __grid_constan
 // not depend on the order the particles had before.
 template <int DIM, bool F32>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
+k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial, int gated)
 {
+    if (skip_rebin(e, gated)) return;
     const sphb_tile t = e.tiles[blockIdx.x];
     const int kk = t.begin + threadIdx.x;
     if (kk >= t.end) return;
@@ -414,21 +462,62 @@ k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial)
         local = 0;
     }
     e.f.cell[k] = local;
+    if (!F32 && !e.f.anchor) return;
+    const double cs = e.scene[s].cell_size;
+    int cx, cy, cz;
+    cell_coords(local, st.n, cx, cy, cz);
+    // position relative to the origin of the particle's own cell
+    const float xr = (float)(x - (double)(st.lo[0] + cx) * cs);
+    const float yr = (float)(y - (double)(st.lo[1] + cy) * cs);
+    const float zr = DIM == 3 ? (float)(z - (double)(st.lo[2] + cz) * cs) : 0.f;
     if (F32) {
-        const double cs = e.scene[s].cell_size;
-        int cx, cy, cz;
-        cell_coords(local, st.n, cx, cy, cz);
-        // position relative to the origin of the particle's own cell
-        const float xr = (float)(x - (double)(st.lo[0] + cx) * cs);
-        const float yr = (float)(y - (double)(st.lo[1] + cy) * cs);
         if (DIM == 2) {
             ((float4 *)e.f.geo)[k] = make_float4(xr, yr, (float)h, (float)m);
             ((float2 *)e.f.vel)[k] = make_float2((float)u, (float)v);
         } else {
-            const float zr = (float)(z - (double)(st.lo[2] + cz) * cs);
             ((float4 *)e.f.geo)[k] = make_float4(xr, yr, zr, (float)h);
             ((float *)e.f.mass)[k] = (float)m;
             ((float4 *)e.f.vel)[k] = make_float4((float)u, (float)v, (float)w, 0.f);
+        }
+    }
+    if (e.f.anchor) {
+        if (DIM == 2) ((float2 *)e.f.anchor)[k] = make_float2(xr, yr);
+        else ((float4 *)e.f.anchor)[k] = make_float4(xr, yr, zr, 0.f);
+    }
+}
+
+// After a rebin decided on the device: the gathered state back into
+// buf[cur], same order (the records, anchors and cells already follow it).
+template <int DIM>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_copy_back(const __grid_constant__ sphb_engine e, int cur, int move_initial, int gated)
+{
+    if (skip_rebin(e, gated)) return;
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int k = t.begin + threadIdx.x;
+    if (k >= t.end) return;
+    const sphb_buffers &S = e.buf[cur ^ 1];
+    const sphb_buffers &D = e.buf[cur];
+    D.x[k] = S.x[k];
+    D.y[k] = S.y[k];
+    D.u[k] = S.u[k];
+    D.v[k] = S.v[k];
+    D.m[k] = S.m[k];
+    D.h[k] = S.h[k];
+    D.idx[k] = S.idx[k];
+    D.tag[k] = S.tag[k];
+    if (DIM == 3) {
+        D.z[k] = S.z[k];
+        D.w[k] = S.w[k];
+    }
+    if (move_initial) {
+        D.x0[k] = S.x0[k];
+        D.y0[k] = S.y0[k];
+        D.u0[k] = S.u0[k];
+        D.v0[k] = S.v0[k];
+        if (DIM == 3) {
+            D.z0[k] = S.z0[k];
+            D.w0[k] = S.w0[k];
         }
     }
 }
@@ -465,9 +554,9 @@ extern "C" int sphb_box_init(const sphb_engine *e, int cur, void *stream)
     int rc = check_engine(e, cur);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    k_box_reset<<<(e->cfg.num_scenes + 127) / 128, 128, 0, st>>>(*e);
+    k_box_reset<<<(e->cfg.num_scenes + 127) / 128, 128, 0, st>>>(*e, 0);
     if (e->num_tiles > 0)
-        k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+        k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, 0);
     return launch_status("sphb_box_init");
 }
 
@@ -487,31 +576,41 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
 {
     int rc = check_engine(e, cur);
     if (rc) return rc;
+    if (flags & ~(SPHB_BIN_MOVE_INITIAL | SPHB_BIN_BOX | SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
     const sphb_config &c = e->cfg;
     cudaStream_t st = (cudaStream_t)stream;
+    const int gated = (flags & SPHB_BIN_IF_NEEDED) ? 1 : 0;
+    // the decision needs the displacements sphb_pc_stage measures from the
+    // anchors
+    if (gated && (!e->f.anchor || !e->f.cell)) return SPHB_ERR_ARG;
+    if (gated) k_bin_decide<<<1, 256, 0, st>>>(*e);
     if (flags & SPHB_BIN_BOX) {
-        k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e);
+        k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e, gated);
         if (e->num_tiles > 0)
-            k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+            k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
     }
-    k_grid_setup<<<1, 1024, 0, st>>>(*e);
+    k_grid_setup<<<1, 1024, 0, st>>>(*e, gated);
     const int nt = e->num_tiles;
-    if (nt > 0) k_hash<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    if (nt > 0) k_hash<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
     const int nb = bin_scan_blocks(c);
-    k_scan_reduce<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e);
-    k_scan_top<<<1, SPHB_SCAN_THREADS, 0, st>>>(*e, nb);
-    k_scan_apply<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e);
+    k_scan_reduce<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e, gated);
+    k_scan_top<<<1, SPHB_SCAN_THREADS, 0, st>>>(*e, nb, gated);
+    k_scan_apply<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e, gated);
     if (nt > 0) {
-        k_scatter<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e);
+        k_scatter<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, gated);
         const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
         if (c.dim == 2 && c.precision == SPHB_FP32C)
-            k_reorder<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+            k_reorder<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
         else if (c.dim == 2)
-            k_reorder<2, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+            k_reorder<2, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
         else if (c.precision == SPHB_FP32C)
-            k_reorder<3, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+            k_reorder<3, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
         else
-            k_reorder<3, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi);
+            k_reorder<3, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
+        if (gated) {
+            if (c.dim == 2) k_copy_back<2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
+            else k_copy_back<3><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
+        }
     }
     return launch_status("sphb_bin");
 }

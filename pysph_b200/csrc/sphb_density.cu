@@ -23,7 +23,11 @@ __global__ void __launch_bounds__(512)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
     const int with_eos = flags & SPHB_DENSITY_EOS;
-    const bool from_list = (flags & SPHB_DENSITY_USE_LIST) && e.f.list_cap > 0;
+    // list reuse: read the lists when the last rebin decision kept them
+    // (work.meta[2]); otherwise record them, with the skin
+    const bool reuse = (flags & SPHB_DENSITY_LIST_IF_VALID) && e.f.list_cap > 0;
+    const bool from_list = e.f.list_cap > 0 && ((flags & SPHB_DENSITY_USE_LIST) ||
+                                                (reuse && e.work.meta[2] == 1));
     const sphb_tile tl = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = tl.seg / A, a = tl.seg - s * A;
@@ -40,17 +44,18 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     unsigned long long np = 0;
     double rho = 0.0;
     // neighbour list of this lane: slots lane, lane + LANES, ... of k,
-    // recorded with the motion skin dt |v|max unless this pass reads them
+    // recorded (unless this pass reads them) with the skin when they are
+    // meant for reuse
     const int N = e.cfg.num_particles;
     uint32_t *__restrict__ nbr = (e.f.list_cap > 0 && !from_list) ? e.f.nbr : nullptr;
     const int cap_lane = e.f.list_cap / LANES;
-    double skin = 0.0;
-    if (nbr && sc.skin_max > 0.0) {
-        skin = st.dt * sqrt(__longlong_as_double((long long)st.max_v2));
-        if (skin > sc.skin_max) {
-            if (threadIdx.x == 0) flag(e, SPHB_ST_SKIN);
-            skin = sc.skin_max;
-        }
+    const double skin = (nbr && reuse) ? sc.skin_max : 0.0;
+    if (nbr && blockIdx.x == 0 && threadIdx.x == 0) {
+        // reusable only when recorded with the skin at the anchors (the
+        // positions of the last rebin, work.meta[3] == 2); no pass of this
+        // kernel reads meta[4], and a plain record also withdraws meta[2]
+        e.work.meta[4] = (reuse && e.work.meta[3] == 2) ? 1 : 0;
+        if (!reuse) e.work.meta[2] = 0;
     }
     int cnt = 0;
     auto record = [&](int j, int o, int dy, int dz) {

@@ -44,6 +44,12 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // the particles move: the lists are not known to be complete until
+        // the next rebin decision, and the positions leave the anchors
+        e.work.meta[2] = 0;
+        e.work.meta[3] = 0;
+    }
     if (stage == 0 && blockIdx.x == 0) {
         // the CFL rule reads the maxima of the corrector's force pass only
         // (dt_fac is reset per calc, S/sph/sph_calc.pyx:324): clear what the
@@ -51,7 +57,6 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         for (int q = threadIdx.x; q < e.cfg.num_scenes; q += blockDim.x) {
             e.sstate[q].max_dtfac = 0ull;
             e.sstate[q].max_acc2 = 0ull;
-            e.sstate[q].max_v2 = 0ull;   // the corrector stage records the next step's
         }
     }
     if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
@@ -60,7 +65,7 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const sphb_buffers &B = e.buf[cur];
     const double dt2 = e.sstate[s].dt / 2;
     double p[3] = {0.0, 0.0, 0.0};
-    double vsq = 0.0;   // |v|^2 after the corrector: the next step's skin
+    double vn[3] = {0.0, 0.0, 0.0};
     if (active) {
         const bool real = B.tag[k] == 0;
         double f[3] = {0.0, 0.0, 0.0};
@@ -88,7 +93,8 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
                 V0[d][k] = v;
                 const double xn = axpy_rn(x, fx, dt2);
                 X[d][k] = xn;
-                V[d][k] = axpy_rn(v, f[d], dt2);
+                vn[d] = axpy_rn(v, f[d], dt2);
+                V[d][k] = vn[d];
                 p[d] = xn;
             } else {
                 const double x0 = X0[d][k], v0 = V0[d][k];
@@ -96,10 +102,9 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
                 const double vh = axpy_rn(v0, f[d], dt2);
                 const double xn = __dadd_rn(2 * xh, -x0);
                 X[d][k] = xn;
-                const double vn = __dadd_rn(2 * vh, -v0);
-                V[d][k] = vn;
+                vn[d] = __dadd_rn(2 * vh, -v0);
+                V[d][k] = vn[d];
                 p[d] = xn;
-                vsq += vn * vn;
             }
         }
     }
@@ -112,9 +117,55 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         if (threadIdx.x == 0 && hi > -INFINITY)
             atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
     }
-    if (stage == 1) {
-        const double bv = block_reduce(isfinite(vsq) ? vsq : 0.0, OpMax(), 0.0);
-        if (threadIdx.x == 0) atomic_max_nonneg(&e.sstate[s].max_v2, bv);
+    // FP32 pair records of the new state, relative to the particle's cell of
+    // the last bin, and how far it has moved from where that bin put it
+    const bool rec = F32 && e.f.geo && e.f.vel;
+    const bool disp = e.f.anchor != nullptr;
+    if (!rec && !disp) return;  // block-uniform
+    float d2 = 0.f;
+    if (active) {
+        const sphb_scene_state &st = e.sstate[s];
+        const double cs = e.scene[s].cell_size;
+        int local = e.f.cell[k];
+        if (local < 0 || local >= st.ncells) {
+            flag(e, SPHB_ST_BAD_INDEX);
+            local = 0;
+        }
+        int c[3];
+        cell_coords(local, st.n, c[0], c[1], c[2]);
+        float xr[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xr[d] = (float)(p[d] - (double)(st.lo[d] + c[d]) * cs);
+        if (rec) {
+            if (DIM == 2) {
+                ((float2 *)e.f.geo)[2 * k] = make_float2(xr[0], xr[1]);
+                ((float2 *)e.f.vel)[k] = make_float2((float)vn[0], (float)vn[1]);
+            } else {
+                ((float4 *)e.f.geo)[k] = make_float4(xr[0], xr[1], xr[2], (float)B.h[k]);
+                ((float4 *)e.f.vel)[k] =
+                    make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
+            }
+        }
+        if (disp) {
+            float q[3] = {0.f, 0.f, 0.f};
+            if (DIM == 2) {
+                const float2 an = ((const float2 *)e.f.anchor)[k];
+                q[0] = xr[0] - an.x;
+                q[1] = xr[1] - an.y;
+            } else {
+                const float4 an = ((const float4 *)e.f.anchor)[k];
+                q[0] = xr[0] - an.x;
+                q[1] = xr[1] - an.y;
+                q[2] = xr[2] - an.z;
+            }
+            d2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            // a non-finite position can never be within the skin
+            if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
+        }
+    }
+    if (disp) {
+        const double bd = block_reduce((double)d2, OpMax(), 0.0);
+        if (threadIdx.x == 0 && bd > 0.0) atomic_max_nonneg(&e.sstate[s].max_disp2, bd);
     }
 }
 
@@ -189,6 +240,14 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
            int dir, double *user, const int *user_offset)
 {
+    // new positions, velocities, masses or smoothing lengths: the lists and
+    // the FP32 records must be rebuilt before they are reused
+    if (dir == 0 && (field <= 5 || field == 12 || field == 13) && blockIdx.x == 0 &&
+        threadIdx.x == 0) {
+        e.work.meta[2] = 0;
+        e.work.meta[3] = 0;
+        e.work.meta[4] = 0;
+    }
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;

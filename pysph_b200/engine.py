@@ -24,7 +24,7 @@ import torch
 from . import _native as nat
 
 ELEM_TILE = 256
-SKIN_MARGIN = 0.05
+SKIN_MARGIN = 0.15
 MASTER = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0", "w0",
           "m", "h")
 USER_PROPS = ("x", "y", "z", "u", "v", "w", "m", "h")
@@ -101,7 +101,7 @@ class Engine:
                  precision: str = "fp32c", stencil: int = 1, lanes: int = 1,
                  pair_block: int = 128, cell_capacity: int | None = None,
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
-                 step_lists: bool = True):
+                 step_lists: bool = True, skin_margin: float | None = None):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -139,11 +139,16 @@ class Engine:
         self.user_n = [int(sizes[:, a].sum()) for a in range(self.A)]
         self._stencil = stencil
         self.use_lists = use_lists
-        # one list per step (the mid-step stage refreshes records instead of
-        # rebinning): cells 5% larger than the support leave room for the
-        # motion skin; off, the cell size is exactly the reference's
+        # list reuse across stages and steps: cells larger than the support
+        # by skin_margin leave room for a skin, and the device rebins only
+        # once some particle has moved half the skin; off, every stage
+        # rebins and the cell size is exactly the reference's
         self.step_lists = bool(use_lists and step_lists)
-        self.skin_margin = SKIN_MARGIN if self.step_lists else 0.0
+        if skin_margin is None:
+            skin_margin = SKIN_MARGIN
+        if self.step_lists and not 0.0 < skin_margin <= 1.0:
+            raise ValueError("skin_margin must be in (0, 1]")
+        self.skin_margin = float(skin_margin) if self.step_lists else 0.0
         self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
@@ -258,11 +263,18 @@ class Engine:
         # per-stage neighbour lists (density pass writes, force pass reads)
         idx_bits = 26 if dim == 2 else 23
         self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
+        if self.step_lists and self.list_cap:
+            # capacity for the skin: entries grow as (1 + margin)^dim
+            grow = (1.0 + self.skin_margin) ** dim
+            self.list_cap = int(math.ceil(self.list_cap * grow / 8.0)) * 8
         if self.list_cap:
             f["nbr"] = torch.zeros(self.list_cap * N, **i32)
             f["nbr_cnt"] = torch.zeros(8 * N, **i32)
         else:
             f["nbr"] = f["nbr_cnt"] = None
+        # binned positions, for the rebin decision of the list reuse
+        f["anchor"] = (torch.zeros(N, 2 if dim == 2 else 4, dtype=torch.float32, device=dev)
+                       if self.step_lists else None)
         self.fields = f
         # scratch
         cfg = self._config(lanes, pair_block)
@@ -395,9 +407,15 @@ class Engine:
         nat.check(rc, name)
 
     def bin(self, flags: int = 0):
+        """Rebin into the other buffer; with BIN_IF_NEEDED the device decides
+        and the state stays in the current buffer either way."""
         if not self._box_valid:
             flags |= nat.BIN_BOX
         self.call("sphb_bin", self.cur, flags)
+        if flags & nat.BIN_IF_NEEDED:
+            # the box is rebuilt only by a rebin that happens; keep asking
+            # for it until a pc_stage has accumulated it again
+            return
         self.cur ^= 1
         self._box_valid = False   # until a pc_stage accumulates it again
 
@@ -458,9 +476,17 @@ class Engine:
         recomputes every scene box from all particles."""
         self._box_valid = False
 
+    def _sync_cells(self):
+        """With list reuse the cell tables are those of the last rebin; a
+        device decision first rebins if any particle has since moved half
+        the skin, so a cell search still finds every pair."""
+        if self.step_lists:
+            self.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
+
     def density(self, dest_mask=None, eos=True):
         if dest_mask is None:
             dest_mask = self.scheme.rho_dests
+        self._sync_cells()
         self.call("sphb_density", self.cur, dest_mask, 1 if eos else 0)
 
     def tait(self, dest_mask=None):
@@ -471,6 +497,8 @@ class Engine:
     def momentum(self, dest_mask=None, gravity=True, mode=0):
         if dest_mask is None:
             dest_mask = self.scheme.mom_dests
+        if not mode & nat.FORCE_USE_LIST:
+            self._sync_cells()
         self.call("sphb_momentum", self.cur, dest_mask, 1 if gravity else 0, mode)
 
     def pc_stage(self, stage: int):
@@ -480,13 +508,13 @@ class Engine:
     def step_begin(self):
         self.call("sphb_step_begin")
 
-    def eval_stage(self, from_list=False):
+    def eval_stage(self):
         """Integrator.eval of the pinned scheme at the current positions:
         SPHRho + Tait (fused), Tait on arrays without SPHRho, then
         MomentumEquation (or SPHPressureGradient) + GravityForce.  The
-        density pass records the neighbour lists the force pass reads, or
-        with from_list reads the lists of the step's first stage."""
-        flags = nat.DENSITY_EOS | (nat.DENSITY_USE_LIST if from_list else 0)
+        density pass records the neighbour lists the force pass reads; with
+        list reuse it reads the lists the last rebin decision kept."""
+        flags = nat.DENSITY_EOS | (nat.DENSITY_LIST_IF_VALID if self.step_lists else 0)
         self.call("sphb_density", self.cur, self.scheme.rho_dests, flags)
         if self.tait_only_mask:
             self.tait(self.tait_only_mask)
@@ -495,20 +523,25 @@ class Engine:
     def pc_step(self, on_half=None):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
         preceded by the Solver's per-step prologue (count, dt).  on_half,
-        when given, is called after the predictor stage."""
+        when given, is called after the predictor stage.  With list reuse
+        both stages rebin only when the device finds it necessary, and the
+        state never changes buffers, so one captured graph replays every
+        step."""
+        reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
         self.step_begin()
-        self.bin(0)
+        self.bin(reuse)
         self.eval_stage()
         self.pc_stage(0)
         if on_half is not None:
             on_half()
-        if self.step_lists:
-            self.call("sphb_refresh", self.cur)
-            self.eval_stage(from_list=True)
-        else:
-            self.bin(nat.BIN_MOVE_INITIAL)
-            self.eval_stage()
+        self.bin(nat.BIN_MOVE_INITIAL | reuse)
+        self.eval_stage()
         self.pc_stage(1)
+
+    def rebin_count(self) -> int:
+        """1 when the last device-decided rebin happened (host sync)."""
+        off = self.work_offsets[nat.WORK_NAMES.index("meta")]
+        return int(self.work_buf[off + 4:off + 8].view(torch.int32).item())
 
     # ---------------------------------------------------------- host sync
     def status(self) -> int:
@@ -554,8 +587,9 @@ class Engine:
         self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 0,
                   v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it
-        if name in ("x", "y", "z", "u", "v", "w"):
-            # the next bin recomputes the boxes and the step's motion skin
+        if name in ("x", "y", "z", "u", "v", "w", "m", "h"):
+            # the next bin recomputes the boxes; the kernel has withdrawn the
+            # lists, so the next device-decided rebin happens
             self._box_valid = False
 
     def exchange_out(self, array: int, name: str, out: torch.Tensor | None = None):
@@ -585,6 +619,7 @@ class Engine:
         FP64 reference predicate: numpy arrays (dest user index, source array,
         source user index), lexicographically sorted."""
         dev = self.device
+        self._sync_cells()
         counts = torch.zeros(self.N, dtype=torch.int32, device=dev)
         dm = 1 << dest_array
         self.call("sphb_neighbors", self.cur, dm, src_mask, counts.data_ptr(),
@@ -615,6 +650,9 @@ class Engine:
     def cell_coords(self, scene: int = 0, array: int = 0):
         """Global integer cell coordinates floor(x / cell_size) per user
         particle of (scene, array)."""
+        if self.step_lists:
+            # cells of the current positions, not of the last rebin
+            self.bin(nat.BIN_MOVE_INITIAL)
         out = torch.zeros(self.N * 3, dtype=torch.int32, device=self.device)
         self.call("sphb_cell_coords", self.cur, out.data_ptr())
         out = out.view(self.N, 3).cpu().numpy()

@@ -241,6 +241,120 @@ def test_nonfinite_position_reported_not_faulted():
     torch.cuda.synchronize()
 
 
+def _decisions(eng, steps):
+    """Run pc_steps; per step the device's rebin decisions (start, mid)."""
+    out = []
+    for _ in range(steps):
+        rec = {}
+        eng.pc_step(on_half=lambda: rec.__setitem__("start", eng.rebin_count()))
+        out.append((rec["start"], eng.rebin_count()))
+    return out
+
+
+def _assert_same_state(a, b, names=("x", "y", "u", "v", "rho"), tol=1e-10):
+    for n in names:
+        ga, gb = a.get(0, n).cpu().numpy(), b.get(0, n).cpu().numpy()
+        assert np.max(np.abs(ga - gb)) <= tol * max(1.0, np.max(np.abs(gb))), n
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("case,margin,steps", [("dam", None, 60), ("drop", 0.02, 20)])
+def test_list_reuse_matches_rebinning_pipeline(precision, case, margin, steps):
+    """Lists kept across stages and steps (the device rebins once a particle
+    has moved half the skin) evaluate the same pairs as rebinning every
+    stage: trajectories agree to round-off (FP64) or to the FP32C
+    trajectory bar, and both device decisions (keep, rebin) occur; the
+    drop with a thin skin rebins on displacement mid-run."""
+    arrays, params, scheme, dim = small_dam() if case == "dam" else drop(dx=0.1)
+    a = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=True,
+               skin_margin=margin)
+    b = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=False)
+    dec = _decisions(a, steps)
+    for _ in range(steps):
+        b.pc_step()
+    a.check_status()
+    b.check_status()
+    flat = [d for pair in dec for d in pair]
+    assert 0 in flat and 1 in flat, dec
+    if case == "drop":
+        assert 1 in flat[2:], dec   # a rebin after the first one
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    _assert_same_state(a, b, tol=tol)
+
+
+def test_fast_motion_rebins_every_stage():
+    """Particles that cross half the skin in one stage force a rebin at
+    every decision, and the result still matches the rebinning pipeline."""
+    arrays, params, scheme, dim = drop(dx=0.1)
+    arrays[0]["u"] = arrays[0]["u"] * 20.0
+    arrays[0]["v"] = arrays[0]["v"] * 20.0
+    p = dict(params, dt=1e-5)
+    a = Engine([(arrays, p)], scheme, dim=2, precision="fp64", step_lists=True,
+               skin_margin=0.02)
+    b = Engine([(arrays, p)], scheme, dim=2, precision="fp64", step_lists=False)
+    dec = _decisions(a, 5)
+    for _ in range(5):
+        b.pc_step()
+    a.check_status()
+    # the first step starts where the engine's initial bin put the particles
+    assert dec[0] == (0, 1) and all(d == (1, 1) for d in dec[1:]), dec
+    _assert_same_state(a, b)
+
+
+def test_state_written_from_host_forces_rebin():
+    """exchange_in of positions between steps withdraws the lists: the next
+    step rebins at its start, and the result matches the rebinning
+    pipeline given the same write."""
+    arrays, params, scheme, dim = small_dam()
+    a = Engine([(arrays, params)], scheme, dim=2, precision="fp64", step_lists=True)
+    b = Engine([(arrays, params)], scheme, dim=2, precision="fp64", step_lists=False)
+    for e in (a, b):
+        for _ in range(3):
+            e.pc_step()
+    x = a.get(0, "x").clone()
+    x[:50] += 0.3 * 0.02
+    for e in (a, b):
+        e.exchange_in(0, "x", x)
+    dec = _decisions(a, 2)
+    for _ in range(2):
+        b.pc_step()
+    assert dec[0][0] == 1, dec
+    _assert_same_state(a, b)
+
+
+def test_graph_replay_matches_eager_steps():
+    """One captured pc_step replayed N times equals N eager steps bit for
+    bit: with list reuse the state never changes buffers, whatever the
+    device decides."""
+    arrays, params, scheme, dim = small_dam()
+    a = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    b = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    for e in (a, b):
+        for _ in range(3):
+            e.pc_step()
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        a.pc_step()
+        b.pc_step()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        a.pc_step()
+    for _ in range(20):
+        g.replay()
+        b.pc_step()
+    torch.cuda.synchronize()
+    a.check_status()
+    b.check_status()
+    # the capture itself runs nothing: both did 4 + 20 steps
+    for n in ("x", "y", "u", "v", "rho", "p"):
+        assert torch.equal(a.get(0, n), b.get(0, n)), n
+    del g
+
+
 def test_grid_overflow_reported():
     arrays, params, scheme, dim = drop(dx=0.1)
     eng = Engine([(arrays, params)], scheme, dim=2, precision="fp64",
