@@ -320,11 +320,15 @@ def run_ours(args, rank, world, local):
     # ---- per-phase timing for the roofline
     kern = kernel_times(eng, flush, stream)
     byts = algorithmic_bytes(wl["dim"], eng.f32)
-    # a full rebin for "bin" (its per-stage average includes the kept lists)
-    per_launch = {"density": kern["density"], "force": kern["force"],
-                  "pc_stage": kern["pc_stage"], "bin": kern["rebin_ms"]}
-    dominant = max(per_launch, key=lambda k: per_launch[k] * (
-        kern["rebins_per_stage"] if k == "bin" else 1.0))
+    rate = kern["rebins_per_stage"]
+    dens = kern.get("density_list", kern["density_record"])
+    # share of a step: each phase's time times how often a stage runs it
+    per_stage = {"density": (1 - rate) * dens + rate * kern["density_record"],
+                 "force": kern["force"], "pc_stage": kern["pc_stage"],
+                 "bin": rate * kern["rebin"] + (1 - rate) * kern.get("bin_kept", 0.0)}
+    dominant = max(per_stage, key=lambda k: per_stage[k])
+    per_launch = {"density": dens, "force": kern["force"], "pc_stage": kern["pc_stage"],
+                  "bin": kern["rebin"]}
     hbm, which = peaks()
     ach = byts[dominant] * N / (per_launch[dominant] * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
@@ -496,60 +500,78 @@ def launches_per_step(eng):
     return 1 + 2 * rebin + 2 * 3 + (2 if eng.tait_only_mask else 0)
 
 
-def kernel_times(eng, flush, stream, reps=40):
-    """Milliseconds of each phase of real steps (eager launches, events
-    around each phase, L2 flushed before every step), averaged per stage,
-    with the device's rebin decisions counted: bin (decision + rebin when
-    taken), density (records the lists after a rebin, reads them
-    otherwise), force (from the lists), pc_stage."""
+def kernel_times(eng, flush, stream, reps=20):
+    """Device time of each phase of the step, each timed alone with CUDA
+    events around its own launches on the engine's stream and the L2
+    flushed (256 MiB write) before every launch: density reading the lists,
+    density searching cells and recording them (the stage after a rebin),
+    force from the lists, pc_stage, a full rebin, and a kept-lists rebin
+    decision (a captured graph of that bin call, whose kernels return at
+    once).  Then the device's rebin decisions over real steps give the rate
+    at which stages rebin."""
     import torch
     from pysph_b200 import _native as nat
-    phases = ["step_begin", "bin0", "density0", "force0", "pc0",
-              "bin1", "density1", "force1", "pc1"]
-    acc = {n: 0.0 for n in phases}
-    reuse = nat.BIN_IF_NEEDED if eng.step_lists else 0
-    moff = eng.work_offsets[nat.WORK_NAMES.index("meta")]
-    meta1 = eng.work_buf[moff + 4:moff + 8].view(torch.int32)
-    took = torch.zeros(reps, 2, dtype=torch.int32, device=eng.device)
-    rebin_ms = [0.0, 0.0]
-    for r in range(reps):
-        flush.zero_()
-        ev = {n: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for n in phases}
 
-        def run(n, fn):
-            ev[n][0].record(stream)
+    def timed(fn, n=reps):
+        tot = 0.0
+        for _ in range(n):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
             fn()
-            ev[n][1].record(stream)
-        run("step_begin", eng.step_begin)
-        for st in (0, 1):
-            flags = reuse | (nat.BIN_MOVE_INITIAL if st else 0)
-            run(f"bin{st}", lambda: eng.bin(flags))
-            took[r, st].copy_(meta1[0])
-            dflags = nat.DENSITY_EOS | (nat.DENSITY_LIST_IF_VALID if eng.step_lists else 0)
-            run(f"density{st}",
-                lambda: eng.call("sphb_density", eng.cur, eng.scheme.rho_dests, dflags))
-            run(f"force{st}", lambda: eng.momentum(
-                mode=eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0)))
-            run(f"pc{st}", lambda: eng.pc_stage(st))
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / n
+
+    mode_f = eng.force_mode | (nat.FORCE_USE_LIST if eng.list_cap else 0)
+    rho = eng.scheme.rho_dests
+    out = {}
+    eng.bin(nat.BIN_MOVE_INITIAL)
+    out["density_record"] = timed(lambda: eng.call("sphb_density", eng.cur, rho,
+                                                   nat.DENSITY_EOS))
+    if eng.list_cap:
+        out["density_list"] = timed(lambda: eng.call(
+            "sphb_density", eng.cur, rho, nat.DENSITY_EOS | nat.DENSITY_USE_LIST))
+    out["force"] = timed(lambda: eng.call("sphb_momentum", eng.cur, eng.scheme.mom_dests,
+                                          1, mode_f))
+    out["pc_stage"] = timed(lambda: eng.pc_stage(0))
+    out["rebin"] = timed(lambda: eng.bin(nat.BIN_MOVE_INITIAL))
+    if eng.step_lists:
+        # positions at the anchors: the decision keeps the lists every time
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(eng.device)
+        s.wait_stream(stream)
+        with torch.cuda.stream(s):
+            eng.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
+        stream.wait_stream(s)
         torch.cuda.synchronize()
-        tk = took[r].tolist()
-        for n in phases:
-            acc[n] += ev[n][0].elapsed_time(ev[n][1])
-        for st in (0, 1):
-            if tk[st] or not eng.step_lists:
-                rebin_ms[0] += ev[f"bin{st}"][0].elapsed_time(ev[f"bin{st}"][1])
-                rebin_ms[1] += 1
+        with torch.cuda.graph(g):
+            eng.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
+        torch.cuda.synchronize()
+        n = 50
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            g.replay()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out["bin_kept"] = a.elapsed_time(b) / n
+        assert eng.rebin_count() == 0
+        del g
+    out["step_begin"] = timed(eng.step_begin)
+    # rebin rate of real steps
+    rebins = 0
+    steps = 20
+    for _ in range(steps):
+        rec = {}
+        eng.pc_step(on_half=lambda: rec.__setitem__("s", eng.rebin_count()))
+        rebins += rec["s"] + eng.rebin_count()
     eng.check_status()
-    t = {n: v / reps for n, v in acc.items()}
-    rebins = int(took.sum().item()) if eng.step_lists else 2 * reps
-    return {"bin": 0.5 * (t["bin0"] + t["bin1"]),
-            "density": 0.5 * (t["density0"] + t["density1"]),
-            "force": 0.5 * (t["force0"] + t["force1"]),
-            "pc_stage": 0.5 * (t["pc0"] + t["pc1"]),
-            "step_begin": t["step_begin"],
-            "rebin_ms": rebin_ms[0] / max(rebin_ms[1], 1),
-            "rebins_per_stage": rebins / (2.0 * reps)}
+    out["rebins_per_stage"] = (rebins / (2.0 * steps)) if eng.step_lists else 1.0
+    return out
 
 
 def fp64_comparison(args, wl, eng32, flush, stream, dev):

@@ -95,7 +95,9 @@ typedef struct {
     double static_hi[3];    /*   moves (+inf / -inf when there are none) */
     int32_t use_cfl;        /* 0: dt kept as set; 1: viscous + force CFL rule;
                                2: viscous rule only (ViscousTimeStep) */
-    int32_t pad0;
+    int32_t uniform_h;      /* 1: every particle of the scene has the same h
+                               (the FP32 pair passes then take h_ab, 1/h_ab
+                               and the kernel normalisation from the dest) */
     double skin_max;        /* list skin: lists hold every pair within
                                (radius_scale h + skin_max)(1 + 1e-5) and
                                stay valid while no particle has moved

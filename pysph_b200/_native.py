@@ -63,7 +63,7 @@ class Scene(ctypes.Structure):
                 ("c0", f64), ("rho0", f64), ("gamma", f64), ("B", f64),
                 ("alpha", f64), ("beta", f64), ("eta", f64), ("g", f64 * 3),
                 ("cfl", f64), ("dt_initial", f64), ("static_lo", f64 * 3),
-                ("static_hi", f64 * 3), ("use_cfl", i32), ("pad0", i32),
+                ("static_hi", f64 * 3), ("use_cfl", i32), ("uniform_h", i32),
                 ("skin_max", f64)]
 
 

@@ -12,6 +12,8 @@
 // with Kahan compensation, the EOS in FP64.  FP64: the reference's
 // arithmetic, with its exact neighbour predicate.
 
+#include <type_traits>
+
 #include "sphb_pairs.cuh"
 
 namespace sphb {
@@ -79,29 +81,70 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const float rad2 = rad * rad;
             const float radl = (float)((hk * sc.radius_scale + skin) * (1.0 + 1e-5));
             const float radl2 = nbr ? radl * radl : rad2;
-            int cx, cy, cz;
-            cell_coords(e.f.cell[k], n, cx, cy, cz);
-            traverse<DIM, R, LANES>(
-                e, from_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
-                [&](int j, int o, int dy, int dz) {
-                    const float4 gj = __ldg(geo + j);
-                    const float dx = (xk - gj.x) - (float)o * csf;
-                    const float ddy = (yk - gj.y) - (float)dy * csf;
-                    float r2 = dx * dx + ddy * ddy;
-                    if (DIM == 3) {
-                        const float ddz = (zk - gj.z) - (float)dz * csf;
-                        r2 += ddz * ddz;
+            const float kf = (float)kfac_unit<DIM>();
+            const float ihk = __fdividef(1.0f, hk);
+            const float fack = DIM == 2 ? kf * ihk * ihk : kf * ihk * ihk * ihk;
+            struct Rec {
+                float4 g;
+                float m, o, dy, dz;
+                bool ok;
+            };
+            auto load = [&](const EntryF &en) {
+                Rec r;
+                r.ok = en.j < N;
+                const int j = r.ok ? en.j : k;
+                r.g = __ldg(geo + j);
+                r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
+                r.o = en.o;
+                r.dy = en.dy;
+                r.dz = en.dz;
+                return r;
+            };
+            auto dist2 = [&](const Rec &r) {
+                const float dx = (xk - r.g.x) - r.o * csf;
+                const float ddy = (yk - r.g.y) - r.dy * csf;
+                float r2 = dx * dx + ddy * ddy;
+                if (DIM == 3) {
+                    const float ddz = (zk - r.g.z) - r.dz * csf;
+                    r2 += ddz * ddz;
+                }
+                return r2;
+            };
+            // uniform h (every particle of the scene): h_ab = h_a, and the
+            // kernel's 1/h and normalisation are the dest's
+            auto pass = [&](auto uniform) {
+                constexpr bool UH = decltype(uniform)::value;
+                auto use = [&](const Rec &r, float r2) {
+                    if (!(r.ok && r2 < rad2)) return;
+                    float ih = ihk, fac = fack;
+                    if (!UH) {
+                        const float hj = DIM == 3 ? r.g.w : r.g.z;
+                        ih = __fdividef(1.0f, 0.5f * (hk + hj));
+                        fac = DIM == 2 ? kf * ih * ih : kf * ih * ih * ih;
                     }
-                    if (r2 < radl2) {
-                        record(j, o, dy, dz);
-                        if (r2 < rad2) {
-                            const float hj = DIM == 3 ? gj.w : gj.z;
-                            const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
-                            acc.add(mj * w_cubic_f<DIM>(r2, 0.5f * (hk + hj)));
-                            ++np;
-                        }
-                    }
-                });
+                    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                    acc.add(r.m * w_cubic_bf(r2 * ir * ih, fac));
+                    ++np;
+                };
+                const int lc = list_count<LANES>(e, from_list, k, lane);
+                if (lc >= 0) {
+                    list_loop<DIM, LANES, 8>(e, k, lane, lc, load,
+                                             [&](const Rec &r) { use(r, dist2(r)); });
+                    return;
+                }
+                int cx, cy, cz;
+                cell_coords(e.f.cell[k], n, cx, cy, cz);
+                for_each_candidate<DIM, R, LANES>(
+                    start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
+                    [&](int j, int o, int dy, int dz) {
+                        const Rec r = load(EntryF{j, (float)o, (float)dy, (float)dz});
+                        const float r2 = dist2(r);
+                        if (r2 < radl2) record(j, o, dy, dz);
+                        use(r, r2);
+                    });
+            };
+            if (sc.uniform_h) pass(std::true_type{});
+            else pass(std::false_type{});
         }
 #pragma unroll
         for (int o = LANES / 2; o > 0; o >>= 1) {

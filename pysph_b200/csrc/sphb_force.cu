@@ -12,6 +12,8 @@
 // GravityForce (S/sph/funcs/external_force.pyx:13-62) adds g afterwards.
 // Per scene the kernel also keeps max dt_fac and max |a|^2 for the CFL rule.
 
+#include <type_traits>
+
 #include "sphb_pairs.cuh"
 
 namespace sphb {
@@ -49,6 +51,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         Kahan ax, ay, az;
         float dtmax = 0.f;
         if (active) {
+            const int N = e.cfg.num_particles;
             const float4 *__restrict__ geo = (const float4 *)e.f.geo;
             const float *__restrict__ mass = (const float *)e.f.mass;
             const float4 *__restrict__ th = (const float4 *)e.f.thermo;
@@ -72,54 +75,98 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             const float rad2 = rad * rad;
             const float alpha = (float)sc.alpha, beta = (float)sc.beta;
             const float eta2 = (float)(sc.eta * sc.eta);
-            int cx, cy, cz;
-            cell_coords(e.f.cell[k], n, cx, cy, cz);
-            traverse<DIM, R, LANES>(
-                e, use_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
-                [&](int j, int o, int dy, int dz) {
-                    const float4 gj = __ldg(geo + j);
-                    const float rx = (xk - gj.x) - (float)o * csf;
-                    const float ry = (yk - gj.y) - (float)dy * csf;
+            const float kf = (float)kfac_unit<DIM>();
+            const float ihk = __fdividef(1.0f, hk);
+            // fac / h of the dest: 2D kf/h^3, 3D kf/h^4
+            const float fihk = DIM == 2 ? kf * ihk * ihk * ihk : kf * ihk * ihk * ihk * ihk;
+            const float eh2k = eta2 * hk * hk;
+            struct Rec {
+                float4 g, t;
+                float vx, vy, vz, m, o, dy, dz;
+                bool ok;
+            };
+            auto load = [&](const EntryF &en) {
+                Rec r;
+                r.ok = en.j < N;
+                const int j = r.ok ? en.j : k;
+                r.g = __ldg(geo + j);
+                r.t = __ldg(th + j);
+                r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
+                if (visc) {
+                    if (DIM == 2) {
+                        const float2 vv = __ldg((const float2 *)e.f.vel + j);
+                        r.vx = vv.x;
+                        r.vy = vv.y;
+                        r.vz = 0.f;
+                    } else {
+                        const float4 vv = __ldg((const float4 *)e.f.vel + j);
+                        r.vx = vv.x;
+                        r.vy = vv.y;
+                        r.vz = vv.z;
+                    }
+                } else {
+                    r.vx = r.vy = r.vz = 0.f;
+                }
+                r.o = en.o;
+                r.dy = en.dy;
+                r.dz = en.dz;
+                return r;
+            };
+            auto pass = [&](auto uniform) {
+                constexpr bool UH = decltype(uniform)::value;
+                auto use = [&](const Rec &r) {
+                    const float rx = (xk - r.g.x) - r.o * csf;
+                    const float ry = (yk - r.g.y) - r.dy * csf;
                     float rz = 0.f;
                     float r2 = rx * rx + ry * ry;
                     if (DIM == 3) {
-                        rz = (zk - gj.z) - (float)dz * csf;
+                        rz = (zk - r.g.z) - r.dz * csf;
                         r2 += rz * rz;
                     }
-                    if (!(r2 < rad2)) return;
+                    if (!(r.ok && r2 < rad2)) return;
                     ++np;
-                    const float hj = DIM == 3 ? gj.w : gj.z;
-                    const float mj = DIM == 3 ? __ldg(mass + j) : gj.w;
-                    const float hab = 0.5f * (hk + hj);
-                    const float4 tj = __ldg(th + j);
-                    float tmp = tk.w + tj.w;
+                    float hab = hk, ih = ihk, fih = fihk, eh2 = eh2k;
+                    if (!UH) {
+                        const float hj = DIM == 3 ? r.g.w : r.g.z;
+                        hab = 0.5f * (hk + hj);
+                        ih = __fdividef(1.0f, hab);
+                        fih = DIM == 2 ? kf * ih * ih * ih : kf * ih * ih * ih * ih;
+                        eh2 = eta2 * hab * hab;
+                    }
+                    float tmp = tk.w + r.t.w;   // P_a/rho_a^2 + P_b/rho_b^2
                     if (visc) {
-                        float vx, vy, vz = 0.f;
-                        if (DIM == 2) {
-                            const float2 vv = __ldg((const float2 *)e.f.vel + j);
-                            vx = uk - vv.x;
-                            vy = vk - vv.y;
-                        } else {
-                            const float4 vv = __ldg((const float4 *)e.f.vel + j);
-                            vx = uk - vv.x;
-                            vy = vk - vv.y;
-                            vz = wk - vv.z;
-                        }
+                        const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
                         float dot = vx * rx + vy * ry;
                         if (DIM == 3) dot += vz * rz;
-                        const float mu = __fdividef(hab * dot, r2 + eta2 * hab * hab);
+                        const float mu = __fdividef(hab * dot, r2 + eh2);
                         dtmax = fmaxf(dtmax, fabsf(mu));
-                        if (dot < 0.f) {
-                            const float cab = 0.5f * (tk.z + tj.z);
-                            const float rhoab = 0.5f * (tk.x + tj.x);
-                            tmp += __fdividef(-alpha * cab * mu + beta * mu * mu, rhoab);
-                        }
+                        // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
+                        const float cab = 0.5f * (tk.z + r.t.z);
+                        const float rhoab = 0.5f * (tk.x + r.t.x);
+                        const float pi = __fdividef(-alpha * cab * mu + beta * mu * mu, rhoab);
+                        tmp += dot < 0.f ? pi : 0.f;
                     }
-                    const float f = -mj * tmp * gw_cubic_f<DIM>(r2, hab);
+                    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                    const float f = -r.m * tmp * gw_cubic_bf(r2 * ir * ih, ir, ih, fih);
                     ax.add(f * rx);
                     ay.add(f * ry);
                     if (DIM == 3) az.add(f * rz);
-                });
+                };
+                const int lc = list_count<LANES>(e, use_list, k, lane);
+                if (lc >= 0) {
+                    list_loop<DIM, LANES, 4>(e, k, lane, lc, load, use);
+                    return;
+                }
+                int cx, cy, cz;
+                cell_coords(e.f.cell[k], n, cx, cy, cz);
+                for_each_candidate<DIM, R, LANES>(
+                    start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
+                    [&](int j, int o, int dy, int dz) {
+                        use(load(EntryF{j, (float)o, (float)dy, (float)dz}));
+                    });
+            };
+            if (sc.uniform_h) pass(std::true_type{});
+            else pass(std::false_type{});
         }
 #pragma unroll
         for (int o = LANES / 2; o > 0; o >>= 1) {

@@ -91,6 +91,71 @@ __device__ __forceinline__ void nbr_unpack(uint32_t v, int &j, int &o, int &dy, 
     dz = DIM == 3 ? (int)((v >> (B + 6)) & 7u) - 2 : 0;
 }
 
+// A list entry unpacked, with the cell offsets as floats.  The 3-bit fields
+// become floats through the exponent of 2^23 (exact, no conversion
+// instruction): float(0x4B000000 | b) = 2^23 + b.
+struct EntryF {
+    int j;
+    float o, dy, dz;
+};
+
+template <int DIM>
+__device__ __forceinline__ EntryF entry_unpack_f(uint32_t v)
+{
+    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
+    constexpr float BIAS = 8388608.0f + 2.0f;
+    EntryF r;
+    r.j = (int)(v & ((1u << B) - 1u));
+    r.o = __int_as_float(0x4B000000 | (int)((v >> B) & 7u)) - BIAS;
+    r.dy = __int_as_float(0x4B000000 | (int)((v >> (B + 3)) & 7u)) - BIAS;
+    r.dz = DIM == 3 ? __int_as_float(0x4B000000 | (int)((v >> (B + 6)) & 7u)) - BIAS : 0.f;
+    return r;
+}
+
+// Entries of dest k this lane owns (-1 when some lane's list overflowed),
+// or -1 when the lists are not to be used.
+template <int LANES>
+__device__ __forceinline__ int list_count(const sphb_engine &e, bool use_list, int k, int lane)
+{
+    if (!use_list) return -1;
+    const int N = e.cfg.num_particles;
+    int mine = 0;
+    bool ok = true;
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) {
+        const int c = __ldg(e.f.nbr_cnt + (size_t)l * N + k);
+        ok = ok && c >= 0;
+        if (l == lane) mine = c;
+    }
+    return ok ? mine : -1;
+}
+
+// use(load(entry)) over the cnt list entries of (k, lane).  U entries and
+// then their neighbour records are loaded before any is used, so each
+// thread keeps U gathers in flight instead of one dependent chain.
+template <int DIM, int LANES, int U, typename Load, typename Use>
+__device__ __forceinline__ void list_loop(const sphb_engine &e, int k, int lane, int cnt,
+                                          Load &&load, Use &&use)
+{
+    const int N = e.cfg.num_particles;
+    const uint32_t *__restrict__ p = e.f.nbr + (size_t)lane * N + k;
+    const size_t stride = (size_t)LANES * N;
+    int c = 0;
+#pragma unroll 1
+    for (; c + U <= cnt; c += U) {
+        uint32_t v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = __ldg(p + (size_t)(c + u) * stride);
+        decltype(load(EntryF{})) r[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) r[u] = load(entry_unpack_f<DIM>(v[u]));
+#pragma unroll
+        for (int u = 0; u < U; ++u) use(r[u]);
+    }
+#pragma unroll 1
+    for (; c < cnt; ++c) use(load(entry_unpack_f<DIM>(__ldg(p + (size_t)c * stride))));
+}
+
 // The pairs of dest k: its list from the last density pass when use_list
 // and every lane's list is complete, else the cell search.
 template <int DIM, int R, int LANES, typename F>
@@ -165,6 +230,27 @@ __device__ __forceinline__ float gw_cubic_f(float r2, float hab)
     float fac = (float)kfac_unit<DIM>() * ih * ih;
     if (DIM == 3) fac *= ih;
     return val * fac;
+}
+
+// Branch-free FP32 cubic spline for the list passes, with t1 = max(2 - q, 0)
+// and t2 = max(1 - q, 0):  W = fac/4 (t1^3 - 4 t2^3) (equal to
+// 1 - 1.5 q^2 (1 - q/2) for q < 1 and (2 - q)^3 / 4 for 1 <= q < 2, zero
+// beyond), and dW/dr / r = fac ih (q < 1 ? (2.25 q - 3) ih : -0.75 t1^2 / r)
+// (S/base/kernels.pyx:355-417).  ir = 1/r (0 for r = 0, where r_ab = 0
+// makes the gradient term vanish anyway).
+__device__ __forceinline__ float w_cubic_bf(float q, float fac)
+{
+    const float t1 = fmaxf(2.0f - q, 0.0f);
+    const float t2 = fmaxf(1.0f - q, 0.0f);
+    return 0.25f * fac * (t1 * t1 * t1 - 4.0f * (t2 * t2 * t2));
+}
+
+__device__ __forceinline__ float gw_cubic_bf(float q, float ir, float ih, float fac_ih)
+{
+    const float t1 = fmaxf(2.0f - q, 0.0f);
+    const float inner = (2.25f * q - 3.0f) * ih;
+    const float outer = -0.75f * t1 * t1 * ir;
+    return fac_ih * (q < 1.0f ? inner : outer);
 }
 
 // FP64 versions with the reference's operations.

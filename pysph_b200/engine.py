@@ -205,6 +205,10 @@ class Engine:
             t.cfl = p.cfl
             t.dt_initial = p.dt_initial
             t.use_cfl = (1 if p.cfl_force else 2) if p.cfl > 0 else 0
+            nonempty = [h for h in hs if len(h)]
+            t.uniform_h = int(bool(nonempty) and
+                              min(float(h.min()) for h in nonempty) ==
+                              max(float(h.max()) for h in nonempty))
         self._scene_host = sc
 
     def _estimate_capacity(self, growth: float) -> int:
@@ -326,6 +330,8 @@ class Engine:
         self.lanes, self.pair_block = lanes, pair_block
         self.pair_tiles = self._make_tiles(pair_block // lanes)
         self._build_desc()
+        # the lists are laid out per lane: record them again
+        self.invalidate_lists()
 
     def _build_desc(self):
         d = nat.EngineDesc()
@@ -362,7 +368,7 @@ class Engine:
             for name in USER_PROPS:
                 if self.dim == 2 and name in ("z", "w"):
                     continue
-                self.exchange_in(a, name, user[a][name])
+                self._exchange_in(a, name, user[a][name])
             self.exchange_tag(a, user[a]["tag"], 0)
         self.bin(0)
         for a in range(self.A):
@@ -470,6 +476,15 @@ class Engine:
         """dt of the next stages for every scene without the CFL rule, set by
         a kernel (no host round trip)."""
         nat.check(self.L.sphb_set_dt(self._pdesc, float(dt), self.stream), "sphb_set_dt")
+
+    def invalidate_lists(self):
+        """The neighbour lists may no longer match the state or the launch
+        shape: the next device rebin decision rebins and they are recorded
+        again (work.meta[2..4] cleared, in stream order)."""
+        if not hasattr(self, "work_buf"):
+            return
+        off = self.work_offsets[nat.WORK_NAMES.index("meta")]
+        self.work_buf[off + 8:off + 20].zero_()
 
     def invalidate_box(self):
         """Positions were changed outside the integrator: the next bin
@@ -581,6 +596,14 @@ class Engine:
     # --------------------------------------------------------- exchange
     def exchange_in(self, array: int, name: str, values: torch.Tensor):
         """User-order FP64 values (scenes concatenated) -> engine."""
+        self._exchange_in(array, name, values)
+        if name == "h" and any(t.uniform_h for t in self._scene_host):
+            # smoothing lengths may now differ within a scene
+            for t in self._scene_host:
+                t.uniform_h = 0
+            self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
+
+    def _exchange_in(self, array: int, name: str, values: torch.Tensor):
         v = values.to(device=self.device, dtype=torch.float64).contiguous()
         if v.numel() != self.user_n[array]:
             raise ValueError("size mismatch")

@@ -143,9 +143,15 @@ def config4_gradient(precision):
 
 def test_adjoint_central_fd_full_rollout():
     """FD in FP64 on 16 random unit directions (seed 0) of the initial
-    velocities.  eps = 1e-5 (velocity units): small enough that few pairs
-    cross the artificial-viscosity switch v.r = 0 (a kink of the loss)
-    between the two evaluations, large against FP64 round-off of the loss."""
+    velocities, eps = 1e-4 (velocity units, |v| ~ 100).  Bars: median over
+    the directions of |FD - adjoint| / |FD| <= 1e-4, and every direction's
+    |FD - adjoint| <= 1e-5 |grad|.  The second form is the meaningful one
+    per direction: a random direction in 100k dimensions sees ~|grad| / 300
+    of the gradient, some far less, and there the FD's own noise (round-off
+    amplified over 200 stiff steps, pairs crossing the artificial-viscosity
+    switch v.r = 0 between the two evaluations) dominates |FD - adjoint| /
+    |FD|.  Measured on B200: median 8e-5, max 5e-7 |grad|; eps from 1e-3
+    to 1e-5 gives the same floor, 1e-6 and below is round-off bound."""
     g, v0, xt, arrays, params, n = config4_gradient("fp64")
     dev = v0.device
     fd = Rollout(arrays, params, fluid_scheme(1), 2, CONFIG4["dt"], CONFIG4["steps"],
@@ -156,16 +162,20 @@ def test_adjoint_central_fd_full_rollout():
         return float(((xf - xt) ** 2).sum() / n)
 
     rng = np.random.default_rng(0)
-    eps = 1e-5
-    errs = []
+    eps = 1e-4
+    gnorm = float(torch.linalg.norm(g))
+    errs, errs_g = [], []
     for _ in range(16):
         d = torch.tensor(rng.standard_normal((2, n)), dtype=torch.float64, device=dev)
         d /= torch.linalg.norm(d)
         fdv = (L(v0 + eps * d) - L(v0 - eps * d)) / (2 * eps)
         adv = float((g * d).sum())
         errs.append(abs(fdv - adv) / max(abs(fdv), 1e-30))
+        errs_g.append(abs(fdv - adv) / gnorm)
     print("FD relative errors:", errs)
-    assert np.median(errs) <= 1e-4 and np.max(errs) <= 1e-3, errs
+    print("FD errors / |grad|:", errs_g)
+    assert np.median(errs) <= 1e-4, errs
+    assert np.max(errs_g) <= 1e-5, errs_g
 
 
 def test_adjoint_fp32c_forward_gradient():

@@ -266,6 +266,8 @@ def test_list_reuse_matches_rebinning_pipeline(precision, case, margin, steps):
     trajectory bar, and both device decisions (keep, rebin) occur; the
     drop with a thin skin rebins on displacement mid-run."""
     arrays, params, scheme, dim = small_dam() if case == "dam" else drop(dx=0.1)
+    if case == "drop":
+        params = dict(params, dt=1e-5)   # c0 dt / h = 0.11
     a = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=True,
                skin_margin=margin)
     b = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=False)
@@ -278,7 +280,9 @@ def test_list_reuse_matches_rebinning_pipeline(precision, case, margin, steps):
     assert 0 in flat and 1 in flat, dec
     if case == "drop":
         assert 1 in flat[2:], dec   # a rebin after the first one
-    tol = 1e-10 if precision == "fp64" else 2e-6
+    # FP32C: the two pipelines sum in different orders, and the FP32 round-off
+    # they differ by grows over the run; 1e-5 of the largest magnitude
+    tol = 1e-10 if precision == "fp64" else 1e-5
     _assert_same_state(a, b, tol=tol)
 
 
