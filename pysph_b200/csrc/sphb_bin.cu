@@ -18,6 +18,8 @@
 // bounded by the grid, so a counting sort replaces the radix sort and the
 // state itself is permuted so every later kernel reads it coalesced.
 
+#include <mutex>
+
 #include "sphb_common.cuh"
 
 namespace sphb {
@@ -34,7 +36,8 @@ __device__ __forceinline__ bool skip_rebin(const sphb_engine &e, int gated)
 // with the skin at those positions (work.meta[4]) and no particle of any
 // scene has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding
 // of the displacement) from its anchor.  max_disp2 restarts either way.
-__global__ void k_bin_decide(const __grid_constant__ sphb_engine e)
+__global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
+                             cudaGraphConditionalHandle cond, int set_cond)
 {
     __shared__ int s_far;
     if (threadIdx.x == 0) s_far = 0;
@@ -53,6 +56,8 @@ __global__ void k_bin_decide(const __grid_constant__ sphb_engine e)
         const bool keep = at_anchor || (lists && !s_far);
         e.work.meta[1] = keep ? 0 : 1;
         e.work.meta[2] = (keep && lists) ? 1 : 0;
+        // inside a captured graph: run the rebin's conditional body or not
+        if (set_cond) cudaGraphSetConditional(cond, keep ? 0u : 1u);
     }
 }
 
@@ -572,18 +577,10 @@ extern "C" int sphb_refresh(const sphb_engine *e, int cur, void *stream)
     return launch_status("sphb_refresh");
 }
 
-extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
+// The kernels of one rebin, gated on work.meta[1] when gated.
+static void launch_rebin(const sphb_engine *e, int cur, int flags, int gated, cudaStream_t st)
 {
-    int rc = check_engine(e, cur);
-    if (rc) return rc;
-    if (flags & ~(SPHB_BIN_MOVE_INITIAL | SPHB_BIN_BOX | SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
     const sphb_config &c = e->cfg;
-    cudaStream_t st = (cudaStream_t)stream;
-    const int gated = (flags & SPHB_BIN_IF_NEEDED) ? 1 : 0;
-    // the decision needs the displacements sphb_pc_stage measures from the
-    // anchors
-    if (gated && (!e->f.anchor || !e->f.cell)) return SPHB_ERR_ARG;
-    if (gated) k_bin_decide<<<1, 256, 0, st>>>(*e);
     if (flags & SPHB_BIN_BOX) {
         k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e, gated);
         if (e->num_tiles > 0)
@@ -612,5 +609,106 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
             else k_copy_back<3><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
         }
     }
+}
+
+// A stream of the library's own per device, to capture the body of the
+// conditional rebin node into (cudaStreamBeginCaptureToGraph needs a stream
+// that is not capturing already); one capture at a time.
+static std::mutex g_body_mu;
+static cudaStream_t g_body_stream[128];
+
+static int body_stream(cudaStream_t *out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return SPHB_ERR_CUDA;
+    if (!g_body_stream[dev] &&
+        cudaStreamCreateWithFlags(&g_body_stream[dev], cudaStreamNonBlocking) != cudaSuccess)
+        return SPHB_ERR_CUDA;
+    *out = g_body_stream[dev];
+    return SPHB_OK;
+}
+
+static int cuda_fail(const char *what, cudaError_t err)
+{
+    record_cuda_error(what, err);
+    return SPHB_ERR_CUDA;
+}
+
+// Captured form of a device-decided rebin: the decision kernel sets a graph
+// conditional handle, and the rebin kernels form the body of an IF node, so
+// a replay that keeps the lists launches none of them.
+static int bin_conditional(const sphb_engine *e, int cur, int flags, cudaStream_t st,
+                           cudaGraph_t graph)
+{
+    cudaError_t err;
+    cudaGraphConditionalHandle cond;
+    if ((err = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault)))
+        return cuda_fail("sphb_bin: conditional handle", err);
+    k_bin_decide<<<1, 256, 0, st>>>(*e, cond, 1);
+    if ((err = cudaGetLastError())) return cuda_fail("sphb_bin: decision", err);
+    cudaStreamCaptureStatus cs;
+    unsigned long long id;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if ((err = cudaStreamGetCaptureInfo(st, &cs, &id, &graph, &deps, &ndeps)))
+        return cuda_fail("sphb_bin: capture info", err);
+    // (the union inside has no default constructor: zeroed storage)
+    alignas(cudaGraphNodeParams) unsigned char pbuf[sizeof(cudaGraphNodeParams)];
+    memset(pbuf, 0, sizeof(pbuf));
+    cudaGraphNodeParams &p = *reinterpret_cast<cudaGraphNodeParams *>(pbuf);
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = cond;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((err = cudaGraphAddNode(&node, graph, deps, ndeps, &p)))
+        return cuda_fail("sphb_bin: conditional node", err);
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    {
+        std::lock_guard<std::mutex> lock(g_body_mu);
+        cudaStream_t bs;
+        if (body_stream(&bs)) return cuda_fail("sphb_bin: body stream", cudaGetLastError());
+        if ((err = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeRelaxed)))
+            return cuda_fail("sphb_bin: body capture", err);
+        launch_rebin(e, cur, flags, 1, bs);
+        const cudaError_t lerr = cudaGetLastError();
+        cudaGraph_t done;
+        err = cudaStreamEndCapture(bs, &done);
+        if (lerr) return cuda_fail("sphb_bin: body launch", lerr);
+        if (err) return cuda_fail("sphb_bin: body capture end", err);
+    }
+    if ((err = cudaStreamUpdateCaptureDependencies(st, &node, 1,
+                                                   cudaStreamSetCaptureDependencies)))
+        return cuda_fail("sphb_bin: capture dependencies", err);
+    return SPHB_OK;
+}
+
+extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
+{
+    int rc = check_engine(e, cur);
+    if (rc) return rc;
+    if (flags & ~(SPHB_BIN_MOVE_INITIAL | SPHB_BIN_BOX | SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int gated = (flags & SPHB_BIN_IF_NEEDED) ? 1 : 0;
+    if (!gated) {
+        launch_rebin(e, cur, flags, 0, st);
+        return launch_status("sphb_bin");
+    }
+    // the decision needs the displacements sphb_pc_stage measures from the
+    // anchors
+    if (!e->f.anchor || !e->f.cell) return SPHB_ERR_ARG;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(st, &cs);
+    if (err) return cuda_fail("sphb_bin: capture status", err);
+    if (cs == cudaStreamCaptureStatusActive) {
+        cudaGraph_t graph;
+        unsigned long long id;
+        if ((err = cudaStreamGetCaptureInfo(st, &cs, &id, &graph, nullptr, nullptr)))
+            return cuda_fail("sphb_bin: capture info", err);
+        return bin_conditional(e, cur, flags, st, graph);
+    }
+    k_bin_decide<<<1, 256, 0, st>>>(*e, cudaGraphConditionalHandle(), 0);
+    launch_rebin(e, cur, flags, 1, st);
     return launch_status("sphb_bin");
 }

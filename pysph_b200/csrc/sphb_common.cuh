@@ -18,6 +18,8 @@ namespace sphb {
 
 // Records the failure of the last launch for sphb_last_cuda_error.
 int launch_status(const char *what);
+// Records err for sphb_last_cuda_error.
+void record_cuda_error(const char *what, cudaError_t err);
 
 __device__ __forceinline__ void flag(const sphb_engine &e, unsigned bits)
 {

@@ -21,6 +21,11 @@ int check_engine_public(const sphb_engine *e, int cur);
 
 static thread_local char g_last_error[256] = "";
 
+void record_cuda_error(const char *what, cudaError_t err)
+{
+    snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(err));
+}
+
 int launch_status(const char *what)
 {
     cudaError_t err = cudaGetLastError();

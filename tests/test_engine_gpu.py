@@ -326,13 +326,22 @@ def test_state_written_from_host_forces_rebin():
     _assert_same_state(a, b)
 
 
-def test_graph_replay_matches_eager_steps():
+@pytest.mark.parametrize("case", ["dam", "drop"])
+def test_graph_replay_matches_eager_steps(case):
     """One captured pc_step replayed N times equals N eager steps bit for
-    bit: with list reuse the state never changes buffers, whatever the
-    device decides."""
-    arrays, params, scheme, dim = small_dam()
-    a = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
-    b = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    bit: with list reuse the state never changes buffers, and inside the
+    graph the rebin is a conditional node the device's decision opens or
+    skips (the drop with a thin skin rebins every few stages, the dam keeps
+    its lists)."""
+    if case == "dam":
+        arrays, params, scheme, dim = small_dam()
+        kw = {}
+    else:
+        arrays, params, scheme, dim = drop(dx=0.1)
+        params = dict(params, dt=1e-5)
+        kw = dict(skin_margin=0.02)
+    a = Engine([(arrays, params)], scheme, dim=2, precision="fp32c", **kw)
+    b = Engine([(arrays, params)], scheme, dim=2, precision="fp32c", **kw)
     for e in (a, b):
         for _ in range(3):
             e.pc_step()
@@ -347,12 +356,16 @@ def test_graph_replay_matches_eager_steps():
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g):
         a.pc_step()
+    rebins = 0
     for _ in range(20):
         g.replay()
         b.pc_step()
+        rebins += b.rebin_count()
     torch.cuda.synchronize()
     a.check_status()
     b.check_status()
+    if case == "drop":
+        assert rebins > 0   # the replays took the rebin branch too
     # the capture itself runs nothing: both did 4 + 20 steps
     for n in ("x", "y", "u", "v", "rho", "p"):
         assert torch.equal(a.get(0, n), b.get(0, n)), n
