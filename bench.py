@@ -199,6 +199,13 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 
 # bytes per particle each kernel must move at least once (FP32C, 2D),
 # counted from the fields it reads and writes at their stored widths
+# DRAM bytes (read + write) per launch from `ncu --set full` on the dam
+# break, FP32C, lanes 1, 256-thread blocks (profiles/k_*_dam_break_fp32c.md)
+NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 47.735e6,
+               ("dam_break", "fp32c", "density"): 41.096e6,
+               ("dam_break", "fp32c", "pc_stage"): 17.976e6}
+
+
 def algorithmic_bytes(dim, f32):
     """Bytes per particle each phase must move once, at the stored widths
     (neighbour re-reads and the neighbour lists, which are scratch, are not
@@ -331,9 +338,14 @@ def run_ours(args, rank, world, local):
                   "bin": kern["rebin"]}
     hbm, which = peaks()
     ach = byts[dominant] * N / (per_launch[dominant] * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC.get((args.workload, args.precision, dominant))
     roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
             "peak": hbm, "peak_kind": which, "unit": "GB/s",
-            "frac": round(ach / hbm, 4), "traffic": None,
+            "frac": round(ach / hbm, 4), "traffic": traffic,
+            "traffic_note": ("dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu "
+                             "capture of this workload and launch shape; includes the "
+                             "neighbour lists, which the algorithmic bytes exclude as "
+                             "scratch") if traffic else None,
             "per_kernel_ms": {k: round(v, 5) for k, v in kern.items()},
             "bytes_per_particle": byts}
 

@@ -92,10 +92,10 @@ k_box_accum(const __grid_constant__ sphb_engine e, int cur, int gated)
     for (int d = 0; d < dim; ++d) {
         double lo = block_reduce(ok ? p[d] : INFINITY, OpMin(), (double)INFINITY);
         if (threadIdx.x == 0 && lo < INFINITY)
-            atomicMin(&e.sstate[s].box[d], enc_double(lo));
+            atomic_min_enc(&e.sstate[s].box[d], enc_double(lo));
         double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
         if (threadIdx.x == 0 && hi > -INFINITY)
-            atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
+            atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi));
     }
 }
 

@@ -52,12 +52,28 @@ __host__ __device__ __forceinline__ double dec_double(unsigned long long e)
 #endif
 }
 
-// Non-negative doubles order like their bit patterns.
+// Non-negative doubles order like their bit patterns.  Every block of a
+// kernel updates the same few maxima, so the atomic is issued only when the
+// value can still raise the stored one (a stale read costs one extra atomic,
+// never a wrong result).
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr,
                                                   double v)
 {
     if (!(v >= 0.0)) return;
-    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    if (b > *(volatile unsigned long long *)addr) atomicMax(addr, b);
+}
+
+// atomicMin / atomicMax on order-encoded doubles, skipped when they cannot
+// change the stored value.
+__device__ __forceinline__ void atomic_min_enc(unsigned long long *addr, unsigned long long v)
+{
+    if (v < *(volatile unsigned long long *)addr) atomicMin(addr, v);
+}
+
+__device__ __forceinline__ void atomic_max_enc(unsigned long long *addr, unsigned long long v)
+{
+    if (v > *(volatile unsigned long long *)addr) atomicMax(addr, v);
 }
 
 // Local cell index -> (cx, cy, cz) within the scene grid.
@@ -118,6 +134,19 @@ struct OpAddU64 {
         return a + b;
     }
 };
+
+// Adds every thread's v into *addr with one global atomic per block.  All
+// threads of the block must call it.
+__device__ __forceinline__ void block_add_u64(unsigned long long *addr, unsigned long long v)
+{
+    __shared__ unsigned long long s_acc;
+    if (threadIdx.x == 0) s_acc = 0ull;
+    __syncthreads();
+    v = warp_reduce(v, OpAddU64());
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_acc, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_acc) atomicAdd(addr, s_acc);
+}
 
 // Kahan-compensated FP32 accumulator: the running value is sum - c.
 struct Kahan {

@@ -218,9 +218,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             if (!isfinite(rho) || !isfinite(p)) flag(e, SPHB_ST_NONFINITE_RHO);
         }
     }
-    // warp-level, so warps that finish early leave without a block barrier
-    const unsigned long long tot = warp_reduce(np, OpAddU64());
-    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&e.work.pairs[0], tot);
+    block_add_u64(&e.work.pairs[0], np);
 }
 
 // Tait alone (rho given).

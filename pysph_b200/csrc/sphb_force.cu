@@ -272,16 +272,15 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         }
         if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
     }
-    // warp-level, so warps that finish early leave without a block barrier
-    const double bdt = warp_reduce(dtf_out, OpMax());
-    const double ba2 = warp_reduce(isfinite(a2) ? a2 : 0.0, OpMax());
-    const unsigned long long tot = warp_reduce(np, OpAddU64());
-    if ((threadIdx.x & 31) == 0) {
+    // one atomic per block and quantity (a block never spans two scenes)
+    const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
+    const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
+    if (threadIdx.x == 0) {
         sphb_scene_state &sw = e.sstate[s];
         atomic_max_nonneg(&sw.max_dtfac, bdt);
         atomic_max_nonneg(&sw.max_acc2, ba2);
-        if (tot) atomicAdd(&e.work.pairs[1], tot);
     }
+    block_add_u64(&e.work.pairs[1], np);
 }
 
 template <int DIM, bool F32>

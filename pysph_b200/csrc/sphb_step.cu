@@ -117,10 +117,10 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     for (int d = 0; d < DIM; ++d) {
         const double lo = block_reduce(ok ? p[d] : INFINITY, OpMin(), (double)INFINITY);
         if (threadIdx.x == 0 && lo < INFINITY)
-            atomicMin(&e.sstate[s].box[d], enc_double(lo));
+            atomic_min_enc(&e.sstate[s].box[d], enc_double(lo));
         const double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
         if (threadIdx.x == 0 && hi > -INFINITY)
-            atomicMax(&e.sstate[s].box[3 + d], enc_double(hi));
+            atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi));
     }
     // FP32 pair records of the new state, relative to the particle's cell of
     // the last bin, and how far it has moved from where that bin put it
