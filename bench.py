@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--pair-block", type=int, default=0)
     ap.add_argument("--stencil", type=int, default=0,
                     help="fix the cell size (support / R); default: autotuned")
+    ap.add_argument("--list-batch", type=int, default=0,
+                    help="list entries the force pass loads ahead (2 or 4); default: autotuned")
     return ap.parse_args()
 
 
@@ -243,17 +245,19 @@ def run_ours(args, rank, world, local):
     dev = torch.device("cuda", local)
     wl = workload(args.workload)
     tune = None
-    if args.lanes or args.pair_block or args.stencil:
+    if args.lanes or args.pair_block or args.stencil or args.list_batch:
         lanes = args.lanes or (4 if wl["dim"] == 3 else 1)
         pb = args.pair_block or 128
         stencil = args.stencil or 1
+        lb = args.list_batch or 4
     else:
         from pysph_b200.autotune import autotune
         tune = autotune(wl["scenes"], wl["scheme"], wl["dim"], args.precision, device=dev)
         lanes, pb, stencil = tune["lanes"], tune["pair_block"], tune["stencil"]
+        lb = tune.get("list_batch", 4)
     args.stencil = stencil
     eng = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=args.precision,
-                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev)
+                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev, list_batch=lb)
     N = eng.N
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -358,11 +362,13 @@ def run_ours(args, rank, world, local):
            "config": {"workload": args.workload, "description": wl["desc"],
                       "particles": N, "precision": args.precision,
                       "stencil": args.stencil, "lanes": lanes, "pair_block": pb,
+                      "list_batch": lb,
                       "cuda_graph": graph is not None,
                       "l2": "flushed (256 MiB write) between timed steps",
                       "parallelism": f"replicas x{world}"},
            "steps_per_s": steps_per_s,
-           "autotune": ({"chosen": {k: tune[k] for k in ("stencil", "lanes", "pair_block")},
+           "autotune": ({"chosen": {k: tune.get(k) for k in ("stencil", "lanes", "pair_block",
+                                                              "list_batch")},
                          "table": tune["table"]} if tune else None),
            "pairs_per_step": pairs / args.steps,
            "gpu_launches": launches_per_step(eng) * args.steps,

@@ -69,10 +69,11 @@ typedef struct {
     int32_t num_arrays;     /* A, arrays per scene, 1..SPHB_MAX_ARRAYS */
     int32_t stencil;        /* R: cell size = support / R; 1 or 2 */
     int32_t lanes;          /* lanes per dest particle in pair kernels: 1,2,4,8 */
-    int32_t pair_block;     /* threads per block of the pair kernels */
+    int32_t pair_block;     /* threads per block of the pair kernels, 32..256 */
     int32_t num_particles;  /* total over all segments */
     int32_t cell_capacity;  /* cell table capacity (all scenes, all arrays) */
-    int32_t pad0;
+    int32_t list_batch;     /* list entries the FP32C force pass loads ahead
+                               per thread: 2 or 4 (0: 4) */
     /* the scheme, per array index (identical for every scene):
      * SPHRho sources, MomentumEquation sources (bitmasks over arrays),
      * TaitEquation dests and integrated arrays (bitmasks) */
@@ -92,7 +93,8 @@ typedef struct {
     double g[3];                 /* GravityForce */
     double cfl, dt_initial;      /* ViscousAndForceBasedTimeStep */
     double static_lo[3];    /* bounds of the particles the integrator never */
-    double static_hi[3];    /*   moves (+inf / -inf when there are none) */
+    double static_hi[3];    /*   moves (+inf / -inf when there are none);
+                               informative, every rebin measures all */
     int32_t use_cfl;        /* 0: dt kept as set; 1: viscous + force CFL rule;
                                2: viscous rule only (ViscousTimeStep) */
     int32_t uniform_h;      /* 1: every particle of the scene has the same h
@@ -111,7 +113,8 @@ typedef struct {
     int32_t n[3];           /* grid dimensions (n[2] == 1 in 2D) */
     int32_t cell_base;      /* first cell key of the scene */
     int32_t ncells;         /* cells per array of this scene */
-    unsigned long long box[6];  /* order-encoded min xyz, max xyz (next bin) */
+    unsigned long long box[6];  /* order-encoded min xyz, max xyz of the
+                                   particles at the last rebin */
     double dt;              /* time step used by the next integrator stage */
     double t;               /* simulated time */
     long long count;        /* completed steps */
@@ -237,10 +240,9 @@ SPHB_API int sphb_box_init(const sphb_engine *e, int cur, void *stream);
  * CellManager.update/_rebin_particles (S/base/cell.pyx:943-986, :1179-1300),
  * RadixSortManager._cl_update (S/base/domain_manager.py:901-972) and the
  * `bin` / `compute_cell_counts` kernels (S/base/radix_sort.cl:31-108).
- * flags: SPHB_BIN_MOVE_INITIAL carries x0..w0 too; SPHB_BIN_BOX first
- * recomputes every scene box from all particles (needed whenever no
- * sphb_pc_stage accumulated it since the last bin).  The grid setup resets
- * each scene's box to its static bounds. */
+ * Every rebin first measures each scene's box from all its particles.
+ * flags: SPHB_BIN_MOVE_INITIAL carries x0..w0 too; SPHB_BIN_BOX is accepted
+ * and has no further effect. */
 #define SPHB_BIN_MOVE_INITIAL 1
 #define SPHB_BIN_BOX 2
 /* SPHB_BIN_IF_NEEDED (needs f.anchor): the device decides whether to
@@ -323,9 +325,9 @@ SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
  * stage 0 = predict (save X0, X = X0 + dt/2 F), stage 1 = correct and
  * final (X = 2 (X0 + dt/2 F) - X0).  Stage 0 also clears the per-scene
  * dt_fac / |a| maxima, so sphb_step_begin sees the corrector's pass only.
- * Accumulates the scene boxes for the next sphb_bin, refreshes the FP32
- * pair records of the moved particles and, with f.anchor, accumulates
- * max_disp2 (cleared by the next SPHB_BIN_IF_NEEDED decision).  PositionStepping
+ * Refreshes the FP32 pair records of the moved particles and, with
+ * f.anchor, accumulates max_disp2 (cleared by the next SPHB_BIN_IF_NEEDED
+ * decision).  PositionStepping
  * (S/sph/funcs/position_funcs.pyx:10-56) supplies F_x = u.
  * PredictorCorrectorIntegrator.integrate (S/solver/integrator.py:646-683),
  * step (:340-367), final_step (:632-644); integrator.cl step_array /

@@ -53,7 +53,7 @@ class Config(ctypes.Structure):
     _fields_ = [("dim", i32), ("precision", i32), ("num_scenes", i32),
                 ("num_arrays", i32), ("stencil", i32), ("lanes", i32),
                 ("pair_block", i32), ("num_particles", i32),
-                ("cell_capacity", i32), ("pad0", i32),
+                ("cell_capacity", i32), ("list_batch", i32),
                 ("rho_src", u32 * MAX_ARRAYS), ("mom_src", u32 * MAX_ARRAYS),
                 ("tait_on", u32), ("step_on", u32)]
 

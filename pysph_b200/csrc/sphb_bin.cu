@@ -189,7 +189,6 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
         const long long total = sh[blockDim.x - 1];
         if (s < S) {
             sphb_scene_state &st = e.sstate[s];
-            const sphb_scene &sc = e.scene[s];
             const long long cb = s_carry + incl - need;
             if (bad || cb + need > cap) {
                 flag(e, SPHB_ST_GRID_OVERFLOW);
@@ -200,10 +199,6 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
                 for (int d = 0; d < 3; ++d) { st.lo[d] = lo[d]; st.n[d] = n[d]; }
                 st.cell_base = (int)cb;
                 st.ncells = n[0] * n[1] * n[2];
-            }
-            for (int d = 0; d < 3; ++d) {
-                st.box[d] = enc_double(sc.static_lo[d]);
-                st.box[3 + d] = enc_double(sc.static_hi[d]);
             }
             st.max_disp2 = 0ull;   // the anchors are the new positions
         }
@@ -581,11 +576,9 @@ extern "C" int sphb_refresh(const sphb_engine *e, int cur, void *stream)
 static void launch_rebin(const sphb_engine *e, int cur, int flags, int gated, cudaStream_t st)
 {
     const sphb_config &c = e->cfg;
-    if (flags & SPHB_BIN_BOX) {
-        k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e, gated);
-        if (e->num_tiles > 0)
-            k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
-    }
+    // every rebin measures the scene boxes afresh (only a rebin needs them)
+    k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e, gated);
+    if (e->num_tiles > 0) k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
     k_grid_setup<<<1, 1024, 0, st>>>(*e, gated);
     const int nt = e->num_tiles;
     if (nt > 0) k_hash<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);

@@ -21,7 +21,7 @@ namespace sphb {
 int check_engine_public(const sphb_engine *e, int cur);
 
 template <int DIM, bool F32, int LANES, int R>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
     const int with_eos = flags & SPHB_DENSITY_EOS;
@@ -43,7 +43,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     const int cell_base = st.cell_base, ncells = st.ncells;
     const sphb_scene &sc = e.scene[s];
     const int *__restrict__ start = e.work.start;
-    unsigned long long np = 0;
+    unsigned int np = 0;   // pairs of this thread
     double rho = 0.0;
     // neighbour list of this lane: slots lane, lane + LANES, ... of k,
     // recorded (unless this pass reads them) with the skin when they are
@@ -122,13 +122,13 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                         ih = __fdividef(1.0f, 0.5f * (hk + hj));
                         fac = DIM == 2 ? kf * ih * ih : kf * ih * ih * ih;
                     }
-                    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                    const float ir = rsqrtf(fmaxf(r2, 1e-30f));   // q = 0 at r = 0
                     acc.add(r.m * w_cubic_bf(r2 * ir * ih, fac));
                     ++np;
                 };
                 const int lc = list_count<LANES>(e, from_list, k, lane);
                 if (lc >= 0) {
-                    list_loop<DIM, LANES, 8>(e, k, lane, lc, load,
+                    list_loop<DIM, LANES, 4>(e, k, lane, lc, load,
                                              [&](const Rec &r) { use(r, dist2(r)); });
                     return;
                 }
@@ -335,7 +335,8 @@ int check_pair_cfg(const sphb_engine *e)
 {
     const sphb_config &c = e->cfg;
     if (c.lanes != 1 && c.lanes != 2 && c.lanes != 4 && c.lanes != 8) return SPHB_ERR_UNSUPPORTED;
-    if (c.pair_block < 32 || c.pair_block > 512 || (c.pair_block & 31)) return SPHB_ERR_ARG;
+    if (c.pair_block < 32 || c.pair_block > 256 || (c.pair_block & 31)) return SPHB_ERR_ARG;
+    if (c.list_batch != 0 && c.list_batch != 2 && c.list_batch != 4) return SPHB_ERR_ARG;
     if (!e->pair_tiles || e->num_pair_tiles < 0) return SPHB_ERR_ARG;
     if (!e->work.start || !e->f.cell) return SPHB_ERR_ARG;
     return SPHB_OK;

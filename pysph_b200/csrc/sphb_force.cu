@@ -21,8 +21,8 @@ namespace sphb {
 int check_engine_public(const sphb_engine *e, int cur);
 int check_pair_cfg(const sphb_engine *e);
 
-template <int DIM, bool F32, int LANES, int R>
-__global__ void __launch_bounds__(512)
+template <int DIM, bool F32, int LANES, int R, int U>
+__global__ void __launch_bounds__(256)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
 {
@@ -43,7 +43,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
     // reuse the density pass's lists when they were built from the same sources
     const bool use_list = (mode & SPHB_FORCE_USE_LIST) && e.f.list_cap > 0 && e.f.nbr &&
                           e.f.nbr_cnt && e.cfg.rho_src[a] == e.cfg.mom_src[a];
-    unsigned long long np = 0;
+    unsigned int np = 0;   // pairs of this thread
     double acc[3] = {0.0, 0.0, 0.0};
     double dtf = 0.0;
 
@@ -141,12 +141,14 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         const float mu = __fdividef(hab * dot, r2 + eh2);
                         dtmax = fmaxf(dtmax, fabsf(mu));
                         // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
+                        // when v_ab . r_ab < 0, i.e. mu < 0; else 0: min(mu, 0)
+                        const float mn = fminf(mu, 0.f);
                         const float cab = 0.5f * (tk.z + r.t.z);
                         const float rhoab = 0.5f * (tk.x + r.t.x);
-                        const float pi = __fdividef(-alpha * cab * mu + beta * mu * mu, rhoab);
-                        tmp += dot < 0.f ? pi : 0.f;
+                        tmp += __fdividef(-alpha * cab * mn + beta * mn * mn, rhoab);
                     }
-                    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                    // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
+                    const float ir = rsqrtf(fmaxf(r2, 1e-30f));
                     const float f = -r.m * tmp * gw_cubic_bf(r2 * ir * ih, ir, ih, fih);
                     ax.add(f * rx);
                     ay.add(f * ry);
@@ -154,7 +156,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                 };
                 const int lc = list_count<LANES>(e, use_list, k, lane);
                 if (lc >= 0) {
-                    list_loop<DIM, LANES, 4>(e, k, lane, lc, load, use);
+                    list_loop<DIM, LANES, U>(e, k, lane, lc, load, use);
                     return;
                 }
                 int cx, cy, cz;
@@ -288,7 +290,13 @@ static void launch_force(const sphb_engine &e, int cur, uint32_t dm, int grav,
                          int mode, cudaStream_t st)
 {
     const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
-#define SPHB_L(LV, RV) k_force<DIM, F32, LV, RV><<<g, b, 0, st>>>(e, cur, dm, grav, mode)
+    // the load-ahead depth only shapes the FP32C list loop
+    const int u = (F32 && e.cfg.list_batch == 2) ? 2 : 4;
+#define SPHB_L(LV, RV)                                                                    \
+    do {                                                                                  \
+        if (u == 2) k_force<DIM, F32, LV, RV, 2><<<g, b, 0, st>>>(e, cur, dm, grav, mode); \
+        else k_force<DIM, F32, LV, RV, 4><<<g, b, 0, st>>>(e, cur, dm, grav, mode);        \
+    } while (0)
     switch (e.cfg.lanes * 10 + e.cfg.stencil) {
     case 11: SPHB_L(1, 1); break;
     case 12: SPHB_L(1, 2); break;

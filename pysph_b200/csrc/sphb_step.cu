@@ -113,15 +113,6 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
             }
         }
     }
-    const bool ok = active && isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
-    for (int d = 0; d < DIM; ++d) {
-        const double lo = block_reduce(ok ? p[d] : INFINITY, OpMin(), (double)INFINITY);
-        if (threadIdx.x == 0 && lo < INFINITY)
-            atomic_min_enc(&e.sstate[s].box[d], enc_double(lo));
-        const double hi = block_reduce(ok ? p[d] : -INFINITY, OpMax(), (double)-INFINITY);
-        if (threadIdx.x == 0 && hi > -INFINITY)
-            atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi));
-    }
     // FP32 pair records of the new state, relative to the particle's cell of
     // the last bin, and how far it has moved from where that bin put it
     const bool rec = F32 && e.f.geo && e.f.vel;
@@ -169,8 +160,10 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         }
     }
     if (disp) {
-        const double bd = block_reduce((double)d2, OpMax(), 0.0);
-        if (threadIdx.x == 0 && bd > 0.0) atomic_max_nonneg(&e.sstate[s].max_disp2, bd);
+        // non-negative floats order like their bits: one warp reduction
+        const float wd = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(d2)));
+        if ((threadIdx.x & 31) == 0 && wd > 0.f)
+            atomic_max_nonneg(&e.sstate[s].max_disp2, (double)wd);
     }
 }
 

@@ -101,7 +101,8 @@ class Engine:
                  precision: str = "fp32c", stencil: int = 1, lanes: int = 1,
                  pair_block: int = 128, cell_capacity: int | None = None,
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
-                 step_lists: bool = True, skin_margin: float | None = None):
+                 step_lists: bool = True, skin_margin: float | None = None,
+                 list_batch: int = 4):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -155,6 +156,9 @@ class Engine:
         if cell_capacity is None:
             cell_capacity = self._estimate_capacity(grid_growth)
         self.cell_capacity = int(cell_capacity)
+        if list_batch not in (2, 4):
+            raise ValueError("list_batch must be 2 or 4")
+        self.list_batch = list_batch
         self._alloc(lanes, pair_block)
         self._upload(scenes)
 
@@ -301,6 +305,7 @@ class Engine:
         cfg.stencil = self._stencil
         cfg.lanes = lanes
         cfg.pair_block = pair_block
+        cfg.list_batch = getattr(self, "list_batch", 4)
         cfg.num_particles = self.N
         cfg.cell_capacity = self.cell_capacity
         rho, mom, tait, step = self.scheme.masks()
@@ -323,10 +328,15 @@ class Engine:
                   "sphb_make_tiles")
         return _struct_to_device(arr, self.device), n.value
 
-    def set_launch(self, lanes: int, pair_block: int):
-        """Pair-kernel launch shape: lanes per dest particle and block size."""
-        if lanes not in (1, 2, 4, 8) or pair_block % 32 or not 32 <= pair_block <= 512:
+    def set_launch(self, lanes: int, pair_block: int, list_batch: int | None = None):
+        """Pair-kernel launch shape: lanes per dest particle, block size and
+        how many list entries the FP32C force pass loads ahead (2 or 4)."""
+        if lanes not in (1, 2, 4, 8) or pair_block % 32 or not 32 <= pair_block <= 256:
             raise ValueError("bad pair-kernel launch shape")
+        if list_batch is not None:
+            if list_batch not in (2, 4):
+                raise ValueError("list_batch must be 2 or 4")
+            self.list_batch = list_batch
         self.lanes, self.pair_block = lanes, pair_block
         self.pair_tiles = self._make_tiles(pair_block // lanes)
         self._build_desc()
