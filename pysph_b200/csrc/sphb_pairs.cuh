@@ -232,17 +232,18 @@ __device__ __forceinline__ float gw_cubic_f(float r2, float hab)
     return val * fac;
 }
 
-// Branch-free FP32 cubic spline for the list passes, with t1 = max(2 - q, 0)
-// and t2 = max(1 - q, 0):  W = fac/4 (t1^3 - 4 t2^3) (equal to
-// 1 - 1.5 q^2 (1 - q/2) for q < 1 and (2 - q)^3 / 4 for 1 <= q < 2, zero
-// beyond), and dW/dr / r = fac ih (q < 1 ? (2.25 q - 3) ih : -0.75 t1^2 / r)
-// (S/base/kernels.pyx:355-417).  ir = 1/r (0 for r = 0, where r_ab = 0
-// makes the gradient term vanish anyway).
+// Branch-free FP32 cubic spline for the list passes (both pieces computed,
+// one selected; t1 = max(2 - q, 0) is zero beyond the support):
+// W = fac (q < 1 ? 1 + q^2 (0.75 q - 1.5) : t1^3 / 4), and
+// dW/dr / r = fac ih (q < 1 ? (2.25 q - 3) ih : -0.75 t1^2 / r)
+// (S/base/kernels.pyx:355-417).  ir = 1/r (huge but finite for r = 0, where
+// r_ab = 0 makes the gradient term vanish anyway).
 __device__ __forceinline__ float w_cubic_bf(float q, float fac)
 {
     const float t1 = fmaxf(2.0f - q, 0.0f);
-    const float t2 = fmaxf(1.0f - q, 0.0f);
-    return 0.25f * fac * (t1 * t1 * t1 - 4.0f * (t2 * t2 * t2));
+    const float inner = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
+    const float outer = 0.25f * (t1 * t1 * t1);
+    return fac * (q < 1.0f ? inner : outer);
 }
 
 __device__ __forceinline__ float gw_cubic_bf(float q, float ir, float ih, float fac_ih)
