@@ -160,12 +160,6 @@ typedef struct {
      * a lane overflowed its list_cap / lanes slots). */
     uint32_t *nbr;
     int32_t *nbr_cnt;
-    /* Optional stage lists (FP32C): the pairs inside the support at the
-     * current positions, written by a pipeline density pass (flags with
-     * SPHB_DENSITY_LIST_IF_VALID or _USE_LIST) for the force pass of the
-     * same stage; same layout and capacity as nbr. */
-    uint32_t *snbr;
-    int32_t *snbr_cnt;
     /* Optional (NULL: no list reuse across stages): FP32 position of every
      * particle at its last rebin, relative to the origin of its cell; 2D
      * float2, 3D float4 {x, y, z, 0}.  sphb_pc_stage measures how far the
@@ -194,9 +188,7 @@ typedef struct {
                                (cleared by anything that moves particles);
                                meta[3] = 2 while the positions are those of
                                the last rebin; meta[4] = 1 when the lists
-                               were recorded with the skin at them;
-                               meta[5] = arrays whose stage lists are
-                               current */
+                               were recorded with the skin at them */
     unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
     unsigned long long *pairs;  /* [4]  pairs evaluated: density, force, -, - */
 } sphb_work;
@@ -324,9 +316,7 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
  * .clt:69-157; S/sph/funcs/external_force.pyx:13-62.
  * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV).
  * mode | SPHB_FORCE_USE_LIST: iterate the lists of the last sphb_density
- * pass (same bin, same sources) instead of searching cells: the stage list
- * of a pipeline density pass at the current positions when there is one
- * for the dest array (work.meta[5]), else the kept lists. */
+ * pass (same bin, same sources) instead of searching cells. */
 #define SPHB_FORCE_USE_LIST 16
 SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
                   int with_gravity, int mode, void *stream);

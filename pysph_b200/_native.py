@@ -86,7 +86,7 @@ class Buffers(ctypes.Structure):
 
 
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
-               "vel", "thermo", "cell", "nbr", "nbr_cnt", "snbr", "snbr_cnt", "anchor")
+               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor")
 FORCE_USE_LIST = 16
 DENSITY_EOS = 1
 DENSITY_USE_LIST = 2

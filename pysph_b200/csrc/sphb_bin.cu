@@ -219,7 +219,6 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
         e.work.meta[2] = 0;
         e.work.meta[3] = 2;
         e.work.meta[4] = 0;
-        e.work.meta[5] = 0;
     }
 }
 

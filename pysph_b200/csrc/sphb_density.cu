@@ -21,7 +21,7 @@ namespace sphb {
 int check_engine_public(const sphb_engine *e, int cur);
 
 template <int DIM, bool F32, int LANES, int R>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
     const int with_eos = flags & SPHB_DENSITY_EOS;
@@ -59,16 +59,6 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
         e.work.meta[4] = (reuse && e.work.meta[3] == 2) ? 1 : 0;
         if (!reuse) e.work.meta[2] = 0;
     }
-    // stage list (FP32C pipeline passes): the pairs inside the support at
-    // this stage's positions, for the force pass that follows
-    const bool pipeline = (flags & (SPHB_DENSITY_LIST_IF_VALID | SPHB_DENSITY_USE_LIST)) != 0;
-    uint32_t *__restrict__ snbr = (F32 && pipeline && e.f.list_cap > 0) ? e.f.snbr : nullptr;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // no kernel pass reads meta[5] while this one writes it
-        if (snbr) atomicOr((unsigned *)&e.work.meta[5], dest_mask);
-        else e.work.meta[5] = 0;
-    }
-    int scnt = 0;
     int cnt = 0;
     auto record = [&](int j, int o, int dy, int dz) {
         if (nbr) {
@@ -97,12 +87,10 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             struct Rec {
                 float4 g;
                 float m, o, dy, dz;
-                uint32_t v;
                 bool ok;
             };
-            auto load = [&](const EntryF &en, uint32_t v) {
+            auto load = [&](const EntryF &en) {
                 Rec r;
-                r.v = v;
                 r.ok = en.j < N;
                 const int j = r.ok ? en.j : k;
                 r.g = __ldg(geo + j);
@@ -128,10 +116,6 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 constexpr bool UH = decltype(uniform)::value;
                 auto use = [&](const Rec &r, float r2) {
                     if (!(r.ok && r2 < rad2)) return;
-                    if (snbr) {
-                        if (scnt < cap_lane) snbr[(size_t)(lane + LANES * scnt) * N + k] = r.v;
-                        ++scnt;
-                    }
                     float ih = ihk, fac = fack;
                     if (!UH) {
                         const float hj = DIM == 3 ? r.g.w : r.g.z;
@@ -142,9 +126,9 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     acc.add(r.m * w_cubic_bf(r2 * ir * ih, fac));
                     ++np;
                 };
-                const int lc = list_count<LANES>(e, e.f.nbr_cnt, from_list, k, lane);
+                const int lc = list_count<LANES>(e, from_list, k, lane);
                 if (lc >= 0) {
-                    list_loop<DIM, LANES, 4>(e, e.f.nbr, k, lane, lc, load,
+                    list_loop<DIM, LANES, 4>(e, k, lane, lc, load,
                                              [&](const Rec &r) { use(r, dist2(r)); });
                     return;
                 }
@@ -153,8 +137,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 for_each_candidate<DIM, R, LANES>(
                     start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
                     [&](int j, int o, int dy, int dz) {
-                        const Rec r = load(EntryF{j, (float)o, (float)dy, (float)dz},
-                                           nbr_pack<DIM>(j, o, dy, dz));
+                        const Rec r = load(EntryF{j, (float)o, (float)dy, (float)dz});
                         const float r2 = dist2(r);
                         if (r2 < radl2) record(j, o, dy, dz);
                         use(r, r2);
@@ -205,7 +188,6 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     }
 
     if (active && nbr) e.f.nbr_cnt[(size_t)lane * N + k] = cnt <= cap_lane ? cnt : -1;
-    if (active && snbr) e.f.snbr_cnt[(size_t)lane * N + k] = scnt <= cap_lane ? scnt : -1;
     if (active && lane == 0) {
         const bool real = e.buf[cur].tag[k] == 0;
         if (!real) rho = 0.0;

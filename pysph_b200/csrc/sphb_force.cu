@@ -85,7 +85,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                 float vx, vy, vz, m, o, dy, dz;
                 bool ok;
             };
-            auto load = [&](const EntryF &en, uint32_t) {
+            auto load = [&](const EntryF &en) {
                 Rec r;
                 r.ok = en.j < N;
                 const int j = r.ok ? en.j : k;
@@ -154,17 +154,9 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     ay.add(f * ry);
                     if (DIM == 3) az.add(f * rz);
                 };
-                // this stage's list from the density pass when it wrote one
-                // for this array, else the kept lists, else the cells
-                const bool stage = use_list && e.f.snbr && ((e.work.meta[5] >> a) & 1);
-                const int sc_ = list_count<LANES>(e, e.f.snbr_cnt, stage, k, lane);
-                if (sc_ >= 0) {
-                    list_loop<DIM, LANES, U>(e, e.f.snbr, k, lane, sc_, load, use);
-                    return;
-                }
-                const int lc = list_count<LANES>(e, e.f.nbr_cnt, use_list, k, lane);
+                const int lc = list_count<LANES>(e, use_list, k, lane);
                 if (lc >= 0) {
-                    list_loop<DIM, LANES, U>(e, e.f.nbr, k, lane, lc, load, use);
+                    list_loop<DIM, LANES, U>(e, k, lane, lc, load, use);
                     return;
                 }
                 int cx, cy, cz;
@@ -172,7 +164,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                 for_each_candidate<DIM, R, LANES>(
                     start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
                     [&](int j, int o, int dy, int dz) {
-                        use(load(EntryF{j, (float)o, (float)dy, (float)dz}, 0u));
+                        use(load(EntryF{j, (float)o, (float)dy, (float)dz}));
                     });
             };
             if (sc.uniform_h) pass(std::true_type{});

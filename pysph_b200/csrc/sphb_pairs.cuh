@@ -112,11 +112,10 @@ __device__ __forceinline__ EntryF entry_unpack_f(uint32_t v)
     return r;
 }
 
-// Entries of dest k this lane owns in the list counted by cnt (-1 when some
-// lane's list overflowed), or -1 when the list is not to be used.
+// Entries of dest k this lane owns (-1 when some lane's list overflowed),
+// or -1 when the lists are not to be used.
 template <int LANES>
-__device__ __forceinline__ int list_count(const sphb_engine &e, const int32_t *cnt, bool use_list,
-                                          int k, int lane)
+__device__ __forceinline__ int list_count(const sphb_engine &e, bool use_list, int k, int lane)
 {
     if (!use_list) return -1;
     const int N = e.cfg.num_particles;
@@ -124,23 +123,22 @@ __device__ __forceinline__ int list_count(const sphb_engine &e, const int32_t *c
     bool ok = true;
 #pragma unroll
     for (int l = 0; l < LANES; ++l) {
-        const int c = __ldg(cnt + (size_t)l * N + k);
+        const int c = __ldg(e.f.nbr_cnt + (size_t)l * N + k);
         ok = ok && c >= 0;
         if (l == lane) mine = c;
     }
     return ok ? mine : -1;
 }
 
-// use(load(entry, raw entry)) over the cnt entries of (k, lane) in list
-// (slot-major [slot][N], slot = lane + LANES c).  U entries and then their
-// neighbour records are loaded before any is used, so each thread keeps U
-// gathers in flight instead of one dependent chain.
+// use(load(entry)) over the cnt list entries of (k, lane).  U entries and
+// then their neighbour records are loaded before any is used, so each
+// thread keeps U gathers in flight instead of one dependent chain.
 template <int DIM, int LANES, int U, typename Load, typename Use>
-__device__ __forceinline__ void list_loop(const sphb_engine &e, const uint32_t *list, int k,
-                                          int lane, int cnt, Load &&load, Use &&use)
+__device__ __forceinline__ void list_loop(const sphb_engine &e, int k, int lane, int cnt,
+                                          Load &&load, Use &&use)
 {
     const int N = e.cfg.num_particles;
-    const uint32_t *__restrict__ p = list + (size_t)lane * N + k;
+    const uint32_t *__restrict__ p = e.f.nbr + (size_t)lane * N + k;
     const size_t stride = (size_t)LANES * N;
     int c = 0;
 #pragma unroll 1
@@ -148,17 +146,14 @@ __device__ __forceinline__ void list_loop(const sphb_engine &e, const uint32_t *
         uint32_t v[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) v[u] = __ldg(p + (size_t)(c + u) * stride);
-        decltype(load(EntryF{}, 0u)) r[U];
+        decltype(load(EntryF{})) r[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) r[u] = load(entry_unpack_f<DIM>(v[u]), v[u]);
+        for (int u = 0; u < U; ++u) r[u] = load(entry_unpack_f<DIM>(v[u]));
 #pragma unroll
         for (int u = 0; u < U; ++u) use(r[u]);
     }
 #pragma unroll 1
-    for (; c < cnt; ++c) {
-        const uint32_t v = __ldg(p + (size_t)c * stride);
-        use(load(entry_unpack_f<DIM>(v), v));
-    }
+    for (; c < cnt; ++c) use(load(entry_unpack_f<DIM>(__ldg(p + (size_t)c * stride))));
 }
 
 // The pairs of dest k: its list from the last density pass when use_list

@@ -54,7 +54,6 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         // the next rebin decision, and the positions leave the anchors
         e.work.meta[2] = 0;
         e.work.meta[3] = 0;
-        e.work.meta[5] = 0;
     }
     if (stage == 0 && blockIdx.x == 0) {
         // the CFL rule reads the maxima of the corrector's force pass only
@@ -246,7 +245,6 @@ k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
         e.work.meta[2] = 0;
         e.work.meta[3] = 0;
         e.work.meta[4] = 0;
-        e.work.meta[5] = 0;
     }
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;

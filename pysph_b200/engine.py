@@ -280,12 +280,6 @@ class Engine:
             f["nbr_cnt"] = torch.zeros(8 * N, **i32)
         else:
             f["nbr"] = f["nbr_cnt"] = None
-        # stage lists: the pairs of the current stage, density pass -> force
-        if self.list_cap and self.f32:
-            f["snbr"] = torch.zeros(self.list_cap * N, **i32)
-            f["snbr_cnt"] = torch.zeros(8 * N, **i32)
-        else:
-            f["snbr"] = f["snbr_cnt"] = None
         # binned positions, for the rebin decision of the list reuse
         f["anchor"] = (torch.zeros(N, 2 if dim == 2 else 4, dtype=torch.float32, device=dev)
                        if self.step_lists else None)
