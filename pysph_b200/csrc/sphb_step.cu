@@ -68,95 +68,96 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const int k = t.begin + threadIdx.x;
     const bool active = k < t.end;
     const sphb_buffers &B = e.buf[cur];
-    const double dt2 = e.sstate[s].dt / 2;
-    double p[3] = {0.0, 0.0, 0.0};
-    double vn[3] = {0.0, 0.0, 0.0};
+    const sphb_scene_state &st = e.sstate[s];
+    const double dt2 = st.dt / 2;
+    const bool rec = F32 && e.f.geo && e.f.vel;   // FP32 pair records
+    const bool disp = e.f.anchor != nullptr;      // displacement check
+    float d2 = 0.f;
     if (active) {
-        const bool real = B.tag[k] == 0;
-        double f[3] = {0.0, 0.0, 0.0};
-        if (real) {
-            if (F32) {
-                f[0] = ((const float *)e.f.au)[k];
-                f[1] = ((const float *)e.f.av)[k];
-                if (DIM == 3) f[2] = ((const float *)e.f.aw)[k];
-            } else {
-                f[0] = ((const double *)e.f.au)[k];
-                f[1] = ((const double *)e.f.av)[k];
-                if (DIM == 3) f[2] = ((const double *)e.f.aw)[k];
-            }
-        }
+        // every load first, so a thread's loads are in flight together
         double *X[3] = {B.x, B.y, B.z};
         double *V[3] = {B.u, B.v, B.w};
         double *X0[3] = {B.x0, B.y0, B.z0};
         double *V0[3] = {B.u0, B.v0, B.w0};
+        const bool real = B.tag[k] == 0;
+        double f[3] = {0.0, 0.0, 0.0}, x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
+        double x0[3] = {0.0, 0.0, 0.0}, v0[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-            const double x = X[d][k], v = V[d][k];
-            const double fx = real ? v : 0.0;  // PositionStepping: F_x = u
-            if (stage == 0) {
-                X0[d][k] = x;
-                V0[d][k] = v;
-                const double xn = axpy_rn(x, fx, dt2);
-                X[d][k] = xn;
-                vn[d] = axpy_rn(v, f[d], dt2);
-                V[d][k] = vn[d];
-                p[d] = xn;
-            } else {
-                const double x0 = X0[d][k], v0 = V0[d][k];
-                const double xh = axpy_rn(x0, fx, dt2);
-                const double vh = axpy_rn(v0, f[d], dt2);
-                const double xn = __dadd_rn(2 * xh, -x0);
-                X[d][k] = xn;
-                vn[d] = __dadd_rn(2 * vh, -v0);
-                V[d][k] = vn[d];
-                p[d] = xn;
+            const void *fa = d == 0 ? e.f.au : (d == 1 ? e.f.av : e.f.aw);
+            f[d] = F32 ? (double)((const float *)fa)[k] : ((const double *)fa)[k];
+            x[d] = X[d][k];
+            v[d] = V[d][k];
+            if (stage == 1) {
+                x0[d] = X0[d][k];
+                v0[d] = V0[d][k];
             }
         }
-    }
-    // FP32 pair records of the new state, relative to the particle's cell of
-    // the last bin, and how far it has moved from where that bin put it
-    const bool rec = F32 && e.f.geo && e.f.vel;
-    const bool disp = e.f.anchor != nullptr;
-    if (!rec && !disp) return;  // block-uniform
-    float d2 = 0.f;
-    if (active) {
-        const sphb_scene_state &st = e.sstate[s];
-        const double cs = e.scene[s].cell_size;
-        int local = e.f.cell[k];
-        if (local < 0 || local >= st.ncells) {
-            flag(e, SPHB_ST_BAD_INDEX);
-            local = 0;
-        }
-        int c[3];
-        cell_coords(local, st.n, c[0], c[1], c[2]);
-        float xr[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) xr[d] = (float)(p[d] - (double)(st.lo[d] + c[d]) * cs);
-        if (rec) {
-            if (DIM == 2) {
-                ((float2 *)e.f.geo)[2 * k] = make_float2(xr[0], xr[1]);
-                ((float2 *)e.f.vel)[k] = make_float2((float)vn[0], (float)vn[1]);
-            } else {
-                ((float4 *)e.f.geo)[k] = make_float4(xr[0], xr[1], xr[2], (float)B.h[k]);
-                ((float4 *)e.f.vel)[k] =
-                    make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
-            }
-        }
+        int local = (rec || disp) ? e.f.cell[k] : 0;
+        float an[3] = {0.f, 0.f, 0.f};
         if (disp) {
-            float q[3] = {0.f, 0.f, 0.f};
             if (DIM == 2) {
-                const float2 an = ((const float2 *)e.f.anchor)[k];
-                q[0] = xr[0] - an.x;
-                q[1] = xr[1] - an.y;
+                const float2 q = ((const float2 *)e.f.anchor)[k];
+                an[0] = q.x;
+                an[1] = q.y;
             } else {
-                const float4 an = ((const float4 *)e.f.anchor)[k];
-                q[0] = xr[0] - an.x;
-                q[1] = xr[1] - an.y;
-                q[2] = xr[2] - an.z;
+                const float4 q = ((const float4 *)e.f.anchor)[k];
+                an[0] = q.x;
+                an[1] = q.y;
+                an[2] = q.z;
             }
-            d2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-            // a non-finite position can never be within the skin
-            if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
+        }
+        const float hk = (rec && DIM == 3) ? (float)B.h[k] : 0.f;
+        // the stage
+        double p[3] = {0.0, 0.0, 0.0}, vn[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double fd = real ? f[d] : 0.0;
+            const double fx = real ? v[d] : 0.0;  // PositionStepping: F_x = u
+            if (stage == 0) {
+                X0[d][k] = x[d];
+                V0[d][k] = v[d];
+                p[d] = axpy_rn(x[d], fx, dt2);
+                vn[d] = axpy_rn(v[d], fd, dt2);
+            } else {
+                const double xh = axpy_rn(x0[d], fx, dt2);
+                const double vh = axpy_rn(v0[d], fd, dt2);
+                p[d] = __dadd_rn(2 * xh, -x0[d]);
+                vn[d] = __dadd_rn(2 * vh, -v0[d]);
+            }
+            X[d][k] = p[d];
+            V[d][k] = vn[d];
+        }
+        // FP32 pair records of the new state, relative to the particle's
+        // cell of the last bin, and how far it has moved from where that bin
+        // put it
+        if (rec || disp) {
+            if (local < 0 || local >= st.ncells) {
+                flag(e, SPHB_ST_BAD_INDEX);
+                local = 0;
+            }
+            const double cs = e.scene[s].cell_size;
+            int c[3];
+            cell_coords(local, st.n, c[0], c[1], c[2]);
+            float xr[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xr[d] = (float)(p[d] - (double)(st.lo[d] + c[d]) * cs);
+            if (rec) {
+                if (DIM == 2) {
+                    ((float2 *)e.f.geo)[2 * k] = make_float2(xr[0], xr[1]);
+                    ((float2 *)e.f.vel)[k] = make_float2((float)vn[0], (float)vn[1]);
+                } else {
+                    ((float4 *)e.f.geo)[k] = make_float4(xr[0], xr[1], xr[2], hk);
+                    ((float4 *)e.f.vel)[k] =
+                        make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
+                }
+            }
+            if (disp) {
+                const float q0 = xr[0] - an[0], q1 = xr[1] - an[1], q2 = xr[2] - an[2];
+                d2 = q0 * q0 + q1 * q1 + q2 * q2;
+                // a non-finite position can never be within the skin
+                if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
+            }
         }
     }
     if (disp) {
