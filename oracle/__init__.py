@@ -32,7 +32,7 @@ _SRC = os.path.join(_HERE, "sph_oracle.c")
 MAX_ARRAYS = 4
 PROPS = ("x", "y", "z", "u", "v", "w", "m", "h", "rho", "p", "cs",
          "au", "av", "aw", "ax", "ay", "az", "dt_fac",
-         "x0", "y0", "z0", "u0", "v0", "w0")
+         "x0", "y0", "z0", "u0", "v0", "w0", "arho", "rho0")
 
 
 def build(force: bool = False) -> str:
@@ -68,6 +68,9 @@ class _System(ctypes.Structure):
         ("nthreads", ctypes.c_int32), ("pad_", ctypes.c_int32),
         ("a", _Array * MAX_ARRAYS),
         ("pairs", ctypes.c_int64),
+        ("rate_src", ctypes.c_uint32 * MAX_ARRAYS),
+        ("xsph_src", ctypes.c_uint32 * MAX_ARRAYS),
+        ("xsph_eps", ctypes.c_double),
     ]
 
 
@@ -105,6 +108,10 @@ def lib():
                                    ctypes.c_double, dp, dp, dp, dp]
         L.orc_pgrad.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
                                 ctypes.c_int, dp, dp, dp]
+        L.orc_density_rate.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_int, dp]
+        L.orc_xsph.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_double, dp, dp, dp]
         L.orc_kernel_w.restype = ctypes.c_double
         L.orc_kernel_w.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int]
         L.orc_kernel_grad.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int, dp]
@@ -154,16 +161,20 @@ class OracleArray:
 
 
 class OracleSystem:
-    """A Particles-like collection plus the pinned scheme (SPHRho -> Tait ->
-    MomentumEquation -> GravityForce -> PositionStepping).
+    """A Particles-like collection plus the scheme, evaluated in the order
+    SPHRho -> TaitEquation -> SPHDensityRate -> MomentumEquation ->
+    GravityForce -> PositionStepping -> XSPHCorrection (summation density:
+    rho_src; continuity equation: rate_src, with xsph_src / xsph_eps).
 
-    rho_src / mom_src map a dest array index to the list of its source array
-    indices; tait_on / step_on list array indices."""
+    rho_src / rate_src / mom_src / xsph_src map a dest array index to the
+    list of its source array indices; tait_on / step_on list array
+    indices."""
 
     def __init__(self, arrays, dim=2, rho_src=None, tait_on=(), mom_src=None,
                  step_on=(), c0=1.0, rho0=1000.0, gamma=7.0, alpha=1.0,
                  beta=1.0, eta=0.1, gravity=(0.0, 0.0, 0.0), nthreads=0,
-                 radius_scale=2.0, cell_scale=2.0):
+                 radius_scale=2.0, cell_scale=2.0, rate_src=None, xsph_src=None,
+                 xsph_eps=0.5):
         self.arrays = list(arrays)
         assert 1 <= len(self.arrays) <= MAX_ARRAYS
         self.dim = dim
@@ -178,6 +189,11 @@ class OracleSystem:
         for d, srcs in (mom_src or {}).items():
             s.mom_src[d] = sum(1 << a for a in srcs)
         s.step_on = sum(1 << a for a in step_on)
+        for d, srcs in (rate_src or {}).items():
+            s.rate_src[d] = sum(1 << a for a in srcs)
+        for d, srcs in (xsph_src or {}).items():
+            s.xsph_src[d] = sum(1 << a for a in srcs)
+        s.xsph_eps = xsph_eps
         s.c0, s.rho0, s.gamma_eos = c0, rho0, gamma
         s.alpha, s.beta, s.gamma_av, s.eta = alpha, beta, 1.4, eta
         s.gx, s.gy, s.gz = gravity

@@ -20,6 +20,9 @@
  *   neighbour predicate, self last . S/base/nnps.pyx:271-356, :525-621
  *   SPHRho ......................... S/sph/funcs/density_funcs.pyx:37-73,
  *                                    S/sph/sph_func.pyx:513-531
+ *   SPHDensityRate ................. S/sph/funcs/density_funcs.pyx:88-161
+ *   XSPHCorrection ................. S/sph/funcs/xsph_funcs.pyx:9-90,
+ *                                    S/sph/sph_func.pyx:500-531 (CSPH eval)
  *   TaitEquation ................... S/sph/funcs/eos_funcs.pyx:88-129
  *   MomentumEquation ............... S/sph/funcs/pressure_funcs.pyx:246-391
  *   SPHPressureGradient ............ S/sph/funcs/pressure_funcs.pyx:62-161
@@ -47,6 +50,8 @@ typedef struct {
     double *ax, *ay, *az;      /* _a_x_1, _a_y_1, _a_z_1 (PositionStepping) */
     double *dt_fac;
     double *x0, *y0, *z0, *u0, *v0, *w0;
+    double *arho;              /* _a_rho_1 (SPHDensityRate) */
+    double *rho0;              /* _rho0 */
     int64_t *tag;              /* 0 == LocalReal */
 } orc_array;
 
@@ -66,6 +71,9 @@ typedef struct {
     int32_t pad_;
     orc_array a[ORC_MAX_ARRAYS];
     int64_t pairs;             /* pair interactions evaluated by orc_eval */
+    uint32_t rate_src[ORC_MAX_ARRAYS]; /* SPHDensityRate sources per dest */
+    uint32_t xsph_src[ORC_MAX_ARRAYS]; /* XSPHCorrection sources per dest */
+    double xsph_eps;
 } orc_system;
 
 typedef struct {
@@ -556,6 +564,85 @@ int orc_pgrad(const orc_system *s, const orc_nnps *c, int da, int sa,
     return 0;
 }
 
+/* SPHDensityRate.eval_nbr (S/sph/funcs/density_funcs.pyx:119-156), hks
+ * off: drho_a += ((v_a - v_b) . grad_a W(r_ab, h_ab)) m_b. */
+int orc_density_rate(const orc_system *s, const orc_nnps *c, int da, int sa,
+                     double *out1)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kfac_unit(dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = 0; continue; }
+        double nr = 0.0;
+        double ha = D->h[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double hb = S->h[j];
+            double hab = 0.5 * (ha + hb);
+            double vx = D->u[i] - S->u[j];
+            double vy = D->v[i] - S->v[j];
+            double vz = D->w[i] - S->w[j];
+            double g[3];
+            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                        hab, dim, kfac, g);
+            double dot = vx * g[0] + vy * g[1] + vz * g[2];
+            nr += dot * S->m[j];
+        }
+        out1[i] += nr;
+    }
+    return 0;
+}
+
+/* XSPHCorrection.eval_nbr_csph (S/sph/funcs/xsph_funcs.pyx:40-86), hks and
+ * kernel correction off, so the CSPH denominator stays 0 and is not applied
+ * (S/sph/sph_func.pyx:513-531): x_a' += eps m_b W_ab (v_b - v_a) / rho_ab,
+ * rho_ab = (rho_b + rho_a) / 2. */
+int orc_xsph(const orc_system *s, const orc_nnps *c, int da, int sa, double eps,
+             double *out1, double *out2, double *out3)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kfac_unit(dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = out2[i] = out3[i] = 0; continue; }
+        double nr0 = 0.0, nr1 = 0.0, nr2 = 0.0;
+        double ha = D->h[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double hb = S->h[j];
+            double hab = 0.5 * (ha + hb);
+            double rhoab = 0.5 * (S->rho[j] + D->rho[i]);
+            double vbx = S->u[j] - D->u[i];
+            double vby = S->v[j] - D->v[i];
+            double vbz = S->w[j] - D->w[i];
+            double mb = S->m[j];
+            double w = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j],
+                                   S->z[j], hab, dim, kfac);
+            double temp = mb * w / rhoab;
+            nr0 += temp * vbx * eps;
+            nr1 += temp * vby * eps;
+            nr2 += temp * vbz * eps;
+        }
+        out1[i] += nr0;
+        out2[i] += nr1;
+        out3[i] += nr2;
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* the pinned scheme: SPHRho -> Tait -> MomentumEquation -> Gravity ->  */
 /* PositionStepping, evaluated as Integrator.eval does                  */
@@ -565,7 +652,8 @@ static uint32_t pair_mask_of(const orc_system *s)
     uint32_t mask = 0;
     for (int d = 0; d < s->narrays; ++d)
         for (int a = 0; a < s->narrays; ++a)
-            if ((s->rho_src[d] | s->mom_src[d]) & (1u << a))
+            if ((s->rho_src[d] | s->mom_src[d] | s->rate_src[d] | s->xsph_src[d]) &
+                (1u << a))
                 mask |= 1u << (d * 4 + a);
     return mask;
 }
@@ -593,6 +681,18 @@ int orc_eval(orc_system *s, const orc_nnps *c)
         const orc_array *D = &s->a[d];
         for (int64_t i = 0; i < D->n; ++i) { D->p[i] = 0.0; D->cs[i] = 0.0; }
         orc_tait(s, d, s->c0, s->rho0, s->gamma_eos, D->p, D->cs);
+    }
+    /* SPHDensityRate (the continuity scheme): integrating, adds into
+     * _a_rho_1 source by source */
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->rate_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int a = 0; a < s->narrays; ++a)
+            if (s->rate_src[d] & (1u << a)) {
+                rc = orc_density_rate(s, c, d, a, D->arho);
+                if (rc) return rc;
+                s->pairs += c->off[d][a][D->n];
+            }
     }
     /* accelerations were reset by reset_accelerations; dt_fac by to_reset */
     for (int d = 0; d < s->narrays; ++d) {
@@ -624,11 +724,28 @@ int orc_eval(orc_system *s, const orc_nnps *c)
             D->az[i] = D->w[i];
         }
     }
+    /* XSPHCorrection: integrating, updates x, y (z) after PositionStepping */
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->xsph_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int a = 0; a < s->narrays; ++a)
+            if (s->xsph_src[d] & (1u << a)) {
+                rc = orc_xsph(s, c, d, a, s->xsph_eps, D->ax, D->ay, D->az);
+                if (rc) return rc;
+                s->pairs += c->off[d][a][D->n];
+            }
+    }
     return 0;
 }
 
 static void reset_acc(const orc_system *s)
 {
+    for (int d = 0; d < s->narrays; ++d) {
+        if (s->rate_src[d]) {
+            const orc_array *D = &s->a[d];
+            for (int64_t i = 0; i < D->n; ++i) D->arho[i] = 0.0;
+        }
+    }
     for (int d = 0; d < s->narrays; ++d) {
         if (!(s->step_on & (1u << d))) continue;
         const orc_array *D = &s->a[d];
@@ -642,6 +759,14 @@ static void reset_acc(const orc_system *s)
 /* Integrator.step: prop = initial + step_arr * dt (numpy, no FMA) */
 static void half_step(const orc_system *s, double dt)
 {
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->rate_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) {
+            double t = D->arho[i] * dt;
+            D->rho[i] = D->rho0[i] + t;
+        }
+    }
     for (int d = 0; d < s->narrays; ++d) {
         if (!(s->step_on & (1u << d))) continue;
         const orc_array *D = &s->a[d];
@@ -666,6 +791,9 @@ int orc_pc_step(orc_system *s, orc_nnps *c, double dt)
     uint32_t pm = pair_mask_of(s);
     int rc = orc_update(s, c, pm);
     if (rc) return rc;
+    for (int d = 0; d < s->narrays; ++d)
+        if (s->rate_src[d])
+            memcpy(s->a[d].rho0, s->a[d].rho, sizeof(double) * (size_t)s->a[d].n);
     for (int d = 0; d < s->narrays; ++d) {
         if (!(s->step_on & (1u << d))) continue;
         const orc_array *D = &s->a[d];
@@ -689,6 +817,11 @@ int orc_pc_step(orc_system *s, orc_nnps *c, double dt)
     rc = orc_eval(s, c);
     if (rc) return rc;
     half_step(s, half);
+    for (int d = 0; d < s->narrays; ++d) {
+        if (!s->rate_src[d]) continue;
+        const orc_array *D = &s->a[d];
+        for (int64_t i = 0; i < D->n; ++i) D->rho[i] = 2 * D->rho[i] - D->rho0[i];
+    }
     for (int d = 0; d < s->narrays; ++d) {
         if (!(s->step_on & (1u << d))) continue;
         const orc_array *D = &s->a[d];

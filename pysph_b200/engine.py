@@ -55,11 +55,32 @@ class SceneParams:
 
 @dataclass
 class Scheme:
-    """Which array indices take part in which operation."""
+    """Which array indices take part in which operation.
+
+    Summation density: rho_src (SPHRho).  Continuity equation: rate_src
+    (SPHDensityRate, rho integrated on its dests), optionally with
+    XSPHCorrection (xsph_src, xsph_eps) added to the position rate."""
     rho_src: dict = field(default_factory=dict)   # dest -> [sources]
     mom_src: dict = field(default_factory=dict)   # dest -> [sources]
     tait_on: tuple = ()
     step_on: tuple = ()
+    rate_src: dict = field(default_factory=dict)  # dest -> [sources]
+    xsph_src: dict = field(default_factory=dict)  # dest -> [sources]
+    xsph_eps: float = 0.5
+
+    @property
+    def continuity(self) -> bool:
+        return any(self.rate_src.values())
+
+    def masks2(self):
+        """Continuity and XSPH source masks per dest array."""
+        rate = [0] * nat.MAX_ARRAYS
+        xs = [0] * nat.MAX_ARRAYS
+        for d, s in self.rate_src.items():
+            rate[d] = sum(1 << a for a in s)
+        for d, s in self.xsph_src.items():
+            xs[d] = sum(1 << a for a in s)
+        return rate, xs
 
     def masks(self):
         rho = [0] * nat.MAX_ARRAYS
@@ -88,6 +109,19 @@ def fluid_scheme(num_arrays: int = 1) -> Scheme:
     all_ = list(range(num_arrays))
     return Scheme(rho_src={a: all_ for a in all_}, mom_src={0: all_},
                   tait_on=tuple(all_), step_on=(0,))
+
+
+def continuity_scheme(num_arrays: int = 1, xsph_eps: float = 0.5) -> Scheme:
+    """The reference's dam-break scheme (examples/dam-break/dam_break.py:
+    184-241, FluidSolver S/solver/fluid_solver.py:55-87): Tait on every
+    array; SPHDensityRate on every array from every array (rho integrated
+    on all of them, walls included); MomentumEquation on the fluid (array
+    0) from every array; the fluid's positions stepped with XSPHCorrection
+    from the fluid (eps = xsph_eps; 0 leaves XSPH out)."""
+    all_ = list(range(num_arrays))
+    return Scheme(mom_src={0: all_}, tait_on=tuple(all_), step_on=(0,),
+                  rate_src={a: all_ for a in all_},
+                  xsph_src={0: [0]} if xsph_eps else {}, xsph_eps=xsph_eps)
 
 
 class Engine:

@@ -50,10 +50,11 @@ def ref_modules(build_dir):
     import pysph.sph.funcs.pressure_funcs as PF
     import pysph.sph.funcs.position_funcs as POS
     import pysph.sph.funcs.external_force as EF
+    import pysph.sph.funcs.xsph_funcs as X
     import pysph.solver.sph_equation as EQ
     import pysph.solver.integrator as I
     import pysph.solver.time_step_functions as T
-    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T)
+    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T, X=X)
 
 
 def make_array(R, props, name, ptype):
@@ -71,31 +72,44 @@ def lists_of(R, particles, src, dst):
     return off, np.concatenate(out) if out else np.zeros(0, np.int32)
 
 
-def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim):
+def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None):
+    """The summation-density scheme, or with xsph_eps the continuity scheme
+    of the reference's dam-break example (examples/dam-break/dam_break.py:
+    184-241): Tait, SPHDensityRate (integrated rho on every array), momentum,
+    gravity, position stepping and XSPHCorrection on the fluid."""
     EQ, D, E, PF, POS, EF = R["EQ"], R["D"], R["E"], R["PF"], R["POS"], R["EF"]
     types = list(range(ntypes))
     vel = ["u", "v", "w"][:dim]
     pos = ["x", "y", "z"][:dim]
-    ops = [EQ.SPHOperation(D.SPHRho.withargs(), on_types=types, from_types=types,
-                           updates=["rho"], id="sd"),
-           EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
-                           updates=["p", "cs"], id="eos"),
-           EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta),
-                             on_types=[0], from_types=types, updates=vel, id="mom")]
+    if xsph_eps is None:
+        ops = [EQ.SPHOperation(D.SPHRho.withargs(), on_types=types, from_types=types,
+                               updates=["rho"], id="sd"),
+               EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
+                               updates=["p", "cs"], id="eos")]
+    else:
+        ops = [EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
+                               updates=["p", "cs"], id="eos"),
+               EQ.SPHIntegration(D.SPHDensityRate.withargs(hks=False), on_types=types,
+                                 from_types=types, updates=["rho"], id="density")]
+    ops.append(EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta),
+                                 on_types=[0], from_types=types, updates=vel, id="mom"))
     if gy:
         ops.append(EQ.SPHIntegration(EF.GravityForce.withargs(gy=gy), on_types=[0],
                                      updates=vel, id="grav"))
     ops.append(EQ.SPHIntegration(POS.PositionStepping.withargs(), on_types=[0],
                                  updates=pos, id="step"))
+    if xsph_eps is not None:
+        ops.append(EQ.SPHIntegration(R["X"].XSPHCorrection.withargs(eps=xsph_eps, hks=False),
+                                     on_types=[0], from_types=[0], updates=pos, id="xsph"))
     return ops
 
 
-def build_sim(R, arrays, types, params, dim):
+def build_sim(R, arrays, types, params, dim, xsph_eps=None):
     pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
     particles = R["P"].Particles(pas)
     kernel = R["K"].CubicSplineKernel(dim=dim)
     ops = scheme_ops(R, len(pas), params["c0"], params["rho0"], params["alpha"],
-                     params["beta"], params["eta"], params["gravity"][1], dim)
+                     params["beta"], params["eta"], params["gravity"][1], dim, xsph_eps)
     calcs = []
     for op in ops:
         calcs.extend(op.get_calcs(particles, kernel))
@@ -211,13 +225,73 @@ def dam(R):
     return out
 
 
+XSPH_EPS = 0.5   # XSPHCorrection's default eps
+
+
+def drop_cont(R):
+    """Elliptical drop with the continuity scheme: first-stage rates, then 10
+    steps of dt = 1e-5."""
+    arrays, types, params = W.elliptical_drop(dx=0.025)
+    pas, particles, integ = build_sim(R, arrays, types, params, 2, XSPH_EPS)
+    out = {f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS}
+    integ.save_initial_arrays()
+    integ.reset_accelerations(step=1)
+    integ.eval()
+    out.update({f"stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                for n in ("p", "cs", "_a_rho_1", "_a_u_1", "_a_v_1", "_a_x_1", "_a_y_1",
+                          "dt_fac")})
+    pas, particles, integ = build_sim(R, arrays, types, params, 2, XSPH_EPS)
+    for step in range(10):
+        particles.update()
+        integ.integrate(1e-5)
+        if step == 0:
+            out.update({f"step1_{k}": v for k, v in state(pas).items()})
+    out.update({f"step10_{k}": v for k, v in state(pas).items()})
+    return out
+
+
+def dam_cont(R):
+    """The dam break (dx = 0.05) with the continuity scheme of the
+    reference's dam-break example: first-stage rates of both arrays, then 5
+    CFL steps."""
+    arrays, types, params = W.dam_break(dx=0.05)
+    pas, particles, integ = build_sim(R, arrays, types, params, 2, XSPH_EPS)
+    out = {f"in{i}_{k}": np.asarray(arrays[i][k]) for i in range(2) for k in PROPS}
+    integ.save_initial_arrays()
+    integ.reset_accelerations(step=1)
+    integ.eval()
+    for i in range(2):
+        names = ("p", "cs", "_a_rho_1") + (("_a_u_1", "_a_v_1", "_a_x_1", "_a_y_1", "dt_fac")
+                                           if i == 0 else ())
+        out.update({f"stage0_{n}_{i}": np.asarray(pas[i].get(n), np.float64).copy()
+                    for n in names})
+    pas, particles, integ = build_sim(R, arrays, types, params, 2, XSPH_EPS)
+    tsf = R["T"].ViscousAndForceBasedTimeStep(cfl=params["cfl"], co=params["c0"],
+                                              particles=particles)
+    sv = _SolverView(integ, params["dt_initial"], 2)
+    dts = []
+    for _ in range(5):
+        sv.count += 1
+        particles.update()
+        dt = tsf.compute_time_step(sv)
+        integ.integrate(dt)
+        dts.append(dt)
+    out["dts"] = np.asarray(dts)
+    out.update({f"step5_{k}": v for k, v in state(pas).items()})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", default=os.path.join(ROOT, "_work", "refbuild"))
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", nargs="*", default=None, help="fixture names to write")
     a = ap.parse_args()
     R = ref_modules(a.build)
-    for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam)):
+    for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
+                     ("drop_cont", drop_cont), ("dam_cont", dam_cont)):
+        if a.only and name not in a.only:
+            continue
         data = fn(R)
         path = os.path.join(a.out, f"{name}.npz")
         np.savez_compressed(path, **data)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import OracleArray, OracleSystem
-from pysph_b200.engine import fluid_scheme
+from pysph_b200.engine import continuity_scheme, fluid_scheme
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 PROPS = ("x", "y", "z", "u", "v", "w", "m", "h", "rho", "p", "cs")
@@ -27,7 +27,9 @@ def oracle_for(g, prefixes, scheme, params, dim):
     arrs = [OracleArray(f"a{i}", **{k: g[f"{p}{k}"].copy() for k in PROPS})
             for i, p in enumerate(prefixes)]
     return OracleSystem(arrs, dim=dim, rho_src=scheme.rho_src, tait_on=scheme.tait_on,
-                        mom_src=scheme.mom_src, step_on=scheme.step_on, **params)
+                        mom_src=scheme.mom_src, step_on=scheme.step_on,
+                        rate_src=scheme.rate_src, xsph_src=scheme.xsph_src,
+                        xsph_eps=scheme.xsph_eps, **params)
 
 
 DROP = dict(c0=1400.0, rho0=1.0, gamma=7.0, alpha=0.1, beta=0.0, eta=0.1)
@@ -125,3 +127,59 @@ def test_square_functions():
     o.tait(0, 1.0, 1000.0, 7.0, p, cs)
     np.testing.assert_array_equal(p, g["tait_0"])
     np.testing.assert_array_equal(cs, g["tait_1"])
+
+
+# -- the continuity scheme (SPHDensityRate + XSPHCorrection) -------------------
+DAM = dict(c0=10.0 * np.sqrt(2 * 9.81 * 2.0), rho0=1000.0, gamma=7.0, alpha=0.1,
+           beta=0.0, eta=0.1, gravity=(0.0, -9.81, 0.0))
+
+
+def test_drop_continuity_first_stage_bit_exact():
+    g = load("drop_cont")
+    o = oracle_for(g, ["in_"], continuity_scheme(1, 0.5), DROP, 2)
+    o.update()
+    o.eval()
+    A = o.arrays[0]
+    for name, got in (("p", A.p), ("cs", A.cs), ("_a_rho_1", A.arho), ("_a_u_1", A.au),
+                      ("_a_v_1", A.av), ("_a_x_1", A.ax), ("_a_y_1", A.ay),
+                      ("dt_fac", A.dt_fac)):
+        np.testing.assert_array_equal(got, g[f"stage0_{name}"], err_msg=name)
+
+
+@pytest.mark.parametrize("steps", [1, 10])
+def test_drop_continuity_trajectory_bit_exact(steps):
+    g = load("drop_cont")
+    o = oracle_for(g, ["in_"], continuity_scheme(1, 0.5), DROP, 2)
+    for _ in range(steps):
+        o.pc_step(1e-5)
+    A = o.arrays[0]
+    for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+        np.testing.assert_array_equal(getattr(A, n), g[f"step{steps}_{n}_0"], err_msg=n)
+
+
+def test_dam_break_continuity_bit_exact():
+    """Walls integrate their density too (SPHDensityRate on every array);
+    XSPH from the fluid only; 5 CFL steps."""
+    g = load("dam_cont")
+    o = oracle_for(g, ["in0_", "in1_"], continuity_scheme(2, 0.5), DAM, 2)
+    o.update()
+    o.eval()
+    for i in range(2):
+        A = o.arrays[i]
+        names = (("p", A.p), ("cs", A.cs), ("_a_rho_1", A.arho))
+        if i == 0:
+            names += (("_a_u_1", A.au), ("_a_v_1", A.av), ("_a_x_1", A.ax),
+                      ("_a_y_1", A.ay), ("dt_fac", A.dt_fac))
+        for name, got in names:
+            np.testing.assert_array_equal(got, g[f"stage0_{name}_{i}"], err_msg=f"{name}_{i}")
+    o = oracle_for(g, ["in0_", "in1_"], continuity_scheme(2, 0.5), DAM, 2)
+    dts = []
+    for _ in range(5):
+        dt = o.cfl_time_step(0.3, DAM["c0"], 1e-4)
+        o.pc_step(dt)
+        dts.append(dt)
+    np.testing.assert_array_equal(np.asarray(dts), g["dts"])
+    for i in range(2):
+        for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+            np.testing.assert_array_equal(getattr(o.arrays[i], n), g[f"step5_{n}_{i}"],
+                                          err_msg=f"{n}_{i}")
