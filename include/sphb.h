@@ -81,6 +81,13 @@ typedef struct {
     uint32_t mom_src[SPHB_MAX_ARRAYS];
     uint32_t tait_on;
     uint32_t step_on;
+    /* continuity-equation scheme (the reference's dam-break / FluidSolver
+     * scheme): SPHDensityRate sources per dest array (its rho is integrated,
+     * buf.rho / rho0 must be set) and XSPHCorrection sources per dest array
+     * (added to the position rate of the integrated arrays); all zero for
+     * the summation-density scheme */
+    uint32_t rate_src[SPHB_MAX_ARRAYS];
+    uint32_t xsph_src[SPHB_MAX_ARRAYS];
 } sphb_config;
 
 /* Per-scene constants, written by the host once. */
@@ -105,6 +112,7 @@ typedef struct {
                                stay valid while no particle has moved
                                skin_max / 2 from where it was binned
                                (0: lists serve one stage only) */
+    double xsph_eps;        /* XSPHCorrection eps */
 } sphb_scene;
 
 /* Per-scene state, written by the kernels (host may seed dt, t, count). */
@@ -141,6 +149,8 @@ typedef struct {
     double *m, *h;
     int32_t *idx;           /* index inside the particle's ParticleArray */
     int32_t *tag;           /* 0 == LocalReal (S/base/particle_array.pxd:20) */
+    double *rho, *rho0;     /* integrated density and its stage-initial copy
+                               (continuity scheme; may be NULL otherwise) */
 } sphb_buffers;
 
 /* Fields recomputed every stage, in the current engine order.  Element type
@@ -165,6 +175,11 @@ typedef struct {
      * float2, 3D float4 {x, y, z, 0}.  sphb_pc_stage measures how far the
      * particles have moved from it. */
     void *anchor;
+    /* continuity scheme outputs of sphb_momentum (T[N]; may be NULL
+     * otherwise): _a_rho_1 of SPHDensityRate and the XSPHCorrection
+     * velocity that sphb_pc_stage adds to the position rate */
+    void *drho;
+    void *xu, *xv, *xw;
     int32_t list_cap;       /* slots per particle, 0 = no lists */
     int32_t pad0;
 } sphb_fields;
@@ -299,6 +314,10 @@ SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
 #define SPHB_DENSITY_EOS 1
 #define SPHB_DENSITY_USE_LIST 2
 #define SPHB_DENSITY_LIST_IF_VALID 4
+/* SPHB_DENSITY_LISTS_ONLY: no density, only the lists (continuity scheme,
+ * where the density is integrated): recorded over every pair function's
+ * sources when the pass would record, nothing otherwise. */
+#define SPHB_DENSITY_LISTS_ONLY 8
 
 /* Refresh the FP32 pair records (positions relative to each particle's
  * cell of the last bin, velocities) from the FP64 state without rebinning.
@@ -347,8 +366,9 @@ SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
  * engine[k] <-> user[seg-local idx[k]], for every scene's segment of that
  * array, with user arrays concatenated over scenes (user_offset[s]).
  * `field` names the engine field: 0..5 x..w, 6..11 x0..w0, 12 m, 13 h,
- * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac. Fields 14..20 are
- * scatter-only.  Gathering x..w, m or h marks the lists invalid
+ * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac; continuity scheme:
+ * 21 the integrated density (buf.rho), 22 its stage-initial copy, 23 its
+ * rate _a_rho_1.  Fields 17..20 and 23 are scatter-only.  Gathering x..w, m or h marks the lists invalid
  * (work.meta[2] = 0): the next SPHB_BIN_IF_NEEDED rebins, which also
  * rebuilds the FP32 pair records from the new state. */
 SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,

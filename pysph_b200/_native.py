@@ -29,6 +29,7 @@ ST_BAD_INDEX = 1 << 5
 ST_NBR_CAPACITY = 1 << 6
 BIN_IF_NEEDED = 4
 DENSITY_LIST_IF_VALID = 4
+DENSITY_LISTS_ONLY = 8
 STATUS_NAMES = {
     ST_GRID_OVERFLOW: "cell grid larger than cell_capacity",
     ST_NONFINITE_POS: "non-finite particle position",
@@ -43,7 +44,10 @@ STATUS_NAMES = {
 FIELDS = {"x": 0, "y": 1, "z": 2, "u": 3, "v": 4, "w": 5,
           "_x0": 6, "_y0": 7, "_z0": 8, "_u0": 9, "_v0": 10, "_w0": 11,
           "m": 12, "h": 13, "rho": 14, "p": 15, "cs": 16,
-          "_a_u_1": 17, "_a_v_1": 18, "_a_w_1": 19, "dt_fac": 20}
+          "_a_u_1": 17, "_a_v_1": 18, "_a_w_1": 19, "dt_fac": 20,
+          # continuity scheme: the integrated density, its stage-initial copy
+          # and its rate (_a_rho_1, scatter only)
+          "rho_state": 21, "_rho0": 22, "_a_rho_1": 23}
 
 i32, u32, f64, vp = ctypes.c_int32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p
 u64, i64 = ctypes.c_uint64, ctypes.c_int64
@@ -55,7 +59,8 @@ class Config(ctypes.Structure):
                 ("pair_block", i32), ("num_particles", i32),
                 ("cell_capacity", i32), ("list_batch", i32),
                 ("rho_src", u32 * MAX_ARRAYS), ("mom_src", u32 * MAX_ARRAYS),
-                ("tait_on", u32), ("step_on", u32)]
+                ("tait_on", u32), ("step_on", u32),
+                ("rate_src", u32 * MAX_ARRAYS), ("xsph_src", u32 * MAX_ARRAYS)]
 
 
 class Scene(ctypes.Structure):
@@ -64,7 +69,7 @@ class Scene(ctypes.Structure):
                 ("alpha", f64), ("beta", f64), ("eta", f64), ("g", f64 * 3),
                 ("cfl", f64), ("dt_initial", f64), ("static_lo", f64 * 3),
                 ("static_hi", f64 * 3), ("use_cfl", i32), ("uniform_h", i32),
-                ("skin_max", f64)]
+                ("skin_max", f64), ("xsph_eps", f64)]
 
 
 class SceneState(ctypes.Structure):
@@ -78,7 +83,7 @@ class Tile(ctypes.Structure):
 
 
 BUFFER_FIELDS = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0",
-                 "w0", "m", "h", "idx", "tag")
+                 "w0", "m", "h", "idx", "tag", "rho", "rho0")
 
 
 class Buffers(ctypes.Structure):
@@ -86,7 +91,7 @@ class Buffers(ctypes.Structure):
 
 
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
-               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor")
+               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor", "drho", "xu", "xv", "xw")
 FORCE_USE_LIST = 16
 DENSITY_EOS = 1
 DENSITY_USE_LIST = 2

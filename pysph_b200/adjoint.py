@@ -37,6 +37,8 @@ class Rollout:
     def __init__(self, arrays, params, scheme: Scheme, dim: int = 2, dt: float = 1e-5,
                  steps: int = 200, checkpoint_every: int = 20, precision: str = "fp32c",
                  device=None, lanes: int = 1, pair_block: int = 128):
+        if scheme.continuity:
+            raise NotImplementedError("the adjoint covers the summation-density scheme")
         if scheme.mom_src and set(scheme.step_on) != set(scheme.mom_src):
             raise ValueError("the integrated arrays must be the MomentumEquation dests")
         self.arrays = arrays

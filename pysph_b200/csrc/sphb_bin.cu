@@ -437,6 +437,8 @@ k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial, int 
     D.h[k] = h;
     D.idx[k] = S.idx[p];
     D.tag[k] = S.tag[p];
+    if (S.rho && D.rho) D.rho[k] = S.rho[p];   // integrated density (continuity)
+    if (move_initial && S.rho0 && D.rho0) D.rho0[k] = S.rho0[p];
     double z = 0.0, w = 0.0;
     if (DIM == 3) {
         z = S.z[p];
@@ -506,6 +508,8 @@ k_copy_back(const __grid_constant__ sphb_engine e, int cur, int move_initial, in
     D.h[k] = S.h[k];
     D.idx[k] = S.idx[k];
     D.tag[k] = S.tag[k];
+    if (S.rho && D.rho) D.rho[k] = S.rho[k];
+    if (move_initial && S.rho0 && D.rho0) D.rho0[k] = S.rho0[k];
     if (DIM == 3) {
         D.z[k] = S.z[k];
         D.w[k] = S.w[k];

@@ -30,11 +30,23 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     const bool reuse = (flags & SPHB_DENSITY_LIST_IF_VALID) && e.f.list_cap > 0;
     const bool from_list = e.f.list_cap > 0 && ((flags & SPHB_DENSITY_USE_LIST) ||
                                                 (reuse && e.work.meta[2] == 1));
+    // lists only (continuity scheme): record the lists after a rebin, no
+    // density; with the lists kept there is nothing to do
+    const bool lists_only = (flags & SPHB_DENSITY_LISTS_ONLY) != 0;
     const sphb_tile tl = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = tl.seg / A, a = tl.seg - s * A;
-    const uint32_t src = e.cfg.rho_src[a];
-    if (!((dest_mask >> a) & 1u) || src == 0u) return;  // block-uniform
+    const uint32_t rsrc = e.cfg.rho_src[a];           // SPHRho sources
+    const uint32_t lsrc = list_sources(e.cfg, a);     // sources the lists hold
+    if (!((dest_mask >> a) & 1u) || (lists_only ? lsrc : rsrc) == 0u) return;  // block-uniform
+    if (lists_only && (from_list || e.f.list_cap == 0)) return;
+    // recording, or reading the lists: every list source; a cell search
+    // without recording: the SPHRho sources alone
+    const bool records = e.f.list_cap > 0 && !from_list;
+    const uint32_t src = (records || from_list) ? lsrc : rsrc;
+    // neighbours outside the SPHRho sources are skipped by the sum
+    const bool filt = src != rsrc;
+    const SegBounds seg(e, s);
     const int lane = threadIdx.x & (LANES - 1);
     const int k = tl.begin + (int)(threadIdx.x / LANES);
     const bool active = k < tl.end;
@@ -93,6 +105,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 Rec r;
                 r.ok = en.j < N;
                 const int j = r.ok ? en.j : k;
+                if (filt) r.ok = r.ok && ((rsrc >> seg.array_of(j)) & 1u);
                 r.g = __ldg(geo + j);
                 r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
                 r.o = en.o;
@@ -115,7 +128,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             auto pass = [&](auto uniform) {
                 constexpr bool UH = decltype(uniform)::value;
                 auto use = [&](const Rec &r, float r2) {
-                    if (!(r.ok && r2 < rad2)) return;
+                    if (lists_only || !(r.ok && r2 < rad2)) return;
                     float ih = ihk, fac = fack;
                     if (!UH) {
                         const float hj = DIM == 3 ? r.g.w : r.g.z;
@@ -174,7 +187,9 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     const double d2 = dist2_ref<DIM>(dx, dy, dz);
                     if (d2 < radl2) {
                         record(j, o, oy, oz);
-                        if (d2 < rad2) {
+                        const bool sums =
+                            !lists_only && (!filt || ((rsrc >> seg.array_of(j)) & 1u));
+                        if (sums && d2 < rad2) {
                             const double hab = 0.5 * (hk + __ldg(B.h + j));
                             sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
                             ++np;
@@ -188,7 +203,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     }
 
     if (active && nbr) e.f.nbr_cnt[(size_t)lane * N + k] = cnt <= cap_lane ? cnt : -1;
-    if (active && lane == 0) {
+    if (active && lane == 0 && !lists_only) {
         const bool real = e.buf[cur].tag[k] == 0;
         if (!real) rho = 0.0;
         const bool eos = with_eos && ((e.cfg.tait_on >> a) & 1u);
@@ -233,9 +248,14 @@ k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
     const sphb_scene &sc = e.scene[s];
-    const bool real = e.buf[cur].tag[k] == 0;
+    const sphb_buffers &B = e.buf[cur];
+    const bool real = B.tag[k] == 0;
+    // continuity scheme: the density is the integrated state, which the
+    // pair passes then read from the same place as a summed one
+    const bool state = B.rho != nullptr && e.cfg.rate_src[a] != 0u;
     double rho;
-    if constexpr (F32) rho = ((const float4 *)e.f.thermo)[k].x;
+    if (state) rho = B.rho[k];
+    else if constexpr (F32) rho = ((const float4 *)e.f.thermo)[k].x;
     else rho = ((const double *)e.f.rho)[k];
     double p = 0.0, c = 0.0;
     if (real) {
@@ -246,13 +266,17 @@ k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
     if constexpr (F32) {
         float4 *th = (float4 *)e.f.thermo;
         float4 v = th[k];
+        if (state) v.x = (float)rho;
         v.y = (float)p;
         v.z = (float)c;
         v.w = v.x != 0.f ? v.y / (v.x * v.x) : 0.f;
         th[k] = v;
+        if (state && !(isfinite(v.x) && isfinite(v.y))) flag(e, SPHB_ST_NONFINITE_RHO);
     } else {
+        if (state) ((double *)e.f.rho)[k] = rho;
         ((double *)e.f.p)[k] = p;
         ((double *)e.f.cs)[k] = c;
+        if (state && !(isfinite(rho) && isfinite(p))) flag(e, SPHB_ST_NONFINITE_RHO);
     }
 }
 
@@ -352,6 +376,9 @@ extern "C" int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
     if ((rc = check_pair_cfg(e))) return rc;
+    if (with_eos & ~(SPHB_DENSITY_EOS | SPHB_DENSITY_USE_LIST | SPHB_DENSITY_LIST_IF_VALID |
+                     SPHB_DENSITY_LISTS_ONLY))
+        return SPHB_ERR_ARG;
     if (e->num_pair_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const sphb_config &c = e->cfg;

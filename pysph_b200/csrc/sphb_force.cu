@@ -21,7 +21,10 @@ namespace sphb {
 int check_engine_public(const sphb_engine *e, int cur);
 int check_pair_cfg(const sphb_engine *e);
 
-template <int DIM, bool F32, int LANES, int R, int U>
+// CONT: the continuity scheme's pair terms too -- SPHDensityRate
+// (density_funcs.pyx:119-156) and XSPHCorrection (xsph_funcs.pyx:40-86),
+// each over its own sources, in the same traversal as the momentum.
+template <int DIM, bool F32, int LANES, int R, int U, bool CONT>
 __global__ void __launch_bounds__(256)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
@@ -29,8 +32,15 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
     const sphb_tile tl = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = tl.seg / A, a = tl.seg - s * A;
-    const uint32_t src = e.cfg.mom_src[a];
-    if (!((dest_mask >> a) & 1u) || src == 0u) return;  // block-uniform
+    const uint32_t mm = e.cfg.mom_src[a];
+    const uint32_t rm = CONT ? e.cfg.rate_src[a] : 0u;
+    const uint32_t xm = CONT ? e.cfg.xsph_src[a] : 0u;
+    if (!((dest_mask >> a) & 1u) || (mm | rm | xm) == 0u) return;  // block-uniform
+    // sources visited: those the lists hold (every pair function's); each
+    // term keeps to its own sources when they differ
+    const uint32_t src = CONT ? list_sources(e.cfg, a) : mm;
+    const bool filt = CONT && ((mm && mm != src) || (rm && rm != src) || (xm && xm != src));
+    const SegBounds seg(e, s);
     const int lane = threadIdx.x & (LANES - 1);
     const int k = tl.begin + (int)(threadIdx.x / LANES);
     const bool active = k < tl.end;
@@ -40,15 +50,18 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
     const sphb_scene &sc = e.scene[s];
     const int *__restrict__ start = e.work.start;
     const bool visc = (mode & 15) == 0;
-    // reuse the density pass's lists when they were built from the same sources
+    // reuse the density pass's lists (recorded over list_sources); without
+    // the per-source filter they must hold the momentum sources exactly
     const bool use_list = (mode & SPHB_FORCE_USE_LIST) && e.f.list_cap > 0 && e.f.nbr &&
-                          e.f.nbr_cnt && e.cfg.rho_src[a] == e.cfg.mom_src[a];
+                          e.f.nbr_cnt && (CONT || list_sources(e.cfg, a) == mm);
     unsigned int np = 0;   // pairs of this thread
     double acc[3] = {0.0, 0.0, 0.0};
     double dtf = 0.0;
+    double drho = 0.0, xs[3] = {0.0, 0.0, 0.0};   // continuity scheme sums
 
     if constexpr (F32) {
         Kahan ax, ay, az;
+        Kahan kr, kxx, kxy, kxz;   // density rate, XSPH velocity (CONT)
         float dtmax = 0.f;
         if (active) {
             const int N = e.cfg.num_particles;
@@ -83,16 +96,18 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             struct Rec {
                 float4 g, t;
                 float vx, vy, vz, m, o, dy, dz;
+                uint32_t bit;   // the source's array as a mask bit (CONT)
                 bool ok;
             };
             auto load = [&](const EntryF &en) {
                 Rec r;
                 r.ok = en.j < N;
                 const int j = r.ok ? en.j : k;
+                r.bit = filt ? 1u << seg.array_of(j) : ~0u;
                 r.g = __ldg(geo + j);
                 r.t = __ldg(th + j);
                 r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
-                if (visc) {
+                if (visc || CONT) {
                     if (DIM == 2) {
                         const float2 vv = __ldg((const float2 *)e.f.vel + j);
                         r.vx = vv.x;
@@ -125,6 +140,9 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     }
                     if (!(r.ok && r2 < rad2)) return;
                     ++np;
+                    const bool mom_on = !CONT || (mm & r.bit);
+                    const bool rate_on = CONT && (rm & r.bit);
+                    const bool xs_on = CONT && (xm & r.bit);
                     float hab = hk, ih = ihk, fih = fihk, eh2 = eh2k;
                     if (!UH) {
                         const float hj = DIM == 3 ? r.g.w : r.g.z;
@@ -134,10 +152,27 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         eh2 = eta2 * hab * hab;
                     }
                     float tmp = tk.w + r.t.w;   // P_a/rho_a^2 + P_b/rho_b^2
+                    const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
+                    float dot = vx * rx + vy * ry;
+                    if (DIM == 3) dot += vz * rz;
+                    // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
+                    const float ir = rsqrtf(fmaxf(r2, 1e-30f));
+                    const float q = r2 * ir * ih;
+                    const float gw = gw_cubic_bf(q, ir, ih, fih);
+                    if (CONT) {
+                        // drho_a += m_b (v_a - v_b) . grad_a W
+                        if (rate_on) kr.add(r.m * (dot * gw));
+                        // XSPH: eps m_b W_ab (v_b - v_a) / rho_ab (eps at the end)
+                        if (xs_on) {
+                            const float w = w_cubic_bf(q, fih * hab);
+                            const float temp = __fdividef(r.m * w, 0.5f * (tk.x + r.t.x));
+                            kxx.add(-temp * vx);
+                            kxy.add(-temp * vy);
+                            if (DIM == 3) kxz.add(-temp * vz);
+                        }
+                        if (!mom_on) return;
+                    }
                     if (visc) {
-                        const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
-                        float dot = vx * rx + vy * ry;
-                        if (DIM == 3) dot += vz * rz;
                         const float mu = __fdividef(hab * dot, r2 + eh2);
                         dtmax = fmaxf(dtmax, fabsf(mu));
                         // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
@@ -147,9 +182,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         const float rhoab = 0.5f * (tk.x + r.t.x);
                         tmp += __fdividef(-alpha * cab * mn + beta * mn * mn, rhoab);
                     }
-                    // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
-                    const float ir = rsqrtf(fmaxf(r2, 1e-30f));
-                    const float f = -r.m * tmp * gw_cubic_bf(r2 * ir * ih, ir, ih, fih);
+                    const float f = -r.m * tmp * gw;
                     ax.add(f * rx);
                     ay.add(f * ry);
                     if (DIM == 3) az.add(f * rz);
@@ -182,6 +215,21 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         acc[1] = ay.value();
         acc[2] = az.value();
         dtf = dtmax;
+        if (CONT) {
+#pragma unroll
+            for (int o = LANES / 2; o > 0; o >>= 1) {
+                kr.merge(__shfl_xor_sync(0xffffffffu, kr.sum, o), __shfl_xor_sync(0xffffffffu, kr.c, o));
+                kxx.merge(__shfl_xor_sync(0xffffffffu, kxx.sum, o), __shfl_xor_sync(0xffffffffu, kxx.c, o));
+                kxy.merge(__shfl_xor_sync(0xffffffffu, kxy.sum, o), __shfl_xor_sync(0xffffffffu, kxy.c, o));
+                if (DIM == 3)
+                    kxz.merge(__shfl_xor_sync(0xffffffffu, kxz.sum, o),
+                              __shfl_xor_sync(0xffffffffu, kxz.c, o));
+            }
+            drho = kr.value();
+            xs[0] = kxx.value() * sc.xsph_eps;
+            xs[1] = kxy.value() * sc.xsph_eps;
+            xs[2] = kxz.value() * sc.xsph_eps;
+        }
     } else {
         if (active) {
             const sphb_buffers &B = e.buf[cur];
@@ -207,9 +255,30 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     const double rab2 = dist2_ref<DIM>(rx, ry, rz);
                     if (!(rab2 < rad2)) return;
                     ++np;
+                    const uint32_t bit = filt ? 1u << seg.array_of(j) : ~0u;
                     const double hab = 0.5 * (hk + __ldg(B.h + j));
                     const double rhob = __ldg(rho + j), Pb = __ldg(pr + j);
                     const double mb = __ldg(B.m + j);
+                    if (CONT) {
+                        const double vbx = __ldg(B.u + j), vby = __ldg(B.v + j);
+                        const double vbz = DIM == 3 ? __ldg(B.w + j) : 0.0;
+                        if (rm & bit) {
+                            // SPHDensityRate: ((v_a - v_b) . grad_a W) m_b
+                            const double g = gw_cubic_d<DIM>(sqrt(rab2), hab);
+                            double d = (uk - vbx) * (rx * g) + (vk - vby) * (ry * g);
+                            if (DIM == 3) d += (wk - vbz) * (rz * g);
+                            drho += d * mb;
+                        }
+                        if (xm & bit) {
+                            // XSPHCorrection: m_b W_ab / rho_ab (v_b - v_a) eps
+                            const double w = w_cubic_d<DIM>(sqrt(rab2), hab);
+                            const double temp = mb * w / (0.5 * (rhob + rhoa));
+                            xs[0] += temp * (vbx - uk) * sc.xsph_eps;
+                            xs[1] += temp * (vby - vk) * sc.xsph_eps;
+                            if (DIM == 3) xs[2] += temp * (vbz - wk) * sc.xsph_eps;
+                        }
+                        if (!(mm & bit)) return;
+                    }
                     double tmp = Pa * rhoa2 + Pb * (1.0 / (rhob * rhob));
                     if (visc) {
                         const double vx = uk - __ldg(B.u + j);
@@ -242,11 +311,33 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             acc[1] += __shfl_xor_sync(0xffffffffu, acc[1], o);
             if (DIM == 3) acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], o);
             dtf = fmax(dtf, __shfl_xor_sync(0xffffffffu, dtf, o));
+            if (CONT) {
+                drho += __shfl_xor_sync(0xffffffffu, drho, o);
+                for (int d = 0; d < DIM; ++d) xs[d] += __shfl_xor_sync(0xffffffffu, xs[d], o);
+            }
         }
     }
 
     double a2 = 0.0, dtf_out = 0.0;
-    if (active && lane == 0) {
+    if (CONT && active && lane == 0) {
+        // non-LocalReal dests get 0 (S/sph/sph_func.pyx:220-227)
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (rm) {
+            const double v = real ? drho : 0.0;
+            if (F32) ((float *)e.f.drho)[k] = (float)v;
+            else ((double *)e.f.drho)[k] = v;
+            if (!isfinite(v)) flag(e, SPHB_ST_NONFINITE_RHO);
+        }
+        if (xm) {
+            void *xo[3] = {e.f.xu, e.f.xv, e.f.xw};
+            for (int d = 0; d < DIM; ++d) {
+                const double v = real ? xs[d] : 0.0;
+                if (F32) ((float *)xo[d])[k] = (float)v;
+                else ((double *)xo[d])[k] = v;
+            }
+        }
+    }
+    if (active && lane == 0 && mm) {
         const bool real = e.buf[cur].tag[k] == 0;
         if (real) {
             if (with_gravity) {
@@ -292,10 +383,14 @@ static void launch_force(const sphb_engine &e, int cur, uint32_t dm, int grav,
     const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
     // the load-ahead depth only shapes the FP32C list loop
     const int u = (F32 && e.cfg.list_batch == 2) ? 2 : 4;
-#define SPHB_L(LV, RV)                                                                    \
-    do {                                                                                  \
-        if (u == 2) k_force<DIM, F32, LV, RV, 2><<<g, b, 0, st>>>(e, cur, dm, grav, mode); \
-        else k_force<DIM, F32, LV, RV, 4><<<g, b, 0, st>>>(e, cur, dm, grav, mode);        \
+    bool cont = false;
+    for (int a = 0; a < SPHB_MAX_ARRAYS; ++a) cont = cont || e.cfg.rate_src[a] || e.cfg.xsph_src[a];
+#define SPHB_L(LV, RV)                                                                         \
+    do {                                                                                       \
+        if (cont) k_force<DIM, F32, LV, RV, 4, true><<<g, b, 0, st>>>(e, cur, dm, grav, mode);  \
+        else if (u == 2)                                                                       \
+            k_force<DIM, F32, LV, RV, 2, false><<<g, b, 0, st>>>(e, cur, dm, grav, mode);       \
+        else k_force<DIM, F32, LV, RV, 4, false><<<g, b, 0, st>>>(e, cur, dm, grav, mode);      \
     } while (0)
     switch (e.cfg.lanes * 10 + e.cfg.stencil) {
     case 11: SPHB_L(1, 1); break;
@@ -324,6 +419,11 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
         return SPHB_ERR_ARG;
     if (!e->f.au || !e->f.av || (e->cfg.dim == 3 && !e->f.aw)) return SPHB_ERR_ARG;
     if ((mode & 15) == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
+    for (int a = 0; a < SPHB_MAX_ARRAYS; ++a) {
+        if (e->cfg.rate_src[a] && !e->f.drho) return SPHB_ERR_ARG;
+        if (e->cfg.xsph_src[a] && (!e->f.xu || !e->f.xv || (e->cfg.dim == 3 && !e->f.xw)))
+            return SPHB_ERR_ARG;
+    }
     if (e->num_pair_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const sphb_config &c = e->cfg;

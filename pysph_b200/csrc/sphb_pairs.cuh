@@ -91,6 +91,32 @@ __device__ __forceinline__ void nbr_unpack(uint32_t v, int &j, int &o, int &dy, 
     dz = DIM == 3 ? (int)((v >> (B + 6)) & 7u) - 2 : 0;
 }
 
+// Sources a dest array's neighbour lists are recorded over: every source
+// of every pair function on it (SPHRho, MomentumEquation, SPHDensityRate,
+// XSPHCorrection), so one list serves all of them.
+__device__ __forceinline__ uint32_t list_sources(const sphb_config &c, int a)
+{
+    return c.rho_src[a] | c.mom_src[a] | c.rate_src[a] | c.xsph_src[a];
+}
+
+// Array index of engine position j inside scene s (segments of a scene are
+// consecutive: seg_offset[s*A + b] is where array b starts).
+struct SegBounds {
+    int b1, b2, b3;   // starts of arrays 1, 2, 3 (INT_MAX when absent)
+    __device__ __forceinline__ SegBounds(const sphb_engine &e, int s)
+    {
+        const int A = e.cfg.num_arrays;
+        const int *so = e.seg_offset + s * A;
+        b1 = A > 1 ? so[1] : 0x7fffffff;
+        b2 = A > 2 ? so[2] : 0x7fffffff;
+        b3 = A > 3 ? so[3] : 0x7fffffff;
+    }
+    __device__ __forceinline__ int array_of(int j) const
+    {
+        return (j >= b1) + (j >= b2) + (j >= b3);
+    }
+};
+
 // A list entry unpacked, with the cell offsets as floats.  The 3-bit fields
 // become floats through the exponent of 2^23 (exact, no conversion
 // instruction): float(0x4B000000 | b) = 2^23 + b.

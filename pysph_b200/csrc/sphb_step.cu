@@ -64,12 +64,27 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
             e.sstate[q].max_acc2 = 0ull;
         }
     }
-    if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
     const int k = t.begin + threadIdx.x;
     const bool active = k < t.end;
     const sphb_buffers &B = e.buf[cur];
     const sphb_scene_state &st = e.sstate[s];
     const double dt2 = st.dt / 2;
+    // continuity scheme: the density of every SPHDensityRate dest is
+    // integrated like the other stepped properties
+    if (active && B.rho && B.rho0 && e.f.drho && e.cfg.rate_src[a]) {
+        const double dr = F32 ? (double)((const float *)e.f.drho)[k] : ((const double *)e.f.drho)[k];
+        if (stage == 0) {
+            const double r0 = B.rho[k];
+            B.rho0[k] = r0;
+            B.rho[k] = axpy_rn(r0, dr, dt2);
+        } else {
+            const double r0 = B.rho0[k];
+            B.rho[k] = __dadd_rn(2 * axpy_rn(r0, dr, dt2), -r0);
+        }
+    }
+    if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
+    // XSPHCorrection adds to PositionStepping's rate
+    const bool xsph = e.cfg.xsph_src[a] && e.f.xu && e.f.xv && (DIM == 2 || e.f.xw);
     const bool rec = F32 && e.f.geo && e.f.vel;   // FP32 pair records
     const bool disp = e.f.anchor != nullptr;      // displacement check
     float d2 = 0.f;
@@ -81,11 +96,15 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         double *V0[3] = {B.u0, B.v0, B.w0};
         const bool real = B.tag[k] == 0;
         double f[3] = {0.0, 0.0, 0.0}, x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
-        double x0[3] = {0.0, 0.0, 0.0}, v0[3] = {0.0, 0.0, 0.0};
+        double x0[3] = {0.0, 0.0, 0.0}, v0[3] = {0.0, 0.0, 0.0}, xv[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const void *fa = d == 0 ? e.f.au : (d == 1 ? e.f.av : e.f.aw);
             f[d] = F32 ? (double)((const float *)fa)[k] : ((const double *)fa)[k];
+            if (xsph) {
+                const void *xa = d == 0 ? e.f.xu : (d == 1 ? e.f.xv : e.f.xw);
+                xv[d] = F32 ? (double)((const float *)xa)[k] : ((const double *)xa)[k];
+            }
             x[d] = X[d][k];
             v[d] = V[d][k];
             if (stage == 1) {
@@ -113,7 +132,8 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const double fd = real ? f[d] : 0.0;
-            const double fx = real ? v[d] : 0.0;  // PositionStepping: F_x = u
+            // PositionStepping: F_x = u (+ the XSPH velocity)
+            const double fx = real ? (xsph ? __dadd_rn(v[d], xv[d]) : v[d]) : 0.0;
             if (stage == 0) {
                 X0[d][k] = x[d];
                 V0[d][k] = v[d];
@@ -230,6 +250,8 @@ __device__ __forceinline__ double *field_ptr(const sphb_engine &e, int cur, int 
     case 11: return B.w0;
     case 12: return B.m;
     case 13: return B.h;
+    case 21: return B.rho;
+    case 22: return B.rho0;
     }
     return nullptr;
 }
@@ -260,10 +282,14 @@ k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
         return;
     }
     const long long ui = (long long)user_offset[s] + li;
-    if (field <= 13) {
+    if (field <= 13 || field == 21 || field == 22) {
         double *f = field_ptr<F32>(e, cur, field);
         if (dir == 0) f[k] = user[ui];
         else user[ui] = f[k];
+        return;
+    }
+    if (field == 23) {   // _a_rho_1, scatter only
+        user[ui] = F32 ? (double)((const float *)e.f.drho)[k] : ((const double *)e.f.drho)[k];
         return;
     }
     if (F32) {
@@ -423,15 +449,15 @@ extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
     if (!user || !user_offset || array < 0 || array >= e->cfg.num_arrays) return SPHB_ERR_ARG;
-    if (field < 0 || field > 20 || (dir != 0 && dir != 1)) return SPHB_ERR_ARG;
-    if (dir == 0 && field >= 17) return SPHB_ERR_ARG;
+    if (field < 0 || field > 23 || (dir != 0 && dir != 1)) return SPHB_ERR_ARG;
+    if (dir == 0 && ((field >= 17 && field <= 20) || field == 23)) return SPHB_ERR_ARG;
     const bool f32 = e->cfg.precision == SPHB_FP32C;
     const sphb_buffers &B = e->buf[cur];
-    const void *ptrs[21] = {B.x, B.y, B.z, B.u, B.v, B.w, B.x0, B.y0, B.z0, B.u0,
+    const void *ptrs[24] = {B.x, B.y, B.z, B.u, B.v, B.w, B.x0, B.y0, B.z0, B.u0,
                             B.v0, B.w0, B.m, B.h,
                             f32 ? e->f.thermo : e->f.rho, f32 ? e->f.thermo : e->f.p,
                             f32 ? e->f.thermo : e->f.cs, e->f.au, e->f.av, e->f.aw,
-                            e->f.dt_fac};
+                            e->f.dt_fac, B.rho, B.rho0, e->f.drho};
     if (!ptrs[field] || !B.idx) return SPHB_ERR_ARG;
     if (e->num_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;

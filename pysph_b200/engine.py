@@ -101,6 +101,14 @@ class Scheme:
     def mom_dests(self) -> int:
         return sum(1 << d for d, s in self.mom_src.items() if s)
 
+    @property
+    def pair_dests(self) -> int:
+        """Arrays that are the dest of any pair function."""
+        m = 0
+        for srcs in (self.rho_src, self.mom_src, self.rate_src, self.xsph_src):
+            m |= sum(1 << d for d, s in srcs.items() if s)
+        return m
+
 
 def fluid_scheme(num_arrays: int = 1) -> Scheme:
     """Array 0 is the fluid; arrays 1.. are fixed walls.  SPHRho and Tait on
@@ -231,6 +239,7 @@ class Engine:
             # list radius (support + skin)(1 + 1e-5) must stay within R cells
             t.skin_max = (p.radius_scale * max_h * (self.skin_margin - 1e-4)
                           if self.skin_margin else 0.0)
+            t.xsph_eps = self.scheme.xsph_eps
             t.radius_scale = p.radius_scale
             t.h_min = h_min
             t.c0, t.rho0, t.gamma = p.c0, p.rho0, p.gamma
@@ -283,6 +292,10 @@ class Engine:
                     b[name] = torch.zeros(N, **f64)
             b["idx"] = torch.zeros(N, **i32)
             b["tag"] = torch.zeros(N, **i32)
+            # the continuity equation integrates the density
+            cont = self.scheme.continuity
+            b["rho"] = torch.zeros(N, **f64) if cont else None
+            b["rho0"] = torch.zeros(N, **f64) if cont else None
             self.bufs.append(b)
         f = {}
         if self.f32:
@@ -302,6 +315,12 @@ class Engine:
             f["aw"] = torch.zeros(N, **f64) if dim == 3 else None
             f["geo"] = f["mass"] = f["vel"] = f["thermo"] = None
         f["cell"] = torch.zeros(N, **i32)
+        # continuity scheme outputs of the pair pass: _a_rho_1, XSPH velocity
+        ft = dict(dtype=torch.float32 if self.f32 else torch.float64, device=dev)
+        f["drho"] = torch.zeros(N, **ft) if self.scheme.continuity else None
+        xs = any(self.scheme.xsph_src.values())
+        for c in ("xu", "xv", "xw"):
+            f[c] = torch.zeros(N, **ft) if xs and (c != "xw" or dim == 3) else None
         # per-stage neighbour lists (density pass writes, force pass reads)
         idx_bits = 26 if dim == 2 else 23
         self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
@@ -348,6 +367,10 @@ class Engine:
             cfg.mom_src[a] = mom[a]
         cfg.tait_on = tait
         cfg.step_on = step
+        rate, xs = self.scheme.masks2()
+        for a in range(nat.MAX_ARRAYS):
+            cfg.rate_src[a] = rate[a]
+            cfg.xsph_src[a] = xs[a]
         return cfg
 
     def _make_tiles(self, tile_size):
@@ -555,7 +578,8 @@ class Engine:
 
     def momentum(self, dest_mask=None, gravity=True, mode=0):
         if dest_mask is None:
-            dest_mask = self.scheme.mom_dests
+            dest_mask = (self.scheme.pair_dests if self.scheme.continuity
+                         else self.scheme.mom_dests)
         if not mode & nat.FORCE_USE_LIST:
             self._sync_cells()
         self.call("sphb_momentum", self.cur, dest_mask, 1 if gravity else 0, mode)
@@ -573,11 +597,21 @@ class Engine:
         MomentumEquation (or SPHPressureGradient) + GravityForce.  The
         density pass records the neighbour lists the force pass reads; with
         list reuse it reads the lists the last rebin decision kept."""
-        flags = nat.DENSITY_EOS | (nat.DENSITY_LIST_IF_VALID if self.step_lists else 0)
-        self.call("sphb_density", self.cur, self.scheme.rho_dests, flags)
+        reuse = nat.DENSITY_LIST_IF_VALID if self.step_lists else 0
+        mode = self.force_mode | (nat.FORCE_USE_LIST if self.list_cap else 0)
+        if self.scheme.continuity:
+            # TaitEquation on the integrated density, then one pair pass:
+            # SPHDensityRate + MomentumEquation + XSPHCorrection; the density
+            # kernel only records the lists (after a rebin)
+            self.call("sphb_density", self.cur, self.scheme.pair_dests,
+                      nat.DENSITY_LISTS_ONLY | reuse)
+            self.tait()
+            self.call("sphb_momentum", self.cur, self.scheme.pair_dests, 1, mode)
+            return
+        self.call("sphb_density", self.cur, self.scheme.rho_dests, nat.DENSITY_EOS | reuse)
         if self.tait_only_mask:
             self.tait(self.tait_only_mask)
-        self.momentum(mode=self.force_mode | (nat.FORCE_USE_LIST if self.list_cap else 0))
+        self.momentum(mode=mode)
 
     def pc_step(self, on_half=None):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
@@ -651,7 +685,7 @@ class Engine:
         v = values.to(device=self.device, dtype=torch.float64).contiguous()
         if v.numel() != self.user_n[array]:
             raise ValueError("size mismatch")
-        self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 0,
+        self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 0,
                   v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it
         if name in ("x", "y", "z", "u", "v", "w", "m", "h"):
@@ -663,9 +697,17 @@ class Engine:
         """Engine -> user-order FP64 tensor (scenes concatenated)."""
         if out is None:
             out = torch.empty(self.user_n[array], dtype=torch.float64, device=self.device)
-        self.call("sphb_exchange", self.cur, array, nat.FIELDS[_canon(name)], 1,
+        self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 1,
                   out.data_ptr(), self.user_offset[array].data_ptr())
         return out
+
+    def _field_id(self, array: int, name: str) -> int:
+        """Exchange id of a property.  With the continuity equation the
+        density of an SPHDensityRate dest is the integrated state."""
+        name = _canon(name)
+        if name == "rho" and self.scheme.rate_src.get(array):
+            return nat.FIELDS["rho_state"]
+        return nat.FIELDS[name]
 
     def exchange_tag(self, array: int, values: torch.Tensor, direction: int):
         v = values.to(device=self.device, dtype=torch.int32).contiguous()

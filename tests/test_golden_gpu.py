@@ -127,3 +127,75 @@ def test_dam_break_cfl(precision):
         rho = eng.get(i, "rho").cpu().numpy()
         ref = g[f"step5_rho_{i}"]
         assert np.max(np.abs(rho - ref) / ref) <= rtol
+
+
+# -- the continuity scheme (SPHDensityRate + XSPHCorrection) -------------------
+from pysph_b200.engine import continuity_scheme  # noqa: E402
+
+DAM = dict(c0=10.0 * np.sqrt(2 * 9.81 * 2.0), rho0=1000.0, gamma=7.0, alpha=0.1,
+           beta=0.0, eta=0.1, gravity=(0.0, -9.81, 0.0), cfl=0.3, dt_initial=1e-4)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_drop_continuity_first_stage(precision):
+    """One evaluation of the continuity scheme: Tait on the given density,
+    then SPHDensityRate + MomentumEquation + XSPH in one pair pass."""
+    g = load("drop_cont")
+    eng = Engine([(arrays(g, ["in_"]), DROP)], continuity_scheme(1, 0.5), dim=2,
+                 precision=precision)
+    eng.eval_stage()
+    eng.check_status()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    for n in ("p", "cs"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"stage0_{n}"]
+        assert np.max(np.abs(got - ref)) <= rtol * np.max(np.abs(ref)) + 1e-300, n
+    atol = 1e-10 if precision == "fp64" else 1e-4
+    for n in ("_a_rho_1", "_a_u_1", "_a_v_1"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"stage0_{n}"]
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, n
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_drop_continuity_ten_steps(precision):
+    """Integrated density and XSPH-corrected positions over 10 steps."""
+    g = load("drop_cont")
+    eng = Engine([(arrays(g, ["in_"]), DROP)], continuity_scheme(1, 0.5), dim=2,
+                 precision=precision)
+    for _ in range(10):
+        eng.pc_step()
+    eng.check_status()
+    dx = 0.025
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"step10_{n}_0"])) / dx <= tol, n
+    rho = eng.get(0, "rho").cpu().numpy()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.max(np.abs(rho - g["step10_rho_0"]) / g["step10_rho_0"]) <= rtol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dam_break_continuity_cfl(precision):
+    """The reference's dam-break scheme: walls integrate their density too;
+    5 CFL steps (dt sequence, positions, both arrays' densities)."""
+    g = load("dam_cont")
+    eng = Engine([(arrays(g, ["in0_", "in1_"]), DAM)], continuity_scheme(2, 0.5), dim=2,
+                 precision=precision)
+    dts = []
+    for _ in range(5):
+        eng.pc_step()
+        dts.append(eng.scene_state()[0].dt)
+    eng.check_status()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    np.testing.assert_allclose(dts, g["dts"], rtol=rtol)
+    dx = 0.05
+    ptol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"step5_{n}_0"])) / dx <= ptol, n
+    for i in range(2):
+        rho = eng.get(i, "rho").cpu().numpy()
+        ref = g[f"step5_rho_{i}"]
+        assert np.max(np.abs(rho - ref) / ref) <= rtol, i
