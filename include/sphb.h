@@ -368,7 +368,8 @@ SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
  * `field` names the engine field: 0..5 x..w, 6..11 x0..w0, 12 m, 13 h,
  * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac; continuity scheme:
  * 21 the integrated density (buf.rho), 22 its stage-initial copy, 23 its
- * rate _a_rho_1.  Fields 17..20 and 23 are scatter-only.  Gathering x..w, m or h marks the lists invalid
+ * rate _a_rho_1; 24..26 the XSPHCorrection velocity.  Fields 17..20 and
+ * 23..26 are scatter-only.  Gathering x..w, m or h marks the lists invalid
  * (work.meta[2] = 0): the next SPHB_BIN_IF_NEEDED rebins, which also
  * rebuilds the FP32 pair records from the new state. */
 SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,

@@ -47,7 +47,9 @@ FIELDS = {"x": 0, "y": 1, "z": 2, "u": 3, "v": 4, "w": 5,
           "_a_u_1": 17, "_a_v_1": 18, "_a_w_1": 19, "dt_fac": 20,
           # continuity scheme: the integrated density, its stage-initial copy
           # and its rate (_a_rho_1, scatter only)
-          "rho_state": 21, "_rho0": 22, "_a_rho_1": 23}
+          "rho_state": 21, "_rho0": 22, "_a_rho_1": 23,
+          # XSPHCorrection velocity (scatter only)
+          "_xsph_u": 24, "_xsph_v": 25, "_xsph_w": 26}
 
 i32, u32, f64, vp = ctypes.c_int32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p
 u64, i64 = ctypes.c_uint64, ctypes.c_int64

@@ -288,8 +288,10 @@ k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
         else user[ui] = f[k];
         return;
     }
-    if (field == 23) {   // _a_rho_1, scatter only
-        user[ui] = F32 ? (double)((const float *)e.f.drho)[k] : ((const double *)e.f.drho)[k];
+    if (field >= 23) {   // _a_rho_1, XSPH velocity: scatter only
+        const void *src = field == 23 ? e.f.drho : field == 24 ? e.f.xu
+                        : field == 25 ? e.f.xv : e.f.xw;
+        user[ui] = F32 ? (double)((const float *)src)[k] : ((const double *)src)[k];
         return;
     }
     if (F32) {
@@ -449,15 +451,16 @@ extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
     if (!user || !user_offset || array < 0 || array >= e->cfg.num_arrays) return SPHB_ERR_ARG;
-    if (field < 0 || field > 23 || (dir != 0 && dir != 1)) return SPHB_ERR_ARG;
-    if (dir == 0 && ((field >= 17 && field <= 20) || field == 23)) return SPHB_ERR_ARG;
+    if (field < 0 || field > 26 || (dir != 0 && dir != 1)) return SPHB_ERR_ARG;
+    if (dir == 0 && ((field >= 17 && field <= 20) || field >= 23)) return SPHB_ERR_ARG;
     const bool f32 = e->cfg.precision == SPHB_FP32C;
     const sphb_buffers &B = e->buf[cur];
-    const void *ptrs[24] = {B.x, B.y, B.z, B.u, B.v, B.w, B.x0, B.y0, B.z0, B.u0,
+    const void *ptrs[27] = {B.x, B.y, B.z, B.u, B.v, B.w, B.x0, B.y0, B.z0, B.u0,
                             B.v0, B.w0, B.m, B.h,
                             f32 ? e->f.thermo : e->f.rho, f32 ? e->f.thermo : e->f.p,
                             f32 ? e->f.thermo : e->f.cs, e->f.au, e->f.av, e->f.aw,
-                            e->f.dt_fac, B.rho, B.rho0, e->f.drho};
+                            e->f.dt_fac, B.rho, B.rho0, e->f.drho,
+                            e->f.xu, e->f.xv, e->f.xw};
     if (!ptrs[field] || !B.idx) return SPHB_ERR_ARG;
     if (e->num_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;

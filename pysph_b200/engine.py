@@ -315,12 +315,12 @@ class Engine:
             f["aw"] = torch.zeros(N, **f64) if dim == 3 else None
             f["geo"] = f["mass"] = f["vel"] = f["thermo"] = None
         f["cell"] = torch.zeros(N, **i32)
-        # continuity scheme outputs of the pair pass: _a_rho_1, XSPH velocity
+        # outputs of SPHDensityRate (_a_rho_1) and XSPHCorrection (velocity):
+        # the continuity scheme's, and any single calc's on this engine
         ft = dict(dtype=torch.float32 if self.f32 else torch.float64, device=dev)
-        f["drho"] = torch.zeros(N, **ft) if self.scheme.continuity else None
-        xs = any(self.scheme.xsph_src.values())
+        f["drho"] = torch.zeros(N, **ft)
         for c in ("xu", "xv", "xw"):
-            f[c] = torch.zeros(N, **ft) if xs and (c != "xw" or dim == 3) else None
+            f[c] = torch.zeros(N, **ft) if (c != "xw" or dim == 3) else None
         # per-stage neighbour lists (density pass writes, force pass reads)
         idx_bits = 26 if dim == 2 else 23
         self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
@@ -493,16 +493,22 @@ class Engine:
         self._box_valid = False   # until a pc_stage accumulates it again
 
     @contextlib.contextmanager
-    def masks(self, rho_src=None, mom_src=None, tait_on=None, step_on=None):
+    def masks(self, rho_src=None, mom_src=None, tait_on=None, step_on=None,
+              rate_src=None, xsph_src=None):
         """Temporarily replace the scheme masks the kernels see (dest array
         -> source bitmask), for evaluating one calc at a time."""
         cfg = self.desc.cfg
-        saved = (list(cfg.rho_src), list(cfg.mom_src), cfg.tait_on, cfg.step_on)
+        saved = (list(cfg.rho_src), list(cfg.mom_src), cfg.tait_on, cfg.step_on,
+                 list(cfg.rate_src), list(cfg.xsph_src))
         try:
             for a, m in (rho_src or {}).items():
                 cfg.rho_src[a] = m
             for a, m in (mom_src or {}).items():
                 cfg.mom_src[a] = m
+            for a, m in (rate_src or {}).items():
+                cfg.rate_src[a] = m
+            for a, m in (xsph_src or {}).items():
+                cfg.xsph_src[a] = m
             if tait_on is not None:
                 cfg.tait_on = tait_on
             if step_on is not None:
@@ -512,6 +518,8 @@ class Engine:
             for a in range(nat.MAX_ARRAYS):
                 cfg.rho_src[a] = saved[0][a]
                 cfg.mom_src[a] = saved[1][a]
+                cfg.rate_src[a] = saved[4][a]
+                cfg.xsph_src[a] = saved[5][a]
             cfg.tait_on, cfg.step_on = saved[2], saved[3]
 
     def update_params(self, scene=None, **kw):
@@ -537,6 +545,15 @@ class Engine:
                 t.g[d] = float(p.gravity[d]) if d < len(p.gravity) else 0.0
             t.cfl, t.dt_initial = p.cfl, p.dt_initial
             t.use_cfl = (1 if p.cfl_force else 2) if p.cfl > 0 else 0
+        self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
+
+    def set_xsph_eps(self, eps: float):
+        """XSPHCorrection eps of every scene (scene table re-uploaded when it
+        changes)."""
+        if all(t.xsph_eps == eps for t in self._scene_host):
+            return
+        for t in self._scene_host:
+            t.xsph_eps = float(eps)
         self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
 
     def set_dt_async(self, dt: float):

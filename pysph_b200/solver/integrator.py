@@ -3,8 +3,10 @@
 PredictorCorrectorIntegrator.integrate(dt) is the hot path.  When its calcs
 are the particle-update scheme -- SPHRho, then TaitEquation, then
 MomentumEquation (or SPHPressureGradient), then GravityForce, then
-PositionStepping, on any arrays -- the whole step runs in the CUDA engine as
-one fused pipeline per stage (rebin, density + EOS, force + gravity,
+PositionStepping, on any arrays -- or its continuity-equation form --
+TaitEquation, SPHDensityRate, MomentumEquation, GravityForce,
+PositionStepping, XSPHCorrection -- the whole step runs in the CUDA engine as
+one fused pipeline per stage (rebin, density + EOS or Tait, one pair pass,
 integrator stage); see fused_plan.  Any other calc list goes through the
 building blocks below (eval: every calc's SPHCalc.sph on the engine; step:
 elementwise updates of the FP64 properties), as the reference does.
@@ -16,7 +18,8 @@ import torch
 from .. import _native as nat
 from ..engine import Scheme, SceneParams
 from ..sph.sph_func import (SPHRho, TaitEquation, MomentumEquation,
-                            SPHPressureGradient, GravityForce, PositionStepping)
+                            SPHPressureGradient, GravityForce, PositionStepping,
+                            SPHDensityRate, XSPHCorrection)
 
 
 class FusedPlan:
@@ -39,9 +42,10 @@ def fused_plan(particles, calcs):
                 return i
         raise ValueError("calc array not in particles")
 
-    order = {SPHRho: 0, TaitEquation: 1, MomentumEquation: 2, SPHPressureGradient: 2,
-             GravityForce: 3, PositionStepping: 4}
+    order = {SPHRho: 0, TaitEquation: 1, SPHDensityRate: 2, MomentumEquation: 3,
+             SPHPressureGradient: 3, GravityForce: 4, PositionStepping: 5, XSPHCorrection: 6}
     rho_src, mom_src, tait_on, step_on, grav_on = {}, {}, set(), set(), set()
+    rate_src, xsph_src = {}, {}
     params = {}
     mode = None
     last = -1
@@ -104,17 +108,30 @@ def fused_plan(particles, calcs):
                 if not calc.integrates or ups[:dim] != pos:
                     return None
                 step_on.add(d)
+            elif cls is SPHDensityRate:
+                if not calc.integrates or ups[:1] != ["rho"] or d in rate_src:
+                    return None
+                rate_src[d] = [b for b in range(len(arrays)) if srcs >> b & 1]
+            elif cls is XSPHCorrection:
+                # added to the position rate of an array already stepped
+                if not calc.integrates or ups[:dim] != pos or d not in step_on or d in xsph_src:
+                    return None
+                agree("xsph_eps", calc.funcs[0].eps)
+                xsph_src[d] = [b for b in range(len(arrays)) if srcs >> b & 1]
     except _NoPlan:
         return None
+    if rho_src and rate_src:
+        return None   # summation density and the continuity equation at once
     if not step_on or set(mom_src) != step_on:
         return None
     if grav_on and grav_on != step_on:
         return None
     if not grav_on:
         params["gravity"] = (0.0, 0.0, 0.0)
-    tait_only = tait_on - set(rho_src)
+    tait_only = tait_on - set(rho_src) if not rate_src else set()
     scheme = Scheme(rho_src=rho_src, mom_src=mom_src, tait_on=tuple(sorted(tait_on)),
-                    step_on=tuple(sorted(step_on)))
+                    step_on=tuple(sorted(step_on)), rate_src=rate_src, xsph_src=xsph_src,
+                    xsph_eps=params.get("xsph_eps", 0.5))
     p = SceneParams(**{k: v for k, v in params.items()
                        if k in SceneParams.__dataclass_fields__})
     return FusedPlan(scheme, p, mode or 0, dim, tuple(sorted(tait_only)))
@@ -239,6 +256,8 @@ class Integrator:
             names = []
             if a in sc.rho_src:
                 names.append("rho")
+            if a in sc.rate_src:
+                names += ["rho", "_rho0", "_a_rho_1"]
             if a in sc.tait_on:
                 names += ["p", "cs"]
             if a in sc.step_on:

@@ -13,7 +13,7 @@ import logging
 
 from ..base.kernels import CubicSplineKernel
 from ..base.particle_types import ParticleType
-from ..sph.sph_func import PositionStepping
+from ..sph.sph_func import PositionStepping, XSPHCorrection
 from .integrator import PredictorCorrectorIntegrator
 from .sph_equation import SPHIntegration, SPHOperation
 from .time_step_functions import TimeStep
@@ -71,15 +71,25 @@ class Solver:
         self.operation_dict.pop(id)
 
     def add_operation_step(self, types, xsph=False, eps=0.5):
-        """Position stepping dx/dt = v on `types` (S/solver/solver.py:186-220)."""
-        if xsph:
-            raise NotImplementedError("XSPH correction is not part of this build")
+        """Position stepping dx/dt = v on `types` (S/solver/solver.py:168-183),
+        followed by the XSPH correction when xsph."""
         updates = ["x", "y", "z"][:self.dim]
         self.add_operation(SPHIntegration(PositionStepping.withargs(), on_types=types,
                                           updates=updates, id="step"))
+        if xsph:
+            self.add_operation_xsph(eps)
 
     def add_operation_xsph(self, eps, hks=False):
-        raise NotImplementedError("XSPH correction is not part of this build")
+        """XSPHCorrection on the arrays the position stepping moves, from
+        those same arrays, added to their position rate
+        (S/solver/solver.py:185-220)."""
+        assert eps > 0, "Invalid value for XSPH epsilon: %f" % eps
+        self.eps = eps
+        assert "step" in self.operation_dict, "position stepping function does not exist!"
+        step = self.operation_dict["step"]
+        self.add_operation(SPHIntegration(
+            XSPHCorrection.withargs(eps=eps, hks=hks), from_types=step.on_types,
+            on_types=step.on_types, updates=step.updates, id="xsph"))
 
     def set_final_time(self, tf):
         self.tf = tf

@@ -4,8 +4,9 @@ from .sph_calc import SPHCalc
 from .sph_func import (Function, SPHFunction, SPHFunctionParticle,
                        CSPHFunctionParticle, SPHRho, TaitEquation,
                        MomentumEquation, SPHPressureGradient, GravityForce,
-                       PositionStepping)
+                       PositionStepping, SPHDensityRate, XSPHCorrection)
 
 __all__ = ["SPHCalc", "Function", "SPHFunction", "SPHFunctionParticle",
            "CSPHFunctionParticle", "SPHRho", "TaitEquation", "MomentumEquation",
-           "SPHPressureGradient", "GravityForce", "PositionStepping"]
+           "SPHPressureGradient", "GravityForce", "PositionStepping",
+           "SPHDensityRate", "XSPHCorrection"]

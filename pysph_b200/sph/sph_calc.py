@@ -148,6 +148,16 @@ def evaluate(calc: SPHCalc, outs):
         with eng.masks(mom_src={a: src_mask}):
             eng.momentum(dest_mask=1 << a, gravity=False, mode=0 if op == "momentum" else 1)
         fields = ["_a_u_1", "_a_v_1", "_a_w_1"][:dim]
+    elif op == "density_rate":
+        # the force pass with only its SPHDensityRate term on
+        with eng.masks(mom_src={a: 0}, rate_src={a: src_mask}):
+            eng.momentum(dest_mask=1 << a, gravity=False, mode=0)
+        fields = ["_a_rho_1"]
+    elif op == "xsph":
+        eng.set_xsph_eps(f0.eps)
+        with eng.masks(mom_src={a: 0}, xsph_src={a: src_mask}):
+            eng.momentum(dest_mask=1 << a, gravity=False, mode=0)
+        fields = ["_xsph_u", "_xsph_v", "_xsph_w"][:dim]
     else:
         raise NotImplementedError(op)
     s.check()

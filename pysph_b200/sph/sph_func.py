@@ -220,3 +220,38 @@ class PositionStepping(SPHFunction):
 
     def set_src_dst_reads(self):
         self.dst_reads = ["u", "v", "w", "tag"]
+
+
+class SPHDensityRate(SPHFunctionParticle):
+    """Continuity equation drho_a/dt = sum_b m_b (v_a - v_b) . grad_a W_ab
+    (S/sph/funcs/density_funcs.pyx:88-171); integrates rho."""
+
+    engine_op = "density_rate"
+    num_outputs = 1
+
+    def __init__(self, source, dest, setup_arrays=True, **kwargs):
+        SPHFunctionParticle.__init__(self, source, dest, setup_arrays, **kwargs)
+        self.id = "densityrate"
+        self.tag = "density"
+
+    def set_src_dst_reads(self):
+        self.src_reads = ["x", "y", "z", "h", "m", "u", "v", "w"]
+        self.dst_reads = ["x", "y", "z", "h", "tag", "u", "v", "w"]
+
+
+class XSPHCorrection(CSPHFunctionParticle):
+    """XSPH velocity added to the position rate:
+    eps sum_b m_b W_ab (v_b - v_a) / rho_ab, rho_ab = (rho_a + rho_b) / 2
+    (S/sph/funcs/xsph_funcs.pyx:9-90)."""
+
+    engine_op = "xsph"
+
+    def __init__(self, source, dest, setup_arrays=True, eps=0.5, **kwargs):
+        CSPHFunctionParticle.__init__(self, source, dest, setup_arrays, **kwargs)
+        self.eps = float(eps)
+        self.id = "xsph"
+        self.tag = "position"
+
+    def set_src_dst_reads(self):
+        self.src_reads = ["x", "y", "z", "h", "m", "rho", "u", "v", "w"]
+        self.dst_reads = ["x", "y", "z", "h", "rho", "u", "v", "w"]

@@ -122,6 +122,9 @@ def test_unsupported_features_fail_loudly():
     with pytest.raises(NotImplementedError):
         sph.MomentumEquation(f, f, deltap=0.1)
     with pytest.raises(NotImplementedError):
+        sph.XSPHCorrection(f, f, hks=True)
+    # as the reference: XSPH needs the position stepping it corrects
+    with pytest.raises(AssertionError):
         solver.Solver(dim=2).add_operation_xsph(eps=0.5)
 
 
@@ -132,3 +135,41 @@ def test_kernel_host_formulas():
     g = base.Point()
     k.py_gradient(base.Point(0.5, 0, 0), base.Point(0, 0, 0), 1.0, g)
     assert g.x < 0 and g.y == 0
+
+
+def continuity_solver(xsph=True):
+    """The reference dam-break example's scheme (examples/dam-break/
+    dam_break.py:184-241)."""
+    f, w = arrays()
+    particles = base.Particles([f, w])
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=62.6, ro=1000.0),
+                                        on_types=[Fluid, Solid], updates=["p", "cs"], id="eos"))
+    s.add_operation(solver.SPHIntegration(sph.SPHDensityRate.withargs(hks=False),
+                                          on_types=[Fluid, Solid], from_types=[Fluid, Solid],
+                                          updates=["rho"], id="density"))
+    s.add_operation(solver.SPHIntegration(sph.MomentumEquation.withargs(alpha=0.1, beta=0.0),
+                                          on_types=[Fluid], from_types=[Fluid, Solid],
+                                          updates=["u", "v"], id="mom"))
+    s.add_operation(solver.SPHIntegration(sph.GravityForce.withargs(gy=-9.81),
+                                          on_types=[Fluid], updates=["u", "v"], id="grav"))
+    s.add_operation_step([Fluid])
+    if xsph:
+        s.add_operation_xsph(eps=0.5)
+    s.setup(particles)
+    return s
+
+
+def test_fused_plan_continuity_scheme():
+    plan = continuity_solver().integrator.plan
+    assert plan is not None
+    sc = plan.scheme
+    assert sc.continuity and sc.rho_src == {}
+    assert sc.rate_src == {0: [0, 1], 1: [0, 1]} and sc.mom_src == {0: [0, 1]}
+    assert sc.xsph_src == {0: [0]} and sc.xsph_eps == 0.5
+    assert sc.tait_on == (0, 1) and sc.step_on == (0,)
+    assert plan.tait_only == ()
+    # rho is integrated on both arrays (S/solver/integrator.py:212-260)
+    for pa in continuity_solver().particles.arrays:
+        assert pa.has_array("_rho0") and pa.has_array("_a_rho_1")
+    assert continuity_solver(xsph=False).integrator.plan.scheme.xsph_src == {}

@@ -231,3 +231,68 @@ def test_host_edits_reach_the_engine():
     osys.pc_step(1e-5)
     assert np.max(np.abs(pa.x.cpu().numpy() - osys.arrays[0].x)) / 0.05 <= 1e-10
     assert np.max(np.abs(pa.u.cpu().numpy() - osys.arrays[0].u)) <= 1e-8 * 50
+
+
+def drop_continuity_solver(dx=0.025, precision=None):
+    """The drop with the continuity scheme: Tait, SPHDensityRate, momentum,
+    position stepping with XSPH (eps 0.5)."""
+    arrays, _, params = W.elliptical_drop(dx=dx)
+    pa = base.get_particle_array(name="fluid", **arrays[0])
+    particles = base.Particles([pa], precision=precision)
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=1400.0, ro=1.0),
+                                        on_types=[Fluid], updates=["p", "cs"], id="eos"))
+    s.add_operation(solver.SPHIntegration(sph.SPHDensityRate.withargs(hks=False),
+                                          on_types=[Fluid], from_types=[Fluid],
+                                          updates=["rho"], id="density"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=0.1, beta=0.0, eta=0.1),
+        on_types=[Fluid], from_types=[Fluid], updates=["u", "v"], id="mom"))
+    s.add_operation_step([Fluid], xsph=True, eps=0.5)
+    s.set_time_step(1e-5)
+    s.set_final_time(1e-4 - 1e-12)
+    s.setup(particles)
+    return s, pa, arrays, params
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_solver_drop_continuity_matches_oracle(precision):
+    """Solver.solve on the continuity scheme runs fused on the engine and
+    tracks the oracle (itself pinned to the reference's fixtures)."""
+    from oracle import OracleArray, OracleSystem
+    from pysph_b200.engine import continuity_scheme
+    s, pa, arrays, params = drop_continuity_solver(precision=precision)
+    assert s.integrator.plan is not None and s.integrator.plan.scheme.continuity
+    s.solve()
+    assert s.count == 10
+    sch = continuity_scheme(1, 0.5)
+    o = OracleSystem([OracleArray("a0", **{k: np.array(v, np.float64)
+                                          for k, v in arrays[0].items()})],
+                     dim=2, tait_on=sch.tait_on, mom_src=sch.mom_src, step_on=sch.step_on,
+                     rate_src=sch.rate_src, xsph_src=sch.xsph_src, xsph_eps=0.5,
+                     c0=1400.0, rho0=1.0, alpha=0.1, beta=0.0, eta=0.1)
+    for _ in range(10):
+        o.pc_step(1e-5)
+    O = o.arrays[0]
+    dx = 0.025
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    assert np.max(np.abs(pa.x.cpu().numpy() - O.x)) / dx <= tol
+    assert np.max(np.abs(pa.y.cpu().numpy() - O.y)) / dx <= tol
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.max(np.abs(pa.rho.cpu().numpy() - O.rho) / O.rho) <= rtol
+    assert np.max(np.abs(pa.get("_rho0").cpu().numpy() - O.rho0) / O.rho0) <= rtol
+
+
+def test_continuity_building_blocks_match_fused():
+    """SPHDensityRate and XSPHCorrection calc by calc (SPHCalc.sph on the
+    engine + elementwise steps) give the fused engine step's result."""
+    s1, pa1, _, _ = drop_continuity_solver(dx=0.05)
+    s2, pa2, _, _ = drop_continuity_solver(dx=0.05)
+    s2.integrator.plan = None
+    for _ in range(3):
+        s1.integrator.integrate(1e-5)
+        s2.integrator.integrate(1e-5)
+    for n in ("x", "y", "u", "v", "rho"):
+        a = pa1.get(n).cpu().numpy()
+        b = pa2.get(n).cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, np.max(np.abs(a))), n
