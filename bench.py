@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dam_break",
-                    choices=["dam_break", "drop", "lattice3d", "batched"])
+                    choices=["dam_break", "dam_break_continuity", "drop", "lattice3d",
+                             "batched"])
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -67,11 +68,16 @@ def parse():
 # ------------------------------------------------------------------ inputs
 def workload(name):
     from pysph_b200 import workloads as W
-    from pysph_b200.engine import fluid_scheme
+    from pysph_b200.engine import continuity_scheme, fluid_scheme
     if name == "dam_break":
         arrays, types, params = W.dam_break()
         return dict(scenes=[(arrays, params)], scheme=fluid_scheme(2), dim=2,
                     desc="2D dam break, dx=0.0025, 320,000 fluid + 12,018 wall, CFL dt")
+    if name == "dam_break_continuity":
+        arrays, types, params = W.dam_break()
+        return dict(scenes=[(arrays, params)], scheme=continuity_scheme(2, 0.5), dim=2,
+                    desc="2D dam break, dx=0.0025, continuity equation + XSPH (eps 0.5), "
+                         "CFL dt")
     if name == "drop":
         arrays, types, params = W.elliptical_drop(dx=0.025)
         return dict(scenes=[(arrays, dict(params, dt=1e-5))], scheme=fluid_scheme(1),
@@ -427,16 +433,20 @@ def timed_steps(eng, steps, flush, stream, graph=True):
 
 
 def other_configs(dev, flush, stream):
-    """The other workloads, briefly: elliptical drop (5,025), the 3D
-    128^3 lattice (one evaluation), 256 batched drops, each FP32C and FP64."""
+    """The other workloads, briefly: the dam break with the continuity
+    equation and XSPH (the reference example's scheme), the elliptical drop
+    (5,025), 256 batched drops and the 3D 128^3 lattice (one evaluation),
+    each FP32C and FP64."""
     import torch
     from pysph_b200.engine import Engine
     out = {}
-    for name, steps in (("drop", 50), ("batched", 10)):
+    for name, steps in (("dam_break_continuity", 100), ("drop", 50), ("batched", 10)):
         wl = workload(name)
         for prec in ("fp32c", "fp64"):
-            eng = Engine(wl["scenes"], wl["scheme"], dim=2, precision=prec, lanes=2,
-                         pair_block=128, stencil=2, device=dev)
+            shape = (dict(lanes=1, pair_block=256, stencil=1) if name.startswith("dam")
+                     else dict(lanes=2, pair_block=128, stencil=2))
+            eng = Engine(wl["scenes"], wl["scheme"], dim=2, precision=prec, device=dev,
+                         **shape)
             ms, pairs = timed_steps(eng, steps, flush, stream)
             out[f"{name}_{prec}"] = {"particles": eng.N, "scenes": eng.S,
                                      "ms_per_step": ms, "steps_per_s": 1e3 / ms,
