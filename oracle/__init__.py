@@ -98,6 +98,8 @@ def lib():
         L.orc_scheme_pairs.argtypes = [P(_System)]
         L.orc_eval.argtypes = [P(_System), ctypes.c_void_p]
         L.orc_pc_step.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_double]
+        L.orc_integrate.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_double,
+                                    ctypes.c_int]
         dp = P(ctypes.c_double)
         L.orc_sph_rho.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
                                   ctypes.c_int, dp]
@@ -275,6 +277,18 @@ class OracleSystem:
 
     def pc_step(self, dt):
         rc = lib().orc_pc_step(ctypes.byref(self._s), self._c, float(dt))
+        if rc:
+            raise RuntimeError(f"oracle step failed ({rc})")
+        self.count += 1
+
+    INTEGRATORS = {"euler": 0, "rk2": 1, "rk4": 2}
+
+    def step(self, dt, integrator="pc"):
+        """One step of the named integrator (pc, euler, rk2, rk4)."""
+        if integrator == "pc":
+            return self.pc_step(dt)
+        rc = lib().orc_integrate(ctypes.byref(self._s), self._c, float(dt),
+                                 self.INTEGRATORS[integrator])
         if rc:
             raise RuntimeError(f"oracle step failed ({rc})")
         self.count += 1

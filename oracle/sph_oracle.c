@@ -31,6 +31,7 @@
  *   SPHFunction.eval (+= / tag) .... S/sph/sph_func.pyx:208-227
  *   SPHCalc.sph resets ............. S/sph/sph_calc.pyx:307-331, :431-440
  *   PredictorCorrector ............. S/solver/integrator.py:262-367, :614-683
+ *   Euler, RK2, RK4 ................ S/solver/integrator.py:420-609
  */
 #include <math.h>
 #include <stdint.h>
@@ -837,4 +838,120 @@ int orc_pc_step(orc_system *s, orc_nnps *c, double dt)
         }
     }
     return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* the other integrators (S/solver/integrator.py:420-609), each preceded  */
+/* by the Solver's particles.update() like orc_pc_step                    */
+/* ------------------------------------------------------------------ */
+static void save_initial(const orc_system *s)
+{
+    for (int d = 0; d < s->narrays; ++d) {
+        const orc_array *D = &s->a[d];
+        size_t nb = sizeof(double) * (size_t)D->n;
+        if (s->rate_src[d]) memcpy(D->rho0, D->rho, nb);
+        if (!(s->step_on & (1u << d))) continue;
+        memcpy(D->x0, D->x, nb);
+        memcpy(D->y0, D->y, nb);
+        memcpy(D->u0, D->u, nb);
+        memcpy(D->v0, D->v, nb);
+        if (s->dim == 3) {
+            memcpy(D->z0, D->z, nb);
+            memcpy(D->w0, D->w, nb);
+        }
+    }
+}
+
+/* the rates of every stepped property, in a fixed order: x y z u v w rho */
+#define ORC_NRATES 7
+static double *rate_ptr(const orc_system *s, int d, int r)
+{
+    const orc_array *D = &s->a[d];
+    int stepped = (s->step_on >> d) & 1u;
+    switch (r) {
+    case 0: return stepped ? D->ax : NULL;
+    case 1: return stepped ? D->ay : NULL;
+    case 2: return stepped && s->dim == 3 ? D->az : NULL;
+    case 3: return stepped ? D->au : NULL;
+    case 4: return stepped ? D->av : NULL;
+    case 5: return stepped && s->dim == 3 ? D->aw : NULL;
+    default: return s->rate_src[d] ? D->arho : NULL;
+    }
+}
+static double *prop_ptr(const orc_system *s, int d, int r, int initial)
+{
+    const orc_array *D = &s->a[d];
+    double *p[ORC_NRATES] = {D->x, D->y, D->z, D->u, D->v, D->w, D->rho};
+    double *p0[ORC_NRATES] = {D->x0, D->y0, D->z0, D->u0, D->v0, D->w0, D->rho0};
+    return initial ? p0[r] : p[r];
+}
+
+/* kind 0: EulerIntegrator.integrate (:420-447); 1: RK2Integrator (:452-499);
+ * 2: RK4Integrator (:504-609). */
+int orc_integrate(orc_system *s, orc_nnps *c, double dt, int kind)
+{
+    uint32_t pm = pair_mask_of(s);
+    int rc = orc_update(s, c, pm);
+    if (rc) return rc;
+    save_initial(s);
+    if (kind == 0 || kind == 1) {
+        reset_acc(s);
+        rc = orc_eval(s, c);
+        if (rc) return rc;
+        half_step(s, kind == 0 ? dt : dt / 2);
+        if (kind == 0) return 0;
+        rc = orc_update(s, c, pm);
+        if (rc) return rc;
+        reset_acc(s);
+        rc = orc_eval(s, c);
+        if (rc) return rc;
+        half_step(s, dt);
+        return 0;
+    }
+    if (kind != 2) return -1;
+    /* RK4: K1..K3 kept per stepped property */
+    double *K[3][ORC_MAX_ARRAYS][ORC_NRATES];
+    memset(K, 0, sizeof(K));
+    for (int d = 0; d < s->narrays; ++d)
+        for (int r = 0; r < ORC_NRATES; ++r)
+            if (rate_ptr(s, d, r))
+                for (int q = 0; q < 3; ++q)
+                    K[q][d][r] = (double *)malloc(sizeof(double) * (size_t)(s->a[d].n + 1));
+    const double h[3] = {dt / 2, dt / 2, dt};
+    for (int q = 0; q < 4; ++q) {
+        if (q > 0) {
+            rc = orc_update(s, c, pm);
+            if (rc) break;
+        }
+        reset_acc(s);
+        rc = orc_eval(s, c);
+        if (rc) break;
+        if (q < 3) {
+            for (int d = 0; d < s->narrays; ++d)
+                for (int r = 0; r < ORC_NRATES; ++r)
+                    if (K[q][d][r])
+                        memcpy(K[q][d][r], rate_ptr(s, d, r), sizeof(double) * (size_t)s->a[d].n);
+            half_step(s, h[q]);
+            continue;
+        }
+        /* X = X0 + fac dt (K1 + 2 K2 + 2 K3 + K4), numpy's order */
+        double fdt = (1.0 / 6.0) * dt;
+        for (int d = 0; d < s->narrays; ++d)
+            for (int r = 0; r < ORC_NRATES; ++r) {
+                double *k4 = rate_ptr(s, d, r);
+                if (!k4) continue;
+                double *x = prop_ptr(s, d, r, 0), *x0 = prop_ptr(s, d, r, 1);
+                for (int64_t i = 0; i < s->a[d].n; ++i) {
+                    double t = K[0][d][r][i] + 2 * K[1][d][r][i];
+                    t = t + 2 * K[2][d][r][i];
+                    t = t + k4[i];
+                    t = fdt * t;
+                    x[i] = x0[i] + t;
+                }
+            }
+    }
+    for (int q = 0; q < 3; ++q)
+        for (int d = 0; d < ORC_MAX_ARRAYS; ++d)
+            for (int r = 0; r < ORC_NRATES; ++r) free(K[q][d][r]);
+    return rc;
 }

@@ -104,7 +104,7 @@ def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None):
     return ops
 
 
-def build_sim(R, arrays, types, params, dim, xsph_eps=None):
+def build_sim(R, arrays, types, params, dim, xsph_eps=None, integrator=None):
     pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
     particles = R["P"].Particles(pas)
     kernel = R["K"].CubicSplineKernel(dim=dim)
@@ -113,7 +113,7 @@ def build_sim(R, arrays, types, params, dim, xsph_eps=None):
     calcs = []
     for op in ops:
         calcs.extend(op.get_calcs(particles, kernel))
-    integ = R["I"].PredictorCorrectorIntegrator(particles, calcs)
+    integ = (integrator or R["I"].PredictorCorrectorIntegrator)(particles, calcs)
     integ.setup_integrator()
     return pas, particles, integ
 
@@ -228,6 +228,25 @@ def dam(R):
 XSPH_EPS = 0.5   # XSPHCorrection's default eps
 
 
+def integrators(R):
+    """The elliptical drop (dx = 0.05) stepped by the reference's Euler, RK2
+    and RK4 integrators, 5 steps of dt = 1e-5, summation density and, for
+    RK2, the continuity scheme too."""
+    arrays, types, params = W.elliptical_drop(dx=0.05)
+    out = {f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS}
+    I = R["I"]
+    for name, cls, eps in (("euler", I.EulerIntegrator, None), ("rk2", I.RK2Integrator, None),
+                           ("rk4", I.RK4Integrator, None), ("rk2cont", I.RK2Integrator, XSPH_EPS)):
+        pas, particles, integ = build_sim(R, arrays, types, params, 2, eps, integrator=cls)
+        for step in range(5):
+            particles.update()
+            integ.integrate(1e-5)
+            if step == 0:
+                out.update({f"{name}_step1_{k}": v for k, v in state(pas).items()})
+        out.update({f"{name}_step5_{k}": v for k, v in state(pas).items()})
+    return out
+
+
 def drop_cont(R):
     """Elliptical drop with the continuity scheme: first-stage rates, then 10
     steps of dt = 1e-5."""
@@ -289,7 +308,8 @@ def main():
     a = ap.parse_args()
     R = ref_modules(a.build)
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
-                     ("drop_cont", drop_cont), ("dam_cont", dam_cont)):
+                     ("drop_cont", drop_cont), ("dam_cont", dam_cont),
+                     ("integrators", integrators)):
         if a.only and name not in a.only:
             continue
         data = fn(R)

@@ -183,3 +183,19 @@ def test_dam_break_continuity_bit_exact():
         for n in ("x", "y", "u", "v", "rho", "p", "cs"):
             np.testing.assert_array_equal(getattr(o.arrays[i], n), g[f"step5_{n}_{i}"],
                                           err_msg=f"{n}_{i}")
+
+
+# -- the other integrators (Euler, RK2, RK4) -----------------------------------
+@pytest.mark.parametrize("name,integ,cont", [("euler", "euler", False), ("rk2", "rk2", False),
+                                             ("rk4", "rk4", False), ("rk2cont", "rk2", True)])
+@pytest.mark.parametrize("steps", [1, 5])
+def test_integrators_bit_exact(name, integ, cont, steps):
+    g = load("integrators")
+    sch = continuity_scheme(1, 0.5) if cont else fluid_scheme(1)
+    o = oracle_for(g, ["in_"], sch, DROP, 2)
+    for _ in range(steps):
+        o.step(1e-5, integ)
+    A = o.arrays[0]
+    for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+        np.testing.assert_array_equal(getattr(A, n), g[f"{name}_step{steps}_{n}_0"],
+                                      err_msg=f"{name} {n}")
