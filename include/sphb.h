@@ -340,9 +340,12 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
 SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
                   int with_gravity, int mode, void *stream);
 
-/* Predictor-corrector stage on the integrated arrays (cfg.step_on):
- * stage 0 = predict (save X0, X = X0 + dt/2 F), stage 1 = correct and
- * final (X = 2 (X0 + dt/2 F) - X0).  Stage 0 also clears the per-scene
+/* Integrator stage on the integrated arrays (cfg.step_on, and the density
+ * of cfg.rate_src dests): stage 0 = predict (save X0, X = X0 + dt/2 F; also
+ * RK2's first stage), stage 1 = correct and final (X = 2 (X0 + dt/2 F) -
+ * X0), stage 2 = Euler (save X0, X = X0 + dt F;
+ * EulerIntegrator.integrate, S/solver/integrator.py:420-447), stage 3 =
+ * RK2's second stage (X = X0 + dt F; RK2Integrator, :452-499).  Stage 0 also clears the per-scene
  * dt_fac / |a| maxima, so sphb_step_begin sees the corrector's pass only.
  * Refreshes the FP32 pair records of the moved particles and, with
  * f.anchor, accumulates max_disp2 (cleared by the next SPHB_BIN_IF_NEEDED
@@ -358,7 +361,8 @@ SPHB_API int sphb_pc_stage(const sphb_engine *e, int cur, int stage, void *strea
  * ViscousAndForceBasedTimeStep.compute_time_step
  * (S/solver/time_step_functions.py:8-57, Integrator.get_max_acceleration
  * S/solver/integrator.py:369-412) using the max dt_fac and |a| of the last
- * sphb_momentum; then t += dt. */
+ * sphb_momentum; then t += dt, and the maxima restart for this step's
+ * force passes. */
 SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
 
 /* Gather (dir 0: user order -> engine order) or scatter (dir 1: engine ->

@@ -69,18 +69,22 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
     const sphb_buffers &B = e.buf[cur];
     const sphb_scene_state &st = e.sstate[s];
     const double dt2 = st.dt / 2;
+    // the stage: 0 save X0, X = X0 + dt/2 F; 1 X = 2 (X0 + dt/2 F) - X0;
+    // 2 save X0, X = X0 + dt F; 3 X = X0 + dt F
+    const bool save = stage == 0 || stage == 2;
+    const double hstep = stage == 0 ? dt2 : st.dt;
+    auto advance = [&](double cur0, double init, double rate) {
+        if (stage == 1) return __dadd_rn(2 * axpy_rn(init, rate, dt2), -init);
+        return axpy_rn(save ? cur0 : init, rate, hstep);
+    };
     // continuity scheme: the density of every SPHDensityRate dest is
     // integrated like the other stepped properties
     if (active && B.rho && B.rho0 && e.f.drho && e.cfg.rate_src[a]) {
         const double dr = F32 ? (double)((const float *)e.f.drho)[k] : ((const double *)e.f.drho)[k];
-        if (stage == 0) {
-            const double r0 = B.rho[k];
-            B.rho0[k] = r0;
-            B.rho[k] = axpy_rn(r0, dr, dt2);
-        } else {
-            const double r0 = B.rho0[k];
-            B.rho[k] = __dadd_rn(2 * axpy_rn(r0, dr, dt2), -r0);
-        }
+        const double r = B.rho[k];
+        const double r0 = save ? r : B.rho0[k];
+        if (save) B.rho0[k] = r;
+        B.rho[k] = advance(r, r0, dr);
     }
     if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
     // XSPHCorrection adds to PositionStepping's rate
@@ -107,7 +111,7 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
             }
             x[d] = X[d][k];
             v[d] = V[d][k];
-            if (stage == 1) {
+            if (!save) {
                 x0[d] = X0[d][k];
                 v0[d] = V0[d][k];
             }
@@ -134,17 +138,12 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
             const double fd = real ? f[d] : 0.0;
             // PositionStepping: F_x = u (+ the XSPH velocity)
             const double fx = real ? (xsph ? __dadd_rn(v[d], xv[d]) : v[d]) : 0.0;
-            if (stage == 0) {
+            if (save) {
                 X0[d][k] = x[d];
                 V0[d][k] = v[d];
-                p[d] = axpy_rn(x[d], fx, dt2);
-                vn[d] = axpy_rn(v[d], fd, dt2);
-            } else {
-                const double xh = axpy_rn(x0[d], fx, dt2);
-                const double vh = axpy_rn(v0[d], fd, dt2);
-                p[d] = __dadd_rn(2 * xh, -x0[d]);
-                vn[d] = __dadd_rn(2 * vh, -v0[d]);
             }
+            p[d] = advance(x[d], x0[d], fx);
+            vn[d] = advance(v[d], v0[d], fd);
             X[d][k] = p[d];
             V[d][k] = vn[d];
         }
@@ -213,6 +212,11 @@ __global__ void k_step_begin(const __grid_constant__ sphb_engine e)
         st.dt = dt;
     }
     st.t += st.dt;
+    // the maxima served this step's rule: the step's own force passes
+    // accumulate them afresh (a single-stage integrator has no stage that
+    // clears them)
+    st.max_dtfac = 0ull;
+    st.max_acc2 = 0ull;
 }
 
 __global__ void k_set_dt(const __grid_constant__ sphb_engine e, double dt)
@@ -398,7 +402,7 @@ extern "C" int sphb_pc_stage(const sphb_engine *e, int cur, int stage, void *str
 {
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
-    if (stage != 0 && stage != 1) return SPHB_ERR_ARG;
+    if (stage < 0 || stage > 3) return SPHB_ERR_ARG;
     if (!e->f.au || !e->f.av) return SPHB_ERR_ARG;
     const sphb_buffers &B = e->buf[cur];
     if (!B.x0 || !B.y0 || !B.u0 || !B.v0) return SPHB_ERR_ARG;

@@ -648,6 +648,28 @@ class Engine:
         self.eval_stage()
         self.pc_stage(1)
 
+    def step(self, integrator: str = "pc", on_half=None):
+        """One step of the named integrator: "pc" (pc_step), "euler"
+        (EulerIntegrator: X = X0 + dt F) or "rk2" (RK2Integrator:
+        X_half = X0 + dt/2 F(X0), X = X0 + dt F(X_half))."""
+        if integrator == "pc":
+            return self.pc_step(on_half)
+        if integrator not in ("euler", "rk2"):
+            raise NotImplementedError(f"{integrator} is not fused on the engine")
+        reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
+        self.step_begin()
+        self.bin(reuse)
+        self.eval_stage()
+        if integrator == "euler":
+            self.pc_stage(2)
+            return
+        self.pc_stage(0)
+        if on_half is not None:
+            on_half()
+        self.bin(nat.BIN_MOVE_INITIAL | reuse)
+        self.eval_stage()
+        self.pc_stage(3)
+
     def rebin_count(self) -> int:
         """1 when the last device-decided rebin happened (host sync)."""
         off = self.work_offsets[nat.WORK_NAMES.index("meta")]

@@ -1,7 +1,7 @@
 """`import pysph_b200.solver.api as solver` -- operations, integrators,
 time-step functions and the Solver of the particle-update path."""
 from .integrator import (Integrator, PredictorCorrectorIntegrator, EulerIntegrator,
-                         fused_plan)
+                         RK2Integrator, RK4Integrator, fused_plan)
 from .solver import Solver
 from .sph_equation import SPHOperation, SPHIntegration
 from .time_step_functions import (TimeStep, ViscousTimeStep,
@@ -9,6 +9,7 @@ from .time_step_functions import (TimeStep, ViscousTimeStep,
 
 HAS_CL = False
 
-__all__ = ["Integrator", "PredictorCorrectorIntegrator", "EulerIntegrator", "Solver",
+__all__ = ["Integrator", "PredictorCorrectorIntegrator", "EulerIntegrator",
+           "RK2Integrator", "RK4Integrator", "Solver",
            "SPHOperation", "SPHIntegration", "TimeStep", "ViscousTimeStep",
            "ViscousAndForceBasedTimeStep", "VelocityBasedTimeStep", "fused_plan"]

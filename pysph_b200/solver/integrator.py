@@ -271,6 +271,21 @@ class Integrator:
             s.mark_engine_newer(a, names)
 
 
+    def _fused_integrate(self, dt, device_dt, kind):
+        """The whole step on the engine (fused plan)."""
+        s = self._fused_session()
+        s.ensure(self._fused_reads(s))
+        eng = s.engine
+        if not device_dt:
+            eng.set_dt_async(dt)
+        eng.step(kind)
+        self._fused_outputs(s)
+        self.time += dt if not device_dt else 0.0
+        self._steps = getattr(self, "_steps", 0) + 1
+        if self.check_every and self._steps % self.check_every == 0:
+            s.check()
+
+
 class PredictorCorrectorIntegrator(Integrator):
     """X(t+h/2) = X0 + h/2 F(X); X(t+h/2) = X0 + h/2 F(X(t+h/2));
     X(t+h) = 2 X(t+h/2) - X0 (S/solver/integrator.py:614-683)."""
@@ -290,18 +305,7 @@ class PredictorCorrectorIntegrator(Integrator):
         """One step.  device_dt: the engine's CFL rule chooses dt (the Solver
         uses it for the viscous / force time-step functions)."""
         if self.plan is not None:
-            s = self._fused_session()
-            s.ensure(self._fused_reads(s))
-            eng = s.engine
-            if not device_dt:
-                eng.set_dt_async(dt)
-            eng.pc_step()
-            self._fused_outputs(s)
-            self.time += dt if not device_dt else 0.0
-            self._steps = getattr(self, "_steps", 0) + 1
-            if self.check_every and self._steps % self.check_every == 0:
-                s.check()
-            return
+            return self._fused_integrate(dt, device_dt, "pc")
         self.save_initial_arrays()
         self.reset_accelerations(step=1)
         self.local_time = self.time
@@ -320,13 +324,85 @@ class PredictorCorrectorIntegrator(Integrator):
 
 
 class EulerIntegrator(Integrator):
-    """Forward Euler: X(t+h) = X0 + h F(X) (S/solver/integrator.py:420-456)."""
+    """Forward Euler: X(t+h) = X0 + h F(X) (S/solver/integrator.py:420-447)."""
 
-    def integrate(self, dt):
+    def integrate(self, dt, device_dt=False):
+        if self.plan is not None:
+            return self._fused_integrate(dt, device_dt, "euler")
         self.save_initial_arrays()
         self.reset_accelerations(step=1)
         self.local_time = self.time
         self.eval()
         self.step(dt)
+        self.particles.update()
+        self.cstep = 1
+
+
+class RK2Integrator(Integrator):
+    """X(t+h/2) = X0 + h/2 F(X); X(t+h) = X0 + h F(X(t+h/2))
+    (S/solver/integrator.py:452-499)."""
+
+    def integrate(self, dt, device_dt=False):
+        if self.plan is not None:
+            return self._fused_integrate(dt, device_dt, "rk2")
+        self.save_initial_arrays()
+        self.reset_accelerations(step=1)
+        self.local_time = self.time
+        self.eval()
+        self.step(dt / 2)
+        self.particles.update()
+        self.cstep = 1
+        self.reset_accelerations(step=1)
+        self.local_time = self.time + dt / 2
+        self.eval()
+        self.step(dt)
+        self.particles.update()
+        self.cstep = 1
+
+
+class RK4Integrator(Integrator):
+    """Classical RK4 with four evaluations and X(t+h) = X0 + h/6 (K1 + 2 K2
+    + 2 K3 + K4) (S/solver/integrator.py:504-609).  Its stages run calc by
+    calc on the engine (no fused plan): the four stage rates live in the
+    particle arrays as the reference keeps them."""
+
+    def __init__(self, particles, calcs):
+        Integrator.__init__(self, particles, calcs)
+        self.nsteps = 4
+
+    def setup_integrator(self):
+        Integrator.setup_integrator(self)
+        self.plan = None
+
+    def final_step(self, dt):
+        fac = 1.0 / 6.0
+        for array in self.arrays:
+            to_step = [self.step_props[array.name][k] for k in (1, 2, 3, 4)]
+            for prop in to_step[0]:
+                init = array.get(to_step[0][prop][0])
+                k1, k2, k3, k4 = (array.get(t[prop][1]) for t in to_step)
+                array.set(**{prop: init + fac * dt * (k1 + 2 * k2 + 2 * k3 + k4)})
+
+    def integrate(self, dt, device_dt=False):
+        self.save_initial_arrays()
+        self.reset_accelerations(step=1)
+        self.local_time = self.time
+        self.eval()
+        self.step(dt / 2)
+        self.particles.update()
+        self.reset_accelerations(step=2)
+        self.local_time = self.time + dt / 2
+        self.eval()
+        self.step(dt / 2)
+        self.particles.update()
+        self.reset_accelerations(step=3)
+        self.local_time = self.time + dt / 2
+        self.eval()
+        self.step(dt)
+        self.particles.update()
+        self.reset_accelerations(step=4)
+        self.local_time = self.time + dt
+        self.eval()
+        self.final_step(dt)
         self.particles.update()
         self.cstep = 1

@@ -14,6 +14,7 @@ def oracle_from(arrays, params, scheme, dim, nthreads=0):
     return OracleSystem(
         oarrs, dim=dim, rho_src=scheme.rho_src, tait_on=scheme.tait_on,
         mom_src=scheme.mom_src, step_on=scheme.step_on,
+        rate_src=scheme.rate_src, xsph_src=scheme.xsph_src, xsph_eps=scheme.xsph_eps,
         c0=params.get("c0", 1.0), rho0=params.get("rho0", 1000.0),
         gamma=params.get("gamma", 7.0), alpha=params.get("alpha", 1.0),
         beta=params.get("beta", 1.0), eta=params.get("eta", 0.1), gravity=g,

@@ -199,3 +199,25 @@ def test_dam_break_continuity_cfl(precision):
         rho = eng.get(i, "rho").cpu().numpy()
         ref = g[f"step5_rho_{i}"]
         assert np.max(np.abs(rho - ref) / ref) <= rtol, i
+
+
+# -- Euler and RK2 fused on the engine; RK4 calc by calc (test_api_gpu) --------
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("name,kind,cont", [("euler", "euler", False), ("rk2", "rk2", False),
+                                            ("rk2cont", "rk2", True)])
+def test_integrators_five_steps(precision, name, kind, cont):
+    g = load("integrators")
+    sch = continuity_scheme(1, 0.5) if cont else fluid_scheme(1)
+    eng = Engine([(arrays(g, ["in_"]), DROP)], sch, dim=2, precision=precision)
+    for _ in range(5):
+        eng.step(kind)
+    eng.check_status()
+    dx = 0.05
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"{name}_step5_{n}_0"])) / dx <= tol, n
+    rho = eng.get(0, "rho").cpu().numpy()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    ref = g[f"{name}_step5_rho_0"]
+    assert np.max(np.abs(rho - ref) / ref) <= rtol
