@@ -211,6 +211,20 @@ class ParticleArray:
     def numpy(self, name):
         return self.get(name).detach().cpu().numpy()
 
+    def get_property_arrays(self, all=False):
+        """Numpy copies of the properties (all=False: the ones not starting
+        with '_', plus _tmpx/_tmpy/_tmpz), and the constants
+        (S/base/particle_array.pyx:634-650)."""
+        if all:
+            props = list(self.properties)
+        else:
+            props = [p for p in self.properties if not p.startswith("_")]
+            props += [p for p in ("_tmpx", "_tmpy", "_tmpz") if p in self.properties]
+        ret = {p: self.get(p, only_real_particles=False).detach().cpu().numpy().copy()
+               for p in props}
+        ret.update(self.constants)
+        return ret
+
 
 def get_particle_array(cl_precision="double", device=None, **props):
     """ParticleArray with the reference's default properties

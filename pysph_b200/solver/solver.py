@@ -10,6 +10,7 @@ simulated time, which the loop needs to know when to stop.
 from __future__ import annotations
 
 import logging
+import os
 
 from ..base.kernels import CubicSplineKernel
 from ..base.particle_types import ParticleType
@@ -17,6 +18,7 @@ from ..sph.sph_func import PositionStepping, XSPHCorrection
 from .integrator import PredictorCorrectorIntegrator
 from .sph_equation import SPHIntegration, SPHOperation
 from .time_step_functions import TimeStep
+from .utils import load, savez
 
 logger = logging.getLogger(__name__)
 
@@ -42,10 +44,20 @@ class Solver:
         self.execute_commands = None
         self.command_interval = 1
         self.print_properties = ["x", "u", "m", "h", "p", "e", "rho"]
+        if dim > 1:
+            self.print_properties.extend(["y", "v"])
+        if dim > 2:
+            self.print_properties.extend(["z", "w"])
         self.particles = None
         self.integrator = None
         self.with_cl = False
-        self.output_directory = "."
+        self.rank = 0
+        # output files (S/solver/solver.py:142-148): <fname>_<count>.npz in
+        # <fname>_output, written at the start of solve() and every pfreq
+        # steps; dump_output=False turns them off
+        self.fname = type(self).__name__
+        self.output_directory = self.fname + "_output"
+        self.dump = True
         self.detailed_output = False
         self.dt_history = []
 
@@ -109,6 +121,42 @@ class Solver:
     def set_output_directory(self, path):
         self.output_directory = path
 
+    # ------------------------------------------------------------ output
+    def dump_output(self, dt, *print_properties):
+        """Write <output_directory>/<fname>_<count>.npz in format version 1
+        (S/solver/solver.py:605-695): solver_data (dt, t, count) and, per
+        particle array, its properties -- all of them with detailed output,
+        else those not starting with '_' plus _tmpx/_tmpy/_tmpz."""
+        if not self.dump:
+            return None
+        os.makedirs(self.output_directory, exist_ok=True)
+        path = os.path.join(self.output_directory, f"{self.fname}_{self.count}.npz")
+        props = {"arrays": {}, "solver_data": {"dt": dt, "t": self.t, "count": self.count}}
+        for array in self.particles.arrays:
+            props["arrays"][array.name] = array.get_property_arrays(all=self.detailed_output)
+        savez(path, version=1, **props)
+        return path
+
+    def load_output(self, count):
+        """Resume from <fname>_<count>.npz (S/solver/solver.py:697-739):
+        the arrays' properties, t and count; '?' lists the counts on disk."""
+        counts = sorted({int(f.rsplit("_", 1)[1][:-4]) for f in os.listdir(self.output_directory)
+                         if f.startswith(self.fname) and f.endswith(".npz")})
+        if count == "?":
+            return counts
+        if int(count) not in counts:
+            raise IOError(f"File with iteration count `{count}` does not exist\n"
+                          f"Valid iteration counts are {counts}")
+        data = load(os.path.join(self.output_directory, f"{self.fname}_{count}.npz"))
+        for pa in self.particles.arrays:
+            src = data["arrays"][pa.name]
+            vals = {n: src.get(n) for n in src.get_property_names()
+                    if pa.has_array(n) and n not in ("group", "local", "pid", "idx")}
+            pa.set(**vals)
+            pa.constants.update(src.constants)
+        self.t = float(data["solver_data"]["t"])
+        self.count = int(data["solver_data"]["count"])
+
     def set_command_handler(self, callable, command_interval=1):
         self.execute_commands = callable
         self.command_interval = command_interval
@@ -131,6 +179,7 @@ class Solver:
 
     def solve(self, show_progress=False):
         dt = self.dt
+        self.dump_output(dt, *self.print_properties)
         self.integrator.time = self.t
         rule = self._device_rule()
         if rule:
@@ -160,6 +209,8 @@ class Solver:
                 array.set_time(self.t)
             for func in self.post_step_functions:
                 func.eval(self)
+            if self.count % self.pfreq == 0:
+                self.dump_output(dt, *self.print_properties)
             if self.execute_commands is not None and self.count % self.command_interval == 0:
                 self.execute_commands(self)
         if rule:

@@ -1,6 +1,8 @@
 """Host-side logic of the reference-shaped API (no device work): particle
 array defaults and properties, operation -> calc grouping, and recognition
 of the fused particle-update scheme."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -173,3 +175,36 @@ def test_fused_plan_continuity_scheme():
     for pa in continuity_solver().particles.arrays:
         assert pa.has_array("_rho0") and pa.has_array("_a_rho_1")
     assert continuity_solver(xsph=False).integrator.plan.scheme.xsph_src == {}
+
+
+def test_output_format_v1_round_trip(tmp_path):
+    """Solver.dump_output writes the reference's format version 1 (an .npz
+    with version, solver_data and arrays as object arrays);
+    solver.utils.load reads it back into ParticleArrays, and
+    Solver.load_output resumes from it."""
+    from pysph_b200.solver import utils
+    s = dam_solver()
+    s.set_output_directory(str(tmp_path))
+    f = s.particles.arrays[0]
+    f.set(u=np.linspace(0.0, 1.0, 11))
+    s.count, s.t = 7, 0.25
+    path = s.dump_output(1e-4, *s.print_properties)
+    assert os.path.basename(path) == "Solver_7.npz"
+    raw = np.load(path, allow_pickle=True)
+    assert int(raw["version"]) == 1 and raw["arrays"].dtype == object
+    data = utils.load(path)
+    assert data["solver_data"] == {"dt": 1e-4, "t": 0.25, "count": 7}
+    g = data["arrays"]["fluid"]
+    assert np.allclose(g.get("u").cpu().numpy(), np.linspace(0.0, 1.0, 11))
+    assert "_u0" not in g.get_property_names() and "_tmpx" in g.get_property_names()
+    s.set_output_printing_level(True)
+    assert "_u0" in utils.load(s.dump_output(1e-4))["arrays"]["fluid"].get_property_names()
+    # resume
+    f.set(u=np.zeros(11))
+    s.count, s.t = 0, 0.0
+    assert s.load_output("?") == [7]
+    s.load_output(7)
+    assert s.count == 7 and s.t == 0.25
+    assert np.allclose(f.get("u").cpu().numpy(), np.linspace(0.0, 1.0, 11))
+    with pytest.raises(IOError):
+        s.load_output(3)
