@@ -71,6 +71,7 @@ class _System(ctypes.Structure):
         ("rate_src", ctypes.c_uint32 * MAX_ARRAYS),
         ("xsph_src", ctypes.c_uint32 * MAX_ARRAYS),
         ("xsph_eps", ctypes.c_double),
+        ("variable_h", ctypes.c_int32), ("hks", ctypes.c_int32),
     ]
 
 
@@ -176,7 +177,7 @@ class OracleSystem:
                  step_on=(), c0=1.0, rho0=1000.0, gamma=7.0, alpha=1.0,
                  beta=1.0, eta=0.1, gravity=(0.0, 0.0, 0.0), nthreads=0,
                  radius_scale=2.0, cell_scale=2.0, rate_src=None, xsph_src=None,
-                 xsph_eps=0.5):
+                 xsph_eps=0.5, variable_h=False, hks=False):
         self.arrays = list(arrays)
         assert 1 <= len(self.arrays) <= MAX_ARRAYS
         self.dim = dim
@@ -196,6 +197,8 @@ class OracleSystem:
         for d, srcs in (xsph_src or {}).items():
             s.xsph_src[d] = sum(1 << a for a in srcs)
         s.xsph_eps = xsph_eps
+        s.variable_h = int(bool(variable_h))
+        s.hks = int(bool(hks))
         s.c0, s.rho0, s.gamma_eos = c0, rho0, gamma
         s.alpha, s.beta, s.gamma_av, s.eta = alpha, beta, 1.4, eta
         s.gx, s.gy, s.gz = gravity

@@ -18,6 +18,9 @@
  *   cell size = scale * max h ...... S/base/cell.pyx:911-941
  *   stencil order (x, y, z) ........ S/base/cell.pyx:95-118, :996-1032
  *   neighbour predicate, self last . S/base/nnps.pyx:271-356, :525-621
+ *   variable h (symmetric lists) ... S/base/nnps.pyx:691-786
+ *   hks (kernel averaged over h_a, h_b) the `if self.hks` branches of each
+ *                                    function
  *   SPHRho ......................... S/sph/funcs/density_funcs.pyx:37-73,
  *                                    S/sph/sph_func.pyx:513-531
  *   SPHDensityRate ................. S/sph/funcs/density_funcs.pyx:88-161
@@ -75,6 +78,8 @@ typedef struct {
     uint32_t rate_src[ORC_MAX_ARRAYS]; /* SPHDensityRate sources per dest */
     uint32_t xsph_src[ORC_MAX_ARRAYS]; /* XSPHCorrection sources per dest */
     double xsph_eps;
+    int32_t variable_h;        /* VarHNbrParticleLocator lists */
+    int32_t hks;               /* kernels averaged over h_a and h_b */
 } orc_system;
 
 typedef struct {
@@ -147,6 +152,38 @@ static void cs_gradient(double pax, double pay, double paz,
     g[0] = rx * (val * fac);
     g[1] = ry * (val * fac);
     g[2] = rz * (val * fac);
+}
+
+/* W and grad W of a pair as the functions evaluate them: at h_ab =
+ * (h_a + h_b) / 2, or with hks the average of the values at h_a and h_b
+ * (e.g. S/sph/funcs/density_funcs.pyx:56-63, pressure_funcs.pyx:371-381). */
+static double pair_w(const orc_system *s, const orc_array *D, int64_t i,
+                     const orc_array *S, int64_t j, double hab, int dim, double kfac)
+{
+    if (s->hks) {
+        double wa = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                                D->h[i], dim, kfac);
+        double wb = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                                S->h[j], dim, kfac);
+        return 0.5 * (wa + wb);
+    }
+    return cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim, kfac);
+}
+
+static void pair_grad(const orc_system *s, const orc_array *D, int64_t i,
+                      const orc_array *S, int64_t j, double hab, int dim, double kfac,
+                      double *g)
+{
+    if (s->hks) {
+        double ga[3], gb[3];
+        cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], D->h[i], dim,
+                    kfac, ga);
+        cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], S->h[j], dim,
+                    kfac, gb);
+        for (int d = 0; d < 3; ++d) g[d] = (ga[d] + gb[d]) * 0.5;
+        return;
+    }
+    cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim, kfac, g);
 }
 
 double orc_kernel_w(double dx, double dy, double dz, double h, int dim)
@@ -296,7 +333,7 @@ static int bin_all(const orc_system *s, orc_nnps *c)
  * swapped to the last slot when source is dest (S/base/nnps.pyx:612-619).
  * Returns the count; writes up to `cap` indices when out != NULL. */
 static int64_t query(const orc_system *s, const orc_nnps *c, int da, int sa,
-                     int64_t i, int32_t *out)
+                     int64_t i, int32_t *out, int swap_self)
 {
     const orc_array *D = &s->a[da];
     const orc_array *S = &s->a[sa];
@@ -331,7 +368,7 @@ static int64_t query(const orc_system *s, const orc_nnps *c, int da, int sa,
             }
         }
     }
-    if (out && da == sa) {
+    if (out && da == sa && swap_self) {
         for (int64_t j = 0; j < cnt - 1; ++j) {
             if (out[j] == (int32_t)i) {
                 out[j] = out[cnt - 1];
@@ -343,19 +380,81 @@ static int64_t query(const orc_system *s, const orc_nnps *c, int da, int sa,
     return cnt;
 }
 
+/* VarHNbrParticleLocator._update_cache (S/base/nnps.pyx:748-784): dest i's
+ * own query (radius from h_i, no self swap), then every source j, in index
+ * order, whose reversed query (radius from h_j, self swapped last) holds i
+ * and that is not yet in i's list. */
+static int build_lists_varh(const orc_system *s, orc_nnps *c, int da, int sa)
+{
+    int64_t nd = s->a[da].n, ns = s->a[sa].n;
+    int64_t *cnt = (int64_t *)calloc((size_t)nd, sizeof(int64_t));
+    int64_t *capa = (int64_t *)calloc((size_t)nd, sizeof(int64_t));
+    int32_t **lst = (int32_t **)calloc((size_t)nd, sizeof(int32_t *));
+    if (!cnt || !capa || !lst) return -3;
+    for (int64_t i = 0; i < nd; ++i) {
+        int64_t m = query(s, c, da, sa, i, NULL, 0);
+        capa[i] = m + 8;
+        lst[i] = (int32_t *)malloc(sizeof(int32_t) * (size_t)capa[i]);
+        if (!lst[i]) return -3;
+        cnt[i] = query(s, c, da, sa, i, lst[i], 0);
+    }
+    int32_t *rev = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nd + 1));
+    if (!rev) return -3;
+    int64_t nsr = 0;   /* the reversed locator covers the real particles */
+    for (int64_t j = 0; j < ns; ++j) nsr += s->a[sa].tag[j] == 0;
+    for (int64_t j = 0; j < nsr; ++j) {
+        int64_t m = query(s, c, sa, da, j, NULL, 1);
+        int32_t *rv = m > nd ? (int32_t *)malloc(sizeof(int32_t) * (size_t)m) : rev;
+        query(s, c, sa, da, j, rv, 1);
+        for (int64_t q = 0; q < m; ++q) {
+            int32_t k = rv[q];
+            int found = 0;
+            for (int64_t t = 0; t < cnt[k]; ++t)
+                if (lst[k][t] == (int32_t)j) { found = 1; break; }
+            if (found) continue;
+            if (cnt[k] == capa[k]) {
+                capa[k] *= 2;
+                lst[k] = (int32_t *)realloc(lst[k], sizeof(int32_t) * (size_t)capa[k]);
+                if (!lst[k]) return -3;
+            }
+            lst[k][cnt[k]++] = (int32_t)j;
+        }
+        if (rv != rev) free(rv);
+    }
+    free(rev);
+    int64_t *off = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nd + 1));
+    if (!off) return -3;
+    off[0] = 0;
+    for (int64_t i = 0; i < nd; ++i) off[i + 1] = off[i] + cnt[i];
+    int32_t *idx = (int32_t *)malloc(sizeof(int32_t) * (size_t)(off[nd] > 0 ? off[nd] : 1));
+    if (!idx) return -3;
+    for (int64_t i = 0; i < nd; ++i) {
+        memcpy(idx + off[i], lst[i], sizeof(int32_t) * (size_t)cnt[i]);
+        free(lst[i]);
+    }
+    free(lst);
+    free(cnt);
+    free(capa);
+    c->off[da][sa] = off;
+    c->idx[da][sa] = idx;
+    c->nn[da] = nd;
+    return 0;
+}
+
 static int build_lists(const orc_system *s, orc_nnps *c, int da, int sa)
 {
+    if (s->variable_h) return build_lists_varh(s, c, da, sa);
     int64_t n = s->a[da].n;
     int64_t *off = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
     if (!off) return -3;
     off[0] = 0;
 #pragma omp parallel for schedule(dynamic, 512)
-    for (int64_t i = 0; i < n; ++i) off[i + 1] = query(s, c, da, sa, i, NULL);
+    for (int64_t i = 0; i < n; ++i) off[i + 1] = query(s, c, da, sa, i, NULL, 1);
     for (int64_t i = 0; i < n; ++i) off[i + 1] += off[i];
     int32_t *idx = (int32_t *)malloc(sizeof(int32_t) * (size_t)(off[n] > 0 ? off[n] : 1));
     if (!idx) { free(off); return -3; }
 #pragma omp parallel for schedule(dynamic, 512)
-    for (int64_t i = 0; i < n; ++i) query(s, c, da, sa, i, idx + off[i]);
+    for (int64_t i = 0; i < n; ++i) query(s, c, da, sa, i, idx + off[i], 1);
     c->off[da][sa] = off;
     c->idx[da][sa] = idx;
     c->nn[da] = n;
@@ -429,8 +528,7 @@ int orc_sph_rho(const orc_system *s, const orc_nnps *c, int da, int sa,
             int32_t j = idx[k];
             double hb = S->h[j];
             double hab = 0.5 * (ha + hb);
-            double w = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j],
-                                   S->z[j], hab, dim, kfac);
+            double w = pair_w(s, D, i, S, j, hab, dim, kfac);
             nr += w * S->m[j];
         }
         out1[i] += nr;
@@ -508,8 +606,7 @@ int orc_momentum(const orc_system *s, const orc_nnps *c, int da, int sa,
             tmp += piab;
             tmp *= -mb;
             double g[3];
-            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
-                        hab, dim, kfac, g);
+            pair_grad(s, D, i, S, j, hab, dim, kfac, g);
             nr0 += tmp * g[0];
             nr1 += tmp * g[1];
             nr2 += tmp * g[2];
@@ -552,8 +649,7 @@ int orc_pgrad(const orc_system *s, const orc_nnps *c, int da, int sa,
             double artificial_stress = 0.0;
             temp = temp + artificial_stress;
             double g[3];
-            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
-                        h, dim, kfac, g);
+            pair_grad(s, D, i, S, j, h, dim, kfac, g);
             nr0 += temp * g[0];
             nr1 += temp * g[1];
             nr2 += temp * g[2];
@@ -591,8 +687,7 @@ int orc_density_rate(const orc_system *s, const orc_nnps *c, int da, int sa,
             double vy = D->v[i] - S->v[j];
             double vz = D->w[i] - S->w[j];
             double g[3];
-            cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
-                        hab, dim, kfac, g);
+            pair_grad(s, D, i, S, j, hab, dim, kfac, g);
             double dot = vx * g[0] + vy * g[1] + vz * g[2];
             nr += dot * S->m[j];
         }
@@ -630,8 +725,7 @@ int orc_xsph(const orc_system *s, const orc_nnps *c, int da, int sa, double eps,
             double vby = S->v[j] - D->v[i];
             double vbz = S->w[j] - D->w[i];
             double mb = S->m[j];
-            double w = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j],
-                                   S->z[j], hab, dim, kfac);
+            double w = pair_w(s, D, i, S, j, hab, dim, kfac);
             double temp = mb * w / rhoab;
             nr0 += temp * vbx * eps;
             nr1 += temp * vby * eps;

@@ -72,7 +72,7 @@ def lists_of(R, particles, src, dst):
     return off, np.concatenate(out) if out else np.zeros(0, np.int32)
 
 
-def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None):
+def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None, hks=False):
     """The summation-density scheme, or with xsph_eps the continuity scheme
     of the reference's dam-break example (examples/dam-break/dam_break.py:
     184-241): Tait, SPHDensityRate (integrated rho on every array), momentum,
@@ -82,16 +82,17 @@ def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None):
     vel = ["u", "v", "w"][:dim]
     pos = ["x", "y", "z"][:dim]
     if xsph_eps is None:
-        ops = [EQ.SPHOperation(D.SPHRho.withargs(), on_types=types, from_types=types,
+        ops = [EQ.SPHOperation(D.SPHRho.withargs(hks=hks), on_types=types, from_types=types,
                                updates=["rho"], id="sd"),
                EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
                                updates=["p", "cs"], id="eos")]
     else:
         ops = [EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
                                updates=["p", "cs"], id="eos"),
-               EQ.SPHIntegration(D.SPHDensityRate.withargs(hks=False), on_types=types,
+               EQ.SPHIntegration(D.SPHDensityRate.withargs(hks=hks), on_types=types,
                                  from_types=types, updates=["rho"], id="density")]
-    ops.append(EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta),
+    ops.append(EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta,
+                                                              hks=hks),
                                  on_types=[0], from_types=types, updates=vel, id="mom"))
     if gy:
         ops.append(EQ.SPHIntegration(EF.GravityForce.withargs(gy=gy), on_types=[0],
@@ -99,17 +100,18 @@ def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None):
     ops.append(EQ.SPHIntegration(POS.PositionStepping.withargs(), on_types=[0],
                                  updates=pos, id="step"))
     if xsph_eps is not None:
-        ops.append(EQ.SPHIntegration(R["X"].XSPHCorrection.withargs(eps=xsph_eps, hks=False),
+        ops.append(EQ.SPHIntegration(R["X"].XSPHCorrection.withargs(eps=xsph_eps, hks=hks),
                                      on_types=[0], from_types=[0], updates=pos, id="xsph"))
     return ops
 
 
-def build_sim(R, arrays, types, params, dim, xsph_eps=None, integrator=None):
+def build_sim(R, arrays, types, params, dim, xsph_eps=None, integrator=None,
+              variable_h=False, hks=False):
     pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
-    particles = R["P"].Particles(pas)
+    particles = R["P"].Particles(pas, variable_h=variable_h)
     kernel = R["K"].CubicSplineKernel(dim=dim)
     ops = scheme_ops(R, len(pas), params["c0"], params["rho0"], params["alpha"],
-                     params["beta"], params["eta"], params["gravity"][1], dim, xsph_eps)
+                     params["beta"], params["eta"], params["gravity"][1], dim, xsph_eps, hks)
     calcs = []
     for op in ops:
         calcs.extend(op.get_calcs(particles, kernel))
@@ -300,6 +302,43 @@ def dam_cont(R):
     return out
 
 
+def varh_drop():
+    """The drop (dx = 0.05) with smoothing lengths growing from 1.0 to 1.4
+    times 1.3 dx across x."""
+    arrays, types, params = W.elliptical_drop(dx=0.05)
+    a = arrays[0]
+    a["h"] = 1.3 * 0.05 * (1.0 + 0.2 * (a["x"] + 1.0))
+    return arrays, types, params
+
+
+def varh(R):
+    """Variable smoothing length: the reference's symmetric neighbour lists
+    (VarHNbrParticleLocator) with hks kernels, summation and continuity
+    schemes: lists, the first stage and 5 PC steps."""
+    arrays, types, params = varh_drop()
+    out = {f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS}
+    for name, eps in (("sum", None), ("cont", XSPH_EPS)):
+        pas, particles, integ = build_sim(R, arrays, types, params, 2, eps,
+                                          variable_h=True, hks=True)
+        if name == "sum":
+            off, idx = lists_of(R, particles, pas[0], pas[0])
+            out["nbr_off"], out["nbr_idx"] = off, idx
+        integ.save_initial_arrays()
+        integ.reset_accelerations(step=1)
+        integ.eval()
+        names = ("rho", "p", "cs", "_a_u_1", "_a_v_1", "dt_fac") + (
+            ("_a_rho_1", "_a_x_1", "_a_y_1") if eps else ())
+        out.update({f"{name}_stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                    for n in names})
+        pas, particles, integ = build_sim(R, arrays, types, params, 2, eps,
+                                          variable_h=True, hks=True)
+        for _ in range(5):
+            particles.update()
+            integ.integrate(1e-5)
+        out.update({f"{name}_step5_{k}": v for k, v in state(pas).items()})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", default=os.path.join(ROOT, "_work", "refbuild"))
@@ -309,7 +348,7 @@ def main():
     R = ref_modules(a.build)
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
                      ("drop_cont", drop_cont), ("dam_cont", dam_cont),
-                     ("integrators", integrators)):
+                     ("integrators", integrators), ("varh", varh)):
         if a.only and name not in a.only:
             continue
         data = fn(R)

@@ -199,3 +199,45 @@ def test_integrators_bit_exact(name, integ, cont, steps):
     for n in ("x", "y", "u", "v", "rho", "p", "cs"):
         np.testing.assert_array_equal(getattr(A, n), g[f"{name}_step{steps}_{n}_0"],
                                       err_msg=f"{name} {n}")
+
+
+# -- variable smoothing length: symmetric lists and hks kernels ---------------
+def oracle_varh(g, scheme):
+    arrs = [OracleArray("a0", **{k: g[f"in_{k}"].copy() for k in PROPS})]
+    return OracleSystem(arrs, dim=2, rho_src=scheme.rho_src, tait_on=scheme.tait_on,
+                        mom_src=scheme.mom_src, step_on=scheme.step_on,
+                        rate_src=scheme.rate_src, xsph_src=scheme.xsph_src,
+                        xsph_eps=scheme.xsph_eps, variable_h=True, hks=True, **DROP)
+
+
+def test_varh_lists_in_reference_order():
+    """VarHNbrParticleLocator: each dest's own radius-h_a list, then every
+    source whose radius-h_b list holds it, in source order."""
+    g = load("varh")
+    o = oracle_varh(g, fluid_scheme(1))
+    o.update()
+    off, idx = o.neighbors(0, 0)
+    np.testing.assert_array_equal(off, g["nbr_off"])
+    np.testing.assert_array_equal(idx, g["nbr_idx"])
+
+
+@pytest.mark.parametrize("name", ["sum", "cont"])
+def test_varh_hks_first_stage_and_steps_bit_exact(name):
+    g = load("varh")
+    sch = fluid_scheme(1) if name == "sum" else continuity_scheme(1, 0.5)
+    o = oracle_varh(g, sch)
+    o.update()
+    o.eval()
+    A = o.arrays[0]
+    got = {"rho": A.rho, "p": A.p, "cs": A.cs, "_a_u_1": A.au, "_a_v_1": A.av,
+           "dt_fac": A.dt_fac, "_a_rho_1": A.arho, "_a_x_1": A.ax, "_a_y_1": A.ay}
+    for key in g:
+        if key.startswith(f"{name}_stage0_"):
+            n = key[len(f"{name}_stage0_"):]
+            np.testing.assert_array_equal(got[n], g[key], err_msg=n)
+    o = oracle_varh(g, sch)
+    for _ in range(5):
+        o.pc_step(1e-5)
+    for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+        np.testing.assert_array_equal(getattr(o.arrays[0], n), g[f"{name}_step5_{n}_0"],
+                                      err_msg=n)
