@@ -113,6 +113,14 @@ typedef struct {
                                skin_max / 2 from where it was binned
                                (0: lists serve one stage only) */
     double xsph_eps;        /* XSPHCorrection eps */
+    int32_t variable_h;     /* 1: symmetric neighbour lists, r < radius_scale
+                               max(h_a, h_b) (VarHNbrParticleLocator,
+                               S/base/nnps.pyx:691-786); 0: r < radius_scale
+                               h_a (FixedDestNbrParticleLocator).  The cells
+                               must cover radius_scale times the largest h */
+    int32_t hks;            /* 1: every pair function averages its kernel over
+                               h_a and h_b instead of using (h_a + h_b) / 2
+                               (the functions' `hks` option) */
 } sphb_scene;
 
 /* Per-scene state, written by the kernels (host may seed dt, t, count). */

@@ -71,7 +71,8 @@ class Scene(ctypes.Structure):
                 ("alpha", f64), ("beta", f64), ("eta", f64), ("g", f64 * 3),
                 ("cfl", f64), ("dt_initial", f64), ("static_lo", f64 * 3),
                 ("static_hi", f64 * 3), ("use_cfl", i32), ("uniform_h", i32),
-                ("skin_max", f64), ("xsph_eps", f64)]
+                ("skin_max", f64), ("xsph_eps", f64),
+                ("variable_h", i32), ("hks", i32)]
 
 
 class SceneState(ctypes.Structure):

@@ -39,6 +39,8 @@ class Rollout:
                  device=None, lanes: int = 1, pair_block: int = 128):
         if scheme.continuity:
             raise NotImplementedError("the adjoint covers the summation-density scheme")
+        if scheme.hks:
+            raise NotImplementedError("the adjoint covers kernels at h_ab only (hks off)")
         if scheme.mom_src and set(scheme.step_on) != set(scheme.mom_src):
             raise ValueError("the integrated arrays must be the MomentumEquation dests")
         self.arrays = arrays

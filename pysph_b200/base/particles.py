@@ -60,7 +60,7 @@ class Session:
             specs.append(d)
         self.engine = Engine([(specs, self.params)], scheme, dim=dim,
                              precision=precision, lanes=lanes, pair_block=pair_block,
-                             device=arrays[0].device)
+                             device=arrays[0].device, variable_h=particles.variable_h)
         self.valid = {}
         for a, pa in enumerate(arrays):
             for name in IMPORTABLE:
@@ -180,7 +180,11 @@ class Session:
 class Locator:
     """Neighbour lists of a (source, dest) pair: FixedDestNbrParticleLocator
     (S/base/nnps.pyx:385-686), computed by the engine with the reference's
-    predicate r^2 < (radius_scale h_dest)^2; self last when source is dest."""
+    predicate r^2 < (radius_scale h_dest)^2; self last when source is dest.
+    With Particles(variable_h=True) the lists are VarHNbrParticleLocator's
+    symmetric sets (S/base/nnps.pyx:691-786), r^2 < (radius_scale h_dest)^2
+    or r^2 < (radius_scale h_source)^2, in ascending source index with self
+    last (the reference lists the same particles in its cell order)."""
 
     def __init__(self, particles, source, dest, radius_scale):
         self.particles = particles
@@ -254,8 +258,6 @@ class Particles:
             assert arr.cl_precision == prec, "All arrays must have the same cl_precision"
         if in_parallel:
             raise NotImplementedError("MPI-distributed particles are not part of this build")
-        if variable_h:
-            raise NotImplementedError("variable-h neighbour search is not part of this build")
         if periodic_domain is not None:
             raise NotImplementedError("periodic domains are not part of this build")
         devs = {str(a.device) for a in arrays}
@@ -263,7 +265,9 @@ class Particles:
             raise ValueError("all arrays must live on one device")
         self.arrays = arrays
         self.in_parallel = False
-        self.variable_h = False
+        # symmetric neighbour sets for varying smoothing lengths
+        # (VarHNbrParticleLocator, S/base/nnps.pyx:691-786)
+        self.variable_h = bool(variable_h)
         self.max_radius_scale = max_radius_scale
         self.precision = precision or ("fp32c" if prec == "single" else "fp64")
         self.kernel = None

@@ -11,6 +11,12 @@
 // FP32C: pair geometry in FP32 from cell-relative positions, the sum in FP32
 // with Kahan compensation, the EOS in FP64.  FP64: the reference's
 // arithmetic, with its exact neighbour predicate.
+//
+// Variable smoothing length (scene.variable_h): the neighbours are the
+// symmetric set of VarHNbrParticleLocator (S/base/nnps.pyx:691-786),
+// r^2 < (radius_scale h_a)^2 or r^2 < (radius_scale h_b)^2.  With scene.hks
+// the pair's W is the mean of W(r, h_a) and W(r, h_b) (density_funcs.pyx:
+// 56-63) instead of W(r, (h_a + h_b) / 2).
 
 #include <type_traits>
 
@@ -96,6 +102,10 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const float kf = (float)kfac_unit<DIM>();
             const float ihk = __fdividef(1.0f, hk);
             const float fack = DIM == 2 ? kf * ihk * ihk : kf * ihk * ihk * ihk;
+            // variable h: symmetric lists and, with hks, W averaged over h_a, h_b
+            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
+            const float rsf = (float)sc.radius_scale;
+            const float skinf = (float)skin;
             struct Rec {
                 float4 g;
                 float m, o, dy, dz;
@@ -128,15 +138,35 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             auto pass = [&](auto uniform) {
                 constexpr bool UH = decltype(uniform)::value;
                 auto use = [&](const Rec &r, float r2) {
-                    if (lists_only || !(r.ok && r2 < rad2)) return;
-                    float ih = ihk, fac = fack;
-                    if (!UH) {
-                        const float hj = DIM == 3 ? r.g.w : r.g.z;
-                        ih = __fdividef(1.0f, 0.5f * (hk + hj));
-                        fac = DIM == 2 ? kf * ih * ih : kf * ih * ih * ih;
+                    if (lists_only || !r.ok) return;
+                    const float hj = DIM == 3 ? r.g.w : r.g.z;
+                    if (UH || !vh) {
+                        if (!(r2 < rad2)) return;
+                    } else {
+                        const float rj = hj * rsf;   // r < radius_scale max(h_a, h_b)
+                        if (!(r2 < rad2 || r2 < rj * rj)) return;
                     }
                     const float ir = rsqrtf(fmaxf(r2, 1e-30f));   // q = 0 at r = 0
-                    acc.add(r.m * w_cubic_bf(r2 * ir * ih, fac));
+                    float w;
+                    if (UH) {
+                        w = w_cubic_bf(r2 * ir * ihk, fack);
+                    } else {
+                        // W(r, h_ab), or with hks (W(r, h_a) + W(r, h_b)) / 2; one
+                        // kernel evaluation in a loop keeps the register count
+                        const float rr = r2 * ir;
+                        float hs = hks ? hk : 0.5f * (hk + hj);
+                        w = 0.f;
+#pragma unroll 1
+                        for (int t = 0;; ++t) {
+                            const float ih = __fdividef(1.0f, hs);
+                            const float fac = DIM == 2 ? kf * ih * ih : kf * ih * ih * ih;
+                            w += w_cubic_bf(rr * ih, fac);
+                            if (!hks || t == 1) break;
+                            hs = hj;
+                        }
+                        if (hks) w *= 0.5f;
+                    }
+                    acc.add(r.m * w);
                     ++np;
                 };
                 const int lc = list_count<LANES>(e, from_list, k, lane);
@@ -152,7 +182,14 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     [&](int j, int o, int dy, int dz) {
                         const Rec r = load(EntryF{j, (float)o, (float)dy, (float)dz});
                         const float r2 = dist2(r);
-                        if (r2 < radl2) record(j, o, dy, dz);
+                        bool rec = r2 < radl2;
+                        if (!UH && vh && nbr && !rec) {
+                            // the larger of the two supports, with the skin
+                            const float hj = DIM == 3 ? r.g.w : r.g.z;
+                            const float rl = (hj * rsf + skinf) * (1.0f + 1e-5f);
+                            rec = hj > hk && r2 < rl * rl;
+                        }
+                        if (rec) record(j, o, dy, dz);
                         use(r, r2);
                     });
             };
@@ -176,6 +213,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const double rad2 = __dmul_rn(rad, rad);
             const double radl = (rad + skin) * (1.0 + 1e-5);
             const double radl2 = nbr ? radl * radl : rad2;
+            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
@@ -185,13 +223,26 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     const double dy = yk - __ldg(B.y + j);
                     const double dz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
                     const double d2 = dist2_ref<DIM>(dx, dy, dz);
-                    if (d2 < radl2) {
+                    const double hb = __ldg(B.h + j);
+                    double radj2 = rad2, radlj2 = radl2;
+                    if (vh) {
+                        // symmetric: r^2 < (radius_scale h_a)^2 or (radius_scale h_b)^2
+                        const double rj = hb * sc.radius_scale;
+                        radj2 = fmax(rad2, __dmul_rn(rj, rj));
+                        const double rl = (fmax(rad, rj) + skin) * (1.0 + 1e-5);
+                        radlj2 = nbr ? rl * rl : radj2;
+                    }
+                    if (d2 < radlj2) {
                         record(j, o, oy, oz);
                         const bool sums =
                             !lists_only && (!filt || ((rsrc >> seg.array_of(j)) & 1u));
-                        if (sums && d2 < rad2) {
-                            const double hab = 0.5 * (hk + __ldg(B.h + j));
-                            sum += w_cubic_d<DIM>(sqrt(d2), hab) * __ldg(B.m + j);
+                        if (sums && d2 < radj2) {
+                            double w;
+                            if (hks)
+                                w = 0.5 * (w_cubic_d<DIM>(sqrt(d2), hk) + w_cubic_d<DIM>(sqrt(d2), hb));
+                            else
+                                w = w_cubic_d<DIM>(sqrt(d2), 0.5 * (hk + hb));
+                            sum += w * __ldg(B.m + j);
                             ++np;
                         }
                     }
@@ -280,7 +331,8 @@ k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
     }
 }
 
-// Neighbour lists with the reference's exact FP64 predicate.
+// Neighbour lists with the reference's exact FP64 predicate (the symmetric
+// one with variable h).
 template <int DIM, int R>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_neighbors(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, uint32_t src_mask,
@@ -298,6 +350,7 @@ k_neighbors(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     const double xk = B.x[k], yk = B.y[k], zk = DIM == 3 ? B.z[k] : 0.0;
     const double rad = B.h[k] * e.scene[s].radius_scale;
     const double rad2 = __dmul_rn(rad, rad);
+    const bool vh = e.scene[s].variable_h != 0;
     int cx, cy, cz;
     cell_coords(e.f.cell[k], n, cx, cy, cz);
     int cnt = 0;
@@ -309,7 +362,14 @@ k_neighbors(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
             const double dx = B.x[j] - xk;
             const double dy = B.y[j] - yk;
             const double dz = DIM == 3 ? B.z[j] - zk : 0.0;
-            if (dist2_ref<DIM>(dx, dy, dz) < rad2) {
+            const double d2 = dist2_ref<DIM>(dx, dy, dz);
+            bool in = d2 < rad2;
+            if (vh && !in) {
+                // variable h: also the particles whose own support holds k
+                const double rj = B.h[j] * e.scene[s].radius_scale;
+                in = d2 < __dmul_rn(rj, rj);
+            }
+            if (in) {
                 if (offs) {
                     const long long pos = base + cnt;
                     if (pos < cap) out[pos] = j;

@@ -11,6 +11,10 @@
 // SPHPressureGradient (:62-161) is the same without Pi and dt_fac.
 // GravityForce (S/sph/funcs/external_force.pyx:13-62) adds g afterwards.
 // Per scene the kernel also keeps max dt_fac and max |a|^2 for the CFL rule.
+// Variable h (scene.variable_h): the symmetric neighbour set r < radius_scale
+// max(h_a, h_b); with scene.hks every pair function's W and grad W are the
+// means of their values at h_a and h_b (pressure_funcs.pyx:141-149,
+// 371-381), the viscosity and dt_fac keep h_ab.
 
 #include <type_traits>
 
@@ -93,6 +97,10 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             // fac / h of the dest: 2D kf/h^3, 3D kf/h^4
             const float fihk = DIM == 2 ? kf * ihk * ihk * ihk : kf * ihk * ihk * ihk * ihk;
             const float eh2k = eta2 * hk * hk;
+            // variable h: symmetric lists and, with hks, W and grad W
+            // averaged over h_a and h_b (the AV and the CFL keep h_ab)
+            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
+            const float rsf = (float)sc.radius_scale;
             struct Rec {
                 float4 g, t;
                 float vx, vy, vz, m, o, dy, dz;
@@ -138,17 +146,21 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         rz = (zk - r.g.z) - r.dz * csf;
                         r2 += rz * rz;
                     }
-                    if (!(r.ok && r2 < rad2)) return;
+                    if (!r.ok) return;
+                    const float hj = DIM == 3 ? r.g.w : r.g.z;
+                    if (UH || !vh) {
+                        if (!(r2 < rad2)) return;
+                    } else {
+                        const float rj = hj * rsf;   // r < radius_scale max(h_a, h_b)
+                        if (!(r2 < rad2 || r2 < rj * rj)) return;
+                    }
                     ++np;
                     const bool mom_on = !CONT || (mm & r.bit);
                     const bool rate_on = CONT && (rm & r.bit);
                     const bool xs_on = CONT && (xm & r.bit);
-                    float hab = hk, ih = ihk, fih = fihk, eh2 = eh2k;
+                    float hab = hk, eh2 = eh2k;
                     if (!UH) {
-                        const float hj = DIM == 3 ? r.g.w : r.g.z;
                         hab = 0.5f * (hk + hj);
-                        ih = __fdividef(1.0f, hab);
-                        fih = DIM == 2 ? kf * ih * ih * ih : kf * ih * ih * ih * ih;
                         eh2 = eta2 * hab * hab;
                     }
                     float tmp = tk.w + r.t.w;   // P_a/rho_a^2 + P_b/rho_b^2
@@ -157,14 +169,38 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     if (DIM == 3) dot += vz * rz;
                     // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
                     const float ir = rsqrtf(fmaxf(r2, 1e-30f));
-                    const float q = r2 * ir * ih;
-                    const float gw = gw_cubic_bf(q, ir, ih, fih);
+                    // grad W / r (and W for XSPH) at h_ab, or with hks the means
+                    // of the values at h_a and h_b: one evaluation in a loop
+                    // keeps the register count of the uniform-h path
+                    float gw, w = 0.f;
+                    if (UH) {
+                        const float q = r2 * ir * ihk;
+                        gw = gw_cubic_bf(q, ir, ihk, fihk);
+                        if (CONT && xs_on) w = w_cubic_bf(q, fihk * hk);
+                    } else {
+                        const float rr = r2 * ir;
+                        float hs = hks ? hk : hab;
+                        gw = 0.f;
+#pragma unroll 1
+                        for (int t = 0;; ++t) {
+                            const float ih = __fdividef(1.0f, hs);
+                            const float fih = DIM == 2 ? kf * ih * ih * ih : kf * ih * ih * ih * ih;
+                            const float q = rr * ih;
+                            gw += gw_cubic_bf(q, ir, ih, fih);
+                            if (CONT && xs_on) w += w_cubic_bf(q, fih * hs);
+                            if (!hks || t == 1) break;
+                            hs = hj;
+                        }
+                        if (hks) {
+                            gw *= 0.5f;
+                            w *= 0.5f;
+                        }
+                    }
                     if (CONT) {
                         // drho_a += m_b (v_a - v_b) . grad_a W
                         if (rate_on) kr.add(r.m * (dot * gw));
                         // XSPH: eps m_b W_ab (v_b - v_a) / rho_ab (eps at the end)
                         if (xs_on) {
-                            const float w = w_cubic_bf(q, fih * hab);
                             const float temp = __fdividef(r.m * w, 0.5f * (tk.x + r.t.x));
                             kxx.add(-temp * vx);
                             kxy.add(-temp * vy);
@@ -244,6 +280,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             const double rad = hk * sc.radius_scale;
             const double rad2 = __dmul_rn(rad, rad);
             const double alpha = sc.alpha, beta = sc.beta, eta = sc.eta;
+            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
@@ -253,25 +290,49 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     const double ry = yk - __ldg(B.y + j);
                     const double rz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
                     const double rab2 = dist2_ref<DIM>(rx, ry, rz);
-                    if (!(rab2 < rad2)) return;
+                    const double hb = __ldg(B.h + j);
+                    double radj2 = rad2;
+                    if (vh) {
+                        // symmetric: r^2 < (radius_scale h_a)^2 or (radius_scale h_b)^2
+                        const double rj = hb * sc.radius_scale;
+                        radj2 = fmax(rad2, __dmul_rn(rj, rj));
+                    }
+                    if (!(rab2 < radj2)) return;
                     ++np;
                     const uint32_t bit = filt ? 1u << seg.array_of(j) : ~0u;
-                    const double hab = 0.5 * (hk + __ldg(B.h + j));
+                    const double hab = 0.5 * (hk + hb);
                     const double rhob = __ldg(rho + j), Pb = __ldg(pr + j);
                     const double mb = __ldg(B.m + j);
+                    // grad_a W: at h_ab, or with hks the mean of the gradients
+                    // at h_a and h_b (pressure_funcs.pyx:371-381)
+                    double gx, gy, gz = 0.0;
+                    if (hks) {
+                        const double ga = gw_cubic_d<DIM>(sqrt(rab2), hk);
+                        const double gb = gw_cubic_d<DIM>(sqrt(rab2), hb);
+                        gx = (rx * ga + rx * gb) * 0.5;
+                        gy = (ry * ga + ry * gb) * 0.5;
+                        if (DIM == 3) gz = (rz * ga + rz * gb) * 0.5;
+                    } else {
+                        const double g = gw_cubic_d<DIM>(sqrt(rab2), hab);
+                        gx = rx * g;
+                        gy = ry * g;
+                        if (DIM == 3) gz = rz * g;
+                    }
                     if (CONT) {
                         const double vbx = __ldg(B.u + j), vby = __ldg(B.v + j);
                         const double vbz = DIM == 3 ? __ldg(B.w + j) : 0.0;
                         if (rm & bit) {
                             // SPHDensityRate: ((v_a - v_b) . grad_a W) m_b
-                            const double g = gw_cubic_d<DIM>(sqrt(rab2), hab);
-                            double d = (uk - vbx) * (rx * g) + (vk - vby) * (ry * g);
-                            if (DIM == 3) d += (wk - vbz) * (rz * g);
+                            double d = (uk - vbx) * gx + (vk - vby) * gy;
+                            if (DIM == 3) d += (wk - vbz) * gz;
                             drho += d * mb;
                         }
                         if (xm & bit) {
                             // XSPHCorrection: m_b W_ab / rho_ab (v_b - v_a) eps
-                            const double w = w_cubic_d<DIM>(sqrt(rab2), hab);
+                            const double w =
+                                hks ? 0.5 * (w_cubic_d<DIM>(sqrt(rab2), hk) +
+                                             w_cubic_d<DIM>(sqrt(rab2), hb))
+                                    : w_cubic_d<DIM>(sqrt(rab2), hab);
                             const double temp = mb * w / (0.5 * (rhob + rhoa));
                             xs[0] += temp * (vbx - uk) * sc.xsph_eps;
                             xs[1] += temp * (vby - vk) * sc.xsph_eps;
@@ -299,10 +360,9 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         }
                     }
                     tmp *= -mb;
-                    const double gw = gw_cubic_d<DIM>(sqrt(rab2), hab);
-                    acc[0] += tmp * (rx * gw);
-                    acc[1] += tmp * (ry * gw);
-                    if (DIM == 3) acc[2] += tmp * (rz * gw);
+                    acc[0] += tmp * gx;
+                    acc[1] += tmp * gy;
+                    if (DIM == 3) acc[2] += tmp * gz;
                 });
         }
 #pragma unroll

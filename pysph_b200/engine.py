@@ -59,7 +59,9 @@ class Scheme:
 
     Summation density: rho_src (SPHRho).  Continuity equation: rate_src
     (SPHDensityRate, rho integrated on its dests), optionally with
-    XSPHCorrection (xsph_src, xsph_eps) added to the position rate."""
+    XSPHCorrection (xsph_src, xsph_eps) added to the position rate.  hks:
+    every pair function averages its kernel over h_a and h_b (the
+    functions' hks option) instead of evaluating it at (h_a + h_b) / 2."""
     rho_src: dict = field(default_factory=dict)   # dest -> [sources]
     mom_src: dict = field(default_factory=dict)   # dest -> [sources]
     tait_on: tuple = ()
@@ -67,6 +69,7 @@ class Scheme:
     rate_src: dict = field(default_factory=dict)  # dest -> [sources]
     xsph_src: dict = field(default_factory=dict)  # dest -> [sources]
     xsph_eps: float = 0.5
+    hks: bool = False
 
     @property
     def continuity(self) -> bool:
@@ -144,7 +147,7 @@ class Engine:
                  pair_block: int = 128, cell_capacity: int | None = None,
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
                  step_lists: bool = True, skin_margin: float | None = None,
-                 list_batch: int = 4):
+                 list_batch: int = 4, variable_h: bool = False):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -192,6 +195,9 @@ class Engine:
         if self.step_lists and not 0.0 < skin_margin <= 1.0:
             raise ValueError("skin_margin must be in (0, 1]")
         self.skin_margin = float(skin_margin) if self.step_lists else 0.0
+        # symmetric neighbour sets r < radius_scale max(h_a, h_b)
+        # (VarHNbrParticleLocator) instead of r < radius_scale h_a
+        self.variable_h = bool(variable_h)
         self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
@@ -210,6 +216,7 @@ class Engine:
         step = set(self.scheme.step_on)
         sc = (nat.Scene * self.S)()
         self._extent = []
+        self._h_cap = []     # largest h the cells of each scene cover
         for s, (arrays, _) in enumerate(scenes):
             p = self.params[s]
             hs = [np.asarray(_np(arr["h"]), np.float64) for arr in arrays]
@@ -234,12 +241,15 @@ class Engine:
                         lo[d] = min(lo[d], pts[d].min())
                         hi[d] = max(hi[d], pts[d].max())
             self._extent.append((alo, ahi, cs))
+            self._h_cap.append(max_h)
             t = sc[s]
             t.cell_size = cs
             # list radius (support + skin)(1 + 1e-5) must stay within R cells
             t.skin_max = (p.radius_scale * max_h * (self.skin_margin - 1e-4)
                           if self.skin_margin else 0.0)
             t.xsph_eps = self.scheme.xsph_eps
+            t.variable_h = int(self.variable_h)
+            t.hks = int(bool(self.scheme.hks))
             t.radius_scale = p.radius_scale
             t.h_min = h_min
             t.c0, t.rho0, t.gamma = p.c0, p.rho0, p.gamma
@@ -547,6 +557,15 @@ class Engine:
             t.use_cfl = (1 if p.cfl_force else 2) if p.cfl > 0 else 0
         self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
 
+    def set_hks(self, hks: bool):
+        """The pair functions' hks option for the next passes (scene table
+        re-uploaded when it changes)."""
+        if all(t.hks == int(bool(hks)) for t in self._scene_host):
+            return
+        for t in self._scene_host:
+            t.hks = int(bool(hks))
+        self.scene_dev.copy_(_struct_to_device(self._scene_host, self.device))
+
     def set_xsph_eps(self, eps: float):
         """XSPHCorrection eps of every scene (scene table re-uploaded when it
         changes)."""
@@ -724,6 +743,15 @@ class Engine:
         v = values.to(device=self.device, dtype=torch.float64).contiguous()
         if v.numel() != self.user_n[array]:
             raise ValueError("size mismatch")
+        if name == "h" and v.numel():
+            # the cells were sized for the largest h at construction
+            off = self.user_offset_host[array]
+            hm = v.cpu().numpy()
+            for s in range(self.S):
+                n = int(self.sizes[s, array])
+                if n and float(hm[off[s]:off[s] + n].max()) > self._h_cap[s]:
+                    raise ValueError("smoothing length above the largest one the cells were "
+                                     "sized for: build a new engine")
         self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 0,
                   v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it

@@ -71,6 +71,10 @@ def fused_plan(particles, calcs):
             d = idx(calc.dest)
             srcs = sum(1 << idx(s) for s in calc.sources)
             ups = list(calc.updates)
+            # one hks option for every pair function of the fused passes
+            for f in calc.funcs:
+                if f.kind == "pair":
+                    agree("hks", bool(f.hks))
             vel = ["u", "v", "w"][:dim]
             pos = ["x", "y", "z"][:dim]
             if cls is SPHRho:
@@ -131,7 +135,7 @@ def fused_plan(particles, calcs):
     tait_only = tait_on - set(rho_src) if not rate_src else set()
     scheme = Scheme(rho_src=rho_src, mom_src=mom_src, tait_on=tuple(sorted(tait_on)),
                     step_on=tuple(sorted(step_on)), rate_src=rate_src, xsph_src=xsph_src,
-                    xsph_eps=params.get("xsph_eps", 0.5))
+                    xsph_eps=params.get("xsph_eps", 0.5), hks=params.get("hks", False))
     p = SceneParams(**{k: v for k, v in params.items()
                        if k in SceneParams.__dataclass_fields__})
     return FusedPlan(scheme, p, mode or 0, dim, tuple(sorted(tait_only)))

@@ -135,6 +135,8 @@ def evaluate(calc: SPHCalc, outs):
     params = f0.params()
     if params:
         eng.update_params(**params)
+    if f0.kind == "pair":
+        eng.set_hks(f0.hks)
     s.ensure(reads)
     dim = calc.kernel.dim
     if op == "density":

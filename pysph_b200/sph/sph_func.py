@@ -85,10 +85,10 @@ class SPHFunctionParticle(SPHFunction):
                  nbr_locator=None, *args, **kwargs):
         SPHFunction.__init__(self, source, dest, setup_arrays)
         self.dest = dest
-        self.hks = hks
+        # hks: W and grad W averaged over h_a and h_b instead of taken at
+        # (h_a + h_b) / 2 (e.g. S/sph/funcs/density_funcs.pyx:56-63)
+        self.hks = bool(hks)
         self.exclude_self = exclude_self
-        if hks:
-            raise NotImplementedError("hks kernel symmetrisation is not part of this build")
         if exclude_self:
             raise NotImplementedError("exclude_self is not part of this build")
 

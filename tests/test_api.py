@@ -120,11 +120,9 @@ def test_fused_plan_rejects_other_orders():
 def test_unsupported_features_fail_loudly():
     f, w = arrays()
     with pytest.raises(NotImplementedError):
-        base.Particles([f], variable_h=True)
+        base.Particles([f], periodic_domain=object())
     with pytest.raises(NotImplementedError):
         sph.MomentumEquation(f, f, deltap=0.1)
-    with pytest.raises(NotImplementedError):
-        sph.XSPHCorrection(f, f, hks=True)
     # as the reference: XSPH needs the position stepping it corrects
     with pytest.raises(AssertionError):
         solver.Solver(dim=2).add_operation_xsph(eps=0.5)
@@ -208,3 +206,33 @@ def test_output_format_v1_round_trip(tmp_path):
     assert np.allclose(f.get("u").cpu().numpy(), np.linspace(0.0, 1.0, 11))
     with pytest.raises(IOError):
         s.load_output(3)
+
+
+def test_variable_h_and_hks_options():
+    """Particles(variable_h=True) selects the symmetric neighbour sets; the
+    functions' hks option reaches the fused scheme when every pair function
+    agrees on it, and calc by calc otherwise."""
+    f, w = arrays()
+    assert base.Particles([f], variable_h=True).variable_h
+    assert sph.XSPHCorrection(f, f, hks=True).hks
+    sc = continuity_solver().integrator.plan.scheme
+    assert not sc.hks
+
+    def solver_hks(rho_hks, mom_hks):
+        f, _ = arrays()
+        particles = base.Particles([f], variable_h=True)
+        s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+        s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(hks=rho_hks), on_types=[Fluid],
+                                            from_types=[Fluid], updates=["rho"], id="sd"))
+        s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=62.6, ro=1000.0),
+                                            on_types=[Fluid], updates=["p", "cs"], id="eos"))
+        s.add_operation(solver.SPHIntegration(
+            sph.MomentumEquation.withargs(alpha=0.1, beta=0.0, hks=mom_hks),
+            on_types=[Fluid], from_types=[Fluid], updates=["u", "v"], id="mom"))
+        s.add_operation_step([Fluid])
+        s.setup(particles)
+        return s.integrator.plan
+
+    assert solver_hks(True, True).scheme.hks
+    assert not solver_hks(False, False).scheme.hks
+    assert solver_hks(True, False) is None

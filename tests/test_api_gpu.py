@@ -331,3 +331,104 @@ def test_solver_other_integrators_match_oracle(integ):
     for n in ("x", "y"):
         assert np.max(np.abs(pa.get(n).cpu().numpy() - getattr(O, n))) / dx <= 1e-10, n
     assert np.max(np.abs(pa.rho.cpu().numpy() - O.rho) / O.rho) <= 1e-12
+
+
+# -- variable smoothing length: Particles(variable_h=True), hks functions -----
+def varh_arrays():
+    """The drop (dx = 0.05) with h growing from 1.0 to 1.4 times 1.3 dx
+    across x."""
+    arrays, _, params = W.elliptical_drop(dx=0.05)
+    a = arrays[0]
+    a["h"] = 1.3 * 0.05 * (1.0 + 0.2 * (a["x"] + 1.0))
+    return arrays, params
+
+
+def varh_oracle(arrays, cont):
+    from oracle import OracleArray, OracleSystem
+    sch = {"rate_src": {0: [0]}, "xsph_src": {0: [0]}} if cont else {"rho_src": {0: [0]}}
+    return OracleSystem([OracleArray("a0", **{k: np.array(v, np.float64)
+                                             for k, v in arrays[0].items()})],
+                        dim=2, tait_on=(0,), mom_src={0: [0]}, step_on=(0,), xsph_eps=0.5,
+                        c0=1400.0, rho0=1.0, alpha=0.1, beta=0.0, eta=0.1,
+                        variable_h=True, hks=True, **sch)
+
+
+def varh_solver(cont, precision=None):
+    arrays, params = varh_arrays()
+    pa = base.get_particle_array(name="fluid", **arrays[0])
+    particles = base.Particles([pa], variable_h=True, precision=precision)
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+    if not cont:
+        s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(hks=True), on_types=[Fluid],
+                                            from_types=[Fluid], updates=["rho"], id="sd"))
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=1400.0, ro=1.0),
+                                        on_types=[Fluid], updates=["p", "cs"], id="eos"))
+    if cont:
+        s.add_operation(solver.SPHIntegration(sph.SPHDensityRate.withargs(hks=True),
+                                              on_types=[Fluid], from_types=[Fluid],
+                                              updates=["rho"], id="density"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=0.1, beta=0.0, eta=0.1, hks=True),
+        on_types=[Fluid], from_types=[Fluid], updates=["u", "v"], id="mom"))
+    s.add_operation_step([Fluid])
+    if cont:
+        s.add_operation_xsph(eps=0.5, hks=True)
+    s.set_time_step(1e-5)
+    s.set_final_time(5e-5 - 1e-12)
+    s.setup(particles)
+    return s, pa, arrays
+
+
+def test_varh_locator_symmetric_sets():
+    """Particles(variable_h=True): the locator hands out the symmetric sets
+    of VarHNbrParticleLocator, self last."""
+    arrays, _ = varh_arrays()
+    pa = base.get_particle_array(name="fluid", **{n: arrays[0][n] for n in ("x", "y", "h", "m")})
+    particles = base.Particles([pa], variable_h=True)
+    particles.kernel = base.CubicSplineKernel(dim=2)
+    loc = particles.nnps_manager.get_neighbor_particle_locator(pa, pa, 2.0)
+    osys = varh_oracle(arrays, False)
+    osys.update_pairs([(0, 0)])
+    off, idx = osys.neighbors(0, 0)
+    for i in range(pa.get_number_of_particles()):
+        got = loc.py_get_nearest_particles(i)
+        ref = idx[off[i]:off[i + 1]]
+        assert got[-1] == i
+        assert sorted(got.tolist()) == sorted(ref.tolist())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("cont", [False, True])
+def test_solver_varh_hks_matches_oracle(precision, cont):
+    """Variable h with hks kernels through Solver.solve (fused on the engine)
+    against the oracle, itself pinned to the reference's fixtures."""
+    s, pa, arrays = varh_solver(cont, precision)
+    plan = s.integrator.plan
+    assert plan is not None and plan.scheme.hks and plan.scheme.continuity == cont
+    s.solve()
+    assert s.count == 5
+    o = varh_oracle(arrays, cont)
+    for _ in range(5):
+        o.pc_step(1e-5)
+    O = o.arrays[0]
+    dx = 0.05
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        assert np.max(np.abs(pa.get(n).cpu().numpy() - getattr(O, n))) / dx <= tol, n
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.max(np.abs(pa.rho.cpu().numpy() - O.rho) / O.rho) <= rtol
+
+
+@pytest.mark.parametrize("cont", [False, True])
+def test_varh_building_blocks_match_fused(cont):
+    """The hks functions calc by calc give the fused step's result."""
+    s1, pa1, _ = varh_solver(cont)
+    s2, pa2, _ = varh_solver(cont)
+    s2.integrator.plan = None
+    for _ in range(3):
+        s1.integrator.integrate(1e-5)
+        s2.integrator.integrate(1e-5)
+    for n in ("x", "y", "u", "v", "rho"):
+        a = pa1.get(n).cpu().numpy()
+        b = pa2.get(n).cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, np.max(np.abs(a))), n

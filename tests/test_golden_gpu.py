@@ -221,3 +221,75 @@ def test_integrators_five_steps(precision, name, kind, cont):
     rtol = 1e-12 if precision == "fp64" else 1e-5
     ref = g[f"{name}_step5_rho_0"]
     assert np.max(np.abs(rho - ref) / ref) <= rtol
+
+
+# -- variable smoothing length: symmetric lists and hks kernels ---------------
+def varh_scheme(cont):
+    sch = continuity_scheme(1, 0.5) if cont else fluid_scheme(1)
+    sch.hks = True
+    return sch
+
+
+def test_varh_neighbour_sets():
+    """Symmetric neighbour sets (VarHNbrParticleLocator): r < 2 max(h_a, h_b),
+    more pairs than the dest's own support gives."""
+    g = load("varh")
+    arr = arrays(g, ["in_"])
+    eng = Engine([(arr, DROP)], varh_scheme(False), dim=2, precision="fp64",
+                 step_lists=False, variable_h=True)
+    di, _, sj = eng.neighbors(0, 1)
+    rdi, rsj = sorted_pairs(g["nbr_off"], g["nbr_idx"])
+    np.testing.assert_array_equal(di, rdi)
+    np.testing.assert_array_equal(sj, rsj)
+    fixed = Engine([(arr, DROP)], fluid_scheme(1), dim=2, precision="fp64", step_lists=False)
+    assert len(fixed.neighbors(0, 1)[0]) < len(rdi)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("name", ["sum", "cont"])
+def test_varh_hks_first_stage(precision, name):
+    """One evaluation with variable h and hks kernels: summation density +
+    Tait + momentum, or Tait + SPHDensityRate + momentum + XSPH."""
+    g = load("varh")
+    cont = name == "cont"
+    eng = Engine([(arrays(g, ["in_"]), DROP)], varh_scheme(cont), dim=2,
+                 precision=precision, variable_h=True)
+    eng.eval_stage()
+    eng.check_status()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    for n in ("rho", "p", "cs"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"{name}_stage0_{n}"]
+        assert np.max(np.abs(got - ref)) <= rtol * np.max(np.abs(ref)) + 1e-300, n
+    atol = 1e-10 if precision == "fp64" else 1e-4
+    names = ["_a_u_1", "_a_v_1", "dt_fac"] + (["_a_rho_1"] if cont else [])
+    for n in names:
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"{name}_stage0_{n}"]
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, n
+    if cont:
+        # position rate: u + the XSPH correction
+        for c, v in (("x", "u"), ("y", "v")):
+            got = (eng.get(0, v) + eng.get(0, f"_xsph_{v}")).cpu().numpy()
+            ref = g[f"cont_stage0__a_{c}_1"]
+            assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, c
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("name", ["sum", "cont"])
+def test_varh_hks_five_steps(precision, name):
+    g = load("varh")
+    eng = Engine([(arrays(g, ["in_"]), DROP)], varh_scheme(name == "cont"), dim=2,
+                 precision=precision, variable_h=True)
+    for _ in range(5):
+        eng.pc_step()
+    eng.check_status()
+    dx = 0.05
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"{name}_step5_{n}_0"])) / dx <= tol, n
+    rho = eng.get(0, "rho").cpu().numpy()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    ref = g[f"{name}_step5_rho_0"]
+    assert np.max(np.abs(rho - ref) / ref) <= rtol
