@@ -72,7 +72,13 @@ class _System(ctypes.Structure):
         ("xsph_src", ctypes.c_uint32 * MAX_ARRAYS),
         ("xsph_eps", ctypes.c_double),
         ("variable_h", ctypes.c_int32), ("hks", ctypes.c_int32),
+        ("kernel", ctypes.c_int32), ("pad2_", ctypes.c_int32),
     ]
+
+# kernel type ids (KernelBase.get_type, S/base/kernels.pyx:31-40) and the
+# support radius of each (radius())
+CUBIC_SPLINE, QUINTIC_SPLINE, WENDLAND_QUINTIC_SPLINE = 1, 3, 4
+KERNEL_RADIUS = {CUBIC_SPLINE: 2.0, QUINTIC_SPLINE: 3.0, WENDLAND_QUINTIC_SPLINE: 2.0}
 
 
 _lib = None
@@ -81,8 +87,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
-            build()
+        build()   # no-op unless sph_oracle.c is newer than the library
         L = ctypes.CDLL(_LIB_PATH)
         P = ctypes.POINTER
         L.orc_nnps_new.restype = ctypes.c_void_p
@@ -118,6 +123,10 @@ def lib():
         L.orc_kernel_w.restype = ctypes.c_double
         L.orc_kernel_w.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int]
         L.orc_kernel_grad.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int, dp]
+        L.orc_kernel_w2.restype = ctypes.c_double
+        L.orc_kernel_w2.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4 + [ctypes.c_int]
+        L.orc_kernel_grad2.argtypes = ([ctypes.c_int] + [ctypes.c_double] * 4
+                                       + [ctypes.c_int, dp])
         L.orc_cell_ids.argtypes = [ctypes.c_int64, dp, dp, dp, ctypes.c_double,
                                    P(ctypes.c_int32)]
         _lib = L
@@ -177,7 +186,7 @@ class OracleSystem:
                  step_on=(), c0=1.0, rho0=1000.0, gamma=7.0, alpha=1.0,
                  beta=1.0, eta=0.1, gravity=(0.0, 0.0, 0.0), nthreads=0,
                  radius_scale=2.0, cell_scale=2.0, rate_src=None, xsph_src=None,
-                 xsph_eps=0.5, variable_h=False, hks=False):
+                 xsph_eps=0.5, variable_h=False, hks=False, kernel=CUBIC_SPLINE):
         self.arrays = list(arrays)
         assert 1 <= len(self.arrays) <= MAX_ARRAYS
         self.dim = dim
@@ -199,6 +208,11 @@ class OracleSystem:
         s.xsph_eps = xsph_eps
         s.variable_h = int(bool(variable_h))
         s.hks = int(bool(hks))
+        if kernel not in KERNEL_RADIUS:
+            raise ValueError("kernel must be 1 (cubic), 3 (quintic) or 4 (Wendland)")
+        if kernel != CUBIC_SPLINE and dim != 2:
+            raise NotImplementedError("the quintic and Wendland kernels are 2D only")
+        s.kernel = kernel
         s.c0, s.rho0, s.gamma_eos = c0, rho0, gamma
         s.alpha, s.beta, s.gamma_av, s.eta = alpha, beta, 1.4, eta
         s.gx, s.gy, s.gz = gravity
@@ -324,13 +338,18 @@ class OracleSystem:
         return dt
 
 
-def kernel_w(dx, dy, dz, h, dim):
-    return lib().orc_kernel_w(dx, dy, dz, h, dim)
+def kernel_w(dx, dy, dz, h, dim, kernel=CUBIC_SPLINE):
+    if kernel == CUBIC_SPLINE:
+        return lib().orc_kernel_w(dx, dy, dz, h, dim)
+    return lib().orc_kernel_w2(kernel, dx, dy, dz, h, dim)
 
 
-def kernel_grad(dx, dy, dz, h, dim):
+def kernel_grad(dx, dy, dz, h, dim, kernel=CUBIC_SPLINE):
     g = (ctypes.c_double * 3)()
-    lib().orc_kernel_grad(dx, dy, dz, h, dim, g)
+    if kernel == CUBIC_SPLINE:
+        lib().orc_kernel_grad(dx, dy, dz, h, dim, g)
+    else:
+        lib().orc_kernel_grad2(kernel, dx, dy, dz, h, dim, g)
     return np.array(g[:])
 
 

@@ -14,6 +14,8 @@
  * x86-64 without FMA contraction.
  *
  *   cubic spline W, grad W ........ S/base/kernels.pyx:349-454 (h_dim :59-66)
+ *   quintic spline, Wendland ....... S/base/kernels.pyx:461-640 (2D only, as
+ *                                    there; their quirks kept, see below)
  *   cell id = floor(x / cs) ........ S/base/cell.pyx:44-84
  *   cell size = scale * max h ...... S/base/cell.pyx:911-941
  *   stencil order (x, y, z) ........ S/base/cell.pyx:95-118, :996-1032
@@ -80,6 +82,8 @@ typedef struct {
     double xsph_eps;
     int32_t variable_h;        /* VarHNbrParticleLocator lists */
     int32_t hks;               /* kernels averaged over h_a and h_b */
+    int32_t kernel;            /* get_type(): 1 cubic, 3 quintic, 4 Wendland */
+    int32_t pad2_;
 } orc_system;
 
 typedef struct {
@@ -154,36 +158,192 @@ static void cs_gradient(double pax, double pay, double paz,
     g[2] = rz * (val * fac);
 }
 
+/* QuinticSplineKernel (S/base/kernels.pyx:461-560), 2D: fac = _fac(1) =
+ * 7 / (478 pi), support 3h.  As in the reference, W adds (1 - q)^5 with
+ * weight 1 (not 15), and the gradient carries +5 (3-q)^4 - 30 (2-q)^4 +
+ * 75 (1-q)^4, the opposite sign of dW/dq. */
+static double qs_fac(void)
+{
+    double h = 1.0;
+    return 7. / (478 * ORC_PI * h * h);
+}
+
+static double qs_function(double pax, double pay, double paz,
+                          double pbx, double pby, double pbz,
+                          double h, int dim, double kfac)
+{
+    double fac = kfac * h_dim(h, dim);
+    double rab = sqrt((pax - pbx) * (pax - pbx) + (pay - pby) * (pay - pby) +
+                      (paz - pbz) * (paz - pbz));
+    double q = rab / h;
+    double val;
+    double tmp1 = (3 - q), tmp2 = (2 - q), tmp3 = (1 - q);
+    if (q > 3.0) {
+        val = 0.0;
+    } else {
+        tmp1 *= (tmp1 * tmp1 * tmp1 * tmp1);
+        if (q > 2.0) {
+            val = tmp1;
+        } else {
+            tmp2 *= (tmp2 * tmp2 * tmp2 * tmp2);
+            val = tmp1 - 6 * tmp2;
+            if (!(q > 1.0)) {
+                tmp3 *= (tmp3 * tmp3 * tmp3 * tmp3);
+                val += tmp3;
+            }
+        }
+    }
+    return val * fac;
+}
+
+static void qs_gradient(double pax, double pay, double paz,
+                        double pbx, double pby, double pbz,
+                        double h, int dim, double kfac, double *g)
+{
+    double fac = kfac * h_dim(h, dim);
+    double rx = pax - pbx, ry = pay - pby, rz = paz - pbz;
+    double rab = sqrt(rx * rx + ry * ry + rz * rz);
+    double q = rab / h;
+    double val;
+    double tmp1 = (3 - q), tmp2 = (2 - q), tmp3 = (1 - q);
+    if (rab < 1e-16) {
+        val = 0.0;
+    } else {
+        fac *= 1. / (h * rab);
+        if (q > 3.0) {
+            val = 0.0;
+        } else {
+            tmp1 *= (tmp1 * tmp1 * tmp1);
+            if (q > 2.0) {
+                val = 5 * tmp1;
+            } else {
+                tmp2 *= (tmp2 * tmp2 * tmp2);
+                val = 5 * tmp1 - 30 * tmp2;
+                if (!(q > 1.0)) {
+                    tmp3 *= (tmp3 * tmp3 * tmp3);
+                    val += 75 * tmp3;
+                }
+            }
+        }
+    }
+    g[0] = rx * (val * fac);
+    g[1] = ry * (val * fac);
+    g[2] = rz * (val * fac);
+}
+
+/* WendlandQuinticSplineKernel (S/base/kernels.pyx:562-640), 2D: support 2h;
+ * _fac(h) is written (7./4*PI*h*h), so fac = _fac(1) = 7 pi / 4 as there. */
+static double wq_fac(void)
+{
+    double h = 1.0;
+    return (7. / 4 * ORC_PI * h * h);
+}
+
+static double wq_function(double pax, double pay, double paz,
+                          double pbx, double pby, double pbz,
+                          double h, int dim, double kfac)
+{
+    double fac = kfac * h_dim(h, dim);
+    double rab = sqrt((pax - pbx) * (pax - pbx) + (pay - pby) * (pay - pby) +
+                      (paz - pbz) * (paz - pbz));
+    double q = rab / h;
+    double val;
+    double tmp = (1 - 0.5 * q);
+    if (q > 2.0) {
+        val = 0.0;
+    } else {
+        tmp *= (tmp * tmp * tmp);
+        tmp *= (2 * q + 1);
+        val = tmp;
+    }
+    return val * fac;
+}
+
+static void wq_gradient(double pax, double pay, double paz,
+                        double pbx, double pby, double pbz,
+                        double h, int dim, double kfac, double *g)
+{
+    double fac = kfac * h_dim(h, dim);
+    double rx = pax - pbx, ry = pay - pby, rz = paz - pbz;
+    double rab = sqrt(rx * rx + ry * ry + rz * rz);
+    double q = rab / h;
+    double val;
+    double tmp = (1 - 0.5 * q);
+    if (rab < 1e-16) {
+        val = 0.0;
+    } else {
+        fac *= 1. / (h * rab);
+        if (q > 2.0) {
+            val = 0;
+        } else {
+            tmp *= (tmp * tmp);
+            val = tmp * -5 * q;
+        }
+    }
+    g[0] = rx * (val * fac);
+    g[1] = ry * (val * fac);
+    g[2] = rz * (val * fac);
+}
+
+/* the kernel's fac = _fac(1.0) and its function / gradient */
+static double kern_fac(const orc_system *s, int dim)
+{
+    if (s->kernel == 3) return qs_fac();
+    if (s->kernel == 4) return wq_fac();
+    return kfac_unit(dim);
+}
+
+static double kern_function(int kernel, double pax, double pay, double paz,
+                            double pbx, double pby, double pbz, double h, int dim,
+                            double kfac)
+{
+    if (kernel == 3) return qs_function(pax, pay, paz, pbx, pby, pbz, h, dim, kfac);
+    if (kernel == 4) return wq_function(pax, pay, paz, pbx, pby, pbz, h, dim, kfac);
+    return cs_function(pax, pay, paz, pbx, pby, pbz, h, dim, kfac);
+}
+
+static void kern_gradient(int kernel, double pax, double pay, double paz,
+                          double pbx, double pby, double pbz, double h, int dim,
+                          double kfac, double *g)
+{
+    if (kernel == 3) qs_gradient(pax, pay, paz, pbx, pby, pbz, h, dim, kfac, g);
+    else if (kernel == 4) wq_gradient(pax, pay, paz, pbx, pby, pbz, h, dim, kfac, g);
+    else cs_gradient(pax, pay, paz, pbx, pby, pbz, h, dim, kfac, g);
+}
+
 /* W and grad W of a pair as the functions evaluate them: at h_ab =
  * (h_a + h_b) / 2, or with hks the average of the values at h_a and h_b
  * (e.g. S/sph/funcs/density_funcs.pyx:56-63, pressure_funcs.pyx:371-381). */
 static double pair_w(const orc_system *s, const orc_array *D, int64_t i,
                      const orc_array *S, int64_t j, double hab, int dim, double kfac)
 {
+    const int k = s->kernel;
     if (s->hks) {
-        double wa = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
-                                D->h[i], dim, kfac);
-        double wb = cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
-                                S->h[j], dim, kfac);
+        double wa = kern_function(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                                  D->h[i], dim, kfac);
+        double wb = kern_function(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j],
+                                  S->h[j], dim, kfac);
         return 0.5 * (wa + wb);
     }
-    return cs_function(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim, kfac);
+    return kern_function(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim,
+                         kfac);
 }
 
 static void pair_grad(const orc_system *s, const orc_array *D, int64_t i,
                       const orc_array *S, int64_t j, double hab, int dim, double kfac,
                       double *g)
 {
+    const int k = s->kernel;
     if (s->hks) {
         double ga[3], gb[3];
-        cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], D->h[i], dim,
-                    kfac, ga);
-        cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], S->h[j], dim,
-                    kfac, gb);
+        kern_gradient(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], D->h[i], dim,
+                      kfac, ga);
+        kern_gradient(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], S->h[j], dim,
+                      kfac, gb);
         for (int d = 0; d < 3; ++d) g[d] = (ga[d] + gb[d]) * 0.5;
         return;
     }
-    cs_gradient(D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim, kfac, g);
+    kern_gradient(k, D->x[i], D->y[i], D->z[i], S->x[j], S->y[j], S->z[j], hab, dim, kfac, g);
 }
 
 double orc_kernel_w(double dx, double dy, double dz, double h, int dim)
@@ -195,6 +355,22 @@ void orc_kernel_grad(double dx, double dy, double dz, double h, int dim,
                      double *g)
 {
     cs_gradient(dx, dy, dz, 0.0, 0.0, 0.0, h, dim, kfac_unit(dim), g);
+}
+
+/* W and grad W of kernel type `kernel` (get_type ids) at (dx, dy, dz) */
+double orc_kernel_w2(int kernel, double dx, double dy, double dz, double h, int dim)
+{
+    orc_system s;
+    s.kernel = kernel;
+    return kern_function(kernel, dx, dy, dz, 0.0, 0.0, 0.0, h, dim, kern_fac(&s, dim));
+}
+
+void orc_kernel_grad2(int kernel, double dx, double dy, double dz, double h, int dim,
+                      double *g)
+{
+    orc_system s;
+    s.kernel = kernel;
+    kern_gradient(kernel, dx, dy, dz, 0.0, 0.0, 0.0, h, dim, kern_fac(&s, dim), g);
 }
 
 /* ------------------------------------------------------------------ */
@@ -517,7 +693,7 @@ int orc_sph_rho(const orc_system *s, const orc_nnps *c, int da, int sa,
     const int32_t *idx = c->idx[da][sa];
     if (!off) return -1;
     int dim = s->dim;
-    double kfac = kfac_unit(dim);
+    double kfac = kern_fac(s, dim);
     set_threads(s);
 #pragma omp parallel for schedule(dynamic, 512)
     for (int64_t i = 0; i < D->n; ++i) {
@@ -563,7 +739,7 @@ int orc_momentum(const orc_system *s, const orc_nnps *c, int da, int sa,
     const int32_t *idx = c->idx[da][sa];
     if (!off) return -1;
     int dim = s->dim;
-    double kfac = kfac_unit(dim);
+    double kfac = kern_fac(s, dim);
     set_threads(s);
 #pragma omp parallel for schedule(dynamic, 512)
     for (int64_t i = 0; i < D->n; ++i) {
@@ -627,7 +803,7 @@ int orc_pgrad(const orc_system *s, const orc_nnps *c, int da, int sa,
     const int32_t *idx = c->idx[da][sa];
     if (!off) return -1;
     int dim = s->dim;
-    double kfac = kfac_unit(dim);
+    double kfac = kern_fac(s, dim);
     set_threads(s);
 #pragma omp parallel for schedule(dynamic, 512)
     for (int64_t i = 0; i < D->n; ++i) {
@@ -672,7 +848,7 @@ int orc_density_rate(const orc_system *s, const orc_nnps *c, int da, int sa,
     const int32_t *idx = c->idx[da][sa];
     if (!off) return -1;
     int dim = s->dim;
-    double kfac = kfac_unit(dim);
+    double kfac = kern_fac(s, dim);
     set_threads(s);
 #pragma omp parallel for schedule(dynamic, 512)
     for (int64_t i = 0; i < D->n; ++i) {
@@ -709,7 +885,7 @@ int orc_xsph(const orc_system *s, const orc_nnps *c, int da, int sa, double eps,
     const int32_t *idx = c->idx[da][sa];
     if (!off) return -1;
     int dim = s->dim;
-    double kfac = kfac_unit(dim);
+    double kfac = kern_fac(s, dim);
     set_threads(s);
 #pragma omp parallel for schedule(dynamic, 512)
     for (int64_t i = 0; i < D->n; ++i) {

@@ -54,7 +54,9 @@ def ref_modules(build_dir):
     import pysph.solver.sph_equation as EQ
     import pysph.solver.integrator as I
     import pysph.solver.time_step_functions as T
-    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T, X=X)
+    from pysph.base.point import Point
+    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T, X=X,
+                Point=Point)
 
 
 def make_array(R, props, name, ptype):
@@ -62,8 +64,8 @@ def make_array(R, props, name, ptype):
     return R["PA"].get_particle_array(name=name, type=ptype, **d)
 
 
-def lists_of(R, particles, src, dst):
-    loc = particles.nnps_manager.get_neighbor_particle_locator(src, dst, 2.0)
+def lists_of(R, particles, src, dst, radius_scale=2.0):
+    loc = particles.nnps_manager.get_neighbor_particle_locator(src, dst, radius_scale)
     n = dst.get_number_of_particles()
     out = [np.asarray(loc.py_get_nearest_particles(i).get_npy_array(), np.int32).copy()
            for i in range(n)]
@@ -106,10 +108,10 @@ def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None, hk
 
 
 def build_sim(R, arrays, types, params, dim, xsph_eps=None, integrator=None,
-              variable_h=False, hks=False):
+              variable_h=False, hks=False, kernel="CubicSplineKernel"):
     pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
     particles = R["P"].Particles(pas, variable_h=variable_h)
-    kernel = R["K"].CubicSplineKernel(dim=dim)
+    kernel = getattr(R["K"], kernel)(dim=dim)
     ops = scheme_ops(R, len(pas), params["c0"], params["rho0"], params["alpha"],
                      params["beta"], params["eta"], params["gravity"][1], dim, xsph_eps, hks)
     calcs = []
@@ -339,6 +341,53 @@ def varh(R):
     return out
 
 
+def kernels(R):
+    """The quintic spline and Wendland quintic kernels (2D): W and grad W on
+    a line of distances, and the drop (dx = 0.05) with each kernel under both
+    schemes: neighbour lists (radius 3h for the quintic), the first stage and
+    5 PC steps.  Wendland's normalisation (7 pi / 4 where 7 / (4 pi) is
+    meant) makes the summed density pi^2 times the rest density, so its
+    summation case takes TaitEquation ro = pi^2 to keep the drop intact."""
+    out = {}
+    arrays, types, params = W.elliptical_drop(dx=0.05)
+    out.update({f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS})
+    rs = np.linspace(0.0, 3.2, 65)
+    for kname in ("QuinticSplineKernel", "WendlandQuinticSplineKernel"):
+        k = getattr(R["K"], kname)(dim=2)
+        pb = R["Point"](0.0, 0.0, 0.0)
+        w, g = [], []
+        for r in rs:
+            pa = R["Point"](0.6 * r, 0.8 * r, 0.0)
+            w.append(k.py_function(pa, pb, 1.1))
+            gr = R["Point"]()
+            k.py_gradient(pa, pb, 1.1, gr)
+            g.append((gr.x, gr.y, gr.z))
+        out[f"{kname}_w"] = np.array(w)
+        out[f"{kname}_grad"] = np.array(g)
+        for name, eps in (("sum", None), ("cont", XSPH_EPS)):
+            p = dict(params)
+            if kname.startswith("Wendland") and name == "sum":
+                p["rho0"] = float(np.pi ** 2)
+            out[f"{kname}_{name}_rho0"] = np.float64(p["rho0"])
+            pas, particles, integ = build_sim(R, arrays, types, p, 2, eps, kernel=kname)
+            if name == "sum":
+                off, idx = lists_of(R, particles, pas[0], pas[0], k.radius())
+                out[f"{kname}_nbr_off"], out[f"{kname}_nbr_idx"] = off, idx
+            integ.save_initial_arrays()
+            integ.reset_accelerations(step=1)
+            integ.eval()
+            names = ("rho", "p", "cs", "_a_u_1", "_a_v_1", "dt_fac") + (
+                ("_a_rho_1", "_a_x_1", "_a_y_1") if eps else ())
+            out.update({f"{kname}_{name}_stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                        for n in names})
+            pas, particles, integ = build_sim(R, arrays, types, p, 2, eps, kernel=kname)
+            for _ in range(5):
+                particles.update()
+                integ.integrate(1e-5)
+            out.update({f"{kname}_{name}_step5_{k_}": v for k_, v in state(pas).items()})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", default=os.path.join(ROOT, "_work", "refbuild"))
@@ -348,7 +397,7 @@ def main():
     R = ref_modules(a.build)
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
                      ("drop_cont", drop_cont), ("dam_cont", dam_cont),
-                     ("integrators", integrators), ("varh", varh)):
+                     ("integrators", integrators), ("varh", varh), ("kernels", kernels)):
         if a.only and name not in a.only:
             continue
         data = fn(R)

@@ -241,3 +241,70 @@ def test_varh_hks_first_stage_and_steps_bit_exact(name):
     for n in ("x", "y", "u", "v", "rho", "p", "cs"):
         np.testing.assert_array_equal(getattr(o.arrays[0], n), g[f"{name}_step5_{n}_0"],
                                       err_msg=n)
+
+
+# -- the quintic spline and Wendland quintic kernels (2D) ---------------------
+KERNELS = {"QuinticSplineKernel": 3, "WendlandQuinticSplineKernel": 4}
+
+
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_values_bit_exact(kname):
+    """W and grad W on a line of distances through q = 0..2.9 (h = 1.1),
+    with the reference's own quirks (the quintic's W weight and gradient
+    sign, Wendland's 7 pi / 4 normalisation)."""
+    from oracle import kernel_grad, kernel_w
+    g = load("kernels")
+    kt = KERNELS[kname]
+    rs = np.linspace(0.0, 3.2, 65)
+    w = [kernel_w(0.6 * r, 0.8 * r, 0.0, 1.1, 2, kt) for r in rs]
+    gr = [kernel_grad(0.6 * r, 0.8 * r, 0.0, 1.1, 2, kt) for r in rs]
+    np.testing.assert_array_equal(np.array(w), g[f"{kname}_w"])
+    np.testing.assert_array_equal(np.array(gr), g[f"{kname}_grad"])
+
+
+def oracle_kernel(g, scheme, kname, name="sum"):
+    from oracle import KERNEL_RADIUS
+    kt = KERNELS[kname]
+    arrs = [OracleArray("a0", **{k: g[f"in_{k}"].copy() for k in PROPS})]
+    par = dict(DROP, rho0=float(g[f"{kname}_{name}_rho0"]))
+    return OracleSystem(arrs, dim=2, rho_src=scheme.rho_src, tait_on=scheme.tait_on,
+                        mom_src=scheme.mom_src, step_on=scheme.step_on,
+                        rate_src=scheme.rate_src, xsph_src=scheme.xsph_src,
+                        xsph_eps=scheme.xsph_eps, kernel=kt, radius_scale=KERNEL_RADIUS[kt],
+                        **par)
+
+
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_lists_in_reference_order(kname):
+    """The locator radius is the kernel's support (3h for the quintic)."""
+    g = load("kernels")
+    o = oracle_kernel(g, fluid_scheme(1), kname)
+    o.update()
+    off, idx = o.neighbors(0, 0)
+    np.testing.assert_array_equal(off, g[f"{kname}_nbr_off"])
+    np.testing.assert_array_equal(idx, g[f"{kname}_nbr_idx"])
+
+
+@pytest.mark.parametrize("name", ["sum", "cont"])
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_first_stage_and_steps_bit_exact(kname, name):
+    g = load("kernels")
+    sch = fluid_scheme(1) if name == "sum" else continuity_scheme(1, 0.5)
+    o = oracle_kernel(g, sch, kname, name)
+    o.update()
+    o.eval()
+    A = o.arrays[0]
+    got = {"rho": A.rho, "p": A.p, "cs": A.cs, "_a_u_1": A.au, "_a_v_1": A.av,
+           "dt_fac": A.dt_fac, "_a_rho_1": A.arho, "_a_x_1": A.ax, "_a_y_1": A.ay}
+    pre = f"{kname}_{name}_stage0_"
+    keys = [k for k in g if k.startswith(pre)]
+    assert keys
+    for key in keys:
+        n = key[len(pre):]
+        np.testing.assert_array_equal(got[n], g[key], err_msg=n)
+    o = oracle_kernel(g, sch, kname, name)
+    for _ in range(5):
+        o.pc_step(1e-5)
+    for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+        np.testing.assert_array_equal(getattr(o.arrays[0], n),
+                                      g[f"{kname}_{name}_step5_{n}_0"], err_msg=n)
