@@ -61,6 +61,15 @@ enum {
 
 enum { SPHB_FP64 = 0, SPHB_FP32C = 1 };   /* plain FP64 / FP32 + Kahan */
 
+/* Smoothing kernels, numbered as KernelBase.get_type (S/base/kernels.pyx:
+ * 31-40).  The quintic spline (support 3h) and the Wendland quintic
+ * (support 2h) are 2D only, as in the reference; 0 means the cubic. */
+enum {
+    SPHB_KERNEL_CUBIC = 1,      /* CubicSplineKernel, support 2h */
+    SPHB_KERNEL_QUINTIC = 3,    /* QuinticSplineKernel */
+    SPHB_KERNEL_WENDLAND = 4    /* WendlandQuinticSplineKernel */
+};
+
 /* Engine-wide configuration. */
 typedef struct {
     int32_t dim;            /* 2 or 3 */
@@ -88,6 +97,9 @@ typedef struct {
      * the summation-density scheme */
     uint32_t rate_src[SPHB_MAX_ARRAYS];
     uint32_t xsph_src[SPHB_MAX_ARRAYS];
+    int32_t kernel;         /* SPHB_KERNEL_*; scene.radius_scale must be its
+                               support (3 for the quintic, else 2) */
+    int32_t reserved;       /* 0 */
 } sphb_config;
 
 /* Per-scene constants, written by the host once. */

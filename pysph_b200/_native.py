@@ -62,7 +62,12 @@ class Config(ctypes.Structure):
                 ("cell_capacity", i32), ("list_batch", i32),
                 ("rho_src", u32 * MAX_ARRAYS), ("mom_src", u32 * MAX_ARRAYS),
                 ("tait_on", u32), ("step_on", u32),
-                ("rate_src", u32 * MAX_ARRAYS), ("xsph_src", u32 * MAX_ARRAYS)]
+                ("rate_src", u32 * MAX_ARRAYS), ("xsph_src", u32 * MAX_ARRAYS),
+                ("kernel", i32), ("reserved", i32)]
+
+# smoothing kernels (KernelBase.get_type ids) and their support radii
+KERNEL_CUBIC, KERNEL_QUINTIC, KERNEL_WENDLAND = 1, 3, 4
+KERNEL_RADIUS = {KERNEL_CUBIC: 2.0, KERNEL_QUINTIC: 3.0, KERNEL_WENDLAND: 2.0}
 
 
 class Scene(ctypes.Structure):

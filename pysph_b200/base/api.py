@@ -1,6 +1,7 @@
 """`import pysph_b200.base.api as base` -- the names of pysph.base.api that
 this build provides."""
-from .kernels import CubicSplineKernel, KernelBase
+from .kernels import (CubicSplineKernel, KernelBase, QuinticSplineKernel,
+                      WendlandQuinticSplineKernel)
 from .particle_array import ParticleArray, get_particle_array
 from .particle_types import (ParticleType, LocalReal, Dummy, LocalDummy,
                              RemoteReal, RemoteDummy, get_local_real_tag,
@@ -12,6 +13,7 @@ from .point import Point
 Fluid = ParticleType.Fluid
 Solid = ParticleType.Solid
 
-__all__ = ["CubicSplineKernel", "KernelBase", "ParticleArray", "get_particle_array",
+__all__ = ["CubicSplineKernel", "QuinticSplineKernel", "WendlandQuinticSplineKernel",
+           "KernelBase", "ParticleArray", "get_particle_array",
            "ParticleType", "Particles", "NeighborLocatorType", "NNPSManager",
            "Locator", "Point", "Fluid", "Solid", "LocalReal"]

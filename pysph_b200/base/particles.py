@@ -37,10 +37,11 @@ class Session:
 
     def __init__(self, particles: "Particles", dim: int, precision: str,
                  scheme: Scheme | None = None, params: SceneParams | None = None,
-                 lanes: int = 1, pair_block: int = 128):
+                 lanes: int = 1, pair_block: int = 128, kernel: int = nat.KERNEL_CUBIC):
         self.particles = particles
         self.dim = dim
         self.precision = precision
+        self.kernel = kernel
         arrays = particles.arrays
         A = len(arrays)
         if scheme is None:
@@ -60,7 +61,8 @@ class Session:
             specs.append(d)
         self.engine = Engine([(specs, self.params)], scheme, dim=dim,
                              precision=precision, lanes=lanes, pair_block=pair_block,
-                             device=arrays[0].device, variable_h=particles.variable_h)
+                             device=arrays[0].device, variable_h=particles.variable_h,
+                             kernel=kernel)
         self.valid = {}
         for a, pa in enumerate(arrays):
             for name in IMPORTABLE:
@@ -286,12 +288,17 @@ class Particles:
         return 3 if any(bool(torch.any(a.properties["z"] != 0)) for a in self.arrays
                         if a.get_number_of_particles()) else 2
 
-    def session(self, dim=None, scheme=None, params=None, lanes=1, pair_block=128):
-        """The engine session; (re)built when the dimension or, when given,
-        the scheme / parameters change."""
+    def session(self, dim=None, scheme=None, params=None, lanes=1, pair_block=128,
+                kernel=None):
+        """The engine session; (re)built when the dimension, the kernel type
+        or, when given, the scheme / parameters change."""
         dim = dim or self._default_dim()
         s = self._session
+        if kernel is None:
+            kernel = (s.kernel if s is not None else
+                      self.kernel.get_type() if self.kernel is not None else nat.KERNEL_CUBIC)
         rebuild = (s is None or s.dim != dim or s.precision != self.precision
+                   or s.kernel != kernel
                    or (scheme is not None and s.scheme != scheme)
                    or (params is not None and s.params != params)
                    or any(s.engine.sizes[0, a] != pa.get_number_of_particles()
@@ -303,7 +310,7 @@ class Particles:
             if s is not None:
                 s.detach()
             self._session = Session(self, dim, self.precision, scheme, params, lanes,
-                                    pair_block)
+                                    pair_block, kernel)
             self._dim = dim
         return self._session
 

@@ -1,5 +1,4 @@
-// sphb_pairs.cuh -- neighbour traversal and the cubic spline for the pair
-// kernels.
+// sphb_pairs.cuh -- neighbour traversal for the pair kernels.
 //
 // Cells are keyed row-major with x fastest, so the 2R+1 cells of one stencil
 // row (cx-R .. cx+R at fixed y, z) hold one contiguous particle range
@@ -213,102 +212,6 @@ __device__ __forceinline__ void traverse(const sphb_engine &e, bool use_list, in
     }
     for_each_candidate<DIM, R, LANES>(start, num_arrays, src_mask, cell_base, ncells, n, cx, cy,
                                       cz, lane, N, e.work.status, f);
-}
-
-// Cubic spline W(r, h) in FP32 (CubicSplineKernel.function,
-// S/base/kernels.pyx:355-378): fac * {1 - 1.5 q^2 (1 - q/2); (2-q)^3 / 4; 0}.
-template <int DIM>
-__device__ __forceinline__ float w_cubic_f(float r2, float hab)
-{
-    const float ih = __fdividef(1.0f, hab);
-    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-    const float q = r * ih;
-    float val;
-    if (q > 2.0f) {
-        val = 0.0f;
-    } else if (q > 1.0f) {
-        const float t = 2.0f - q;
-        val = 0.25f * t * t * t;
-    } else {
-        val = 1.0f - 1.5f * (q * q) * (1.0f - 0.5f * q);
-    }
-    float fac = (float)kfac_unit<DIM>() * ih * ih;
-    if (DIM == 3) fac *= ih;
-    return val * fac;
-}
-
-// dW/dr / r, so grad W = (x_a - x_b) * gw (CubicSplineKernel.gradient,
-// S/base/kernels.pyx:380-417), FP32.
-template <int DIM>
-__device__ __forceinline__ float gw_cubic_f(float r2, float hab)
-{
-    const float ih = __fdividef(1.0f, hab);
-    const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
-    const float q = r2 * ir * ih;
-    float val = 0.0f;
-    if (q > 2.0f) {
-    } else if (q >= 1.0f) {
-        const float t = 2.0f - q;
-        val = -0.75f * t * t * ih * ir;
-    } else if (q > 1e-14f) {
-        val = 3.0f * (0.75f * q - 1.0f) * ih * ih;
-    }
-    float fac = (float)kfac_unit<DIM>() * ih * ih;
-    if (DIM == 3) fac *= ih;
-    return val * fac;
-}
-
-// Branch-free FP32 cubic spline for the list passes (both pieces computed,
-// one selected; t1 = max(2 - q, 0) is zero beyond the support):
-// W = fac (q < 1 ? 1 + q^2 (0.75 q - 1.5) : t1^3 / 4), and
-// dW/dr / r = fac ih (q < 1 ? (2.25 q - 3) ih : -0.75 t1^2 / r)
-// (S/base/kernels.pyx:355-417).  ir = 1/r (huge but finite for r = 0, where
-// r_ab = 0 makes the gradient term vanish anyway).
-__device__ __forceinline__ float w_cubic_bf(float q, float fac)
-{
-    const float t1 = fmaxf(2.0f - q, 0.0f);
-    const float inner = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
-    const float outer = 0.25f * (t1 * t1 * t1);
-    return fac * (q < 1.0f ? inner : outer);
-}
-
-__device__ __forceinline__ float gw_cubic_bf(float q, float ir, float ih, float fac_ih)
-{
-    const float t1 = fmaxf(2.0f - q, 0.0f);
-    const float inner = (2.25f * q - 3.0f) * ih;
-    const float outer = -0.75f * t1 * t1 * ir;
-    return fac_ih * (q < 1.0f ? inner : outer);
-}
-
-// FP64 versions with the reference's operations.
-template <int DIM>
-__device__ __forceinline__ double w_cubic_d(double rab, double h)
-{
-    const double q = rab / h;
-    double val;
-    const double fac = (DIM == 2 ? 1.0 / (h * h) : 1.0 / (h * h * h)) * kfac_unit<DIM>();
-    if (q > 2.0)
-        val = 0.0;
-    else if (q > 1.0)
-        val = 0.25 * (2 - q) * (2 - q) * (2 - q);
-    else
-        val = 1 - 1.5 * (q * q) * (1 - 0.5 * q);
-    return val * fac;
-}
-
-template <int DIM>
-__device__ __forceinline__ double gw_cubic_d(double rab, double h)
-{
-    const double q = rab / h;
-    double val = 0.0;
-    const double fac = (DIM == 2 ? 1.0 / (h * h) : 1.0 / (h * h * h)) * kfac_unit<DIM>();
-    if (q > 2.0) {
-    } else if (q >= 1.0) {
-        val = -0.75 * (2 - q) * (2 - q) / (h * rab);
-    } else if (q > 1e-14) {
-        val = 3.0 * (0.75 * q - 1) / (h * h);
-    }
-    return val * fac;
 }
 
 // Squared distance with the reference's rounding (no FMA contraction):

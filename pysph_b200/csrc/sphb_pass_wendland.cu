@@ -1,0 +1,14 @@
+// sphb_pass_wendland.cu -- the density and force passes with the Wendland quintic
+// kernel in 2D.
+
+#include "sphb_density_pass.cuh"
+#include "sphb_force_pass.cuh"
+
+namespace sphb {
+
+template void launch_density_kt<SPHB_KERNEL_WENDLAND, 2>(const sphb_engine &, int, uint32_t, int,
+                                           cudaStream_t);
+template void launch_force_kt<SPHB_KERNEL_WENDLAND, 2>(const sphb_engine &, int, uint32_t, int, int,
+                                         cudaStream_t);
+
+}  // namespace sphb

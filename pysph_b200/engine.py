@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes
+import dataclasses
 import math
 from dataclasses import dataclass, field
 
@@ -44,7 +45,7 @@ class SceneParams:
     dt: float = 1e-4
     cfl: float = 0.0            # > 0: ViscousAndForceBasedTimeStep
     dt_initial: float = 1e-4     # solver.dt, used by the CFL rule at step 1
-    radius_scale: float = 2.0    # cubic-spline support / h
+    radius_scale: float = 2.0    # kernel support / h (set from the engine's kernel)
     cfl_force: bool = True       # CFL rule with the force criterion too
 
     @staticmethod
@@ -147,7 +148,8 @@ class Engine:
                  pair_block: int = 128, cell_capacity: int | None = None,
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
                  step_lists: bool = True, skin_margin: float | None = None,
-                 list_batch: int = 4, variable_h: bool = False):
+                 list_batch: int = 4, variable_h: bool = False,
+                 kernel: int = nat.KERNEL_CUBIC):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -164,8 +166,18 @@ class Engine:
         self.A = len(scenes[0][0])
         if self.S < 1 or not 1 <= self.A <= nat.MAX_ARRAYS:
             raise ValueError("need >= 1 scene and 1..4 arrays per scene")
-        self.params = [p if isinstance(p, SceneParams) else SceneParams.from_dict(p)
-                       for _, p in scenes]
+        # smoothing kernel (KernelBase.get_type ids); the quintic spline and
+        # the Wendland quintic are 2D only, as in the reference
+        if kernel not in nat.KERNEL_RADIUS:
+            raise ValueError("kernel must be 1 (cubic), 3 (quintic) or 4 (Wendland quintic)")
+        if kernel != nat.KERNEL_CUBIC and dim != 2:
+            raise NotImplementedError("the quintic and Wendland kernels are 2D only")
+        self.kernel = kernel
+        params = [p if isinstance(p, SceneParams) else SceneParams.from_dict(p)
+                  for _, p in scenes]
+        # the neighbour radius is the kernel's support
+        self.params = [dataclasses.replace(p, radius_scale=nat.KERNEL_RADIUS[kernel])
+                       for p in params]
         sizes = np.zeros((self.S, self.A), np.int64)
         for s, (arrays, _) in enumerate(scenes):
             if len(arrays) != self.A:
@@ -334,9 +346,11 @@ class Engine:
         # per-stage neighbour lists (density pass writes, force pass reads)
         idx_bits = 26 if dim == 2 else 23
         self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
-        if self.step_lists and self.list_cap:
-            # capacity for the skin: entries grow as (1 + margin)^dim
-            grow = (1.0 + self.skin_margin) ** dim
+        if self.list_cap:
+            # capacity for the skin and the kernel's support (3h for the
+            # quintic): entries grow as (radius (1 + margin))^dim; a lane
+            # whose list overflows searches its cells instead
+            grow = ((1.0 + self.skin_margin) * nat.KERNEL_RADIUS[self.kernel] / 2.0) ** dim
             self.list_cap = int(math.ceil(self.list_cap * grow / 8.0)) * 8
         if self.list_cap:
             f["nbr"] = torch.zeros(self.list_cap * N, **i32)
@@ -369,6 +383,7 @@ class Engine:
         cfg.lanes = lanes
         cfg.pair_block = pair_block
         cfg.list_batch = getattr(self, "list_batch", 4)
+        cfg.kernel = self.kernel
         cfg.num_particles = self.N
         cfg.cell_capacity = self.cell_capacity
         rho, mom, tait, step = self.scheme.masks()

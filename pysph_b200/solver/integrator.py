@@ -23,12 +23,13 @@ from ..sph.sph_func import (SPHRho, TaitEquation, MomentumEquation,
 
 
 class FusedPlan:
-    def __init__(self, scheme, params, mode, dim, tait_only):
+    def __init__(self, scheme, params, mode, dim, tait_only, kernel=1):
         self.scheme = scheme
         self.params = params
         self.mode = mode
         self.dim = dim
         self.tait_only = tait_only
+        self.kernel = kernel    # smoothing kernel type (KernelBase.get_type)
 
 
 def fused_plan(particles, calcs):
@@ -50,6 +51,7 @@ def fused_plan(particles, calcs):
     mode = None
     last = -1
     dim = None
+    ktype = None
 
     def agree(key, val):
         if key in params and params[key] != val:
@@ -66,7 +68,11 @@ def fused_plan(particles, calcs):
                 return None
             last = stage
             dim = dim or calc.kernel.dim
-            if calc.kernel.dim != dim or calc.kernel.radius() != 2.0:
+            ktype = ktype or calc.kernel.get_type()
+            # one kernel for every calc, one the pair passes evaluate
+            if calc.kernel.dim != dim or calc.kernel.get_type() != ktype:
+                return None
+            if ktype not in (1, 3, 4) or (ktype != 1 and dim != 2):
                 return None
             d = idx(calc.dest)
             srcs = sum(1 << idx(s) for s in calc.sources)
@@ -138,7 +144,7 @@ def fused_plan(particles, calcs):
                     xsph_eps=params.get("xsph_eps", 0.5), hks=params.get("hks", False))
     p = SceneParams(**{k: v for k, v in params.items()
                        if k in SceneParams.__dataclass_fields__})
-    return FusedPlan(scheme, p, mode or 0, dim, tuple(sorted(tait_only)))
+    return FusedPlan(scheme, p, mode or 0, dim, tuple(sorted(tait_only)), ktype or 1)
 
 
 class _NoPlan(Exception):
@@ -237,7 +243,7 @@ class Integrator:
     # --------------------------------------------------------------- fused
     def _fused_session(self):
         s = self.particles.session(dim=self.plan.dim, scheme=self.plan.scheme,
-                                   params=self.plan.params)
+                                   params=self.plan.params, kernel=self.plan.kernel)
         s.engine.force_mode = self.plan.mode
         s.engine.tait_only_mask = sum(1 << a for a in self.plan.tait_only)
         return s

@@ -121,7 +121,7 @@ def evaluate(calc: SPHCalc, outs):
         raise NotImplementedError(f"{type(f0).__name__} is not part of this build")
 
     P = calc.particles
-    s = P.session(dim=calc.kernel.dim)
+    s = P.session(dim=calc.kernel.dim, kernel=calc.kernel.get_type())
     eng = s.engine
     a = s.index(dest)
     src_mask = 0

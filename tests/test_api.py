@@ -236,3 +236,43 @@ def test_variable_h_and_hks_options():
     assert solver_hks(True, True).scheme.hks
     assert not solver_hks(False, False).scheme.hks
     assert solver_hks(True, False) is None
+
+
+def test_other_kernels_host_formulas():
+    """QuinticSplineKernel / WendlandQuinticSplineKernel host formulas
+    against the values the reference's own kernels gave (fixture), quirks
+    included; 2D only, as in the reference."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "kernels.npz"))
+    rs = np.linspace(0.0, 3.2, 65)
+    for kname, radius in (("QuinticSplineKernel", 3.0), ("WendlandQuinticSplineKernel", 2.0)):
+        k = getattr(base, kname)(dim=2)
+        assert k.radius() == radius
+        w, gr = [], []
+        for r in rs:
+            pa, pb = base.Point(0.6 * r, 0.8 * r, 0.0), base.Point(0.0, 0.0, 0.0)
+            w.append(k.py_function(pa, pb, 1.1))
+            q = base.Point()
+            k.py_gradient(pa, pb, 1.1, q)
+            gr.append((q.x, q.y, q.z))
+        np.testing.assert_allclose(w, g[f"{kname}_w"], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(gr, g[f"{kname}_grad"], rtol=1e-12, atol=1e-14)
+        with pytest.raises(NotImplementedError):
+            getattr(base, kname)(dim=3)
+
+
+def test_fused_plan_kernel_type():
+    f, _ = arrays()
+    particles = base.Particles([f])
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator,
+                      kernel=base.QuinticSplineKernel(dim=2))
+    s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid],
+                                        from_types=[Fluid], updates=["rho"], id="sd"))
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=62.6, ro=1000.0),
+                                        on_types=[Fluid], updates=["p", "cs"], id="eos"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=0.1, beta=0.0), on_types=[Fluid],
+        from_types=[Fluid], updates=["u", "v"], id="mom"))
+    s.add_operation_step([Fluid])
+    s.setup(particles)
+    assert s.integrator.plan.kernel == 3
+    assert dam_solver().integrator.plan.kernel == 1

@@ -432,3 +432,69 @@ def test_varh_building_blocks_match_fused(cont):
         a = pa1.get(n).cpu().numpy()
         b = pa2.get(n).cpu().numpy()
         assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, np.max(np.abs(a))), n
+
+
+# -- the quintic spline and Wendland quintic kernels --------------------------
+def kernel_solver(kernel, rho0=1.0, cont=False):
+    arrays, _, params = W.elliptical_drop(dx=0.05)
+    pa = base.get_particle_array(name="fluid", **arrays[0])
+    particles = base.Particles([pa])
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator,
+                      kernel=kernel(dim=2))
+    if not cont:
+        s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid],
+                                            from_types=[Fluid], updates=["rho"], id="sd"))
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=1400.0, ro=rho0),
+                                        on_types=[Fluid], updates=["p", "cs"], id="eos"))
+    if cont:
+        s.add_operation(solver.SPHIntegration(sph.SPHDensityRate.withargs(),
+                                              on_types=[Fluid], from_types=[Fluid],
+                                              updates=["rho"], id="density"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=0.1, beta=0.0, eta=0.1),
+        on_types=[Fluid], from_types=[Fluid], updates=["u", "v"], id="mom"))
+    s.add_operation_step([Fluid])
+    if cont:
+        s.add_operation_xsph(eps=0.5)
+    s.set_time_step(1e-5)
+    s.set_final_time(5e-5 - 1e-12)
+    s.setup(particles)
+    return s, pa, arrays
+
+
+@pytest.mark.parametrize("cont", [False, True])
+@pytest.mark.parametrize("kname", ["QuinticSplineKernel", "WendlandQuinticSplineKernel"])
+def test_solver_other_kernels_match_oracle(kname, cont):
+    """Solver(kernel=QuinticSplineKernel / WendlandQuinticSplineKernel) runs
+    fused on the engine and tracks the oracle (pinned to the reference)."""
+    from oracle import KERNEL_RADIUS, OracleArray, OracleSystem
+    kernel = getattr(base, kname)
+    rho0 = float(np.pi ** 2) if kname.startswith("Wendland") and not cont else 1.0
+    s, pa, arrays = kernel_solver(kernel, rho0, cont)
+    plan = s.integrator.plan
+    kt = kernel(dim=2).get_type()
+    assert plan is not None and plan.kernel == kt
+    s.solve()
+    assert s.count == 5
+    sch = ({"rate_src": {0: [0]}, "xsph_src": {0: [0]}} if cont else {"rho_src": {0: [0]}})
+    o = OracleSystem([OracleArray("a0", **{k: np.array(v, np.float64)
+                                          for k, v in arrays[0].items()})],
+                     dim=2, tait_on=(0,), mom_src={0: [0]}, step_on=(0,), xsph_eps=0.5,
+                     c0=1400.0, rho0=rho0, alpha=0.1, beta=0.0, eta=0.1, kernel=kt,
+                     radius_scale=KERNEL_RADIUS[kt], **sch)
+    for _ in range(5):
+        o.pc_step(1e-5)
+    O = o.arrays[0]
+    dx = 0.05
+    for n in ("x", "y"):
+        assert np.max(np.abs(pa.get(n).cpu().numpy() - getattr(O, n))) / dx <= 1e-10, n
+    assert np.max(np.abs(pa.rho.cpu().numpy() - O.rho) / O.rho) <= 1e-12
+    # calc by calc gives the fused result
+    s2, pa2, _ = kernel_solver(kernel, rho0, cont)
+    s2.integrator.plan = None
+    for _ in range(5):
+        s2.integrator.integrate(1e-5)
+    for n in ("x", "y", "rho"):
+        a = pa.get(n).cpu().numpy()
+        b = pa2.get(n).cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, np.max(np.abs(a))), n

@@ -293,3 +293,72 @@ def test_varh_hks_five_steps(precision, name):
     rtol = 1e-12 if precision == "fp64" else 1e-5
     ref = g[f"{name}_step5_rho_0"]
     assert np.max(np.abs(rho - ref) / ref) <= rtol
+
+
+# -- the quintic spline and Wendland quintic kernels (2D) ---------------------
+KERNELS = {"QuinticSplineKernel": 3, "WendlandQuinticSplineKernel": 4}
+
+
+def kernel_engine(g, kname, name, precision, **kw):
+    sch = continuity_scheme(1, 0.5) if name == "cont" else fluid_scheme(1)
+    par = dict(DROP, rho0=float(g[f"{kname}_{name}_rho0"]))
+    return Engine([(arrays(g, ["in_"]), par)], sch, dim=2, precision=precision,
+                  kernel=KERNELS[kname], **kw)
+
+
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_neighbour_sets(kname):
+    """The neighbour radius is the kernel's support (3h for the quintic)."""
+    g = load("kernels")
+    eng = kernel_engine(g, kname, "sum", "fp64", step_lists=False)
+    di, _, sj = eng.neighbors(0, 1)
+    rdi, rsj = sorted_pairs(g[f"{kname}_nbr_off"], g[f"{kname}_nbr_idx"])
+    np.testing.assert_array_equal(di, rdi)
+    np.testing.assert_array_equal(sj, rsj)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("name", ["sum", "cont"])
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_first_stage(kname, name, precision):
+    g = load("kernels")
+    cont = name == "cont"
+    eng = kernel_engine(g, kname, name, precision)
+    eng.eval_stage()
+    eng.check_status()
+    pre = f"{kname}_{name}_stage0_"
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    for n in ("rho", "p", "cs"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[pre + n]
+        assert np.max(np.abs(got - ref)) <= rtol * np.max(np.abs(ref)) + 1e-300, n
+    atol = 1e-10 if precision == "fp64" else 1e-4
+    for n in ["_a_u_1", "_a_v_1", "dt_fac"] + (["_a_rho_1"] if cont else []):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[pre + n]
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, n
+    if cont:
+        for c, v in (("x", "u"), ("y", "v")):
+            got = (eng.get(0, v) + eng.get(0, f"_xsph_{v}")).cpu().numpy()
+            ref = g[f"{pre}_a_{c}_1"]
+            assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, c
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("name", ["sum", "cont"])
+@pytest.mark.parametrize("kname", sorted(KERNELS))
+def test_other_kernels_five_steps(kname, name, precision):
+    g = load("kernels")
+    eng = kernel_engine(g, kname, name, precision)
+    for _ in range(5):
+        eng.pc_step()
+    eng.check_status()
+    dx = 0.05
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"{kname}_{name}_step5_{n}_0"])) / dx <= tol, n
+    rho = eng.get(0, "rho").cpu().numpy()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    ref = g[f"{kname}_{name}_step5_rho_0"]
+    assert np.max(np.abs(rho - ref) / ref) <= rtol
