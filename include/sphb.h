@@ -200,6 +200,12 @@ typedef struct {
      * velocity that sphb_pc_stage adds to the position rate */
     void *drho;
     void *xu, *xv, *xw;
+    /* Optional (FP32C): the second copy of the pair records for the
+     * integrator stage fused into sphb_momentum (SPHB_FORCE_STAGE): the
+     * pass reads geo / vel and writes the moved particles' new records
+     * here, so the caller swaps geo <-> geo_next and vel <-> vel_next after
+     * it.  When set, the rebin and sphb_refresh write both copies. */
+    void *geo_next, *vel_next;
     int32_t list_cap;       /* slots per particle, 0 = no lists */
     int32_t pad0;
 } sphb_fields;
@@ -357,6 +363,18 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
  * mode | SPHB_FORCE_USE_LIST: iterate the lists of the last sphb_density
  * pass (same bin, same sources) instead of searching cells. */
 #define SPHB_FORCE_USE_LIST 16
+/* mode | SPHB_FORCE_NO_MAXIMA: leave the per-scene dt_fac / |a| maxima
+ * alone (a predictor's pass, whose maxima the CFL rule does not read). */
+#define SPHB_FORCE_NO_MAXIMA 32
+/* mode | SPHB_FORCE_STAGE(kind), FP32C with f.geo_next / vel_next: the
+ * sphb_pc_stage stage `kind` (0..3) of every dest particle in the pass's
+ * epilogue, on the accelerations, density rate and XSPH velocity it has
+ * just computed.  The new records go to geo_next / vel_next; every stepped
+ * array (cfg.step_on) and density-rate dest must be a dest of the pass.
+ * Unlike sphb_pc_stage, stage 0 does not clear the CFL maxima: give the
+ * predictor's pass SPHB_FORCE_NO_MAXIMA instead. */
+#define SPHB_FORCE_STAGE(kind) (((kind) + 1) << 8)
+#define SPHB_FORCE_STAGE_MASK 0x700
 SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
                   int with_gravity, int mode, void *stream);
 

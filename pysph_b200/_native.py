@@ -99,8 +99,16 @@ class Buffers(ctypes.Structure):
 
 
 FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
-               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor", "drho", "xu", "xv", "xw")
+               "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor", "drho", "xu", "xv", "xw",
+               "geo_next", "vel_next")
 FORCE_USE_LIST = 16
+FORCE_NO_MAXIMA = 32
+
+
+def FORCE_STAGE(kind: int) -> int:
+    """sphb_momentum mode bits of the fused integrator stage `kind`."""
+    return (kind + 1) << 8
+
 DENSITY_EOS = 1
 DENSITY_USE_LIST = 2
 

@@ -124,16 +124,23 @@ k_refresh(const __grid_constant__ sphb_engine e, int cur)
     const float xr = (float)(B.x[k] - (double)(st.lo[0] + cx) * cs);
     const float yr = (float)(B.y[k] - (double)(st.lo[1] + cy) * cs);
     float4 *geo = (float4 *)e.f.geo;
+    const float4 g = geo[k];
+    // both copies of the records when the force pass steps the state
+    float4 gn;
     if (DIM == 2) {
-        const float4 g = geo[k];
-        geo[k] = make_float4(xr, yr, g.z, g.w);
-        ((float2 *)e.f.vel)[k] = make_float2((float)B.u[k], (float)B.v[k]);
+        gn = make_float4(xr, yr, g.z, g.w);
+        const float2 vv = make_float2((float)B.u[k], (float)B.v[k]);
+        ((float2 *)e.f.vel)[k] = vv;
+        if (e.f.vel_next) ((float2 *)e.f.vel_next)[k] = vv;
     } else {
         const float zr = (float)(B.z[k] - (double)(st.lo[2] + cz) * cs);
-        const float4 g = geo[k];
-        geo[k] = make_float4(xr, yr, zr, g.w);
-        ((float4 *)e.f.vel)[k] = make_float4((float)B.u[k], (float)B.v[k], (float)B.w[k], 0.f);
+        gn = make_float4(xr, yr, zr, g.w);
+        const float4 vv = make_float4((float)B.u[k], (float)B.v[k], (float)B.w[k], 0.f);
+        ((float4 *)e.f.vel)[k] = vv;
+        if (e.f.vel_next) ((float4 *)e.f.vel_next)[k] = vv;
     }
+    geo[k] = gn;
+    if (e.f.geo_next) ((float4 *)e.f.geo_next)[k] = gn;
 }
 
 // ----------------------------------------------------------- grid setup --
@@ -473,13 +480,20 @@ k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial, int 
     const float yr = (float)(y - (double)(st.lo[1] + cy) * cs);
     const float zr = DIM == 3 ? (float)(z - (double)(st.lo[2] + cz) * cs) : 0.f;
     if (F32) {
+        // both copies of the records when the force pass steps the state
+        const float4 g = DIM == 2 ? make_float4(xr, yr, (float)h, (float)m)
+                                  : make_float4(xr, yr, zr, (float)h);
+        ((float4 *)e.f.geo)[k] = g;
+        if (e.f.geo_next) ((float4 *)e.f.geo_next)[k] = g;
         if (DIM == 2) {
-            ((float4 *)e.f.geo)[k] = make_float4(xr, yr, (float)h, (float)m);
-            ((float2 *)e.f.vel)[k] = make_float2((float)u, (float)v);
+            const float2 vv = make_float2((float)u, (float)v);
+            ((float2 *)e.f.vel)[k] = vv;
+            if (e.f.vel_next) ((float2 *)e.f.vel_next)[k] = vv;
         } else {
-            ((float4 *)e.f.geo)[k] = make_float4(xr, yr, zr, (float)h);
             ((float *)e.f.mass)[k] = (float)m;
-            ((float4 *)e.f.vel)[k] = make_float4((float)u, (float)v, (float)w, 0.f);
+            const float4 vv = make_float4((float)u, (float)v, (float)w, 0.f);
+            ((float4 *)e.f.vel)[k] = vv;
+            if (e.f.vel_next) ((float4 *)e.f.vel_next)[k] = vv;
         }
     }
     if (e.f.anchor) {

@@ -20,8 +20,25 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
     if ((rc = check_pair_cfg(e))) return rc;
-    if ((mode & ~SPHB_FORCE_USE_LIST) != 0 && (mode & ~SPHB_FORCE_USE_LIST) != 1)
-        return SPHB_ERR_ARG;
+    const int fmode = mode & ~(SPHB_FORCE_USE_LIST | SPHB_FORCE_NO_MAXIMA | SPHB_FORCE_STAGE_MASK);
+    if (fmode != 0 && fmode != 1) return SPHB_ERR_ARG;
+    const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
+    if (kind > 3) return SPHB_ERR_ARG;
+    if (kind >= 0) {
+        // the fused stage: FP32C, both record copies, the stage buffers,
+        // and every stepped / density-rate array a dest of this pass
+        const sphb_config &c = e->cfg;
+        if (c.precision != SPHB_FP32C || !e->f.geo_next || !e->f.vel_next) return SPHB_ERR_ARG;
+        const sphb_buffers &B = e->buf[cur];
+        if (!B.x0 || !B.y0 || !B.u0 || !B.v0 || (c.dim == 3 && (!B.z0 || !B.w0)))
+            return SPHB_ERR_ARG;
+        for (int a = 0; a < c.num_arrays; ++a) {
+            const bool pair_dest = ((dest_mask >> a) & 1u) &&
+                                   (c.mom_src[a] | c.rate_src[a] | c.xsph_src[a]) != 0u;
+            if ((((c.step_on >> a) & 1u) || c.rate_src[a]) && !pair_dest) return SPHB_ERR_ARG;
+            if (c.rate_src[a] && (!B.rho || !B.rho0)) return SPHB_ERR_ARG;
+        }
+    }
     if (!e->f.au || !e->f.av || (e->cfg.dim == 3 && !e->f.aw)) return SPHB_ERR_ARG;
     if ((mode & 15) == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
     for (int a = 0; a < SPHB_MAX_ARRAYS; ++a) {

@@ -24,14 +24,18 @@
 #include "sphb_kernels.cuh"
 #include "sphb_launch.cuh"
 #include "sphb_pairs.cuh"
+#include "sphb_stage.cuh"
 
 namespace sphb {
 
 // CONT: the continuity scheme's pair terms too -- SPHDensityRate
 // (density_funcs.pyx:119-156) and XSPHCorrection (xsph_funcs.pyx:40-86),
 // each over its own sources, in the same traversal as the momentum.
+// The 2D FP32C momentum-only variants are held to 80 registers (three
+// 256-thread blocks per SM); left alone, the fused stage in the epilogue
+// would take them to 96 (two blocks).
 template <int KT, int DIM, bool F32, int LANES, int R, int U, bool CONT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? 3 : 1)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
 {
@@ -427,13 +431,44 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         }
         if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
     }
-    // one atomic per block and quantity (a block never spans two scenes)
-    const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
-    const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
-    if (threadIdx.x == 0) {
-        sphb_scene_state &sw = e.sstate[s];
-        atomic_max_nonneg(&sw.max_dtfac, bdt);
-        atomic_max_nonneg(&sw.max_acc2, ba2);
+    if (!(mode & SPHB_FORCE_NO_MAXIMA)) {
+        // one atomic per block and quantity (a block never spans two scenes)
+        const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
+        const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
+        if (threadIdx.x == 0) {
+            sphb_scene_state &sw = e.sstate[s];
+            atomic_max_nonneg(&sw.max_dtfac, bdt);
+            atomic_max_nonneg(&sw.max_acc2, ba2);
+        }
+    }
+    if constexpr (F32) {
+        // the integrator stage fused into the epilogue (FP32C): the rates
+        // as stored above, the new records into the second copy
+        const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
+        if (kind >= 0) {
+            const bool stepped = (e.cfg.step_on >> a) & 1u;
+            float d2 = 0.f;
+            if (active && lane == 0 && (stepped || rm)) {
+                const bool real = e.buf[cur].tag[k] == 0;
+                double f[3], xv[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    f[d] = (double)(float)acc[d];
+                    xv[d] = (double)(float)(real ? xs[d] : 0.0);
+                }
+                const double dr = (double)(float)(real ? drho : 0.0);
+                const float4 g_old = ((const float4 *)e.f.geo)[k];
+                d2 = stage_particle<DIM, true>(e, cur, k, s, a, kind, f, xm != 0u, xv, dr,
+                                               (float4 *)e.f.geo_next, e.f.vel_next, g_old);
+            }
+            if (stepped && e.f.anchor) warp_max_disp(e, s, d2);
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                // the particles move: the lists are not known to be complete
+                // until the next rebin decision, and they leave the anchors
+                e.work.meta[2] = 0;
+                e.work.meta[3] = 0;
+            }
+        }
     }
     block_add_u64(&e.work.pairs[1], np);
 }

@@ -1,19 +1,12 @@
-// sphb_step.cu -- predictor-corrector stages, the per-step prologue (count,
-// CFL time step), user <-> engine order exchange, and the host helpers of
-// the C ABI (sm_100a).
-//
-// PredictorCorrectorIntegrator (S/solver/integrator.py:614-683):
-//   predict   X0 = X;  X = X0 + dt/2 F(X)                      (step, :340-367)
-//   correct   X = X0 + dt/2 F(X_half);  final  X = 2 X - X0    (:632-644)
-// F is the acceleration for u, v, w and, through PositionStepping
-// (S/sph/funcs/position_funcs.pyx:10-56), the velocity for x, y, z.  The
-// state stays FP64; products and sums round separately (numpy's
-// `initial + step * dt`, no FMA), so FP64 runs track the reference closely.
+// sphb_step.cu -- integrator stages (the per-particle stage itself is in
+// sphb_stage.cuh), the per-step prologue (count, CFL time step), user <->
+// engine order exchange, and the host helpers of the C ABI (sm_100a).
 
 #include <stdio.h>
 #include <string.h>
 
 #include "sphb_common.cuh"
+#include "sphb_stage.cuh"
 
 namespace sphb {
 
@@ -35,11 +28,6 @@ int launch_status(const char *what)
         return SPHB_ERR_CUDA;
     }
     return SPHB_OK;
-}
-
-__device__ __forceinline__ double axpy_rn(double x0, double a, double dt)
-{
-    return __dadd_rn(x0, __dmul_rn(a, dt));
 }
 
 template <int DIM, bool F32>
@@ -65,126 +53,36 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         }
     }
     const int k = t.begin + threadIdx.x;
-    const bool active = k < t.end;
-    const sphb_buffers &B = e.buf[cur];
-    const sphb_scene_state &st = e.sstate[s];
-    const double dt2 = st.dt / 2;
-    // the stage: 0 save X0, X = X0 + dt/2 F; 1 X = 2 (X0 + dt/2 F) - X0;
-    // 2 save X0, X = X0 + dt F; 3 X = X0 + dt F
-    const bool save = stage == 0 || stage == 2;
-    const double hstep = stage == 0 ? dt2 : st.dt;
-    auto advance = [&](double cur0, double init, double rate) {
-        if (stage == 1) return __dadd_rn(2 * axpy_rn(init, rate, dt2), -init);
-        return axpy_rn(save ? cur0 : init, rate, hstep);
-    };
-    // continuity scheme: the density of every SPHDensityRate dest is
-    // integrated like the other stepped properties
-    if (active && B.rho && B.rho0 && e.f.drho && e.cfg.rate_src[a]) {
-        const double dr = F32 ? (double)((const float *)e.f.drho)[k] : ((const double *)e.f.drho)[k];
-        const double r = B.rho[k];
-        const double r0 = save ? r : B.rho0[k];
-        if (save) B.rho0[k] = r;
-        B.rho[k] = advance(r, r0, dr);
-    }
-    if (!((e.cfg.step_on >> a) & 1u)) return;  // block-uniform
-    // XSPHCorrection adds to PositionStepping's rate
-    const bool xsph = e.cfg.xsph_src[a] && e.f.xu && e.f.xv && (DIM == 2 || e.f.xw);
-    const bool rec = F32 && e.f.geo && e.f.vel;   // FP32 pair records
-    const bool disp = e.f.anchor != nullptr;      // displacement check
+    const bool rate = e.buf[cur].rho && e.f.drho && e.cfg.rate_src[a];
+    const bool stepped = (e.cfg.step_on >> a) & 1u;
+    if (!rate && !stepped) return;   // block-uniform
     float d2 = 0.f;
-    if (active) {
-        // every load first, so a thread's loads are in flight together
-        double *X[3] = {B.x, B.y, B.z};
-        double *V[3] = {B.u, B.v, B.w};
-        double *X0[3] = {B.x0, B.y0, B.z0};
-        double *V0[3] = {B.u0, B.v0, B.w0};
-        const bool real = B.tag[k] == 0;
-        double f[3] = {0.0, 0.0, 0.0}, x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
-        double x0[3] = {0.0, 0.0, 0.0}, v0[3] = {0.0, 0.0, 0.0}, xv[3] = {0.0, 0.0, 0.0};
+    if (k < t.end) {
+        // the rates the force pass left: accelerations, XSPH velocity,
+        // density rate
+        auto ld = [&](const void *q) {
+            return F32 ? (double)((const float *)q)[k] : ((const double *)q)[k];
+        };
+        const bool xsph = e.cfg.xsph_src[a] && e.f.xu && e.f.xv && (DIM == 2 || e.f.xw);
+        double f[3] = {0.0, 0.0, 0.0}, xv[3] = {0.0, 0.0, 0.0};
+        if (stepped) {
+            const void *fa[3] = {e.f.au, e.f.av, e.f.aw};
+            const void *xa[3] = {e.f.xu, e.f.xv, e.f.xw};
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            const void *fa = d == 0 ? e.f.au : (d == 1 ? e.f.av : e.f.aw);
-            f[d] = F32 ? (double)((const float *)fa)[k] : ((const double *)fa)[k];
-            if (xsph) {
-                const void *xa = d == 0 ? e.f.xu : (d == 1 ? e.f.xv : e.f.xw);
-                xv[d] = F32 ? (double)((const float *)xa)[k] : ((const double *)xa)[k];
-            }
-            x[d] = X[d][k];
-            v[d] = V[d][k];
-            if (!save) {
-                x0[d] = X0[d][k];
-                v0[d] = V0[d][k];
+            for (int d = 0; d < DIM; ++d) {
+                f[d] = ld(fa[d]);
+                if (xsph) xv[d] = ld(xa[d]);
             }
         }
-        int local = (rec || disp) ? e.f.cell[k] : 0;
-        float an[3] = {0.f, 0.f, 0.f};
-        if (disp) {
-            if (DIM == 2) {
-                const float2 q = ((const float2 *)e.f.anchor)[k];
-                an[0] = q.x;
-                an[1] = q.y;
-            } else {
-                const float4 q = ((const float4 *)e.f.anchor)[k];
-                an[0] = q.x;
-                an[1] = q.y;
-                an[2] = q.z;
-            }
-        }
-        const float hk = (rec && DIM == 3) ? (float)B.h[k] : 0.f;
-        // the stage
-        double p[3] = {0.0, 0.0, 0.0}, vn[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            const double fd = real ? f[d] : 0.0;
-            // PositionStepping: F_x = u (+ the XSPH velocity)
-            const double fx = real ? (xsph ? __dadd_rn(v[d], xv[d]) : v[d]) : 0.0;
-            if (save) {
-                X0[d][k] = x[d];
-                V0[d][k] = v[d];
-            }
-            p[d] = advance(x[d], x0[d], fx);
-            vn[d] = advance(v[d], v0[d], fd);
-            X[d][k] = p[d];
-            V[d][k] = vn[d];
-        }
-        // FP32 pair records of the new state, relative to the particle's
-        // cell of the last bin, and how far it has moved from where that bin
-        // put it
-        if (rec || disp) {
-            if (local < 0 || local >= st.ncells) {
-                flag(e, SPHB_ST_BAD_INDEX);
-                local = 0;
-            }
-            const double cs = e.scene[s].cell_size;
-            int c[3];
-            cell_coords(local, st.n, c[0], c[1], c[2]);
-            float xr[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) xr[d] = (float)(p[d] - (double)(st.lo[d] + c[d]) * cs);
-            if (rec) {
-                if (DIM == 2) {
-                    ((float2 *)e.f.geo)[2 * k] = make_float2(xr[0], xr[1]);
-                    ((float2 *)e.f.vel)[k] = make_float2((float)vn[0], (float)vn[1]);
-                } else {
-                    ((float4 *)e.f.geo)[k] = make_float4(xr[0], xr[1], xr[2], hk);
-                    ((float4 *)e.f.vel)[k] =
-                        make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
-                }
-            }
-            if (disp) {
-                const float q0 = xr[0] - an[0], q1 = xr[1] - an[1], q2 = xr[2] - an[2];
-                d2 = q0 * q0 + q1 * q1 + q2 * q2;
-                // a non-finite position can never be within the skin
-                if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
-            }
-        }
+        const double dr = rate ? ld(e.f.drho) : 0.0;
+        // FP32 pair records rewritten in place
+        const bool rec = F32 && e.f.geo && e.f.vel && stepped;
+        float4 *geo = rec ? (float4 *)e.f.geo : nullptr;
+        const float4 g_old = rec ? geo[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        d2 = stage_particle<DIM, F32>(e, cur, k, s, a, stage, f, xsph, xv, dr, geo,
+                                      rec ? e.f.vel : nullptr, g_old);
     }
-    if (disp) {
-        // non-negative floats order like their bits: one warp reduction
-        const float wd = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(d2)));
-        if ((threadIdx.x & 31) == 0 && wd > 0.f)
-            atomic_max_nonneg(&e.sstate[s].max_disp2, (double)wd);
-    }
+    if (stepped && e.f.anchor) warp_max_disp(e, s, d2);
 }
 
 // Solver.solve per-step prologue for every scene.

@@ -149,7 +149,7 @@ class Engine:
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
                  step_lists: bool = True, skin_margin: float | None = None,
                  list_batch: int = 4, variable_h: bool = False,
-                 kernel: int = nat.KERNEL_CUBIC):
+                 kernel: int = nat.KERNEL_CUBIC, fuse_stage: bool = True):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -210,6 +210,8 @@ class Engine:
         # symmetric neighbour sets r < radius_scale max(h_a, h_b)
         # (VarHNbrParticleLocator) instead of r < radius_scale h_a
         self.variable_h = bool(variable_h)
+        # run the integrator stage in the force pass's epilogue (FP32C)
+        self.fuse_stage = bool(fuse_stage)
         self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
         self._host_scene_tables(scenes)
@@ -331,11 +333,16 @@ class Engine:
             f["mass"] = torch.zeros(N, **f32) if dim == 3 else None
             f["vel"] = torch.zeros(N, 2 if dim == 2 else 4, **f32)
             f["thermo"] = torch.zeros(N, 4, **f32)
+            # the second copy of the records: the force pass that runs the
+            # integrator stage writes the moved particles' records there
+            f["geo_next"] = torch.zeros_like(f["geo"])
+            f["vel_next"] = torch.zeros_like(f["vel"])
         else:
             for n in ("rho", "p", "cs", "au", "av", "dt_fac"):
                 f[n] = torch.zeros(N, **f64)
             f["aw"] = torch.zeros(N, **f64) if dim == 3 else None
             f["geo"] = f["mass"] = f["vel"] = f["thermo"] = None
+            f["geo_next"] = f["vel_next"] = None
         f["cell"] = torch.zeros(N, **i32)
         # outputs of SPHDensityRate (_a_rho_1) and XSPHCorrection (velocity):
         # the continuity scheme's, and any single calc's on this engine
@@ -639,17 +646,54 @@ class Engine:
         self.call("sphb_pc_stage", self.cur, stage)
         self._box_valid = True
 
+    @property
+    def fuses_stage(self) -> bool:
+        """Whether the integrator stage runs in the force pass's epilogue
+        (FP32C, with every stepped and density-rate array a force dest)."""
+        if not (self.f32 and self.fuse_stage):
+            return False
+        dests = self.scheme.pair_dests if self.scheme.continuity else self.scheme.mom_dests
+        need = sum(1 << a for a in self.scheme.step_on)
+        need |= sum(1 << d for d, s in self.scheme.rate_src.items() if s)
+        return need & ~dests == 0
+
+    def _swap_records(self):
+        f = self.fields
+        f["geo"], f["geo_next"] = f["geo_next"], f["geo"]
+        f["vel"], f["vel_next"] = f["vel_next"], f["vel"]
+        for name in ("geo", "geo_next", "vel", "vel_next"):
+            setattr(self.desc.f, name, f[name].data_ptr())
+
+    def _stage(self, kind: int):
+        """Integrator.eval at the current positions, then stage `kind` of
+        sphb_pc_stage: fused into the force pass when the engine allows it
+        (the predictor's pass then leaves the CFL maxima alone), else as its
+        own pass.  A fused stage swaps the two record copies, so a captured
+        graph must hold an even number of them (a PC or RK2 step does)."""
+        if self.fuses_stage:
+            self.eval_stage(stage=kind)
+            self._box_valid = True
+        else:
+            self.eval_stage()
+            self.pc_stage(kind)
+
     def step_begin(self):
         self.call("sphb_step_begin")
 
-    def eval_stage(self):
+    def eval_stage(self, stage: int | None = None):
         """Integrator.eval of the pinned scheme at the current positions:
         SPHRho + Tait (fused), Tait on arrays without SPHRho, then
         MomentumEquation (or SPHPressureGradient) + GravityForce.  The
         density pass records the neighbour lists the force pass reads; with
-        list reuse it reads the lists the last rebin decision kept."""
+        list reuse it reads the lists the last rebin decision kept.  With
+        `stage` (engines where fuses_stage) the force pass also runs that
+        integrator stage and the record copies swap."""
         reuse = nat.DENSITY_LIST_IF_VALID if self.step_lists else 0
         mode = self.force_mode | (nat.FORCE_USE_LIST if self.list_cap else 0)
+        if stage is not None:
+            if not self.fuses_stage:
+                raise ValueError("this engine runs the integrator stage on its own")
+            mode |= nat.FORCE_STAGE(stage) | (nat.FORCE_NO_MAXIMA if stage == 0 else 0)
         if self.scheme.continuity:
             # TaitEquation on the integrated density, then one pair pass:
             # SPHDensityRate + MomentumEquation + XSPHCorrection; the density
@@ -658,11 +702,13 @@ class Engine:
                       nat.DENSITY_LISTS_ONLY | reuse)
             self.tait()
             self.call("sphb_momentum", self.cur, self.scheme.pair_dests, 1, mode)
-            return
-        self.call("sphb_density", self.cur, self.scheme.rho_dests, nat.DENSITY_EOS | reuse)
-        if self.tait_only_mask:
-            self.tait(self.tait_only_mask)
-        self.momentum(mode=mode)
+        else:
+            self.call("sphb_density", self.cur, self.scheme.rho_dests, nat.DENSITY_EOS | reuse)
+            if self.tait_only_mask:
+                self.tait(self.tait_only_mask)
+            self.momentum(mode=mode)
+        if stage is not None:
+            self._swap_records()
 
     def pc_step(self, on_half=None):
         """One PredictorCorrectorIntegrator.integrate(dt) of every scene,
@@ -674,13 +720,11 @@ class Engine:
         reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
         self.step_begin()
         self.bin(reuse)
-        self.eval_stage()
-        self.pc_stage(0)
+        self._stage(0)
         if on_half is not None:
             on_half()
         self.bin(nat.BIN_MOVE_INITIAL | reuse)
-        self.eval_stage()
-        self.pc_stage(1)
+        self._stage(1)
 
     def step(self, integrator: str = "pc", on_half=None):
         """One step of the named integrator: "pc" (pc_step), "euler"
@@ -693,16 +737,14 @@ class Engine:
         reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
         self.step_begin()
         self.bin(reuse)
-        self.eval_stage()
         if integrator == "euler":
-            self.pc_stage(2)
+            self._stage(2)
             return
-        self.pc_stage(0)
+        self._stage(0)
         if on_half is not None:
             on_half()
         self.bin(nat.BIN_MOVE_INITIAL | reuse)
-        self.eval_stage()
-        self.pc_stage(3)
+        self._stage(3)
 
     def rebin_count(self) -> int:
         """1 when the last device-decided rebin happened (host sync)."""

@@ -435,3 +435,34 @@ def test_continuity_against_oracle_with_walls_and_ghosts():
             got = eng.get(i, n).cpu().numpy()
             ref = getattr(O, n)
             assert np.max(np.abs(got - ref)) <= 1e-10 * max(1.0, np.max(np.abs(ref))), (i, n)
+
+
+@pytest.mark.parametrize("case,cont,integ", [("dam", False, "pc"), ("dam", True, "pc"),
+                                             ("drop", False, "euler"), ("drop", True, "rk2")])
+def test_fused_stage_matches_separate_pass(case, cont, integ):
+    """The integrator stage in the force pass's epilogue (FP32C) against the
+    same stage as its own pass: the same rates in the same arithmetic, so
+    the states, the CFL time steps and the rebin decisions agree bit for
+    bit."""
+    from pysph_b200.engine import continuity_scheme
+    arrays, params, scheme, dim = CASES[case]()
+    if cont:
+        scheme = continuity_scheme(len(arrays), 0.5)
+    a = Engine([(arrays, params)], scheme, dim=dim, precision="fp32c")
+    b = Engine([(arrays, params)], scheme, dim=dim, precision="fp32c", fuse_stage=False)
+    assert a.fuses_stage and not b.fuses_stage
+    dts, rebins = [], 0
+    for _ in range(30):
+        a.step(integ)
+        b.step(integ)
+        rebins += a.rebin_count()
+        assert a.rebin_count() == b.rebin_count()
+        dts.append((a.scene_state()[0].dt, b.scene_state()[0].dt))
+    a.check_status()
+    b.check_status()
+    assert all(x == y for x, y in dts)
+    for i in range(len(arrays)):
+        for n in ("x", "y", "u", "v", "rho", "p"):
+            assert torch.equal(a.get(i, n), b.get(i, n)), (i, n)
+    if case == "dam":
+        assert rebins > 0
