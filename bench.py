@@ -580,8 +580,8 @@ def kernel_times(eng, flush, stream, reps=20):
         # records it writes go to the second copy, which the rebin below
         # rewrites)
         mode_s = mode_f | nat.FORCE_STAGE(0) | nat.FORCE_NO_MAXIMA
-        out["force_stage"] = timed(lambda: eng.call("sphb_momentum", eng.cur,
-                                                    eng.scheme.mom_dests, 1, mode_s))
+        dests = eng.scheme.pair_dests if eng.scheme.continuity else eng.scheme.mom_dests
+        out["force_stage"] = timed(lambda: eng.call("sphb_momentum", eng.cur, dests, 1, mode_s))
     out["rebin"] = timed(lambda: eng.bin(nat.BIN_MOVE_INITIAL))
     if eng.step_lists:
         # positions at the anchors: the decision keeps the lists every time

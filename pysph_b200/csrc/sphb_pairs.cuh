@@ -155,30 +155,43 @@ __device__ __forceinline__ int list_count(const sphb_engine &e, bool use_list, i
     return ok ? mine : -1;
 }
 
-// use(load(entry)) over the cnt list entries of (k, lane).  U entries and
-// then their neighbour records are loaded before any is used, so each
-// thread keeps U gathers in flight instead of one dependent chain.
+// use(load(entry)) over the cnt list entries of (k, lane), in batches of
+// U: a batch's U neighbour records are loaded before any is used, and the
+// next batch's list entries are fetched before this batch's records, so a
+// thread keeps U record gathers and U list loads in flight instead of one
+// dependent chain.  The last batch is padded with entries whose index is
+// out of range, which load() marks as not ok.
 template <int DIM, int LANES, int U, typename Load, typename Use>
 __device__ __forceinline__ void list_loop(const sphb_engine &e, int k, int lane, int cnt,
                                           Load &&load, Use &&use)
 {
+    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
+    constexpr uint32_t PAD = (1u << B) - 1u;   // index >= num_particles
     const int N = e.cfg.num_particles;
     const uint32_t *__restrict__ p = e.f.nbr + (size_t)lane * N + k;
     const size_t stride = (size_t)LANES * N;
-    int c = 0;
-#pragma unroll 1
-    for (; c + U <= cnt; c += U) {
-        uint32_t v[U];
+    const int nb = (cnt + U - 1) / U;
+    auto fetch = [&](int b, uint32_t *v) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) v[u] = __ldg(p + (size_t)(c + u) * stride);
+        for (int u = 0; u < U; ++u) {
+            const int c = b * U + u;
+            v[u] = c < cnt ? __ldg(p + (size_t)c * stride) : PAD;
+        }
+    };
+    uint32_t v[U];
+    if (nb > 0) fetch(0, v);
+#pragma unroll 1
+    for (int b = 0; b < nb; ++b) {
+        uint32_t w[U];
+        if (b + 1 < nb) fetch(b + 1, w);
         decltype(load(EntryF{})) r[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) r[u] = load(entry_unpack_f<DIM>(v[u]));
 #pragma unroll
         for (int u = 0; u < U; ++u) use(r[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = w[u];
     }
-#pragma unroll 1
-    for (; c < cnt; ++c) use(load(entry_unpack_f<DIM>(__ldg(p + (size_t)c * stride))));
 }
 
 // The pairs of dest k: its list from the last density pass when use_list
