@@ -209,9 +209,12 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 # counted from the fields it reads and writes at their stored widths
 # DRAM bytes (read + write) per launch from `ncu --set full` on the dam
 # break, FP32C, lanes 1, 256-thread blocks (profiles/k_*_dam_break_fp32c.md)
-NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 47.735e6,
-               ("dam_break", "fp32c", "density"): 41.096e6,
-               ("dam_break", "fp32c", "pc_stage"): 17.976e6}
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu --set full
+# on the bench's own workload and launch shape; the force pass with the
+# integrator stage fused into it)
+NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 71.933e6 + 4.520e6,
+               ("dam_break", "fp32c", "density"): 40.980e6 + 0.008e6,
+               ("dam_break", "fp32c", "pc_stage"): 17.951e6 + 0.000256e6}
 
 
 def algorithmic_bytes(dim, f32):
