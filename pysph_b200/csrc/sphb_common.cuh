@@ -183,4 +183,24 @@ __host__ __device__ __forceinline__ double kfac_unit()
                     : 1.0 / 3.141592653589793;
 }
 
+// x^y of the Tait EOS.  The FP32C path rounds p and cs to float, so an
+// integral exponent up to 16 (gamma = 7 gives 7 and 3) is taken by
+// repeated squaring in FP64, a few roundings far below the float rounding
+// that follows; otherwise, and always on the FP64 path, pow.
+template <bool F32>
+__device__ __forceinline__ double eos_pow(double x, double y)
+{
+    if (F32 && rint(y) == y && fabs(y) <= 16.0) {
+        int n = (int)fabs(y);
+        double b = x, acc = 1.0;
+        while (n) {
+            if (n & 1) acc *= b;
+            b *= b;
+            n >>= 1;
+        }
+        return y < 0.0 ? 1.0 / acc : acc;
+    }
+    return pow(x, y);
+}
+
 }  // namespace sphb

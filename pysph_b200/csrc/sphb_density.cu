@@ -38,8 +38,8 @@ k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
     double p = 0.0, c = 0.0;
     if (real) {
         const double ratio = rho / sc.rho0;
-        p = (pow(ratio, sc.gamma) - 1.0) * sc.B;
-        c = pow(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
+        p = (eos_pow<F32>(ratio, sc.gamma) - 1.0) * sc.B;
+        c = eos_pow<F32>(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
     }
     if constexpr (F32) {
         float4 *th = (float4 *)e.f.thermo;
