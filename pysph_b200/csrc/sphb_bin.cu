@@ -39,6 +39,9 @@ __device__ __forceinline__ bool skip_rebin(const sphb_engine &e, int gated)
 __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
                              cudaGraphConditionalHandle cond, int set_cond)
 {
+    // launched as a programmatic dependent of the stage before: its
+    // displacements and meta must be complete
+    pdl_wait();
     __shared__ int s_far;
     if (threadIdx.x == 0) s_far = 0;
     __syncthreads();
@@ -655,8 +658,8 @@ static int bin_conditional(const sphb_engine *e, int cur, int flags, cudaStream_
     cudaGraphConditionalHandle cond;
     if ((err = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault)))
         return cuda_fail("sphb_bin: conditional handle", err);
-    k_bin_decide<<<1, 256, 0, st>>>(*e, cond, 1);
-    if ((err = cudaGetLastError())) return cuda_fail("sphb_bin: decision", err);
+    if ((err = launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cond, 1)))
+        return cuda_fail("sphb_bin: decision", err);
     cudaStreamCaptureStatus cs;
     unsigned long long id;
     const cudaGraphNode_t *deps = nullptr;
@@ -719,7 +722,7 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
             return cuda_fail("sphb_bin: capture info", err);
         return bin_conditional(e, cur, flags, st, graph);
     }
-    k_bin_decide<<<1, 256, 0, st>>>(*e, cudaGraphConditionalHandle(), 0);
+    launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cudaGraphConditionalHandle(), 0);
     launch_rebin(e, cur, flags, 1, st);
     return launch_status("sphb_bin");
 }

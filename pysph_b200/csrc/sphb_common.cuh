@@ -26,6 +26,40 @@ __device__ __forceinline__ void flag(const sphb_engine &e, unsigned bits)
     atomicOr(e.work.status, bits);
 }
 
+// Programmatic dependent launch.  A kernel launched with launch_pdl may start
+// while its predecessor in the stream is still running; pdl_wait() holds it
+// until that predecessor has completed and its writes are visible (at once
+// when there is none).  pdl_trigger() lets this grid's own dependent launch
+// as soon as every block of this grid has started.
+__device__ __forceinline__ void pdl_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void pdl_trigger()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch with programmatic stream serialization: the kernel must call
+// pdl_wait() before it reads anything its predecessor writes.
+template <typename... KArgs, typename... Args>
+static inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                                     cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Monotone map double -> uint64 so atomicMin/atomicMax order doubles.
 __host__ __device__ __forceinline__ unsigned long long enc_double(double v)
 {

@@ -19,6 +19,8 @@ template <bool F32>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_tait(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask)
 {
+    // the force pass that follows may launch once every block has started
+    pdl_trigger();
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;

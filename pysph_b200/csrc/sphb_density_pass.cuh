@@ -37,6 +37,8 @@ template <int KT, int DIM, bool F32, int LANES, int R>
 __global__ void __launch_bounds__(256, (F32 && DIM == 2) ? 5 : 1)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
+    // the force pass that follows may launch once every block has started
+    pdl_trigger();
     const int with_eos = flags & SPHB_DENSITY_EOS;
     // list reuse: read the lists when the last rebin decision kept them
     // (work.meta[2]); otherwise record them, with the skin

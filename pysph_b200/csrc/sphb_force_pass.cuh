@@ -39,6 +39,11 @@ __global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? 3 : 1)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
 {
+    // launched as a programmatic dependent of the density pass: everything
+    // below reads what that pass wrote; the next rebin decision may launch
+    // once every block of this pass has started
+    pdl_wait();
+    pdl_trigger();
     const sphb_tile tl = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = tl.seg / A, a = tl.seg - s * A;
@@ -479,18 +484,19 @@ static void launch_force_lr(const sphb_engine &e, int cur, uint32_t dm, int grav
 {
     const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
     if (cont) {
-        k_force<KT, DIM, F32, LV, RV, 4, true><<<g, b, 0, st>>>(e, cur, dm, grav, mode);
+        launch_pdl(k_force<KT, DIM, F32, LV, RV, 4, true>, g, b, st, e, cur, dm, grav, mode);
         return;
     }
     // the load-ahead depth only shapes the FP32C list loop of the cubic (the
     // other kernels and FP64 load 4 ahead)
     if constexpr (F32 && KT == SPHB_KERNEL_CUBIC) {
         if (e.cfg.list_batch == 2) {
-            k_force<KT, DIM, F32, LV, RV, 2, false><<<g, b, 0, st>>>(e, cur, dm, grav, mode);
+            launch_pdl(k_force<KT, DIM, F32, LV, RV, 2, false>, g, b, st, e, cur, dm, grav,
+                       mode);
             return;
         }
     }
-    k_force<KT, DIM, F32, LV, RV, 4, false><<<g, b, 0, st>>>(e, cur, dm, grav, mode);
+    launch_pdl(k_force<KT, DIM, F32, LV, RV, 4, false>, g, b, st, e, cur, dm, grav, mode);
 }
 
 template <int KT, int DIM, bool F32>
