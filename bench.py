@@ -498,7 +498,8 @@ def other_configs(dev, flush, stream):
 def adjoint_measure(dev, stream):
     """Differentiable rollout: elliptical drop, 50k particles (dx = 0.0079),
     200 steps of dt = 2e-6, checkpoints every 20, FP32C forward, FP64
-    adjoint; times forward and backward with CUDA events."""
+    adjoint; times forward and backward with CUDA events, after a warm-up
+    pair that captures the rollout's graphs."""
     import torch
     from pysph_b200 import workloads as W
     from pysph_b200.adjoint import Rollout
@@ -513,7 +514,10 @@ def adjoint_measure(dev, stream):
                  device=dev).forward({0: vt})[0][0]
     r = Rollout(arrays, params, fluid_scheme(1), 2, 2e-6, 200, checkpoint_every=20,
                 precision="fp32c", device=dev)
-    r.forward({0: v0})  # warm
+    # warm: the first forward and backward run eagerly and capture the
+    # step and segment graphs that the timed pair replays
+    xw = r.forward({0: v0})[0][0]
+    r.backward({0: (2.0 * (xw - xt) / n, torch.zeros_like(xw))})
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     torch.cuda.synchronize()
     ev[0].record(stream)

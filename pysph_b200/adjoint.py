@@ -22,6 +22,12 @@ With X0, V0 the state at the start of a step and F = F(X0, V0):
 
 RolloutFunction wraps it as a torch.autograd.Function of the initial
 velocities.
+
+With graphs=True (CUDA devices) the forward step, a segment's recompute
+(with every step's two stage states exported) and the segment's adjoint
+are each captured once in a CUDA graph and replayed: one launch per step
+forward and two per segment backward instead of thousands, with the
+results of the eager calls.
 """
 from __future__ import annotations
 
@@ -36,7 +42,7 @@ from .engine import Engine, Scheme, SceneParams
 class Rollout:
     def __init__(self, arrays, params, scheme: Scheme, dim: int = 2, dt: float = 1e-5,
                  steps: int = 200, checkpoint_every: int = 20, precision: str = "fp32c",
-                 device=None, lanes: int = 1, pair_block: int = 128):
+                 device=None, lanes: int = 1, pair_block: int = 128, graphs: bool = True):
         if scheme.continuity:
             raise NotImplementedError("the adjoint covers the summation-density scheme")
         if scheme.hks:
@@ -60,6 +66,8 @@ class Rollout:
         self.moving = list(scheme.step_on)
         self.checkpoints = []
         self._scratch = None
+        self.graphs = bool(graphs)
+        self._g = {}   # captured graphs and their fixed buffers
 
     # ---------------------------------------------------------------- state
     def _comps(self):
@@ -92,7 +100,7 @@ class Rollout:
         eng = self.fwd
         eng.set_dt_async(self.dt)
         for n in range(self.steps):
-            eng.pc_step()
+            self._fwd_step()
             if (n + 1) % self.k == 0 and n + 1 < self.steps:
                 ck = self._clone(self.get_state())
                 self.checkpoints.append(ck)
@@ -111,19 +119,22 @@ class Rollout:
     def _clone(state):
         return {a: (X.clone(), V.clone()) for a, (X, V) in state.items()}
 
-    def _segment_states(self, start_state, nsteps):
-        """Recompute nsteps steps from start_state on the forward engine;
-        per step the states (X0, V0) and (Xh, Vh) of its two stages."""
-        eng = self.fwd
-        self.set_state(start_state)
-        eng.set_dt_async(self.dt)
-        out = []
-        for _ in range(nsteps):
-            s0 = self.get_state()
-            half = {}
-            eng.pc_step(on_half=lambda: half.__setitem__("sh", self.get_state()))
-            out.append((s0, half["sh"]))
-        return out
+    # ------------------------------------------------------------- graphs
+    def _fwd_step(self):
+        """One forward step: eager the first time, captured the second,
+        replayed after that."""
+        g = self._g.get("fwd")
+        if not self.graphs or g is None:
+            if self.graphs:
+                self._g["fwd"] = "warm"
+            self.fwd.pc_step()
+            return
+        if g == "warm":
+            torch.cuda.synchronize(self.device)
+            g = self._g["fwd"] = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.fwd.pc_step()
+        g.replay()
 
     # ---------------------------------------------------------------- VJP
     def vjp_F(self, state, lam_F):
@@ -191,12 +202,76 @@ class Rollout:
         for si in reversed(range(nseg)):
             start = si * self.k
             n = min(self.k, self.steps - start)
-            states = self._segment_states(self.checkpoints[si], n)
-            for s0, sh in reversed(states):
-                lam = self.step_adjoint(s0, sh, lam)
+            # the segment's states, recomputed from its checkpoint, then its
+            # steps' adjoints in reverse: one graph replay each
+            self.set_state(self.checkpoints[si])
+            self.fwd.set_dt_async(self.dt)
+            states = self._segment_rec(n)
+            lam = self._clone(self._segment_adj(n, states, lam))
         self.adj.check_status()
         self.fwd.check_status()
         return lam
+
+    def _recompute(self, n):
+        """n forward steps from the engine's state; per step the states
+        (X0, V0) and (Xh, Vh) of its two stages."""
+        out = []
+        for _ in range(n):
+            s0 = self.get_state()
+            half = {}
+            self.fwd.pc_step(on_half=lambda: half.__setitem__("sh", self.get_state()))
+            out.append((s0, half["sh"]))
+        return out
+
+    def _adjoint(self, states, lam):
+        for s0, sh in reversed(states):
+            lam = self.step_adjoint(s0, sh, lam)
+        return lam
+
+    # A segment's recompute and its adjoint each run eagerly the first time
+    # (warming every kernel and allocation), are captured the second time
+    # and replayed after that.  The captured adjoint reads the recompute
+    # graph's own output tensors and a fixed copy of the incoming lam.
+    def _segment_rec(self, n):
+        key = ("rec", n)
+        g = self._g.get(key)
+        if not self.graphs or g is None:
+            if self.graphs:
+                self._g[key] = "warm"
+            return self._recompute(n)
+        if g == "warm":
+            torch.cuda.synchronize(self.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                out = self._recompute(n)
+            g = self._g[key] = (graph, out)
+        graph, out = g
+        graph.replay()
+        return out
+
+    def _segment_adj(self, n, states, lam):
+        key = ("adj", n)
+        g = self._g.get(key)
+        if not self.graphs or g is None:
+            if self.graphs:
+                self._g[key] = "warm"
+            return self._adjoint(states, lam)
+        if g == "warm":
+            buf = self._clone(lam)
+            torch.cuda.synchronize(self.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                out = self._adjoint(states, buf)
+            g = self._g[key] = (graph, states, buf, out)
+            lam = None   # the buffer holds it already
+        graph, cap_states, buf, out = g
+        if states is not cap_states:
+            raise RuntimeError("the adjoint graph reads the recompute graph's outputs")
+        for a, (X, V) in (lam or {}).items():
+            buf[a][0].copy_(X)
+            buf[a][1].copy_(V)
+        graph.replay()
+        return out
 
 
 class RolloutFunction(torch.autograd.Function):

@@ -31,25 +31,27 @@ struct V3 {
 // g(s) with grad W = r g and dg/ds (the cubic spline of
 // CubicSplineKernel.gradient, S/base/kernels.pyx:380-417, and its
 // derivative).  Returns g, writes dg/ds / s into dgs (for r (x) r terms).
+// Two reciprocals (1/h, 1/s) replace the divisions of the textbook form.
 template <int DIM>
 __device__ __forceinline__ double kernel_g(double s, double h, double &dgs)
 {
-    const double q = s / h;
-    const double fac = (DIM == 2 ? 1.0 / (h * h) : 1.0 / (h * h * h)) * kfac_unit<DIM>();
+    const double ih = 1.0 / h;
+    const double q = s * ih;
+    const double fac = (DIM == 2 ? ih * ih : ih * ih * ih) * kfac_unit<DIM>();
     double g = 0.0;
     dgs = 0.0;
     if (q > 2.0) {
     } else if (q >= 1.0) {
-        // g = -0.75 (2 - q)^2 / (h s) * fac
+        const double is = 1.0 / s;
+        // g = -0.75 (2 - q)^2 / (h s) fac
         const double t = 2.0 - q;
-        g = -0.75 * t * t / (h * s) * fac;
-        // dg/ds = fac * (1.5 t / (h^2 s) + 0.75 t^2 / (h s^2))
-        const double dg = fac * (1.5 * t / (h * h * s) + 0.75 * t * t / (h * s * s));
-        dgs = dg / s;
+        g = -0.75 * t * t * ih * is * fac;
+        // dg/ds = fac (1.5 t / (h^2 s) + 0.75 t^2 / (h s^2))
+        const double dg = fac * ih * is * (1.5 * t * ih + 0.75 * t * t * is);
+        dgs = dg * is;
     } else if (q > 1e-14) {
-        g = 3.0 * (0.75 * q - 1.0) / (h * h) * fac;
-        const double dg = fac * 2.25 / (h * h * h);
-        dgs = dg / s;
+        g = 3.0 * (0.75 * q - 1.0) * ih * ih * fac;
+        dgs = fac * 2.25 * ih * ih * ih / s;
     }
     return g;
 }
@@ -89,6 +91,7 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     double vk[3] = {B.u[k], B.v[k], DIM == 3 ? B.w[k] : 0.0};
     const double hk = B.h[k], mk = B.m[k];
     const double rhok = rho[k], pk = pr[k], ck = cs[k];
+    const double irhok = 1.0 / rhok;
     const bool k_dest = ((dest_mask >> a) & 1u) && B.tag[k] == 0;
     double lk[3] = {0, 0, 0};
     for (int d = 0; d < DIM; ++d) lk[d] = k_dest ? P.lam_a[(size_t)d * N + k] : 0.0;
@@ -129,30 +132,36 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
             const double rhoj = rho[j], pj = pr[j], cj = cs[j], mj = B.m[j];
             const double v[3] = {vk[0] - vj[0], vk[1] - vj[1], vk[2] - vj[2]};
             const double dot = v[0] * r[0] + v[1] * r[1] + v[2] * r[2];
-            const double den = r2 + eta2 * h * h;
-            const double mu = h * dot / den;
+            // reciprocals once per pair instead of a division per term
+            const double iden = 1.0 / (r2 + eta2 * h * h);
+            const double mu = h * dot * iden;
             const double rhobar = 0.5 * (rhok + rhoj), cbar = 0.5 * (ck + cj);
+            const double irb = 1.0 / rhobar;
+            const double irhoj = 1.0 / rhoj;
             double Pi = 0.0, dPi_dmu = 0.0;
             if (dot < 0.0) {
-                Pi = (-alpha * cbar * mu + beta * mu * mu) / rhobar;
-                dPi_dmu = (-alpha * cbar + 2.0 * beta * mu) / rhobar;
+                Pi = (-alpha * cbar * mu + beta * mu * mu) * irb;
+                dPi_dmu = (-alpha * cbar + 2.0 * beta * mu) * irb;
             }
             // dmu/dr = h (v / den - 2 dot r / den^2); dmu/dv_a = h r / den
             double dmu_dr[3], dmu_dv[3];
             for (int d = 0; d < 3; ++d) {
-                dmu_dr[d] = h * (v[d] / den - 2.0 * dot * r[d] / (den * den));
-                dmu_dv[d] = h * r[d] / den;
+                dmu_dr[d] = h * iden * (v[d] - 2.0 * dot * r[d] * iden);
+                dmu_dv[d] = h * r[d] * iden;
             }
+            // 1 / rho of each particle of the pair
+            const double irho_k = irhok;
             // The pair term T = -m_b (A + Pi) G(r) is symmetric in which
             // particle is "a"; both roles use r = x_a - x_b.
-            auto accumulate = [&](const double *lam, double mb, double rho_a, double p_a,
-                                  double rho_b, double p_b, double sign_r, bool k_is_a) {
+            auto accumulate = [&](const double *lam, double mb, double irho_a, double p_a,
+                                  double irho_b, double p_b, double sign_r, bool k_is_a) {
                 // r_role = sign_r * r (role 2 has a = j, so r_role = -r)
                 double rr[3] = {sign_r * r[0], sign_r * r[1], sign_r * r[2]};
                 double GG[3] = {sign_r * G[0], sign_r * G[1], sign_r * G[2]};
                 const double lg = lam[0] * GG[0] + lam[1] * GG[1] + lam[2] * GG[2];
                 const double lr = lam[0] * rr[0] + lam[1] * rr[1] + lam[2] * rr[2];
-                const double AP = (p_a / (rho_a * rho_a) + p_b / (rho_b * rho_b)) + Pi;
+                const double pa_r2 = p_a * irho_a * irho_a, pb_r2 = p_b * irho_b * irho_b;
+                const double AP = (pa_r2 + pb_r2) + Pi;
                 // lam^T dT/dr_role = -m_b [ (A+Pi)(g lam + (lam.r) dgs r) + (lam.G) dPi/dr ]
                 double dT_dr[3];
                 for (int d = 0; d < 3; ++d) {
@@ -163,11 +172,11 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
                 double dT_dva[3];
                 for (int d = 0; d < 3; ++d)
                     dT_dva[d] = -mb * lg * dPi_dmu * sign_r * dmu_dv[d];
-                const double dT_drho_a = -mb * lg * (-2.0 * p_a / (rho_a * rho_a * rho_a) - 0.5 * Pi / rhobar);
-                const double dT_drho_b = -mb * lg * (-2.0 * p_b / (rho_b * rho_b * rho_b) - 0.5 * Pi / rhobar);
-                const double dT_dp_a = -mb * lg / (rho_a * rho_a);
-                const double dT_dp_b = -mb * lg / (rho_b * rho_b);
-                const double dT_dc = (dot < 0.0) ? -mb * lg * (-alpha * mu * 0.5 / rhobar) : 0.0;
+                const double dT_drho_a = -mb * lg * (-2.0 * pa_r2 * irho_a - 0.5 * Pi * irb);
+                const double dT_drho_b = -mb * lg * (-2.0 * pb_r2 * irho_b - 0.5 * Pi * irb);
+                const double dT_dp_a = -mb * lg * irho_a * irho_a;
+                const double dT_dp_b = -mb * lg * irho_b * irho_b;
+                const double dT_dc = (dot < 0.0) ? -mb * lg * (-alpha * mu * 0.5 * irb) : 0.0;
                 if (k_is_a) {
                     for (int d = 0; d < DIM; ++d) {
                         gx[d] += dT_dr[d];    // dr/dx_a = +I
@@ -186,11 +195,11 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
                     gc += dT_dc;
                 }
             };
-            if (r1) accumulate(lk, mj, rhok, pk, rhoj, pj, 1.0, true);
+            if (r1) accumulate(lk, mj, irho_k, pk, irhoj, pj, 1.0, true);
             if (role2) {
                 double lj[3] = {0, 0, 0};
                 for (int d = 0; d < DIM; ++d) lj[d] = P.lam_a[(size_t)d * N + j];
-                accumulate(lj, mk, rhoj, pj, rhok, pk, -1.0, false);
+                accumulate(lj, mk, irhoj, pj, irho_k, pk, -1.0, false);
             }
         });
     for (int d = 0; d < DIM; ++d) {
