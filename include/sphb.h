@@ -441,7 +441,10 @@ SPHB_API int sphb_permute(const sphb_engine *e, int cur, int array, int dir, dou
  * The reference has no gradients; these are the reverse-mode kernels of the
  * differentiable rollout (FP64 engines only).  Vectors are SoA [dim][N] in
  * engine order.  Each needs the forward quantities of the stage (positions,
- * velocities, rho, p, cs from sphb_density) and its bin. */
+ * velocities, rho, p, cs from sphb_density) and its bin.  In a scene of
+ * uniform h, the pair kernels walk the neighbour lists that sphb_density
+ * recorded for that bin (every array with SPHRho sources, f.list_cap > 0);
+ * otherwise they search the cells. */
 
 /* Given lam_a, the adjoint of the MomentumEquation acceleration of the dest
  * arrays in dest_mask: lam_x += (da/dx)^T lam_a, lam_v += (da/dv)^T lam_a;

@@ -105,8 +105,13 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     // array decides the dest-role sources, mom_src of the neighbour's array
     // the source role
     const uint32_t all = (1u << A) - 1u;
-    for_each_candidate<DIM, R, 1>(
-        e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, 0, N, e.work.status,
+    // the lists of the density pass (recorded one lane per particle) hold
+    // every pair of both roles when h is uniform (the predicate is then
+    // symmetric)
+    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
+                          e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
+    traverse<DIM, R, 1>(
+        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
         [&](int j, int, int, int) {
             if (j == k) return;
             double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};
@@ -258,8 +263,13 @@ k_density_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
     int cx, cy, cz;
     cell_coords(e.f.cell[k], n, cx, cy, cz);
     const uint32_t all = (1u << A) - 1u;
-    for_each_candidate<DIM, R, 1>(
-        e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, 0, N, e.work.status,
+    // the lists of the density pass (recorded one lane per particle) hold
+    // every pair of both roles when h is uniform (the predicate is then
+    // symmetric)
+    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
+                          e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
+    traverse<DIM, R, 1>(
+        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
         [&](int j, int, int, int) {
             if (j == k) return;
             const double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};
