@@ -32,9 +32,11 @@ namespace sphb {
 
 // The 2D FP32C variants are held to 48 registers, five 256-thread blocks per
 // SM (62 registers and four blocks otherwise): 2-12% shorter passes on the
-// dam break, the list-recording pass gaining most.
+// dam break, the list-recording pass gaining most.  The 3D FP32C variants are
+// held to four blocks (64 registers) and the FP64 ones to three (80; they
+// would take 86 and fit two).
 template <int KT, int DIM, bool F32, int LANES, int R>
-__global__ void __launch_bounds__(256, (F32 && DIM == 2) ? 5 : 1)
+__global__ void __launch_bounds__(256, F32 ? (DIM == 2 ? 5 : 4) : 3)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
     // the force pass that follows may launch once every block has started
@@ -222,7 +224,10 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             const double rad2 = __dmul_rn(rad, rad);
             const double radl = (rad + skin) * (1.0 + 1e-5);
             const double radl2 = nbr ? radl * radl : rad2;
-            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
+            // with one h in the scene the symmetric set and the averaged
+            // kernel are the plain ones
+            const bool uh = sc.uniform_h != 0;
+            const bool vh = !uh && sc.variable_h != 0, hks = !uh && sc.hks != 0;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
@@ -232,10 +237,10 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     const double dy = yk - __ldg(B.y + j);
                     const double dz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
                     const double d2 = dist2_ref<DIM>(dx, dy, dz);
-                    const double hb = __ldg(B.h + j);
-                    double radj2 = rad2, radlj2 = radl2;
+                    double hb = 0.0, radj2 = rad2, radlj2 = radl2;
                     if (vh) {
                         // symmetric: r^2 < (radius_scale h_a)^2 or (radius_scale h_b)^2
+                        hb = __ldg(B.h + j);
                         const double rj = hb * sc.radius_scale;
                         radj2 = fmax(rad2, __dmul_rn(rj, rj));
                         const double rl = (fmax(rad, rj) + skin) * (1.0 + 1e-5);
@@ -246,6 +251,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                         const bool sums =
                             !lists_only && (!filt || ((rsrc >> seg.array_of(j)) & 1u));
                         if (sums && d2 < radj2) {
+                            if (!vh) hb = uh ? hk : __ldg(B.h + j);
                             double w;
                             if (hks)
                                 w = 0.5 * (Kern<KT>::template w_d<DIM>(sqrt(d2), hk) + Kern<KT>::template w_d<DIM>(sqrt(d2), hb));

@@ -33,9 +33,11 @@ namespace sphb {
 // each over its own sources, in the same traversal as the momentum.
 // The 2D FP32C momentum-only variants are held to 80 registers (three
 // 256-thread blocks per SM); left alone, the fused stage in the epilogue
-// would take them to 96 (two blocks).
+// would take them to 96 (two blocks).  Every other variant is held to 128
+// (two blocks): the FP64 continuity pass would otherwise take 132 and fit
+// one block per SM.
 template <int KT, int DIM, bool F32, int LANES, int R, int U, bool CONT>
-__global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? 3 : 1)
+__global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? 3 : 2)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
 {
@@ -291,7 +293,10 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             const double rad = hk * sc.radius_scale;
             const double rad2 = __dmul_rn(rad, rad);
             const double alpha = sc.alpha, beta = sc.beta, eta = sc.eta;
-            const bool vh = sc.variable_h != 0, hks = sc.hks != 0;
+            // with one h in the scene the symmetric set and the averaged
+            // kernels are the plain ones
+            const bool uh = sc.uniform_h != 0;
+            const bool vh = !uh && sc.variable_h != 0, hks = !uh && sc.hks != 0;
             int cx, cy, cz;
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
@@ -301,14 +306,15 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                     const double ry = yk - __ldg(B.y + j);
                     const double rz = DIM == 3 ? zk - __ldg(B.z + j) : 0.0;
                     const double rab2 = dist2_ref<DIM>(rx, ry, rz);
-                    const double hb = __ldg(B.h + j);
-                    double radj2 = rad2;
+                    double hb = 0.0, radj2 = rad2;
                     if (vh) {
                         // symmetric: r^2 < (radius_scale h_a)^2 or (radius_scale h_b)^2
+                        hb = __ldg(B.h + j);
                         const double rj = hb * sc.radius_scale;
                         radj2 = fmax(rad2, __dmul_rn(rj, rj));
                     }
                     if (!(rab2 < radj2)) return;
+                    if (!vh) hb = uh ? hk : __ldg(B.h + j);
                     ++np;
                     const uint32_t bit = filt ? 1u << seg.array_of(j) : ~0u;
                     const double hab = 0.5 * (hk + hb);
