@@ -264,9 +264,11 @@ def run_ours(args, rank, world, local):
         tune = autotune(wl["scenes"], wl["scheme"], wl["dim"], args.precision, device=dev)
         lanes, pb, stencil = tune["lanes"], tune["pair_block"], tune["stencil"]
         lb = tune.get("list_batch", 4)
+    skin = tune.get("skin_margin") if tune else None
     args.stencil = stencil
     eng = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=args.precision,
-                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev, list_batch=lb)
+                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev, list_batch=lb,
+                 skin_margin=skin)
     N = eng.N
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -378,13 +380,13 @@ def run_ours(args, rank, world, local):
            "config": {"workload": args.workload, "description": wl["desc"],
                       "particles": N, "precision": args.precision,
                       "stencil": args.stencil, "lanes": lanes, "pair_block": pb,
-                      "list_batch": lb,
+                      "list_batch": lb, "skin_margin": eng.skin_margin,
                       "cuda_graph": graph is not None,
                       "l2": "flushed (256 MiB write) between timed steps",
                       "parallelism": f"replicas x{world}"},
            "steps_per_s": steps_per_s,
            "autotune": ({"chosen": {k: tune.get(k) for k in ("stencil", "lanes", "pair_block",
-                                                              "list_batch")},
+                                                              "list_batch", "skin_margin")},
                          "table": tune["table"]} if tune else None),
            "pairs_per_step": pairs / args.steps,
            "gpu_launches": launches_per_step(eng) * args.steps,
@@ -453,8 +455,11 @@ def other_configs(dev, flush, stream):
     for name, steps in (("dam_break_continuity", 100), ("drop", 50), ("batched", 10)):
         wl = workload(name)
         for prec in ("fp32c", "fp64"):
-            shape = (dict(lanes=1, pair_block=256, stencil=1) if name.startswith("dam")
-                     else dict(lanes=2, pair_block=128, stencil=2))
+            # launch shapes and skins measured on B200 for these workloads
+            shape = {"dam_break_continuity": dict(lanes=1, pair_block=256, stencil=1),
+                     "drop": dict(lanes=1, pair_block=128, stencil=1),
+                     "batched": dict(lanes=1, pair_block=128, stencil=1,
+                                     skin_margin=0.25)}[name]
             eng = Engine(wl["scenes"], wl["scheme"], dim=2, precision=prec, device=dev,
                          **shape)
             ms, pairs = timed_steps(eng, steps, flush, stream)

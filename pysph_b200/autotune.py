@@ -2,9 +2,12 @@
 
 For a workload it times whole predictor-corrector steps for every candidate
 of cell size (stencil R: cell = support / R), lanes per dest particle and
-threads per block, and returns the fastest.  Results are cached per
-(dim, precision, particle-count bucket, scene-count bucket), in memory and,
-when PYSPH_B200_TUNE_CACHE names a file, in that JSON file.
+threads per block, and returns the fastest.  On that shape it then tries
+the force pass's load-ahead depth (FP32C) and the skin of the kept
+neighbour lists: a wider skin means longer lists but fewer rebins, which
+pays where particles move fast.  Results are cached per (dim, precision,
+particle-count bucket, scene-count bucket), in memory and, when
+PYSPH_B200_TUNE_CACHE names a file, in that JSON file.
 """
 from __future__ import annotations
 
@@ -19,6 +22,7 @@ from .engine import Engine
 LANES = (1, 2, 4, 8)
 BLOCKS = (64, 128, 256)
 STENCILS = (1, 2)
+SKINS = (0.1, 0.15, 0.25)
 
 _cache: dict = {}
 
@@ -98,6 +102,22 @@ def autotune(scenes, scheme, dim, precision="fp32c", device=None, stencils=STENC
         if ms < best["ms_per_step"]:
             best = dict(table[-1])
         del eng
+    # the skin, on enough steps for the rebins to show (fresh engines, so
+    # every candidate starts from the same state)
+    skin_table = []
+    for skin in SKINS:
+        eng = Engine(scenes, scheme, dim=dim, precision=precision, stencil=best["stencil"],
+                     lanes=best["lanes"], pair_block=best["pair_block"], device=device,
+                     list_batch=best.get("list_batch", 4), skin_margin=skin)
+        ms = time_steps(eng, 4 * steps, warm=steps)
+        eng.check_status()
+        skin_table.append(dict(stencil=best["stencil"], lanes=best["lanes"],
+                               pair_block=best["pair_block"],
+                               list_batch=best.get("list_batch", 4), skin_margin=skin,
+                               ms_per_step=ms))
+        del eng
+    table.extend(skin_table)
+    best = dict(min(skin_table, key=lambda r: r["ms_per_step"]))
     res = dict(best, key=key, table=table)
     _cache[key] = res
     _store()

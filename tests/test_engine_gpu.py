@@ -468,3 +468,21 @@ def test_fused_stage_matches_separate_pass(case, cont, integ):
             assert torch.equal(a.get(i, n), b.get(i, n)), (i, n)
     if case == "dam" and not cont:
         assert rebins > 0   # the rebin path ran too
+
+
+def test_autotune_returns_a_timed_shape(tmp_path, monkeypatch):
+    """The autotuner times the candidate shapes, then the skin on the best
+    one, and caches the result per workload bucket (in a file when asked)."""
+    from pysph_b200 import autotune as T
+    monkeypatch.setenv("PYSPH_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    T._cache.clear()
+    arrays, params, scheme, dim = drop(dx=0.05)
+    scenes = [(arrays, dict(params, dt=1e-5))]
+    kw = dict(lanes=(1, 2), blocks=(128,), stencils=(1,), steps=2)
+    res = T.autotune(scenes, scheme, dim, "fp32c", **kw)
+    assert res["lanes"] in (1, 2) and res["pair_block"] == 128 and res["stencil"] == 1
+    assert res["skin_margin"] in T.SKINS and res["ms_per_step"] > 0
+    assert len(res["table"]) == 2 + 1 + len(T.SKINS)
+    assert (tmp_path / "tune.json").exists()
+    assert T.autotune(scenes, scheme, dim, "fp32c", **kw) is res   # cached
+    T._cache.clear()
