@@ -484,5 +484,7 @@ def test_autotune_returns_a_timed_shape(tmp_path, monkeypatch):
     assert res["skin_margin"] in T.SKINS and res["ms_per_step"] > 0
     assert len(res["table"]) == 2 + 1 + len(T.SKINS)
     assert (tmp_path / "tune.json").exists()
-    assert T.autotune(scenes, scheme, dim, "fp32c", **kw) is res   # cached
+    again = T.autotune(scenes, scheme, dim, "fp32c", **kw)   # from the cache file
+    assert {k: again[k] for k in ("lanes", "pair_block", "stencil", "skin_margin")} == \
+        {k: res[k] for k in ("lanes", "pair_block", "stencil", "skin_margin")}
     T._cache.clear()
