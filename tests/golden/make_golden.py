@@ -341,6 +341,42 @@ def varh(R):
     return out
 
 
+def varh3d_case():
+    """A jittered 10^3 lattice with h growing from 1.2 to 1.56 dx along z
+    and random velocities (so the viscosity acts)."""
+    arrays, types, params = W.lattice3d(n=10)
+    a = arrays[0]
+    dx = 0.1
+    a["h"] = 1.2 * dx * (1.0 + 0.3 * a["z"])
+    rng = np.random.default_rng(3)
+    for c in ("u", "v", "w"):
+        a[c] = rng.normal(0.0, 0.5, len(a["x"]))
+    params = dict(c0=10.0, rho0=1.0, alpha=0.1, beta=0.0, eta=0.1, gravity=(0.0, 0.0, 0.0))
+    return arrays, types, params
+
+
+def varh3d(R):
+    """Variable h with hks kernels in 3D (summation scheme): the symmetric
+    lists, the first stage and 3 PC steps."""
+    arrays, types, params = varh3d_case()
+    out = {f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS}
+    pas, particles, integ = build_sim(R, arrays, types, params, 3, variable_h=True, hks=True)
+    off, idx = lists_of(R, particles, pas[0], pas[0])
+    out["nbr_off"], out["nbr_idx"] = off, idx
+    integ.save_initial_arrays()
+    integ.reset_accelerations(step=1)
+    integ.eval()
+    out.update({f"stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                for n in ("rho", "p", "cs", "_a_u_1", "_a_v_1", "_a_w_1", "dt_fac")})
+    pas, particles, integ = build_sim(R, arrays, types, params, 3, variable_h=True, hks=True)
+    for _ in range(3):
+        particles.update()
+        integ.integrate(1e-4)
+    out.update({f"step3_{k}": v for k, v in state(pas, ("x", "y", "z", "u", "v", "w", "rho",
+                                                         "p")).items()})
+    return out
+
+
 def kernels(R):
     """The quintic spline and Wendland quintic kernels (2D): W and grad W on
     a line of distances, and the drop (dx = 0.05) with each kernel under both
@@ -397,7 +433,8 @@ def main():
     R = ref_modules(a.build)
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
                      ("drop_cont", drop_cont), ("dam_cont", dam_cont),
-                     ("integrators", integrators), ("varh", varh), ("kernels", kernels)):
+                     ("integrators", integrators), ("varh", varh), ("kernels", kernels),
+                     ("varh3d", varh3d)):
         if a.only and name not in a.only:
             continue
         data = fn(R)

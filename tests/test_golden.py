@@ -308,3 +308,35 @@ def test_other_kernels_first_stage_and_steps_bit_exact(kname, name):
     for n in ("x", "y", "u", "v", "rho", "p", "cs"):
         np.testing.assert_array_equal(getattr(o.arrays[0], n),
                                       g[f"{kname}_{name}_step5_{n}_0"], err_msg=n)
+
+
+# -- variable h with hks in 3D --------------------------------------------------
+VARH3D = dict(c0=10.0, rho0=1.0, gamma=7.0, alpha=0.1, beta=0.0, eta=0.1)
+
+
+def oracle_varh3d(g):
+    arrs = [OracleArray("a0", **{k: g[f"in_{k}"].copy() for k in PROPS})]
+    sch = fluid_scheme(1)
+    return OracleSystem(arrs, dim=3, rho_src=sch.rho_src, tait_on=sch.tait_on,
+                        mom_src=sch.mom_src, step_on=sch.step_on, variable_h=True, hks=True,
+                        **VARH3D)
+
+
+def test_varh3d_lists_stage_and_steps_bit_exact():
+    g = load("varh3d")
+    o = oracle_varh3d(g)
+    o.update()
+    off, idx = o.neighbors(0, 0)
+    np.testing.assert_array_equal(off, g["nbr_off"])
+    np.testing.assert_array_equal(idx, g["nbr_idx"])
+    o.eval()
+    A = o.arrays[0]
+    got = {"rho": A.rho, "p": A.p, "cs": A.cs, "_a_u_1": A.au, "_a_v_1": A.av,
+           "_a_w_1": A.aw, "dt_fac": A.dt_fac}
+    for n, v in got.items():
+        np.testing.assert_array_equal(v, g[f"stage0_{n}"], err_msg=n)
+    o = oracle_varh3d(g)
+    for _ in range(3):
+        o.pc_step(1e-4)
+    for n in ("x", "y", "z", "u", "v", "w", "rho", "p"):
+        np.testing.assert_array_equal(getattr(o.arrays[0], n), g[f"step3_{n}_0"], err_msg=n)

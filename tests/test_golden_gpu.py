@@ -362,3 +362,41 @@ def test_other_kernels_five_steps(kname, name, precision):
     rtol = 1e-12 if precision == "fp64" else 1e-5
     ref = g[f"{kname}_{name}_step5_rho_0"]
     assert np.max(np.abs(rho - ref) / ref) <= rtol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_varh3d_hks(precision):
+    """3D, variable h with hks kernels: symmetric neighbour sets, the first
+    stage and 3 PC steps against the reference's fixture."""
+    g = load("varh3d")
+    par = dict(c0=10.0, rho0=1.0, gamma=7.0, alpha=0.1, beta=0.0, eta=0.1, dt=1e-4)
+    eng = Engine([(arrays(g, ["in_"]), par)], varh_scheme(False), dim=3, precision=precision,
+                 variable_h=True, lanes=4)
+    if precision == "fp64":
+        di, _, sj = eng.neighbors(0, 1)
+        rdi, rsj = sorted_pairs(g["nbr_off"], g["nbr_idx"])
+        np.testing.assert_array_equal(di, rdi)
+        np.testing.assert_array_equal(sj, rsj)
+    eng.eval_stage()
+    eng.check_status()
+    rtol = 1e-12 if precision == "fp64" else 1e-5
+    for n in ("rho", "p", "cs"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"stage0_{n}"]
+        assert np.max(np.abs(got - ref)) <= rtol * np.max(np.abs(ref)), n
+    atol = 1e-10 if precision == "fp64" else 1e-4
+    for n in ("_a_u_1", "_a_v_1", "_a_w_1", "dt_fac"):
+        got = eng.get(0, n).cpu().numpy()
+        ref = g[f"stage0_{n}"]
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= atol, n
+    eng = Engine([(arrays(g, ["in_"]), par)], varh_scheme(False), dim=3, precision=precision,
+                 variable_h=True, lanes=4)
+    for _ in range(3):
+        eng.pc_step()
+    eng.check_status()
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y", "z"):
+        got = eng.get(0, n).cpu().numpy()
+        assert np.max(np.abs(got - g[f"step3_{n}_0"])) / 0.1 <= tol, n
+    rho = eng.get(0, "rho").cpu().numpy()
+    assert np.max(np.abs(rho - g["step3_rho_0"]) / g["step3_rho_0"]) <= rtol
