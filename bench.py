@@ -212,9 +212,52 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu --set full
 # on the bench's own workload and launch shape; the force pass with the
 # integrator stage fused into it)
-NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 71.933e6 + 4.520e6,
-               ("dam_break", "fp32c", "density"): 40.980e6 + 0.008e6,
+NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 71.932e6 + 3.265e6,
+               ("dam_break", "fp32c", "density"): 40.985e6 + 0.021e6,
                ("dam_break", "fp32c", "pc_stage"): 17.951e6 + 0.000256e6}
+
+
+# FP32 work of one launch, from the same capture: flops = 2 FFMA + FADD +
+# FMUL + 4 FFMA2 + 2 FADD2 + 2 FMUL2 (sm__sass_thread_inst_executed_op_*),
+# and the fraction of cycles the schedulers issued
+# (smsp__issue_active.avg.pct_of_peak_sustained_active)
+NCU_FP32 = {("dam_break", "fp32c", "force"): {"flops": 398.5e6, "issue_active": 0.518},
+            ("dam_break", "fp32c", "density"): {"flops": 228.9e6, "issue_active": 0.739}}
+
+
+def fma_peaks(dev):
+    """Measured FP32 and FP64 FMA rates (TFLOP/s) of this GPU: sphb_fma_probe
+    on 8 full blocks per SM, the compute denominators of the pair passes'
+    roofline."""
+    import torch
+    from pysph_b200 import _native as nat
+    L = nat.lib()
+    props = torch.cuda.get_device_properties(dev)
+    blocks = props.multi_processor_count * 8
+    out = {}
+    for name, fp64, dtype in (("fp32_tflops", 0, torch.float32), ("fp64_tflops", 1, torch.float64)):
+        buf = torch.empty(blocks, dtype=dtype, device=dev)
+        iters = 400 if fp64 else 1600
+        stream = torch.cuda.current_stream(dev)
+        run = lambda: nat.check(L.sphb_fma_probe(fp64, buf.data_ptr(), blocks, iters,
+                                                 ctypes_stream(stream)), "sphb_fma_probe")
+        run()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        flops = 5.0 * blocks * 256 * iters * 256
+        out[name] = flops / (a.elapsed_time(b) * 1e-3) / 1e12
+    return out
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
 
 
 def algorithmic_bytes(dim, f32):
@@ -370,6 +413,19 @@ def run_ours(args, rank, world, local):
                              "scratch") if traffic else None,
             "per_kernel_ms": {k: round(v, 5) for k, v in kern.items()},
             "bytes_per_particle": byts}
+    # the pair passes are bound by FP32 issue: their FP32 flop rate against
+    # the measured FMA peak, and the issue-active fraction ncu saw
+    peaks_c = fma_peaks(dev)
+    fp = NCU_FP32.get((args.workload, args.precision, dominant))
+    if fp:
+        ach_c = fp["flops"] / (per_launch[dominant] * 1e-3) / 1e12
+        roof["compute"] = {"bound": "fp32", "achieved": round(ach_c, 2),
+                           "peak": round(peaks_c["fp32_tflops"], 2), "unit": "TFLOP/s",
+                           "frac": round(ach_c / peaks_c["fp32_tflops"], 4),
+                           "issue_active": fp["issue_active"],
+                           "note": ("flops per launch from one ncu capture; peak from "
+                                    "sphb_fma_probe on this GPU")}
+    roof["fma_peaks_measured"] = {k: round(v, 2) for k, v in peaks_c.items()}
 
     out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
