@@ -669,8 +669,10 @@ class Engine:
         sphb_pc_stage: fused into the force pass when the engine allows it
         (the predictor's pass then leaves the CFL maxima alone), else as its
         own pass.  A fused stage swaps the two record copies, so a captured
-        graph must hold an even number of them (a PC or RK2 step does)."""
-        if self.fuses_stage:
+        graph must hold an even number of them: a PC or RK2 step does, and
+        an Euler step (one stage) being captured runs its stage on its own."""
+        capturing = self.device.type == "cuda" and torch.cuda.is_current_stream_capturing()
+        if self.fuses_stage and not (kind == 2 and capturing):
             self.eval_stage(stage=kind)
             self._box_valid = True
         else:

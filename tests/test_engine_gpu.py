@@ -488,3 +488,27 @@ def test_autotune_returns_a_timed_shape(tmp_path, monkeypatch):
     assert {k: again[k] for k in ("lanes", "pair_block", "stencil", "skin_margin")} == \
         {k: res[k] for k in ("lanes", "pair_block", "stencil", "skin_margin")}
     T._cache.clear()
+
+
+def test_euler_step_graph_replays_like_eager_steps():
+    """A captured Euler step (one stage) keeps the record copies in place, so
+    its replays match eager steps."""
+    arrays, params, scheme, dim = drop(dx=0.05)
+    params = dict(params, dt=1e-5)
+    a = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    b = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    for e in (a, b):
+        e.step("euler")
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        a.step("euler")
+    for _ in range(5):
+        g.replay()
+        b.step("euler")
+    torch.cuda.synchronize()
+    a.check_status()
+    b.check_status()
+    for n in ("x", "y", "u", "v", "rho"):
+        assert torch.equal(a.get(0, n), b.get(0, n)), n
+    del g
