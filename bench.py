@@ -526,10 +526,11 @@ def other_configs(dev, flush, stream):
             torch.cuda.empty_cache()
     wl = workload("lattice3d")
     for prec in ("fp32c", "fp64"):
-        # the launch shape measured best for this lattice on B200 (both
-        # precisions): cells of half the support, 2 lanes per particle
-        eng = Engine(wl["scenes"], wl["scheme"], dim=3, precision=prec, lanes=2,
-                     pair_block=128, stencil=2, device=dev)
+        # the launch shapes measured best for this lattice on B200: cells of
+        # half the support, 1 lane per particle (FP32C) or 2 (FP64)
+        eng = Engine(wl["scenes"], wl["scheme"], dim=3, precision=prec,
+                     lanes=1 if prec == "fp32c" else 2, pair_block=128, stencil=2,
+                     device=dev)
         # one evaluation: rebin + SPHRho + SPHPressureGradient
         def one():
             eng.bin(0)
