@@ -229,7 +229,10 @@ typedef struct {
                                (cleared by anything that moves particles);
                                meta[3] = 2 while the positions are those of
                                the last rebin; meta[4] = 1 when the lists
-                               were recorded with the skin at them */
+                               were recorded with the skin at them;
+                               meta[5] = 1 after the host wrote positions or
+                               velocities, until sphb_refresh has rebuilt the
+                               records and measured the displacements */
     unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
     unsigned long long *pairs;  /* [4]  pairs evaluated: density, force, -, - */
 } sphb_work;
@@ -346,7 +349,11 @@ SPHB_API int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
 #define SPHB_DENSITY_LISTS_ONLY 8
 
 /* Refresh the FP32 pair records (positions relative to each particle's
- * cell of the last bin, velocities) from the FP64 state without rebinning.
+ * cell of the last bin, velocities) from the FP64 state without rebinning,
+ * and, with f.anchor, measure every particle's displacement from its anchor
+ * into the scenes' max_disp2, so that the next SPHB_BIN_IF_NEEDED decision
+ * may keep the lists after positions or velocities written by the host
+ * (work.meta[5]; without this call it rebins).
  * sphb_pc_stage refreshes them itself; this is for state written by other
  * means.  No-op for SPHB_FP64. */
 SPHB_API int sphb_refresh(const sphb_engine *e, int cur, void *stream);
@@ -411,9 +418,11 @@ SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
  * 14 rho, 15 p, 16 cs, 17 au, 18 av, 19 aw, 20 dt_fac; continuity scheme:
  * 21 the integrated density (buf.rho), 22 its stage-initial copy, 23 its
  * rate _a_rho_1; 24..26 the XSPHCorrection velocity.  Fields 17..20 and
- * 23..26 are scatter-only.  Gathering x..w, m or h marks the lists invalid
- * (work.meta[2] = 0): the next SPHB_BIN_IF_NEEDED rebins, which also
- * rebuilds the FP32 pair records from the new state. */
+ * 23..26 are scatter-only.  Gathering m or h withdraws the lists: the next
+ * SPHB_BIN_IF_NEEDED rebins, which also rebuilds the FP32 pair records.
+ * Gathering x..w marks them unchecked (work.meta[5]): the next decision
+ * rebins unless sphb_refresh has since measured that no particle left half
+ * the skin around its anchor. */
 SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
                   int dir, double *user, const int32_t *user_offset,
                   void *stream);

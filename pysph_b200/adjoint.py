@@ -80,6 +80,9 @@ class Rollout:
                     torch.stack([eng.get(a, c) for c in pv])) for a in self.moving}
 
     def set_state(self, state, eng=None):
+        """The state into an engine, rebinned there: every restart from the
+        same state (the forward's checkpoints, the backward's recomputes, the
+        VJPs) then starts from the same order and lists."""
         eng = eng or self.fwd
         px, pv = self._comps()
         for a, (X, V) in state.items():
@@ -88,6 +91,7 @@ class Rollout:
             for d, c in enumerate(pv):
                 eng.exchange_in(a, c, V[d])
         eng.invalidate_box()
+        eng.rebin_now()
 
     # -------------------------------------------------------------- forward
     def forward(self, velocities):
@@ -141,7 +145,6 @@ class Rollout:
         """(d F / d(X, V))^T lam_F at state: {array: (lX, lV)}."""
         eng = self.adj
         self.set_state(state, eng)
-        eng.bin(nat.BIN_MOVE_INITIAL)
         eng.density()
         N = eng.N
         dim = self.dim

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "sphb_common.cuh"
+#include "sphb_stage.cuh"
 
 namespace sphb {
 
@@ -55,7 +56,8 @@ __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
     __syncthreads();
     if (threadIdx.x == 0) {
         const bool at_anchor = e.work.meta[3] == 2;
-        const bool lists = e.work.meta[4] == 1;
+        // host-written state nobody has measured: no trusting the lists
+        const bool lists = e.work.meta[4] == 1 && e.work.meta[5] == 0;
         const bool keep = at_anchor || (lists && !s_far);
         e.work.meta[1] = keep ? 0 : 1;
         e.work.meta[2] = (keep && lists) ? 1 : 0;
@@ -102,48 +104,72 @@ k_box_accum(const __grid_constant__ sphb_engine e, int cur, int gated)
     }
 }
 
-// FP32 pair records from the FP64 state without reordering: positions
-// relative to the origin of each particle's cell of the last bin (still
-// within a skin of that cell), velocities.
-template <int DIM>
+// FP32 pair records from the FP64 state without reordering (FP32C):
+// positions relative to the origin of each particle's cell of the last bin,
+// velocities, into both record copies.  With anchors, every particle's
+// displacement from its anchor goes into its scene's max_disp2, and the
+// host-written state counts as measured (meta[5]).
+template <int DIM, bool F32>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_refresh(const __grid_constant__ sphb_engine e, int cur)
 {
     const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A;
-    const sphb_scene_state &st = e.sstate[s];
-    const double cs = e.scene[s].cell_size;
-    const sphb_buffers &B = e.buf[cur];
-    int local = e.f.cell[k];
-    if (local < 0 || local >= st.ncells) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        local = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) e.work.meta[5] = 0;
+    float d2 = 0.f;
+    if (k < t.end) {
+        const sphb_scene_state &st = e.sstate[s];
+        const double cs = e.scene[s].cell_size;
+        const sphb_buffers &B = e.buf[cur];
+        int local = e.f.cell[k];
+        if (local < 0 || local >= st.ncells) {
+            flag(e, SPHB_ST_BAD_INDEX);
+            local = 0;
+        }
+        int cx, cy, cz;
+        cell_coords(local, st.n, cx, cy, cz);
+        const float xr = (float)(B.x[k] - (double)(st.lo[0] + cx) * cs);
+        const float yr = (float)(B.y[k] - (double)(st.lo[1] + cy) * cs);
+        const float zr = DIM == 3 ? (float)(B.z[k] - (double)(st.lo[2] + cz) * cs) : 0.f;
+        if (F32) {
+            float4 *geo = (float4 *)e.f.geo;
+            const float4 g = geo[k];
+            // both copies of the records when the force pass steps the state
+            const float4 gn = DIM == 2 ? make_float4(xr, yr, g.z, g.w)
+                                       : make_float4(xr, yr, zr, g.w);
+            geo[k] = gn;
+            if (e.f.geo_next) ((float4 *)e.f.geo_next)[k] = gn;
+            if (DIM == 2) {
+                const float2 vv = make_float2((float)B.u[k], (float)B.v[k]);
+                ((float2 *)e.f.vel)[k] = vv;
+                if (e.f.vel_next) ((float2 *)e.f.vel_next)[k] = vv;
+            } else {
+                const float4 vv = make_float4((float)B.u[k], (float)B.v[k], (float)B.w[k], 0.f);
+                ((float4 *)e.f.vel)[k] = vv;
+                if (e.f.vel_next) ((float4 *)e.f.vel_next)[k] = vv;
+            }
+        }
+        if (e.f.anchor) {
+            float q0, q1, q2 = 0.f;
+            if (DIM == 2) {
+                const float2 an = ((const float2 *)e.f.anchor)[k];
+                q0 = xr - an.x;
+                q1 = yr - an.y;
+            } else {
+                const float4 an = ((const float4 *)e.f.anchor)[k];
+                q0 = xr - an.x;
+                q1 = yr - an.y;
+                q2 = zr - an.z;
+            }
+            d2 = q0 * q0 + q1 * q1 + q2 * q2;
+            // a non-finite position can never be within the skin
+            if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
+        }
     }
-    int cx, cy, cz;
-    cell_coords(local, st.n, cx, cy, cz);
-    const float xr = (float)(B.x[k] - (double)(st.lo[0] + cx) * cs);
-    const float yr = (float)(B.y[k] - (double)(st.lo[1] + cy) * cs);
-    float4 *geo = (float4 *)e.f.geo;
-    const float4 g = geo[k];
-    // both copies of the records when the force pass steps the state
-    float4 gn;
-    if (DIM == 2) {
-        gn = make_float4(xr, yr, g.z, g.w);
-        const float2 vv = make_float2((float)B.u[k], (float)B.v[k]);
-        ((float2 *)e.f.vel)[k] = vv;
-        if (e.f.vel_next) ((float2 *)e.f.vel_next)[k] = vv;
-    } else {
-        const float zr = (float)(B.z[k] - (double)(st.lo[2] + cz) * cs);
-        gn = make_float4(xr, yr, zr, g.w);
-        const float4 vv = make_float4((float)B.u[k], (float)B.v[k], (float)B.w[k], 0.f);
-        ((float4 *)e.f.vel)[k] = vv;
-        if (e.f.vel_next) ((float4 *)e.f.vel_next)[k] = vv;
-    }
-    geo[k] = gn;
-    if (e.f.geo_next) ((float4 *)e.f.geo_next)[k] = gn;
+    // a block never spans two scenes
+    if (e.f.anchor) warp_max_disp(e, s, d2);
 }
 
 // ----------------------------------------------------------- grid setup --
@@ -229,6 +255,7 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
         e.work.meta[2] = 0;
         e.work.meta[3] = 2;
         e.work.meta[4] = 0;
+        e.work.meta[5] = 0;
     }
 }
 
@@ -585,11 +612,18 @@ extern "C" int sphb_refresh(const sphb_engine *e, int cur, void *stream)
 {
     int rc = check_engine(e, cur);
     if (rc) return rc;
-    if (e->cfg.precision != SPHB_FP32C || e->num_tiles == 0) return SPHB_OK;
-    if (!e->f.geo || !e->f.vel || !e->f.cell) return SPHB_ERR_ARG;
+    if (e->num_tiles == 0) return SPHB_OK;
+    const bool f32 = e->cfg.precision == SPHB_FP32C;
+    if (!e->f.cell || (f32 && (!e->f.geo || !e->f.vel))) return SPHB_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if (e->cfg.dim == 2) k_refresh<2><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
-    else k_refresh<3><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    const int nt = e->num_tiles;
+    if (e->cfg.dim == 2) {
+        if (f32) k_refresh<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+        else k_refresh<2, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    } else {
+        if (f32) k_refresh<3, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+        else k_refresh<3, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
+    }
     return launch_status("sphb_refresh");
 }
 

@@ -163,13 +163,16 @@ __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
            int dir, double *user, const int *user_offset)
 {
-    // new positions, velocities, masses or smoothing lengths: the lists and
-    // the FP32 records must be rebuilt before they are reused
+    // new masses or smoothing lengths: the lists must be recorded again;
+    // new positions or velocities: the records are stale and the particles
+    // may have left their anchors, so the next decision rebins unless
+    // sphb_refresh measures them first (meta[5])
     if (dir == 0 && (field <= 5 || field == 12 || field == 13) && blockIdx.x == 0 &&
         threadIdx.x == 0) {
         e.work.meta[2] = 0;
         e.work.meta[3] = 0;
-        e.work.meta[4] = 0;
+        if (field <= 5) e.work.meta[5] = 1;
+        else e.work.meta[4] = 0;
     }
     const sphb_tile t = e.tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;

@@ -513,9 +513,15 @@ class Engine:
 
     def bin(self, flags: int = 0):
         """Rebin into the other buffer; with BIN_IF_NEEDED the device decides
-        and the state stays in the current buffer either way."""
+        and the state stays in the current buffer either way.  After
+        positions or velocities written from the host the records are
+        refreshed and every displacement measured first, so the decision
+        may keep the lists."""
         if not self._box_valid:
             flags |= nat.BIN_BOX
+        if (flags & nat.BIN_IF_NEEDED) and getattr(self, "_host_state", False):
+            self.call("sphb_refresh", self.cur)
+        self._host_state = False
         self.call("sphb_bin", self.cur, flags)
         if flags & nat.BIN_IF_NEEDED:
             # the box is rebuilt only by a rebin that happens; keep asking
@@ -610,6 +616,17 @@ class Engine:
             return
         off = self.work_offsets[nat.WORK_NAMES.index("meta")]
         self.work_buf[off + 8:off + 20].zero_()
+
+    def rebin_now(self):
+        """Rebin at once, the state staying in its buffer (a device-decided
+        rebin with the lists withdrawn; a plain rebin without list reuse),
+        e.g. after the host rewrote the state: every later launch sees the
+        same buffers, so graphs captured around it replay."""
+        if not self.step_lists:
+            return self.bin(nat.BIN_MOVE_INITIAL)
+        self.invalidate_lists()
+        self._host_state = False
+        self.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
 
     def invalidate_box(self):
         """Positions were changed outside the integrator: the next bin
@@ -815,9 +832,12 @@ class Engine:
                   v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it
         if name in ("x", "y", "z", "u", "v", "w", "m", "h"):
-            # the next bin recomputes the boxes; the kernel has withdrawn the
-            # lists, so the next device-decided rebin happens
+            # the next bin recomputes the boxes; new m or h withdraw the
+            # lists, new positions or velocities need the records refreshed
+            # and the displacements measured before the lists are trusted
             self._box_valid = False
+            if name not in ("m", "h"):
+                self._host_state = True
 
     def exchange_out(self, array: int, name: str, out: torch.Tensor | None = None):
         """Engine -> user-order FP64 tensor (scenes concatenated)."""

@@ -512,3 +512,36 @@ def test_euler_step_graph_replays_like_eager_steps():
     for n in ("x", "y", "u", "v", "rho"):
         assert torch.equal(a.get(0, n), b.get(0, n)), n
     del g
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_host_written_state_within_the_skin_keeps_the_lists(precision):
+    """Positions and velocities written from the host: the engine refreshes
+    the records and measures every displacement before its next decision,
+    which keeps the lists while no particle has left half the skin (and
+    rebins otherwise), with results matching the rebinning pipeline."""
+    arrays, params, scheme, dim = small_dam()
+    a = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=True)
+    b = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=False)
+    for e in (a, b):
+        for _ in range(3):
+            e.pc_step()
+    skin = a._scene_host[0].skin_max
+    x = a.get(0, "x").clone()
+    u = a.get(0, "u").clone()
+    x[:50] += 0.1 * skin
+    u[:50] += 0.5
+    for e in (a, b):
+        e.exchange_in(0, "x", x)
+        e.exchange_in(0, "u", u)
+    dec = _decisions(a, 2)
+    for _ in range(2):
+        b.pc_step()
+    assert dec[0][0] == 0, dec   # kept: nobody left half the skin
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    _assert_same_state(a, b, tol=tol)
+    # three skins: the measured displacement forces the rebin
+    x = a.get(0, "x").clone()
+    x[:5] += 3.0 * skin
+    a.exchange_in(0, "x", x)
+    assert _decisions(a, 1)[0][0] == 1
