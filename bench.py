@@ -726,8 +726,10 @@ def e2e(eng, wl, stream, dev, args):
     step and reads back x, y, u, v, rho, p into pinned host memory.  The
     copies run on two copy streams, double-buffered on the device, so the
     upload of the next step's state and the read-back of the last step's
-    results overlap the current step's kernels.  Reported in the metric's
-    unit (pair-interactions/s, the kernels' own pair counts) and in steps/s."""
+    results overlap the current step's kernels; the device part of a step
+    (state in, the PC step, results out) is one CUDA graph per buffer.
+    Reported in the metric's unit (pair-interactions/s, the kernels' own
+    pair counts) and in steps/s."""
     import torch
     a = 0
     n = eng.user_n[a]
@@ -752,6 +754,29 @@ def e2e(eng, wl, stream, dev, args):
                 dev_in[b][k].copy_(ins[k], non_blocking=True)
         in_ready[b].record(h2d)
 
+    def device_step(b):
+        for k in ins:
+            eng.exchange_in(a, k, dev_in[b][k])
+        eng.invalidate_box()
+        eng.pc_step()
+        for k in outs:
+            eng.exchange_out(a, k, out=dev_out[b][k])
+
+    # one graph per buffer, captured after an eager warm-up of each (on the
+    # real state)
+    for b in range(2):
+        for k in ins:
+            dev_in[b][k].copy_(ins[k])
+    graphs = []
+    for b in range(2):
+        device_step(b)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            device_step(b)
+        graphs.append(g)
+    torch.cuda.synchronize()
+
     for e in in_free + out_free:
         e.record(stream)
     torch.cuda.synchronize()
@@ -763,17 +788,12 @@ def e2e(eng, wl, stream, dev, args):
     for i in range(k_steps):
         b = i % 2
         stream.wait_event(in_ready[b])
-        for k in ins:
-            eng.exchange_in(a, k, dev_in[b][k])
+        stream.wait_event(out_free[b])   # the read-back two steps ago is done
+        graphs[b].replay()
         in_free[b].record(stream)
+        out_ready[b].record(stream)
         if i + 1 < k_steps:
             upload(1 - b)
-        eng.invalidate_box()
-        eng.pc_step()
-        stream.wait_event(out_free[b])   # the read-back two steps ago is done
-        for k in outs:
-            eng.exchange_out(a, k, out=dev_out[b][k])
-        out_ready[b].record(stream)
         d2h.wait_event(out_ready[b])
         with torch.cuda.stream(d2h):
             for k in outs:
@@ -785,6 +805,7 @@ def e2e(eng, wl, stream, dev, args):
     ms = t0.elapsed_time(t1)
     pd, pf = eng.pair_counts()
     eng.check_status()
+    del graphs
     return {"value": (pd + pf) / (ms / 1e3), "unit": "pair-interactions/s",
             "steps_per_s": k_steps / (ms / 1e3),
             "h2d_bytes_per_step": 8 * n * len(ins),
