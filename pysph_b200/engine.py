@@ -828,8 +828,9 @@ class Engine:
                 if n and float(hm[off[s]:off[s] + n].max()) > self._h_cap[s]:
                     raise ValueError("smoothing length above the largest one the cells were "
                                      "sized for: build a new engine")
-        self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 0,
-                  v.data_ptr(), self.user_offset[array].data_ptr())
+        if v.numel():   # (an array without particles has nothing to copy)
+            self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 0,
+                      v.data_ptr(), self.user_offset[array].data_ptr())
         self._keep = v  # keep alive until the stream passes it
         if name in ("x", "y", "z", "u", "v", "w", "m", "h"):
             # the next bin recomputes the boxes; new m or h withdraw the
@@ -843,8 +844,9 @@ class Engine:
         """Engine -> user-order FP64 tensor (scenes concatenated)."""
         if out is None:
             out = torch.empty(self.user_n[array], dtype=torch.float64, device=self.device)
-        self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 1,
-                  out.data_ptr(), self.user_offset[array].data_ptr())
+        if self.user_n[array]:
+            self.call("sphb_exchange", self.cur, array, self._field_id(array, name), 1,
+                      out.data_ptr(), self.user_offset[array].data_ptr())
         return out
 
     def _field_id(self, array: int, name: str) -> int:
@@ -857,8 +859,9 @@ class Engine:
 
     def exchange_tag(self, array: int, values: torch.Tensor, direction: int):
         v = values.to(device=self.device, dtype=torch.int32).contiguous()
-        self.call("sphb_exchange_tag", self.cur, array, direction, v.data_ptr(),
-                  self.user_offset[array].data_ptr())
+        if v.numel():
+            self.call("sphb_exchange_tag", self.cur, array, direction, v.data_ptr(),
+                      self.user_offset[array].data_ptr())
         return v
 
     def get(self, array: int, name: str, scene: int | None = None):
