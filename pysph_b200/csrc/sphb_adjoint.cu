@@ -111,7 +111,7 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
                           e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
     traverse<DIM, R, 1>(
-        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
+        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, CellTrim{},
         [&](int j, int, int, int) {
             if (j == k) return;
             double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};
@@ -269,7 +269,7 @@ k_density_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
     const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
                           e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
     traverse<DIM, R, 1>(
-        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
+        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, CellTrim{},
         [&](int j, int, int, int) {
             if (j == k) return;
             const double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};

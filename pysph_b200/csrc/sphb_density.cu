@@ -86,7 +86,7 @@ k_neighbors(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     const long long base = offs ? offs[k] : 0;
     for_each_candidate<DIM, R, 1>(
         e.work.start, A, src_mask, st.cell_base, st.ncells, n, cx, cy, cz, 0,
-        e.cfg.num_particles, e.work.status,
+        e.cfg.num_particles, e.work.status, CellTrim{},
         [&](int j, int, int, int) {
             const double dx = B.x[j] - xk;
             const double dy = B.y[j] - yk;

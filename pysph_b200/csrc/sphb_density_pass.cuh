@@ -190,7 +190,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 cell_coords(e.f.cell[k], n, cx, cy, cz);
                 for_each_candidate<DIM, R, LANES>(
                     start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
-                    [&](int j, int o, int dy, int dz) {
+                    cell_trim_rel(e, xk, yk, zk, csf), [&](int j, int o, int dy, int dz) {
                         const Rec r = load(EntryF{j, (float)o, (float)dy, (float)dz});
                         const float r2 = dist2(r);
                         bool rec = r2 < radl2;
@@ -232,6 +232,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
                 e, from_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
+                cell_trim_abs<DIM>(e, st, sc.cell_size, xk, yk, zk, cx, cy, cz),
                 [&](int j, int o, int oy, int oz) {
                     const double dx = xk - __ldg(B.x + j);
                     const double dy = yk - __ldg(B.y + j);

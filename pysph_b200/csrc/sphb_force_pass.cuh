@@ -245,7 +245,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                 cell_coords(e.f.cell[k], n, cx, cy, cz);
                 for_each_candidate<DIM, R, LANES>(
                     start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
-                    [&](int j, int o, int dy, int dz) {
+                    cell_trim_rel(e, xk, yk, zk, csf), [&](int j, int o, int dy, int dz) {
                         use(load(EntryF{j, (float)o, (float)dy, (float)dz}));
                     });
             };
@@ -301,6 +301,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             cell_coords(e.f.cell[k], n, cx, cy, cz);
             traverse<DIM, R, LANES>(
                 e, use_list, k, lane, start, A, src, cell_base, ncells, n, cx, cy, cz,
+                cell_trim_abs<DIM>(e, st, sc.cell_size, xk, yk, zk, cx, cy, cz),
                 [&](int j, int, int, int) {
                     const double rx = xk - __ldg(B.x + j);
                     const double ry = yk - __ldg(B.y + j);
