@@ -85,7 +85,7 @@ def workload(name):
     if name == "lattice3d":
         arrays, types, params = W.lattice3d(n=128)
         return dict(scenes=[(arrays, dict(params, dt=1e-6))], scheme=fluid_scheme(1),
-                    dim=3, desc="3D jittered 128^3 lattice (1,048,576), h=1.2dx")
+                    dim=3, desc="3D jittered 128^3 lattice (2,097,152 particles), h=1.2dx")
     if name == "batched":
         scenes = W.batched_drops(num_scenes=256, seed=0)
         return dict(scenes=[(a, dict(p, dt=1e-5)) for a, _, p in scenes],
