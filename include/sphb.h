@@ -422,7 +422,9 @@ SPHB_API int sphb_step_begin(const sphb_engine *e, void *stream);
  * SPHB_BIN_IF_NEEDED rebins, which also rebuilds the FP32 pair records.
  * Gathering x..w marks them unchecked (work.meta[5]): the next decision
  * rebins unless sphb_refresh has since measured that no particle left half
- * the skin around its anchor. */
+ * the skin around its anchor.  `user` and `user_offset` must not be NULL
+ * (SPHB_ERR_ARG): an array without particles has nothing to exchange and
+ * the call is simply not made. */
 SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
                   int dir, double *user, const int32_t *user_offset,
                   void *stream);
