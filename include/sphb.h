@@ -303,6 +303,10 @@ SPHB_API int sphb_box_init(const sphb_engine *e, int cur, void *stream);
  * support + skin while every particle stays within skin / 2 of its binned
  * position.  Without the flag, sphb_bin always rebins into buf[cur ^ 1]. */
 #define SPHB_BIN_IF_NEEDED 4
+/* SPHB_BIN_STEP_BEGIN (with SPHB_BIN_IF_NEEDED only): the decision first
+ * runs sphb_step_begin's prologue for every scene, in the same launch, so
+ * that a step's first bin replaces the sphb_step_begin call. */
+#define SPHB_BIN_STEP_BEGIN 8
 SPHB_API int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream);
 
 /* Neighbour lists of every particle of the dest arrays in dest_mask among

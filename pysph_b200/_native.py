@@ -28,6 +28,7 @@ ST_NONFINITE_ACC = 1 << 4
 ST_BAD_INDEX = 1 << 5
 ST_NBR_CAPACITY = 1 << 6
 BIN_IF_NEEDED = 4
+BIN_STEP_BEGIN = 8     # the first bin of a step runs the step prologue too
 DENSITY_LIST_IF_VALID = 4
 DENSITY_LISTS_ONLY = 8
 STATUS_NAMES = {

@@ -38,7 +38,7 @@ __device__ __forceinline__ bool skip_rebin(const sphb_engine &e, int gated)
 // scene has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding
 // of the displacement) from its anchor.  max_disp2 restarts either way.
 __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
-                             cudaGraphConditionalHandle cond, int set_cond)
+                             cudaGraphConditionalHandle cond, int set_cond, int step_begin)
 {
     // launched as a programmatic dependent of the stage before: its
     // displacements and meta must be complete
@@ -47,6 +47,7 @@ __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
     if (threadIdx.x == 0) s_far = 0;
     __syncthreads();
     for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) {
+        if (step_begin) step_begin_scene(e, s);
         sphb_scene_state &st = e.sstate[s];
         const double d2 = __longlong_as_double((long long)st.max_disp2);
         const double lim = 0.5 * e.scene[s].skin_max * (1.0 - 1e-4);
@@ -692,7 +693,8 @@ static int bin_conditional(const sphb_engine *e, int cur, int flags, cudaStream_
     cudaGraphConditionalHandle cond;
     if ((err = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault)))
         return cuda_fail("sphb_bin: conditional handle", err);
-    if ((err = launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cond, 1)))
+    if ((err = launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cond, 1,
+                          (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0)))
         return cuda_fail("sphb_bin: decision", err);
     cudaStreamCaptureStatus cs;
     unsigned long long id;
@@ -736,7 +738,10 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
 {
     int rc = check_engine(e, cur);
     if (rc) return rc;
-    if (flags & ~(SPHB_BIN_MOVE_INITIAL | SPHB_BIN_BOX | SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
+    if (flags & ~(SPHB_BIN_MOVE_INITIAL | SPHB_BIN_BOX | SPHB_BIN_IF_NEEDED |
+                  SPHB_BIN_STEP_BEGIN))
+        return SPHB_ERR_ARG;
+    if ((flags & SPHB_BIN_STEP_BEGIN) && !(flags & SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const int gated = (flags & SPHB_BIN_IF_NEEDED) ? 1 : 0;
     if (!gated) {
@@ -756,7 +761,8 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
             return cuda_fail("sphb_bin: capture info", err);
         return bin_conditional(e, cur, flags, st, graph);
     }
-    launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cudaGraphConditionalHandle(), 0);
+    launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cudaGraphConditionalHandle(), 0,
+               (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0);
     launch_rebin(e, cur, flags, 1, st);
     return launch_status("sphb_bin");
 }

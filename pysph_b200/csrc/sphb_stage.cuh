@@ -146,4 +146,38 @@ __device__ __forceinline__ void warp_max_disp(const sphb_engine &e, int s, float
     if ((threadIdx.x & 31) == 0 && wd > 0.f) atomic_max_nonneg(&e.sstate[s].max_disp2, (double)wd);
 }
 
+// The Solver's per-step prologue for scene s (S/solver/solver.py:546-566):
+// count += 1; with use_cfl, dt from ViscousAndForceBasedTimeStep
+// (S/solver/time_step_functions.py:8-57) over the maxima of the last force
+// passes; t += dt; the maxima restart.  Run by k_step_begin, or by the rebin
+// decision of a step's first bin (SPHB_BIN_STEP_BEGIN).
+__device__ __forceinline__ void step_begin_scene(const sphb_engine &e, int s)
+{
+    const sphb_scene &sc = e.scene[s];
+    sphb_scene_state &st = e.sstate[s];
+    st.count += 1;
+    if (sc.use_cfl) {
+        const double dtfac = __longlong_as_double((long long)st.max_dtfac);
+        const double acc2 = __longlong_as_double((long long)st.max_acc2);
+        double dt = 1.0;
+        // ViscousTimeStep: min(cfl * h / (co + max dt_fac))
+        const double dv = __ddiv_rn(__dmul_rn(sc.cfl, sc.h_min), __dadd_rn(sc.c0, dtfac));
+        dt = dv < dt ? dv : dt;
+        // force criterion (use_cfl == 1): cfl * min(sqrt(h / fmax)), with
+        // fmax = solver.dt at count 1; use_cfl == 2 is ViscousTimeStep alone
+        if (sc.use_cfl == 1) {
+            const double fmax = st.count == 1 ? sc.dt_initial : sqrt(acc2);
+            const double df = __dmul_rn(sc.cfl, sqrt(__ddiv_rn(sc.h_min, fmax)));
+            dt = dt < df ? dt : df;
+        }
+        st.dt = dt;
+    }
+    st.t += st.dt;
+    // the maxima served this step's rule: the step's own force passes
+    // accumulate them afresh (a single-stage integrator has no stage that
+    // clears them)
+    st.max_dtfac = 0ull;
+    st.max_acc2 = 0ull;
+}
+
 }  // namespace sphb

@@ -737,13 +737,21 @@ class Engine:
         state never changes buffers, so one captured graph replays every
         step."""
         reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
-        self.step_begin()
-        self.bin(reuse)
+        self._begin_and_bin(reuse)
         self._stage(0)
         if on_half is not None:
             on_half()
         self.bin(nat.BIN_MOVE_INITIAL | reuse)
         self._stage(1)
+
+    def _begin_and_bin(self, reuse):
+        """The step prologue and the first bin: one launch (the rebin
+        decision runs the prologue) when the device decides the rebin."""
+        if reuse:
+            self.bin(reuse | nat.BIN_STEP_BEGIN)
+        else:
+            self.step_begin()
+            self.bin(reuse)
 
     def step(self, integrator: str = "pc", on_half=None):
         """One step of the named integrator: "pc" (pc_step), "euler"
@@ -754,8 +762,7 @@ class Engine:
         if integrator not in ("euler", "rk2"):
             raise NotImplementedError(f"{integrator} is not fused on the engine")
         reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
-        self.step_begin()
-        self.bin(reuse)
+        self._begin_and_bin(reuse)
         if integrator == "euler":
             self._stage(2)
             return
