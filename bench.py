@@ -609,7 +609,9 @@ def launches_per_step(eng):
     rebin = 7 + (2 if eng.step_lists else 0)
     # per stage: density, force, and pc_stage unless the force pass runs it
     stage = 2 if eng.fuses_stage else 3
-    return 1 + 2 * rebin + 2 * stage + (2 if eng.tait_only_mask else 0)
+    # the step prologue: its own launch, or inside the first decision
+    begin = 0 if eng.step_lists else 1
+    return begin + 2 * rebin + 2 * stage + (2 if eng.tait_only_mask else 0)
 
 
 def kernel_times(eng, flush, stream, reps=20):
