@@ -100,6 +100,9 @@ def lib():
         L.orc_nbr_total.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_nbr_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                    P(ctypes.c_int64), P(ctypes.c_int32)]
+        L.orc_nbr_copy_sorted.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          P(ctypes.c_int64), P(ctypes.c_int32),
+                                          ctypes.c_int]
         L.orc_scheme_pairs.restype = ctypes.c_uint32
         L.orc_scheme_pairs.argtypes = [P(_System)]
         L.orc_eval.argtypes = [P(_System), ctypes.c_void_p]
@@ -265,6 +268,20 @@ class OracleSystem:
         lib().orc_nbr_copy(self._c, d, s,
                            off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                            idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        return off, idx[:tot]
+
+    def neighbors_sorted(self, d, s):
+        """neighbors(d, s) with every dest's list in ascending order (the
+        canonical form sets are compared in)."""
+        tot = lib().orc_nbr_total(self._c, d, s)
+        if tot < 0:
+            raise RuntimeError("neighbour lists not built for this pair")
+        off = np.empty(self.arrays[d].n + 1, np.int64)
+        idx = np.empty(max(tot, 1), np.int32)
+        lib().orc_nbr_copy_sorted(self._c, d, s,
+                                  off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                  idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                  int(self._s.nthreads))
         return off, idx[:tot]
 
     # -- functions --------------------------------------------------------

@@ -680,6 +680,31 @@ int orc_nbr_copy(const orc_nnps *c, int da, int sa, int64_t *off, int32_t *idx)
     return 0;
 }
 
+static int cmp_i32(const void *a, const void *b)
+{
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* The lists of orc_nbr_copy with each dest's list sorted ascending: the
+ * canonical form neighbour sets are compared in (a comparison aid, not a
+ * reference routine). */
+int orc_nbr_copy_sorted(const orc_nnps *c, int da, int sa, int64_t *off, int32_t *idx,
+                        int nthreads)
+{
+    if (orc_nbr_copy(c, da, sa, off, idx)) return -1;
+    const int64_t n = c->nn[da];
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < n; ++i)
+        qsort(idx + off[i], (size_t)(off[i + 1] - off[i]), sizeof(int32_t), cmp_i32);
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* SPH functions, function-level semantics of SPHFunction.eval:        */
 /* out[i] += result for LocalReal dests, out[i] = 0 otherwise.          */

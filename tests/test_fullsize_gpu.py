@@ -1,0 +1,291 @@
+"""Parity of the CUDA path with the oracle at the benchmark workloads' own
+sizes, through the C ABI.
+
+* 2D dam break, dx = 0.0025 (320,000 fluid + 12,018 wall particles): cell
+  coordinates and neighbour sets bit-exact; FP64 and FP32C densities,
+  pressures, accelerations and dt_fac after the first evaluation; two full
+  CFL predictor-corrector steps (the dt sequence and the state).
+* 3D jittered 128^3 lattice (2,097,152 particles): neighbour sets
+  bit-exact in both precisions; SPHRho and SPHPressureGradient.
+* 256 batched elliptical drops (N_s ~ U[1k, 20k]): two steps, every scene.
+* 2D elliptical drop (5,025 particles): the full 100 FP64 steps.
+
+Integer work is compared bit for bit.  Floating point: FP64 against the
+oracle to round-off (1e-12 density, 1e-10 accelerations relative to the
+largest); FP32C to the FP32 path's bar, 1e-5 relative density error, with
+accelerations to 1e-4 of the largest.  Every comparison prints its
+measured error (pytest -s shows them).
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import oracle_from, oracle_density_eos, oracle_momentum, rel_err
+from pysph_b200 import workloads as W
+from pysph_b200.engine import Engine, fluid_scheme
+
+pytestmark = pytest.mark.gpu
+
+RHO_TOL = {"fp64": 1e-12, "fp32c": 1e-5}
+ACC_TOL = {"fp64": 1e-10, "fp32c": 1e-4}
+# the bench's launch shape for the dam break (one lane per particle,
+# 256-thread blocks, cells of the whole support)
+DAM_SHAPE = dict(lanes=1, pair_block=256, stencil=1)
+
+
+def report(name, **errs):
+    print(f"[parity] {name}: " + ", ".join(f"{k}={v:.3e}" for k, v in errs.items()))
+
+
+def max_rel(got, ref):
+    return float(np.max(np.abs(got - ref) / np.abs(ref)))
+
+
+@pytest.fixture(scope="module")
+def dam():
+    arrays, types, params = W.dam_break()
+    return arrays, params, fluid_scheme(2)
+
+
+@pytest.fixture(scope="module")
+def dam_oracle(dam):
+    arrays, params, scheme = dam
+    osys = oracle_from(arrays, params, scheme, 2)
+    osys.update()
+    return osys
+
+
+def assert_lists_equal(eng, osys, A, scene=0):
+    for d in range(A):
+        for s in range(A):
+            off, lst = eng.neighbor_csr(d, s, scene=scene)
+            ooff, olst = osys.neighbors_sorted(d, s)
+            np.testing.assert_array_equal(off, ooff)
+            np.testing.assert_array_equal(lst, olst)
+
+
+def test_dam_break_cells_bit_exact(dam):
+    """Cell coordinates floor(x / cs) with the reference's cell size
+    2 max h, every fluid and wall particle."""
+    import oracle
+    arrays, params, scheme = dam
+    eng = Engine([(arrays, params)], scheme, dim=2, precision="fp64", step_lists=False,
+                 **DAM_SHAPE)
+    cs = eng.cell_size()
+    assert cs == 2.0 * max(float(np.max(a["h"])) for a in arrays)
+    for a, arr in enumerate(arrays):
+        got = eng.cell_coords(0, a)
+        ref = oracle.cell_ids(arr["x"], arr["y"], arr["z"], cs)
+        ref[:, 2] = 0
+        np.testing.assert_array_equal(got, ref)
+    eng.check_status()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dam_break_neighbor_sets_bit_exact(dam, dam_oracle, precision):
+    """Sorted neighbour lists of every (dest, source) array pair, against
+    the reference's NNPS restated: bit-exact."""
+    arrays, params, scheme = dam
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision, **DAM_SHAPE)
+    assert_lists_equal(eng, dam_oracle, 2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dam_break_first_evaluation(dam, precision):
+    """SPHRho + Tait on fluid and walls, MomentumEquation + gravity and
+    dt_fac on the fluid, from the initial state; the pair counts of both
+    passes equal the oracle's neighbour totals."""
+    arrays, params, scheme = dam
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision, **DAM_SHAPE)
+    osys = oracle_from(arrays, params, scheme, 2)
+    osys.update()
+    oracle_density_eos(osys, scheme)
+    oracle_momentum(osys, scheme)
+    eng.reset_pair_counts()
+    eng.eval_stage()
+    eng.check_status()
+    B = params["c0"] ** 2 * params["rho0"] / params["gamma"]
+    errs = {}
+    for a in range(2):
+        O = osys.arrays[a]
+        errs[f"rho{a}"] = max_rel(eng.get(a, "rho").cpu().numpy(), O.rho)
+        errs[f"p{a}"] = rel_err(eng.get(a, "p").cpu().numpy(), O.p, scale=B)
+    O = osys.arrays[0]
+    scale = max(np.max(np.abs(O.au)), np.max(np.abs(O.av)))
+    errs["au"] = rel_err(eng.get(0, "au").cpu().numpy(), O.au, scale)
+    errs["av"] = rel_err(eng.get(0, "av").cpu().numpy(), O.av, scale)
+    errs["dt_fac"] = rel_err(eng.get(0, "dt_fac").cpu().numpy(), O.dt_fac)
+    report(f"dam break first evaluation {precision}", **errs)
+    for a in range(2):
+        assert errs[f"rho{a}"] <= RHO_TOL[precision]
+        assert errs[f"p{a}"] <= 10 * RHO_TOL[precision]
+    for k in ("au", "av", "dt_fac"):
+        assert errs[k] <= ACC_TOL[precision], k
+    pd, pf = eng.pair_counts()
+    tot_rho = sum(len(osys.neighbors(d, s)[1]) for d in (0, 1) for s in (0, 1))
+    tot_mom = sum(len(osys.neighbors(0, s)[1]) for s in (0, 1))
+    if precision == "fp64":
+        assert (pd, pf) == (tot_rho, tot_mom)
+    else:
+        # FP32 geometry may decide a pair within ~1e-7 of the support radius
+        # the other way (W = grad W = 0 there)
+        assert abs(pd - tot_rho) <= tot_rho * 1e-5 and abs(pf - tot_mom) <= tot_mom * 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dam_break_two_cfl_steps(dam, precision):
+    """Two PC steps with the CFL time step computed on the device: the dt
+    sequence and the fluid state after them."""
+    arrays, params, scheme = dam
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision, **DAM_SHAPE)
+    osys = oracle_from(arrays, params, scheme, 2)
+    dts = []
+    for _ in range(2):
+        dt = osys.cfl_time_step(params["cfl"], params["c0"], params["dt_initial"])
+        osys.pc_step(dt)
+        eng.pc_step()
+        dts.append((eng.scene_state()[0].dt, dt))
+    eng.check_status()
+    errs = {f"dt{i}": abs(g - r) / r for i, (g, r) in enumerate(dts)}
+    O = osys.arrays[0]
+    dx = 0.0025
+    for n in ("x", "y"):
+        errs[n + "/dx"] = float(np.max(np.abs(eng.get(0, n).cpu().numpy() - getattr(O, n)))) / dx
+    vscale = max(np.max(np.abs(O.u)), np.max(np.abs(O.v)))
+    for n in ("u", "v"):
+        errs[n] = rel_err(eng.get(0, n).cpu().numpy(), getattr(O, n), vscale)
+    for a in range(2):
+        errs[f"rho{a}"] = max_rel(eng.get(a, "rho").cpu().numpy(), osys.arrays[a].rho)
+    report(f"dam break two CFL steps {precision}", **errs)
+    dt_tol = 1e-12 if precision == "fp64" else 1e-5
+    assert errs["dt0"] <= dt_tol and errs["dt1"] <= dt_tol
+    # positions move by dt^2 a ~ 1e-4 dx per step: FP64 to round-off; FP32C
+    # accelerations carry <= 1e-4 of the largest
+    pos_tol = 1e-10 if precision == "fp64" else 1e-6
+    assert errs["x/dx"] <= pos_tol and errs["y/dx"] <= pos_tol
+    assert errs["u"] <= ACC_TOL[precision] and errs["v"] <= ACC_TOL[precision]
+    assert errs["rho0"] <= RHO_TOL[precision] and errs["rho1"] <= RHO_TOL[precision]
+
+
+@pytest.fixture(scope="module")
+def lattice():
+    arrays, types, params = W.lattice3d(n=128)
+    osys = oracle_from(arrays, params, fluid_scheme(1), 3)
+    osys.update()
+    return arrays, params, osys
+
+
+def lattice_engine(arrays, params, precision):
+    # the bench's shape for one evaluation of the lattice: cells of half
+    # the support, lists without a skin
+    return Engine([(arrays, params)], fluid_scheme(1), dim=3, precision=precision,
+                  lanes=1 if precision == "fp32c" else 2, pair_block=128, stencil=2,
+                  step_lists=False)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_lattice_128_neighbor_sets_bit_exact(lattice, precision):
+    """2,097,152 particles, about 58 neighbours each (122 M list entries):
+    the sorted lists equal the reference NNPS's."""
+    arrays, params, osys = lattice
+    eng = lattice_engine(arrays, params, precision)
+    off, lst = eng.neighbor_csr(0, 0)
+    ooff, olst = osys.neighbors_sorted(0, 0)
+    assert len(olst) > 100_000_000
+    np.testing.assert_array_equal(off, ooff)
+    np.testing.assert_array_equal(lst, olst)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_lattice_128_density_and_pressure_gradient(lattice, precision):
+    """One evaluation as the benchmark times it -- bin, SPHRho,
+    SPHPressureGradient -- on the jittered lattice with Tait pressures
+    from perturbed densities."""
+    arrays, params, osys = lattice
+    O = osys.arrays[0]
+    rho = np.zeros_like(O.rho)
+    osys.sph_rho(0, 0, rho)
+    au, av, aw = (np.zeros_like(O.rho) for _ in range(3))
+    osys.pgrad(0, 0, au, av, aw)
+    eng = lattice_engine(arrays, params, precision)
+    eng.bin(0)
+    eng.density(eos=False)
+    errs = {"rho": max_rel(eng.get(0, "rho").cpu().numpy(), rho)}
+    # the pressure gradient of the input densities and pressures
+    for n in ("rho", "p"):
+        eng.exchange_in(0, n, torch.as_tensor(arrays[0][n]))
+    eng.momentum(gravity=False, mode=1 | 16)
+    eng.check_status()
+    scale = max(np.max(np.abs(a)) for a in (au, av, aw))
+    for n, ref in (("au", au), ("av", av), ("aw", aw)):
+        errs[n] = rel_err(eng.get(0, n).cpu().numpy(), ref, scale)
+    report(f"lattice 128^3 {precision}", **errs)
+    assert errs["rho"] <= RHO_TOL[precision]
+    for n in ("au", "av", "aw"):
+        assert errs[n] <= ACC_TOL[precision], n
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_batched_256_scenes_two_steps(precision):
+    """All 256 drops (about 2.9 M particles) advanced together for two PC
+    steps; every scene against its own oracle."""
+    scenes = W.batched_drops(num_scenes=256, seed=0)
+    specs = [(arrs, dict(p, dt=1e-5)) for arrs, _, p in scenes]
+    eng = Engine(specs, fluid_scheme(1), dim=2, precision=precision, lanes=1,
+                 pair_block=128, stencil=1)
+    for _ in range(2):
+        eng.pc_step()
+    eng.check_status()
+    x_all = eng.get(0, "x").cpu().numpy()
+    u_all = eng.get(0, "u").cpu().numpy()
+    rho_all = eng.get(0, "rho").cpu().numpy()
+    off = eng.user_offset_host[0]
+    worst = {"x/dx": 0.0, "u": 0.0, "rho": 0.0}
+    for s, (arrs, p) in enumerate(specs):
+        osys = oracle_from(arrs, p, fluid_scheme(1), 2)
+        for _ in range(2):
+            osys.pc_step(1e-5)
+        O = osys.arrays[0]
+        n = len(O.x)
+        sl = slice(int(off[s]), int(off[s]) + n)
+        dx = float(arrs[0]["h"][0]) / 1.3
+        worst["x/dx"] = max(worst["x/dx"], float(np.max(np.abs(x_all[sl] - O.x))) / dx)
+        worst["u"] = max(worst["u"], rel_err(u_all[sl], O.u))
+        worst["rho"] = max(worst["rho"], max_rel(rho_all[sl], O.rho))
+    report(f"256 drops two steps {precision}", **worst)
+    assert worst["x/dx"] <= (1e-10 if precision == "fp64" else 2e-6)
+    assert worst["u"] <= (1e-12 if precision == "fp64" else 2e-6)
+    assert worst["rho"] <= RHO_TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_drop_100_steps(precision):
+    """The elliptical drop's full run: 100 PC steps of dt = 1e-5."""
+    arrays, _, params = W.elliptical_drop(dx=0.025)
+    params = dict(params, dt=1e-5)
+    eng = Engine([(arrays, params)], fluid_scheme(1), dim=2, precision=precision)
+    osys = oracle_from(arrays, params, fluid_scheme(1), 2)
+    for _ in range(100):
+        eng.pc_step()
+        osys.pc_step(1e-5)
+    eng.check_status()
+    O = osys.arrays[0]
+    errs = {n + "/dx": float(np.max(np.abs(eng.get(0, n).cpu().numpy() - getattr(O, n)))) / 0.025
+            for n in ("x", "y")}
+    for n in ("u", "v"):
+        errs[n] = rel_err(eng.get(0, n).cpu().numpy(), getattr(O, n))
+    errs["rho"] = max_rel(eng.get(0, "rho").cpu().numpy(), O.rho)
+    report(f"drop 100 steps {precision}", **errs)
+    st = eng.scene_state()[0]
+    assert st.count == 100 and st.t == pytest.approx(1e-3)
+    # FP64 to round-off.  FP32C: the accelerations' ~1e-7..1e-6 relative
+    # error (the Tait EOS with c0 = 1400 amplifies density round-off) is
+    # integrated 200 times, so velocity errors grow linearly and position
+    # errors quadratically with the step count: measured on B200 after 100
+    # steps 4.7e-5 / 1.1e-4 spacings (x / y), 7.1e-5 / 2.3e-4 of the largest
+    # velocity (u / v), densities 6.7e-6 (the FP32 path's bar is 1e-5)
+    pos_tol = 1e-10 if precision == "fp64" else 3e-4
+    vel_tol = 1e-10 if precision == "fp64" else 6e-4
+    assert errs["x/dx"] <= pos_tol and errs["y/dx"] <= pos_tol
+    assert errs["u"] <= vel_tol and errs["v"] <= vel_tol
+    assert errs["rho"] <= RHO_TOL[precision]
