@@ -56,7 +56,10 @@ enum {
     SPHB_ST_NONFINITE_RHO = 1u << 3,  /* NaN/Inf density or pressure */
     SPHB_ST_NONFINITE_ACC = 1u << 4,  /* NaN/Inf acceleration */
     SPHB_ST_BAD_INDEX = 1u << 5,      /* an index failed its bounds check */
-    SPHB_ST_NBR_CAPACITY = 1u << 6    /* neighbour list output too small */
+    SPHB_ST_NBR_CAPACITY = 1u << 6,   /* neighbour list output too small */
+    SPHB_ST_STAGE_TIMEOUT = 1u << 7   /* a tiled pass's shared-memory staging
+                                         did not complete in its wait limit
+                                         (the block's dests were skipped) */
 };
 
 enum { SPHB_FP64 = 0, SPHB_FP32C = 1 };   /* plain FP64 / FP32 + Kahan */
@@ -99,8 +102,19 @@ typedef struct {
     uint32_t xsph_src[SPHB_MAX_ARRAYS];
     int32_t kernel;         /* SPHB_KERNEL_*; scene.radius_scale must be its
                                support (3 for the quintic, else 2) */
-    int32_t reserved;       /* 0 */
+    int32_t pair_mode;      /* how the pair passes find neighbours:
+                               SPHB_PAIRS_LISTS (0): neighbour lists recorded
+                               by sphb_density (f.nbr, list_cap slots) and
+                               read back by later passes;
+                               SPHB_PAIRS_TILED (1): every pass searches the
+                               stencil cells of a block's dests from shared
+                               memory, where the block stages their
+                               particles' records (2D FP32C, fixed h per
+                               pair (no variable_h / hks), summation
+                               density scheme); no lists */
 } sphb_config;
+
+enum { SPHB_PAIRS_LISTS = 0, SPHB_PAIRS_TILED = 1 };
 
 /* Per-scene constants, written by the host once. */
 typedef struct {
@@ -234,7 +248,10 @@ typedef struct {
                                velocities, until sphb_refresh has rebuilt the
                                records and measured the displacements */
     unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
-    unsigned long long *pairs;  /* [4]  pairs evaluated: density, force, -, - */
+    unsigned long long *pairs;  /* [4]  pairs evaluated: density, force;
+                                   [2]: blocks of the tiled passes that read
+                                   their records from global memory (their
+                                   ranges exceeded the shared memory); [3]: - */
 } sphb_work;
 
 /* Everything the kernels see.  Tables are device pointers. */

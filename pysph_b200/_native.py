@@ -27,6 +27,7 @@ ST_NONFINITE_RHO = 1 << 3
 ST_NONFINITE_ACC = 1 << 4
 ST_BAD_INDEX = 1 << 5
 ST_NBR_CAPACITY = 1 << 6
+ST_STAGE_TIMEOUT = 1 << 7
 BIN_IF_NEEDED = 4
 BIN_STEP_BEGIN = 8     # the first bin of a step runs the step prologue too
 DENSITY_LIST_IF_VALID = 4
@@ -39,6 +40,7 @@ STATUS_NAMES = {
     ST_NONFINITE_ACC: "non-finite acceleration",
     ST_BAD_INDEX: "index failed a bounds check",
     ST_NBR_CAPACITY: "neighbour list output too small",
+    ST_STAGE_TIMEOUT: "shared-memory staging of a tiled pass timed out",
 }
 
 # engine field ids of sphb_exchange
@@ -64,7 +66,7 @@ class Config(ctypes.Structure):
                 ("rho_src", u32 * MAX_ARRAYS), ("mom_src", u32 * MAX_ARRAYS),
                 ("tait_on", u32), ("step_on", u32),
                 ("rate_src", u32 * MAX_ARRAYS), ("xsph_src", u32 * MAX_ARRAYS),
-                ("kernel", i32), ("reserved", i32)]
+                ("kernel", i32), ("pair_mode", i32)]
 
 # smoothing kernels (KernelBase.get_type ids) and their support radii
 KERNEL_CUBIC, KERNEL_QUINTIC, KERNEL_WENDLAND = 1, 3, 4
@@ -103,6 +105,8 @@ FIELD_NAMES = ("rho", "p", "cs", "au", "av", "aw", "dt_fac", "geo", "mass",
                "vel", "thermo", "cell", "nbr", "nbr_cnt", "anchor", "drho", "xu", "xv", "xw",
                "geo_next", "vel_next")
 FORCE_USE_LIST = 16
+# cfg.pair_mode: neighbour lists (0) or shared-memory tiles (1)
+PAIRS_LISTS, PAIRS_TILED = 0, 1
 FORCE_NO_MAXIMA = 32
 
 

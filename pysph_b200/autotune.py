@@ -2,7 +2,8 @@
 
 For a workload it times whole predictor-corrector steps for every candidate
 of cell size (stencil R: cell = support / R), lanes per dest particle and
-threads per block, and returns the fastest.  On that shape it then tries
+threads per block, with the neighbour lists and (2D FP32C summation
+density) with the shared-memory tiles, and returns the fastest.  On that shape it then tries
 the force pass's load-ahead depth (FP32C) and the skin of the kept
 neighbour lists: a wider skin means longer lists but fewer rebins, which
 pays where particles move fast.  Results are cached per (dim, precision,
@@ -65,10 +66,17 @@ def time_steps(eng: Engine, steps: int = 4, warm: int = 2) -> float:
     return a.elapsed_time(b) / steps
 
 
+def tiled_ok(scheme, dim, precision, variable_h=False) -> bool:
+    """Whether the tiled pair passes apply (2D FP32C, summation density, one
+    h per pair)."""
+    return (dim == 2 and precision == "fp32c" and not scheme.continuity and not scheme.hks
+            and not variable_h)
+
+
 def autotune(scenes, scheme, dim, precision="fp32c", device=None, stencils=STENCILS,
-             lanes=LANES, blocks=BLOCKS, steps=4, force=False):
-    """Best {"stencil", "lanes", "pair_block", "ms_per_step"} plus the table of
-    every candidate timed."""
+             lanes=LANES, blocks=BLOCKS, steps=4, force=False, tiled=True):
+    """Best {"pairs", "stencil", "lanes", "pair_block", "ms_per_step"} plus the
+    table of every candidate timed."""
     _load()
     n = sum(len(a["x"]) for arrays, _ in scenes for a in arrays)
     key = _key(dim, precision, n, len(scenes))
@@ -85,19 +93,31 @@ def autotune(scenes, scheme, dim, precision="fp32c", device=None, stencils=STENC
                 eng.set_launch(L, B)
                 ms = time_steps(eng, steps)
                 eng.check_status()
-                table.append({"stencil": R, "lanes": L, "pair_block": B,
+                table.append({"pairs": "lists", "stencil": R, "lanes": L, "pair_block": B,
                               "ms_per_step": ms})
         del eng
+        if tiled and tiled_ok(scheme, dim, precision):
+            eng = Engine(scenes, scheme, dim=dim, precision=precision, stencil=R,
+                         device=device, pairs="tiled")
+            for B in blocks:
+                if B < 128:
+                    continue
+                eng.set_launch(1, B)
+                ms = time_steps(eng, steps)
+                eng.check_status()
+                table.append({"pairs": "tiled", "stencil": R, "lanes": 1, "pair_block": B,
+                              "ms_per_step": ms})
+            del eng
     best = min(table, key=lambda r: r["ms_per_step"])
     best = dict(best, list_batch=4)
-    if precision == "fp32c":
+    if precision == "fp32c" and best["pairs"] == "lists":
         # load-ahead depth of the force pass's list loop, on the best shape
         eng = Engine(scenes, scheme, dim=dim, precision=precision, stencil=best["stencil"],
                      lanes=best["lanes"], pair_block=best["pair_block"], device=device,
                      list_batch=2)
         ms = time_steps(eng, steps)
         eng.check_status()
-        table.append({"stencil": best["stencil"], "lanes": best["lanes"],
+        table.append({"pairs": "lists", "stencil": best["stencil"], "lanes": best["lanes"],
                       "pair_block": best["pair_block"], "list_batch": 2, "ms_per_step": ms})
         if ms < best["ms_per_step"]:
             best = dict(table[-1])
@@ -108,10 +128,11 @@ def autotune(scenes, scheme, dim, precision="fp32c", device=None, stencils=STENC
     for skin in SKINS:
         eng = Engine(scenes, scheme, dim=dim, precision=precision, stencil=best["stencil"],
                      lanes=best["lanes"], pair_block=best["pair_block"], device=device,
-                     list_batch=best.get("list_batch", 4), skin_margin=skin)
+                     list_batch=best.get("list_batch", 4), skin_margin=skin,
+                     pairs=best["pairs"])
         ms = time_steps(eng, 4 * steps, warm=steps)
         eng.check_status()
-        skin_table.append(dict(stencil=best["stencil"], lanes=best["lanes"],
+        skin_table.append(dict(pairs=best["pairs"], stencil=best["stencil"], lanes=best["lanes"],
                                pair_block=best["pair_block"],
                                list_batch=best.get("list_batch", 4), skin_margin=skin,
                                ms_per_step=ms))

@@ -255,7 +255,9 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
         e.work.meta[1] = 1;
         e.work.meta[2] = 0;
         e.work.meta[3] = 2;
-        e.work.meta[4] = 0;
+        // tiled pair passes search the cells, which stay complete while no
+        // particle has moved half the skin from where this rebin put it
+        e.work.meta[4] = e.cfg.pair_mode == SPHB_PAIRS_TILED ? 1 : 0;
         e.work.meta[5] = 0;
     }
 }

@@ -135,6 +135,14 @@ int check_pair_cfg(const sphb_engine *e)
     if (!e->pair_tiles || e->num_pair_tiles < 0) return SPHB_ERR_ARG;
     if (!e->work.start || !e->f.cell) return SPHB_ERR_ARG;
     if (!pass_variant(c)) return SPHB_ERR_UNSUPPORTED;   // kernel type / dimension
+    if (c.pair_mode != SPHB_PAIRS_LISTS && c.pair_mode != SPHB_PAIRS_TILED) return SPHB_ERR_ARG;
+    if (c.pair_mode == SPHB_PAIRS_TILED) {
+        // 2D FP32C, one thread per dest, the summation-density scheme
+        if (c.dim != 2 || c.precision != SPHB_FP32C || c.lanes != 1) return SPHB_ERR_UNSUPPORTED;
+        for (int a = 0; a < SPHB_MAX_ARRAYS; ++a)
+            if (c.rate_src[a] || c.xsph_src[a]) return SPHB_ERR_UNSUPPORTED;
+        if (c.num_particles >= (1 << SPHB_NBR_IDX_BITS_2D)) return SPHB_ERR_UNSUPPORTED;
+    }
     return SPHB_OK;
 }
 
@@ -151,6 +159,8 @@ extern "C" int sphb_density(const sphb_engine *e, int cur, uint32_t dest_mask,
     if (with_eos & ~(SPHB_DENSITY_EOS | SPHB_DENSITY_USE_LIST | SPHB_DENSITY_LIST_IF_VALID |
                      SPHB_DENSITY_LISTS_ONLY))
         return SPHB_ERR_ARG;
+    if (e->cfg.pair_mode == SPHB_PAIRS_TILED && (with_eos & SPHB_DENSITY_LISTS_ONLY))
+        return SPHB_ERR_UNSUPPORTED;
     if (e->num_pair_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const sphb_config &c = e->cfg;

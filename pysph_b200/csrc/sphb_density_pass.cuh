@@ -30,6 +30,49 @@
 
 namespace sphb {
 
+// The outputs of dest k after its density sum: rho (0 for non-LocalReal
+// dests), the Tait EOS when asked and the array is a Tait dest, the FP32C
+// record {rho, p, cs, p / rho^2}, and the pair count.  Every thread of the
+// block calls it; rho is valid in lane 0 of each dest.
+template <bool F32>
+__device__ __forceinline__ void density_finish(const sphb_engine &e, int cur, int k, int s, int a,
+                                               bool active, int lane, double rho, int with_eos,
+                                               unsigned int np)
+{
+    const sphb_scene &sc = e.scene[s];
+    if (active && lane == 0) {
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (!real) rho = 0.0;
+        const bool eos = with_eos && ((e.cfg.tait_on >> a) & 1u);
+        double p = 0.0, c = 0.0;
+        if (eos && real) {
+            const double ratio = rho / sc.rho0;
+            p = (eos_pow<F32>(ratio, sc.gamma) - 1.0) * sc.B;
+            c = eos_pow<F32>(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
+        }
+        if constexpr (F32) {
+            float4 *th = (float4 *)e.f.thermo;
+            float4 t = th[k];
+            t.x = (float)rho;
+            if (eos) {
+                t.y = (float)p;
+                t.z = (float)c;
+            }
+            t.w = t.x != 0.f ? t.y / (t.x * t.x) : 0.f;
+            th[k] = t;
+            if (!isfinite(t.x) || !isfinite(t.y)) flag(e, SPHB_ST_NONFINITE_RHO);
+        } else {
+            ((double *)e.f.rho)[k] = rho;
+            if (eos) {
+                ((double *)e.f.p)[k] = p;
+                ((double *)e.f.cs)[k] = c;
+            }
+            if (!isfinite(rho) || !isfinite(p)) flag(e, SPHB_ST_NONFINITE_RHO);
+        }
+    }
+    block_add_u64(&e.work.pairs[0], np);
+}
+
 // The 2D FP32C variants are held to 48 registers, five 256-thread blocks per
 // SM (62 registers and four blocks otherwise): 2-12% shorter passes on the
 // dam break, the list-recording pass gaining most.  The 3D FP32C variants are
@@ -270,37 +313,7 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     }
 
     if (active && nbr) e.f.nbr_cnt[(size_t)lane * N + k] = cnt <= cap_lane ? cnt : -1;
-    if (active && lane == 0 && !lists_only) {
-        const bool real = e.buf[cur].tag[k] == 0;
-        if (!real) rho = 0.0;
-        const bool eos = with_eos && ((e.cfg.tait_on >> a) & 1u);
-        double p = 0.0, c = 0.0;
-        if (eos && real) {
-            const double ratio = rho / sc.rho0;
-            p = (eos_pow<F32>(ratio, sc.gamma) - 1.0) * sc.B;
-            c = eos_pow<F32>(ratio, 0.5 * (sc.gamma - 1.0)) * sc.c0;
-        }
-        if constexpr (F32) {
-            float4 *th = (float4 *)e.f.thermo;
-            float4 t = th[k];
-            t.x = (float)rho;
-            if (eos) {
-                t.y = (float)p;
-                t.z = (float)c;
-            }
-            t.w = t.x != 0.f ? t.y / (t.x * t.x) : 0.f;
-            th[k] = t;
-            if (!isfinite(t.x) || !isfinite(t.y)) flag(e, SPHB_ST_NONFINITE_RHO);
-        } else {
-            ((double *)e.f.rho)[k] = rho;
-            if (eos) {
-                ((double *)e.f.p)[k] = p;
-                ((double *)e.f.cs)[k] = c;
-            }
-            if (!isfinite(rho) || !isfinite(p)) flag(e, SPHB_ST_NONFINITE_RHO);
-        }
-    }
-    block_add_u64(&e.work.pairs[0], np);
+    density_finish<F32>(e, cur, k, s, a, active && !lists_only, lane, rho, with_eos, np);
 }
 
 template <int KT, int DIM, bool F32>
@@ -325,6 +338,12 @@ static void launch_density_p(const sphb_engine &e, int cur, uint32_t dm, int eos
 template <int KT, int DIM>
 void launch_density_kt(const sphb_engine &e, int cur, uint32_t dm, int flags, cudaStream_t st)
 {
+    if constexpr (DIM == 2) {
+        if (e.cfg.pair_mode == SPHB_PAIRS_TILED) {
+            launch_density_tiled<KT>(e, cur, dm, flags, st);
+            return;
+        }
+    }
     if (e.cfg.precision == SPHB_FP32C) launch_density_p<KT, DIM, true>(e, cur, dm, flags, st);
     else launch_density_p<KT, DIM, false>(e, cur, dm, flags, st);
 }

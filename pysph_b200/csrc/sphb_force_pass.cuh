@@ -28,6 +28,108 @@
 
 namespace sphb {
 
+// Everything after the pair sums of dest k: its outputs (non-LocalReal
+// dests get 0), gravity, dt_fac, the per-scene CFL maxima, the integrator
+// stage fused into the epilogue (FP32C) and the pair count.  Every thread
+// of the block calls it (block reductions inside); acc, dtf, drho and xs
+// are valid in lane 0 of each dest.
+template <int DIM, bool F32, bool CONT>
+__device__ __forceinline__ void force_finish(const sphb_engine &e, int cur, int k, int s, int a,
+                                             bool active, int lane, double *acc, double dtf,
+                                             double drho, const double *xs, bool visc,
+                                             uint32_t mm, uint32_t rm, uint32_t xm,
+                                             int with_gravity, int mode, unsigned int np)
+{
+    const sphb_scene &sc = e.scene[s];
+    double a2 = 0.0, dtf_out = 0.0;
+    if (CONT && active && lane == 0) {
+        // non-LocalReal dests get 0 (S/sph/sph_func.pyx:220-227)
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (rm) {
+            const double v = real ? drho : 0.0;
+            if (F32) ((float *)e.f.drho)[k] = (float)v;
+            else ((double *)e.f.drho)[k] = v;
+            if (!isfinite(v)) flag(e, SPHB_ST_NONFINITE_RHO);
+        }
+        if (xm) {
+            void *xo[3] = {e.f.xu, e.f.xv, e.f.xw};
+            for (int d = 0; d < DIM; ++d) {
+                const double v = real ? xs[d] : 0.0;
+                if (F32) ((float *)xo[d])[k] = (float)v;
+                else ((double *)xo[d])[k] = v;
+            }
+        }
+    }
+    if (active && lane == 0 && mm) {
+        const bool real = e.buf[cur].tag[k] == 0;
+        if (real) {
+            if (with_gravity) {
+                acc[0] += sc.g[0];
+                acc[1] += sc.g[1];
+                if (DIM == 3) acc[2] += sc.g[2];
+            }
+            dtf_out = visc ? dtf : 0.0;
+        } else {
+            acc[0] = acc[1] = acc[2] = 0.0;
+        }
+        if (F32) {
+            const float fx = (float)acc[0], fy = (float)acc[1], fz = (float)acc[2];
+            ((float *)e.f.au)[k] = fx;
+            ((float *)e.f.av)[k] = fy;
+            if (DIM == 3) ((float *)e.f.aw)[k] = fz;
+            if (visc) ((float *)e.f.dt_fac)[k] = (float)dtf_out;
+            a2 = (double)fx * fx + (double)fy * fy + (double)fz * fz;
+        } else {
+            ((double *)e.f.au)[k] = acc[0];
+            ((double *)e.f.av)[k] = acc[1];
+            if (DIM == 3) ((double *)e.f.aw)[k] = acc[2];
+            if (visc) ((double *)e.f.dt_fac)[k] = dtf_out;
+            a2 = acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2];
+        }
+        if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
+    }
+    if (!(mode & SPHB_FORCE_NO_MAXIMA)) {
+        // one atomic per block and quantity (a block never spans two scenes)
+        const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
+        const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
+        if (threadIdx.x == 0) {
+            sphb_scene_state &sw = e.sstate[s];
+            atomic_max_nonneg(&sw.max_dtfac, bdt);
+            atomic_max_nonneg(&sw.max_acc2, ba2);
+        }
+    }
+    if constexpr (F32) {
+        // the integrator stage fused into the epilogue (FP32C): the rates
+        // as stored above, the new records into the second copy
+        const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
+        if (kind >= 0) {
+            const bool stepped = (e.cfg.step_on >> a) & 1u;
+            float d2 = 0.f;
+            if (active && lane == 0 && (stepped || rm)) {
+                const bool real = e.buf[cur].tag[k] == 0;
+                double f[3], xv[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    f[d] = (double)(float)acc[d];
+                    xv[d] = (double)(float)(real ? xs[d] : 0.0);
+                }
+                const double dr = (double)(float)(real ? drho : 0.0);
+                const float4 g_old = ((const float4 *)e.f.geo)[k];
+                d2 = stage_particle<DIM, true>(e, cur, k, s, a, kind, f, xm != 0u, xv, dr,
+                                               (float4 *)e.f.geo_next, e.f.vel_next, g_old);
+            }
+            if (stepped && e.f.anchor) warp_max_disp(e, s, d2);
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                // the particles move: the lists are not known to be complete
+                // until the next rebin decision, and they leave the anchors
+                e.work.meta[2] = 0;
+                e.work.meta[3] = 0;
+            }
+        }
+    }
+    block_add_u64(&e.work.pairs[1], np);
+}
+
 // CONT: the continuity scheme's pair terms too -- SPHDensityRate
 // (density_funcs.pyx:119-156) and XSPHCorrection (xsph_funcs.pyx:40-86),
 // each over its own sources, in the same traversal as the momentum.
@@ -396,93 +498,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         }
     }
 
-    double a2 = 0.0, dtf_out = 0.0;
-    if (CONT && active && lane == 0) {
-        // non-LocalReal dests get 0 (S/sph/sph_func.pyx:220-227)
-        const bool real = e.buf[cur].tag[k] == 0;
-        if (rm) {
-            const double v = real ? drho : 0.0;
-            if (F32) ((float *)e.f.drho)[k] = (float)v;
-            else ((double *)e.f.drho)[k] = v;
-            if (!isfinite(v)) flag(e, SPHB_ST_NONFINITE_RHO);
-        }
-        if (xm) {
-            void *xo[3] = {e.f.xu, e.f.xv, e.f.xw};
-            for (int d = 0; d < DIM; ++d) {
-                const double v = real ? xs[d] : 0.0;
-                if (F32) ((float *)xo[d])[k] = (float)v;
-                else ((double *)xo[d])[k] = v;
-            }
-        }
-    }
-    if (active && lane == 0 && mm) {
-        const bool real = e.buf[cur].tag[k] == 0;
-        if (real) {
-            if (with_gravity) {
-                acc[0] += sc.g[0];
-                acc[1] += sc.g[1];
-                if (DIM == 3) acc[2] += sc.g[2];
-            }
-            dtf_out = visc ? dtf : 0.0;
-        } else {
-            acc[0] = acc[1] = acc[2] = 0.0;
-        }
-        if (F32) {
-            const float fx = (float)acc[0], fy = (float)acc[1], fz = (float)acc[2];
-            ((float *)e.f.au)[k] = fx;
-            ((float *)e.f.av)[k] = fy;
-            if (DIM == 3) ((float *)e.f.aw)[k] = fz;
-            if (visc) ((float *)e.f.dt_fac)[k] = (float)dtf_out;
-            a2 = (double)fx * fx + (double)fy * fy + (double)fz * fz;
-        } else {
-            ((double *)e.f.au)[k] = acc[0];
-            ((double *)e.f.av)[k] = acc[1];
-            if (DIM == 3) ((double *)e.f.aw)[k] = acc[2];
-            if (visc) ((double *)e.f.dt_fac)[k] = dtf_out;
-            a2 = acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2];
-        }
-        if (!isfinite(a2)) flag(e, SPHB_ST_NONFINITE_ACC);
-    }
-    if (!(mode & SPHB_FORCE_NO_MAXIMA)) {
-        // one atomic per block and quantity (a block never spans two scenes)
-        const double bdt = block_reduce(dtf_out, OpMax(), 0.0);
-        const double ba2 = block_reduce(isfinite(a2) ? a2 : 0.0, OpMax(), 0.0);
-        if (threadIdx.x == 0) {
-            sphb_scene_state &sw = e.sstate[s];
-            atomic_max_nonneg(&sw.max_dtfac, bdt);
-            atomic_max_nonneg(&sw.max_acc2, ba2);
-        }
-    }
-    if constexpr (F32) {
-        // the integrator stage fused into the epilogue (FP32C): the rates
-        // as stored above, the new records into the second copy
-        const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
-        if (kind >= 0) {
-            const bool stepped = (e.cfg.step_on >> a) & 1u;
-            float d2 = 0.f;
-            if (active && lane == 0 && (stepped || rm)) {
-                const bool real = e.buf[cur].tag[k] == 0;
-                double f[3], xv[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    f[d] = (double)(float)acc[d];
-                    xv[d] = (double)(float)(real ? xs[d] : 0.0);
-                }
-                const double dr = (double)(float)(real ? drho : 0.0);
-                const float4 g_old = ((const float4 *)e.f.geo)[k];
-                d2 = stage_particle<DIM, true>(e, cur, k, s, a, kind, f, xm != 0u, xv, dr,
-                                               (float4 *)e.f.geo_next, e.f.vel_next, g_old);
-            }
-            if (stepped && e.f.anchor) warp_max_disp(e, s, d2);
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
-                // the particles move: the lists are not known to be complete
-                // until the next rebin decision, and they leave the anchors
-                e.work.meta[2] = 0;
-                e.work.meta[3] = 0;
-            }
-        }
-    }
-    block_add_u64(&e.work.pairs[1], np);
+    force_finish<DIM, F32, CONT>(e, cur, k, s, a, active, lane, acc, dtf, drho, xs, visc, mm,
+                                 rm, xm, with_gravity, mode, np);
 }
 
 template <int KT, int DIM, bool F32, int LV, int RV>
@@ -530,6 +547,12 @@ template <int KT, int DIM>
 void launch_force_kt(const sphb_engine &e, int cur, uint32_t dm, int grav, int mode,
                      cudaStream_t st)
 {
+    if constexpr (DIM == 2) {
+        if (e.cfg.pair_mode == SPHB_PAIRS_TILED) {
+            launch_force_tiled<KT>(e, cur, dm, grav, mode, st);
+            return;
+        }
+    }
     if (e.cfg.precision == SPHB_FP32C) launch_force_p<KT, DIM, true>(e, cur, dm, grav, mode, st);
     else launch_force_p<KT, DIM, false>(e, cur, dm, grav, mode, st);
 }

@@ -17,6 +17,14 @@ template <int KT, int DIM>
 void launch_force_kt(const sphb_engine &e, int cur, uint32_t dm, int grav, int mode,
                      cudaStream_t st);
 
+// the same passes with shared-memory staging (pair_mode SPHB_PAIRS_TILED,
+// 2D FP32C; sphb_tiled.cuh)
+template <int KT>
+void launch_density_tiled(const sphb_engine &e, int cur, uint32_t dm, int flags, cudaStream_t st);
+template <int KT>
+void launch_force_tiled(const sphb_engine &e, int cur, uint32_t dm, int grav, int mode,
+                        cudaStream_t st);
+
 // kernel * 10 + dim of the built pair passes (the cubic in 2D and 3D, the
 // quintic and Wendland kernels in 2D, as the reference has them); 0 if the
 // configuration has no pass

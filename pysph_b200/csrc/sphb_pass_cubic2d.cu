@@ -3,6 +3,7 @@
 
 #include "sphb_density_pass.cuh"
 #include "sphb_force_pass.cuh"
+#include "sphb_tiled.cuh"
 
 namespace sphb {
 

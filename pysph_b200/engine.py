@@ -149,7 +149,8 @@ class Engine:
                  grid_growth: float = 2.0, device=None, use_lists: bool = True,
                  step_lists: bool = True, skin_margin: float | None = None,
                  list_batch: int = 4, variable_h: bool = False,
-                 kernel: int = nat.KERNEL_CUBIC, fuse_stage: bool = True):
+                 kernel: int = nat.KERNEL_CUBIC, fuse_stage: bool = True,
+                 pairs: str = "lists"):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
         if precision not in ("fp64", "fp32c"):
@@ -173,6 +174,21 @@ class Engine:
         if kernel != nat.KERNEL_CUBIC and dim != 2:
             raise NotImplementedError("the quintic and Wendland kernels are 2D only")
         self.kernel = kernel
+        # how the pair passes find neighbours: "lists" (recorded by the
+        # density pass after a rebin, read back while the skin holds) or
+        # "tiled" (every pass searches the cells from shared memory, where
+        # each block stages its dests' stencil rows; 2D FP32C summation
+        # density with one h per pair, one thread per dest)
+        if pairs not in ("lists", "tiled"):
+            raise ValueError("pairs must be 'lists' or 'tiled'")
+        if pairs == "tiled":
+            if dim != 2 or precision != "fp32c":
+                raise NotImplementedError("tiled pair passes are 2D FP32C")
+            if scheme.continuity or scheme.hks or variable_h:
+                raise NotImplementedError("tiled pair passes: summation density, one h per pair")
+            if lanes != 1:
+                raise ValueError("tiled pair passes run one thread per dest (lanes=1)")
+        self.pairs = pairs
         params = [p if isinstance(p, SceneParams) else SceneParams.from_dict(p)
                   for _, p in scenes]
         # the neighbour radius is the kernel's support
@@ -353,7 +369,11 @@ class Engine:
         # per-stage neighbour lists (density pass writes, force pass reads)
         idx_bits = 26 if dim == 2 else 23
         self.list_cap = (64 if dim == 2 else 160) if (self.use_lists and N < 2 ** idx_bits) else 0
-        if self.list_cap:
+        if self.list_cap and self.pairs == "tiled":
+            # per-stage lists: the entries the density pass accepted (within
+            # the support, no skin), for the force pass of the same stage
+            self.list_cap = 48
+        elif self.list_cap:
             # capacity for the skin and the kernel's support (3h for the
             # quintic): entries grow as (radius (1 + margin))^dim; a lane
             # whose list overflows searches its cells instead
@@ -391,6 +411,7 @@ class Engine:
         cfg.pair_block = pair_block
         cfg.list_batch = getattr(self, "list_batch", 4)
         cfg.kernel = self.kernel
+        cfg.pair_mode = nat.PAIRS_TILED if getattr(self, "pairs", "lists") == "tiled" else 0
         cfg.num_particles = self.N
         cfg.cell_capacity = self.cell_capacity
         rho, mom, tait, step = self.scheme.masks()
@@ -422,6 +443,8 @@ class Engine:
         how many list entries the FP32C force pass loads ahead (2 or 4)."""
         if lanes not in (1, 2, 4, 8) or pair_block % 32 or not 32 <= pair_block <= 256:
             raise ValueError("bad pair-kernel launch shape")
+        if self.pairs == "tiled" and lanes != 1:
+            raise ValueError("tiled pair passes run one thread per dest (lanes=1)")
         if list_batch is not None:
             if list_batch not in (2, 4):
                 raise ValueError("list_batch must be 2 or 4")
@@ -651,11 +674,13 @@ class Engine:
             dest_mask = sum(1 << a for a in self.scheme.tait_on)
         self.call("sphb_tait", self.cur, dest_mask)
 
-    def momentum(self, dest_mask=None, gravity=True, mode=0):
+    def momentum(self, dest_mask=None, gravity=True, mode=0, synced=False):
+        """The force pass; synced: the cells are known to cover every pair
+        (the stage's rebin decision has just run), so no decision first."""
         if dest_mask is None:
             dest_mask = (self.scheme.pair_dests if self.scheme.continuity
                          else self.scheme.mom_dests)
-        if not mode & nat.FORCE_USE_LIST:
+        if not mode & nat.FORCE_USE_LIST and not synced:
             self._sync_cells()
         self.call("sphb_momentum", self.cur, dest_mask, 1 if gravity else 0, mode)
 
@@ -725,7 +750,8 @@ class Engine:
             self.call("sphb_density", self.cur, self.scheme.rho_dests, nat.DENSITY_EOS | reuse)
             if self.tait_only_mask:
                 self.tait(self.tait_only_mask)
-            self.momentum(mode=mode)
+            # the density pass above searched the same cells
+            self.momentum(mode=mode, synced=True)
         if stage is not None:
             self._swap_records()
 
@@ -795,6 +821,13 @@ class Engine:
         off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
         v = self.work_buf[off:off + 32].view(torch.int64).tolist()
         return v[0], v[1]
+
+    def fallback_blocks(self) -> int:
+        """Blocks of the tiled pair passes (since the last
+        reset_pair_counts) whose stencil rows did not fit shared memory and
+        that read their records from global memory instead."""
+        off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
+        return int(self.work_buf[off + 16:off + 24].view(torch.int64).item())
 
     def reset_pair_counts(self):
         off = self.work_offsets[nat.WORK_NAMES.index("pairs")]

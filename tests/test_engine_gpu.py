@@ -478,7 +478,7 @@ def test_autotune_returns_a_timed_shape(tmp_path, monkeypatch):
     T._cache.clear()
     arrays, params, scheme, dim = drop(dx=0.05)
     scenes = [(arrays, dict(params, dt=1e-5))]
-    kw = dict(lanes=(1, 2), blocks=(128,), stencils=(1,), steps=2)
+    kw = dict(lanes=(1, 2), blocks=(128,), stencils=(1,), steps=2, tiled=False)
     res = T.autotune(scenes, scheme, dim, "fp32c", **kw)
     assert res["lanes"] in (1, 2) and res["pair_block"] == 128 and res["stencil"] == 1
     assert res["skin_margin"] in T.SKINS and res["ms_per_step"] > 0
