@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--pair-block", type=int, default=0)
     ap.add_argument("--stencil", type=int, default=0,
                     help="fix the cell size (support / R); default: autotuned")
+    ap.add_argument("--pairs", default="auto", choices=["auto", "lists", "tiled"],
+                    help="neighbour lists or shared-memory tiles; default: autotuned")
     ap.add_argument("--list-batch", type=int, default=0,
                     help="list entries the force pass loads ahead (2 or 4); default: autotuned")
     return ap.parse_args()
@@ -88,9 +90,9 @@ def workload(name):
                     dim=3, desc="3D jittered 128^3 lattice (2,097,152 particles), h=1.2dx")
     if name == "batched":
         scenes = W.batched_drops(num_scenes=256, seed=0)
-        return dict(scenes=[(a, dict(p, dt=1e-5)) for a, _, p in scenes],
+        return dict(scenes=[(a, p) for a, _, p in scenes],
                     scheme=fluid_scheme(1), dim=2,
-                    desc="256 elliptical drops, N_s ~ U[1k,20k], dt=1e-5")
+                    desc="256 elliptical drops, N_s ~ U[1k,20k], dt_s = 1e-5 dx_s / 0.025")
     raise ValueError(name)
 
 
@@ -102,8 +104,10 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, dev):
+        # nvidia-smi numbers GPUs physically and ignores CUDA_VISIBLE_DEVICES:
+        # name the device by its UUID so the samples are this GPU's
+        self.index = gpu_id(dev)
         self.proc = None
         self.lines = []
 
@@ -156,7 +160,18 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "gpu": self.index}
+
+
+def gpu_id(dev):
+    """nvidia-smi's -i argument for a torch device: its UUID (GPU-...), else
+    the CUDA ordinal."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(getattr(dev, "index", dev) or 0)
 
 
 # ------------------------------------------------------------------ helpers
@@ -212,17 +227,18 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu --set full
 # on the bench's own workload and launch shape; the force pass with the
 # integrator stage fused into it)
-NCU_TRAFFIC = {("dam_break", "fp32c", "force"): 71.932e6 + 3.265e6,
-               ("dam_break", "fp32c", "density"): 40.985e6 + 0.021e6,
-               ("dam_break", "fp32c", "pc_stage"): 17.951e6 + 0.000256e6}
+NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 71.932e6 + 3.265e6,
+               ("dam_break", "fp32c", "lists", "density"): 40.985e6 + 0.021e6,
+               ("dam_break", "fp32c", "lists", "pc_stage"): 17.951e6 + 0.000256e6}
 
 
 # FP32 work of one launch, from the same capture: flops = 2 FFMA + FADD +
 # FMUL + 4 FFMA2 + 2 FADD2 + 2 FMUL2 (sm__sass_thread_inst_executed_op_*),
 # and the fraction of cycles the schedulers issued
 # (smsp__issue_active.avg.pct_of_peak_sustained_active)
-NCU_FP32 = {("dam_break", "fp32c", "force"): {"flops": 398.5e6, "issue_active": 0.518},
-            ("dam_break", "fp32c", "density"): {"flops": 228.9e6, "issue_active": 0.739}}
+NCU_FP32 = {("dam_break", "fp32c", "lists", "force"): {"flops": 398.5e6, "issue_active": 0.518},
+            ("dam_break", "fp32c", "lists", "density"): {"flops": 228.9e6,
+                                                         "issue_active": 0.739}}
 
 
 def fma_peaks(dev):
@@ -290,58 +306,75 @@ def algorithmic_bytes(dim, f32):
 
 
 # ------------------------------------------------------------------ our arm
+def launch_shape(wl, precision, args, dev, force_tune=False):
+    """The engine's launch shape: fixed from the command line, else the
+    autotuner's (both pair modes, every cell size / lanes / block / skin)."""
+    if not force_tune and (args.lanes or args.pair_block or args.stencil or args.list_batch
+                           or args.pairs != "auto"):
+        pairs = "lists" if args.pairs == "auto" else args.pairs
+        return dict(pairs=pairs, lanes=args.lanes or (4 if wl["dim"] == 3 else 1),
+                    pair_block=args.pair_block or 128, stencil=args.stencil or 1,
+                    list_batch=args.list_batch or 4, skin_margin=None), None
+    from pysph_b200.autotune import autotune
+    tune = autotune(wl["scenes"], wl["scheme"], wl["dim"], precision, device=dev)
+    shape = {k: tune.get(k) for k in ("pairs", "lanes", "pair_block", "stencil", "list_batch",
+                                      "skin_margin")}
+    shape["pairs"] = shape["pairs"] or "lists"
+    shape["list_batch"] = shape["list_batch"] or 4
+    return shape, tune
+
+
+def make_engine(wl, precision, shape, dev):
+    from pysph_b200.engine import Engine
+    return Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=precision,
+                  stencil=shape["stencil"], lanes=shape["lanes"],
+                  pair_block=shape["pair_block"], device=dev,
+                  list_batch=shape["list_batch"], skin_margin=shape["skin_margin"],
+                  pairs=shape["pairs"])
+
+
+def capture_step(eng, stream):
+    """One PC step captured in a CUDA graph (after a side-stream warm-up)."""
+    import torch
+    s = torch.cuda.Stream(eng.device)
+    s.wait_stream(stream)
+    with torch.cuda.stream(s):
+        eng.pc_step()
+    stream.wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        eng.pc_step()
+    torch.cuda.synchronize()
+    return g
+
+
 def run_ours(args, rank, world, local):
     import torch
-    from pysph_b200.engine import Engine
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wl = workload(args.workload)
-    tune = None
-    if args.lanes or args.pair_block or args.stencil or args.list_batch:
-        lanes = args.lanes or (4 if wl["dim"] == 3 else 1)
-        pb = args.pair_block or 128
-        stencil = args.stencil or 1
-        lb = args.list_batch or 4
-    else:
-        from pysph_b200.autotune import autotune
-        tune = autotune(wl["scenes"], wl["scheme"], wl["dim"], args.precision, device=dev)
-        lanes, pb, stencil = tune["lanes"], tune["pair_block"], tune["stencil"]
-        lb = tune.get("list_batch", 4)
-    skin = tune.get("skin_margin") if tune else None
-    args.stencil = stencil
-    eng = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision=args.precision,
-                 stencil=stencil, lanes=lanes, pair_block=pb, device=dev, list_batch=lb,
-                 skin_margin=skin)
+    shape, tune = launch_shape(wl, args.precision, args, dev)
+    eng = make_engine(wl, args.precision, shape, dev)
     N = eng.N
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     # clocks are sampled from the warm-up through the end of the timed region
-    clk = ClockSampler(local).__enter__()
+    clk = ClockSampler(dev).__enter__()
+    # the warm-up advances the state: the timed steps are steps W+1 .. W+K of
+    # the run from the workload's initial state
     for _ in range(max(args.warmup, 3)):
         eng.pc_step()
     torch.cuda.synchronize()
     eng.check_status()
-
     graph = None
     if not args.no_graph:
-        try:
-            s = torch.cuda.Stream(dev)
-            s.wait_stream(stream)
-            with torch.cuda.stream(s):
-                eng.pc_step()   # warm the side stream
-            stream.wait_stream(s)
-            torch.cuda.synchronize()
-            graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph):
-                eng.pc_step()
-            torch.cuda.synchronize()
-            graph.replay()
-            torch.cuda.synchronize()
-            eng.check_status()
-        except Exception as ex:  # report, fall back to eager launches
-            print(f"graph capture failed: {ex}", file=sys.stderr)
-            graph = None
+        graph = capture_step(eng, stream)
+        graph.replay()
+        torch.cuda.synchronize()
+        eng.check_status()
+    start_step = max(args.warmup, 3) + (2 if graph is not None else 0)
 
     def step():
         if graph is not None:
@@ -370,6 +403,7 @@ def run_ours(args, rank, world, local):
     ms = sum(starts[i].elapsed_time(ends[i]) for i in range(args.steps))
     eng.check_status()
     pairs_d, pairs_f = eng.pair_counts()
+    rebins = eng.device_rebins()
     pairs = pairs_d + pairs_f
     job = replica_result(ms, pairs, args.steps, world)
     ms_max, value, steps_per_s = job["ms"], job["value"], job["steps_per_s"]
@@ -377,21 +411,71 @@ def run_ours(args, rank, world, local):
     if args.no_extras:
         out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
                "n_gpus": world, "steps": args.steps, "ms_per_step": ms_max / args.steps,
-               "steps_per_s": steps_per_s, "config": {"workload": args.workload},
+               "steps_per_s": steps_per_s, "config": {"workload": args.workload,
+                                                      "pairs": shape["pairs"]},
                "clocks": clk.summary()}
         del graph
         return out
 
-    # ---- per-phase timing for the roofline
+    roof = roofline(eng, args.workload, args.precision, flush, stream,
+                    rebins / (2.0 * args.steps))
+    out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32+kahan pair sums, fp64 state" if eng.f32 else "fp64",
+           "data": "synthetic",
+           "config": {"workload": args.workload, "description": wl["desc"],
+                      "particles": N, "precision": args.precision,
+                      "pairs": shape["pairs"], "stencil": shape["stencil"],
+                      "lanes": shape["lanes"], "pair_block": shape["pair_block"],
+                      "list_batch": shape["list_batch"], "skin_margin": eng.skin_margin,
+                      "cuda_graph": graph is not None,
+                      "timed_steps": f"steps {start_step + 1}..{start_step + args.steps} of "
+                                     "the run from the initial state",
+                      "l2": "flushed (256 MiB write) between timed steps",
+                      "parallelism": f"replicas x{world}"},
+           "steps_per_s": steps_per_s,
+           "rebins_per_stage": rebins / (2.0 * args.steps),
+           "autotune": ({"chosen": {k: tune.get(k) for k in ("pairs", "stencil", "lanes",
+                                                              "pair_block", "list_batch",
+                                                              "skin_margin")},
+                         "table": tune["table"]} if tune else None),
+           "pairs_per_step": pairs / args.steps,
+           "gpu_launches": launches_per_step(eng) * args.steps,
+           "roofline": roof, "clocks": clk.summary()}
+    del graph
+    if rank == 0:
+        if args.workload == "dam_break":
+            out["full_run"] = full_run(wl, args.precision, shape, dev, stream, 2000)
+        if args.precision == "fp32c":
+            out["fp64_gpu"] = fp64_comparison(args, wl, shape, flush, stream, dev)
+            out["fp64_gpu"]["fp32c_speedup_steps"] = steps_per_s / out["fp64_gpu"]["steps_per_s"]
+        out["e2e"] = e2e_facade(wl, args, shape, dev, stream)
+        out["e2e"]["engine_api"] = e2e_engine(eng, stream, dev, args)
+        del eng
+        torch.cuda.empty_cache()
+        if args.workload == "dam_break":
+            out["batched"] = batched_config(dev, flush, stream)
+            out["adjoint"] = adjoint_measure(dev, stream)
+            out["other_configs"] = other_configs(dev, flush, stream)
+        if not args.no_cpu:
+            out["cpu_baseline"] = cpu_baseline(args, shape, dev)
+    return out
+
+
+def roofline(eng, workload_name, precision, flush, stream, rebins_per_stage):
+    """Per-kernel times (each alone, L2 flushed) and the HBM roofline of the
+    dominant kernel: its algorithmic bytes per particle times the particles
+    of one launch, over its CUDA-event launch time, against the measured copy
+    peak.  A stage's time weighs the kept-cells and rebinning variants by
+    the rebin rate of the timed steps."""
     kern = kernel_times(eng, flush, stream)
-    byts = algorithmic_bytes(wl["dim"], eng.f32)
-    rate = kern["rebins_per_stage"]
-    dens = kern.get("density_list", kern["density_record"])
-    # share of a step: each phase's time times how often a stage runs it;
-    # with the stage fused, the force pass carries the stage's bytes too
+    byts = algorithmic_bytes(eng.dim, eng.f32)
+    rate = rebins_per_stage
     fused = "force_stage" in kern
     t_force = kern["force_stage"] if fused else kern["force"]
-    per_stage = {"density": (1 - rate) * dens + rate * kern["density_record"],
+    per_stage = {"density": (1 - rate) * kern["density"] + rate * kern["density_record"],
                  "force": t_force,
                  "bin": rate * kern["rebin"] + (1 - rate) * kern.get("bin_kept", 0.0)}
     if not fused:
@@ -399,24 +483,23 @@ def run_ours(args, rank, world, local):
     else:
         byts = dict(byts, force=byts["force"] + byts["pc_stage"])
     dominant = max(per_stage, key=lambda k: per_stage[k])
-    per_launch = {"density": dens, "force": t_force, "pc_stage": kern["pc_stage"],
+    per_launch = {"density": kern["density"], "force": t_force, "pc_stage": kern["pc_stage"],
                   "bin": kern["rebin"]}
     hbm, which = peaks()
-    ach = byts[dominant] * N / (per_launch[dominant] * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC.get((args.workload, args.precision, dominant))
+    ach = byts[dominant] * eng.N / (per_launch[dominant] * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC.get((workload_name, precision, eng.pairs, dominant))
     roof = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
             "peak": hbm, "peak_kind": which, "unit": "GB/s",
             "frac": round(ach / hbm, 4), "traffic": traffic,
             "traffic_note": ("dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu "
-                             "capture of this workload and launch shape; includes the "
-                             "neighbour lists, which the algorithmic bytes exclude as "
-                             "scratch") if traffic else None,
+                             "capture of this workload and launch shape") if traffic else None,
             "per_kernel_ms": {k: round(v, 5) for k, v in kern.items()},
+            "per_stage_ms": {k: round(v, 5) for k, v in per_stage.items()},
             "bytes_per_particle": byts}
-    # the pair passes are bound by FP32 issue: their FP32 flop rate against
-    # the measured FMA peak, and the issue-active fraction ncu saw
-    peaks_c = fma_peaks(dev)
-    fp = NCU_FP32.get((args.workload, args.precision, dominant))
+    # the pair passes are bound by instruction issue: their FP32 flop rate
+    # against the measured FMA peak, and the issue-active fraction ncu saw
+    peaks_c = fma_peaks(eng.device)
+    fp = NCU_FP32.get((workload_name, precision, eng.pairs, dominant))
     if fp:
         ach_c = fp["flops"] / (per_launch[dominant] * 1e-3) / 1e12
         roof["compute"] = {"bound": "fp32", "achieved": round(ach_c, 2),
@@ -426,96 +509,110 @@ def run_ours(args, rank, world, local):
                            "note": ("flops per launch from one ncu capture; peak from "
                                     "sphb_fma_probe on this GPU")}
     roof["fma_peaks_measured"] = {k: round(v, 2) for k, v in peaks_c.items()}
-
-    out = {"metric": METRIC, "value": value, "unit": "pair-interactions/s",
-           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None,
-           "dtype": "fp32+kahan pair sums, fp64 state" if eng.f32 else "fp64",
-           "data": "synthetic",
-           "config": {"workload": args.workload, "description": wl["desc"],
-                      "particles": N, "precision": args.precision,
-                      "stencil": args.stencil, "lanes": lanes, "pair_block": pb,
-                      "list_batch": lb, "skin_margin": eng.skin_margin,
-                      "cuda_graph": graph is not None,
-                      "l2": "flushed (256 MiB write) between timed steps",
-                      "parallelism": f"replicas x{world}"},
-           "steps_per_s": steps_per_s,
-           "autotune": ({"chosen": {k: tune.get(k) for k in ("stencil", "lanes", "pair_block",
-                                                              "list_batch", "skin_margin")},
-                         "table": tune["table"]} if tune else None),
-           "pairs_per_step": pairs / args.steps,
-           "gpu_launches": launches_per_step(eng) * args.steps,
-           "roofline": roof, "clocks": clk.summary()}
-
-    if rank == 0:
-        if args.precision == "fp32c":
-            out["fp64_gpu"] = fp64_comparison(args, wl, eng, flush, stream, dev)
-            out["fp64_gpu"]["fp32c_speedup_steps"] = steps_per_s / out["fp64_gpu"]["steps_per_s"]
-        out["e2e"] = e2e(eng, wl, stream, dev, args)
-        if args.workload == "dam_break":
-            out["adjoint"] = adjoint_measure(dev, stream)
-            out["other_configs"] = other_configs(dev, flush, stream)
-        if not args.no_cpu:
-            out["cpu_baseline"] = cpu_baseline(args)
-    del graph
-    return out
+    return roof
 
 
-def timed_steps(eng, steps, flush, stream, graph=True):
-    """ms per PC step of an engine (CUDA graph replay, L2 flushed between
-    steps, events around each step) and pair-interactions per step."""
+def full_run(wl, precision, shape, dev, stream, steps):
+    """The workload's whole run: `steps` PC steps from the initial state (a
+    fresh engine), replayed from one captured graph in chunks timed with CUDA
+    events (no L2 flush: the state, ~200 MB, exceeds the L2), with the
+    device's rebin count over the run."""
     import torch
-    for _ in range(3):
-        eng.pc_step()
-    g = None
-    if graph:
-        s = torch.cuda.Stream(eng.device)
-        s.wait_stream(stream)
-        with torch.cuda.stream(s):
-            eng.pc_step()
-        stream.wait_stream(s)
-        torch.cuda.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            eng.pc_step()
-        torch.cuda.synchronize()
+    eng = make_engine(wl, precision, shape, dev)
     eng.reset_pair_counts()
+    eng.pc_step()                       # step 1 (eager)
+    g = capture_step(eng, stream)       # steps 2 (warm-up) and 3 (capture)
+    done = 3
     tot = 0.0
-    for _ in range(steps):
-        flush.zero_()
+    chunk = 100
+    while done < steps:
+        n = min(chunk, steps - done)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        if g is not None:
+        for _ in range(n):
             g.replay()
-        else:
-            eng.pc_step()
         b.record(stream)
         torch.cuda.synchronize()
         tot += a.elapsed_time(b)
+        done += n
     eng.check_status()
+    st = eng.scene_state()[0]
     pd, pf = eng.pair_counts()
-    del g
-    return tot / steps, (pd + pf) / steps
+    rebins = eng.device_rebins()
+    timed = steps - 3
+    out = {"steps": steps, "timed_steps": timed, "ms_per_step": tot / timed,
+           "steps_per_s": timed / (tot * 1e-3), "simulated_time_s": st.t,
+           "pairs_per_step": (pd + pf) / steps,
+           "rebins_per_stage": rebins / (2.0 * steps),
+           "note": "steps 4..N timed (graph replays, L2 not flushed); rebins counted by the "
+                   "device decisions over all N steps"}
+    del g, eng
+    torch.cuda.empty_cache()
+    return out
+
+
+def batched_config(dev, flush, stream, steps=500):
+    """256 elliptical drops (N_s ~ U[1k, 20k]) advanced together, one launch
+    per kernel over all scenes, under a captured CUDA graph: the autotuned
+    shape, `steps` steps timed with CUDA events, per-kernel times and the
+    roofline of the dominant kernel; the FP64 path on its own autotuned shape
+    beside it."""
+    import torch
+
+    class A:
+        pass
+    args = A()
+    args.lanes = args.pair_block = args.stencil = args.list_batch = 0
+    args.pairs = "auto"
+    wl = workload("batched")
+    out = {"workload": wl["desc"]}
+    for prec, nsteps in (("fp32c", steps), ("fp64", max(50, steps // 10))):
+        shape, tune = launch_shape(wl, prec, args, dev)
+        eng = make_engine(wl, prec, shape, dev)
+        eng.pc_step()
+        g = capture_step(eng, stream)
+        eng.reset_pair_counts()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(nsteps):
+            g.replay()
+        b.record(stream)
+        torch.cuda.synchronize()
+        eng.check_status()
+        ms = a.elapsed_time(b) / nsteps
+        pd, pf = eng.pair_counts()
+        rebins = eng.device_rebins()
+        del g
+        r = {"particles": eng.N, "scenes": eng.S, "steps": nsteps, "ms_per_step": ms,
+             "steps_per_s": 1e3 / ms, "pair_interactions_per_s": (pd + pf) / nsteps / (ms / 1e3),
+             "rebins_per_stage": rebins / (2.0 * nsteps),
+             "shape": shape, "cuda_graph": True,
+             "l2": "not flushed (the state, ~1.7 GB, exceeds the L2)"}
+        if prec == "fp32c":
+            r["roofline"] = roofline(eng, "batched", prec, flush, stream,
+                                     r["rebins_per_stage"])
+        out[prec] = r
+        del eng
+        torch.cuda.empty_cache()
+    out["fp32c_speedup_steps"] = out["fp32c"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    return out
 
 
 def other_configs(dev, flush, stream):
     """The other workloads, briefly: the dam break with the continuity
     equation and XSPH (the reference example's scheme), the elliptical drop
-    (5,025), 256 batched drops and the 3D 128^3 lattice (one evaluation),
-    each FP32C and FP64."""
+    (5,025) and the 3D 128^3 lattice (one evaluation), each FP32C and FP64."""
     import torch
     from pysph_b200.engine import Engine
     out = {}
-    for name, steps in (("dam_break_continuity", 100), ("drop", 50), ("batched", 10)):
+    for name, steps in (("dam_break_continuity", 100), ("drop", 50)):
         wl = workload(name)
         for prec in ("fp32c", "fp64"):
-            # launch shapes and skins measured on B200 for these workloads
+            # launch shapes measured on B200 for these workloads
             shape = {"dam_break_continuity": dict(lanes=1, pair_block=256, stencil=1),
-                     "drop": dict(lanes=1, pair_block=128, stencil=1),
-                     "batched": dict(lanes=1, pair_block=128, stencil=1,
-                                     skin_margin=0.25)}[name]
+                     "drop": dict(lanes=1, pair_block=128, stencil=1)}[name]
             eng = Engine(wl["scenes"], wl["scheme"], dim=2, precision=prec, device=dev,
                          **shape)
             ms, pairs = timed_steps(eng, steps, flush, stream)
@@ -529,11 +626,11 @@ def other_configs(dev, flush, stream):
         # the launch shapes measured best for this lattice on B200: cells of
         # half the support, 1 lane per particle (FP32C) or 2 (FP64).  One
         # evaluation reuses no lists, so they carry no skin (the density pass
-        # records them for the force pass of the same evaluation): 3.34 ->
-        # 2.71 ms FP32C against the stepping engines' skin of 0.15
+        # records them for the force pass of the same evaluation)
         eng = Engine(wl["scenes"], wl["scheme"], dim=3, precision=prec,
                      lanes=1 if prec == "fp32c" else 2, pair_block=128, stencil=2,
                      step_lists=False, device=dev)
+
         # one evaluation: rebin + SPHRho + SPHPressureGradient
         def one():
             eng.bin(0)
@@ -560,6 +657,33 @@ def other_configs(dev, flush, stream):
         del eng
         torch.cuda.empty_cache()
     return out
+
+
+def timed_steps(eng, steps, flush, stream, graph=True):
+    """ms per PC step of an engine (CUDA graph replay, L2 flushed between
+    steps, events around each step) and pair-interactions per step."""
+    import torch
+    for _ in range(3):
+        eng.pc_step()
+    g = capture_step(eng, stream) if graph else None
+    eng.reset_pair_counts()
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        if g is not None:
+            g.replay()
+        else:
+            eng.pc_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    eng.check_status()
+    pd, pf = eng.pair_counts()
+    del g
+    return tot / steps, (pd + pf) / steps
 
 
 def adjoint_measure(dev, stream):
@@ -617,12 +741,12 @@ def launches_per_step(eng):
 def kernel_times(eng, flush, stream, reps=20):
     """Device time of each phase of the step, each timed alone with CUDA
     events around its own launches on the engine's stream and the L2
-    flushed (256 MiB write) before every launch: density reading the lists,
-    density searching cells and recording them (the stage after a rebin),
-    force from the lists, pc_stage, a full rebin, and a kept-lists rebin
-    decision (a captured graph of that bin call, whose kernels return at
-    once).  Then the device's rebin decisions over real steps give the rate
-    at which stages rebin."""
+    flushed (256 MiB write) before every launch: the density pass of a stage
+    that keeps its cells (lists: reading them; tiled: the same pass as every
+    stage), the density pass after a rebin (lists: searching cells and
+    recording them), force, pc_stage, the force pass with the stage fused, a
+    full rebin, and a kept-cells rebin decision (a captured graph of that bin
+    call, whose kernels return at once)."""
     import torch
     from pysph_b200 import _native as nat
 
@@ -645,9 +769,11 @@ def kernel_times(eng, flush, stream, reps=20):
     eng.bin(nat.BIN_MOVE_INITIAL)
     out["density_record"] = timed(lambda: eng.call("sphb_density", eng.cur, rho,
                                                    nat.DENSITY_EOS))
-    if eng.list_cap:
-        out["density_list"] = timed(lambda: eng.call(
+    if eng.list_cap and eng.pairs == "lists":
+        out["density"] = timed(lambda: eng.call(
             "sphb_density", eng.cur, rho, nat.DENSITY_EOS | nat.DENSITY_USE_LIST))
+    else:
+        out["density"] = out["density_record"]
     out["force"] = timed(lambda: eng.call("sphb_momentum", eng.cur, eng.scheme.mom_dests,
                                           1, mode_f))
     out["pc_stage"] = timed(lambda: eng.pc_stage(0))
@@ -660,7 +786,7 @@ def kernel_times(eng, flush, stream, reps=20):
         out["force_stage"] = timed(lambda: eng.call("sphb_momentum", eng.cur, dests, 1, mode_s))
     out["rebin"] = timed(lambda: eng.bin(nat.BIN_MOVE_INITIAL))
     if eng.step_lists:
-        # positions at the anchors: the decision keeps the lists every time
+        # positions at the anchors: the decision keeps the cells every time
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(eng.device)
         s.wait_stream(stream)
@@ -683,140 +809,178 @@ def kernel_times(eng, flush, stream, reps=20):
         assert eng.rebin_count() == 0
         del g
     out["step_begin"] = timed(eng.step_begin)
-    # rebin rate of real steps
-    rebins = 0
-    steps = 20
-    for _ in range(steps):
-        rec = {}
-        eng.pc_step(on_half=lambda: rec.__setitem__("s", eng.rebin_count()))
-        rebins += rec["s"] + eng.rebin_count()
     eng.check_status()
-    out["rebins_per_stage"] = (rebins / (2.0 * steps)) if eng.step_lists else 1.0
     return out
 
 
-def fp64_comparison(args, wl, eng32, flush, stream, dev):
-    """The plain FP64 GPU path on the same workload and the FP32C density
-    error against it after one step from the same state."""
+def fp64_comparison(args, wl, shape32, flush, stream, dev):
+    """The plain FP64 GPU path on the same workload, on its own autotuned
+    launch shape (and, for comparison, on the FP32C shape), timed like the
+    FP32C line: one captured step replayed, L2 flushed between steps."""
     import torch
-    from pysph_b200.engine import Engine
-    e64 = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision="fp64",
-                 stencil=args.stencil, lanes=eng32.lanes, pair_block=eng32.pair_block,
-                 device=dev)
-    e32 = Engine(wl["scenes"], wl["scheme"], dim=wl["dim"], precision="fp32c",
-                 stencil=args.stencil, lanes=eng32.lanes, pair_block=eng32.pair_block,
-                 device=dev)
-    e64.pc_step()
-    e32.pc_step()
-    err = 0.0
-    for a in range(e64.A):
-        r64 = e64.get(a, "rho")
-        r32 = e32.get(a, "rho")
-        err = max(err, float(((r32 - r64).abs() / r64.abs()).max().item()))
-    del e32
-    # same method as the FP32C line: one captured step replayed, L2 flushed
-    # between steps, events around each step
+    shape64, tune64 = launch_shape(wl, "fp64", args, dev, force_tune=True)
     k = max(10, args.steps // 4)
+    e64 = make_engine(wl, "fp64", shape64, dev)
+    for _ in range(max(args.warmup, 3)):
+        e64.pc_step()
     ms, pairs = timed_steps(e64, k, flush, stream, graph=True)
     del e64
+    # the FP32C shape on FP64 (lists only: the tiled passes are FP32C)
+    same = dict(shape32, pairs="lists")
+    e64b = make_engine(wl, "fp64", same, dev)
+    for _ in range(max(args.warmup, 3)):
+        e64b.pc_step()
+    ms_b, _ = timed_steps(e64b, k, flush, stream, graph=True)
+    del e64b
     torch.cuda.empty_cache()
     return {"steps_per_s": 1e3 / ms, "value": pairs / (ms / 1e3),
             "unit": "pair-interactions/s", "steps": k, "cuda_graph": True,
-            "rho_rel_err_fp32c_vs_fp64": err}
+            "shape": shape64, "autotune_table": tune64["table"] if tune64 else None,
+            "steps_per_s_on_fp32c_shape": 1e3 / ms_b, "fp32c_shape": same}
 
 
-def e2e(eng, wl, stream, dev, args):
-    """Through the public engine API with host buffers: every step uploads
-    the fluid state (x, y, u, v) from pinned host memory, advances one PC
-    step and reads back x, y, u, v, rho, p into pinned host memory.  The
-    copies run on two copy streams, double-buffered on the device, so the
-    upload of the next step's state and the read-back of the last step's
-    results overlap the current step's kernels; the device part of a step
-    (state in, the PC step, results out) is one CUDA graph per buffer.
-    Reported in the metric's unit (pair-interactions/s, the kernels' own
-    pair counts) and in steps/s."""
+def e2e_engine(eng, stream, dev, args):
+    """Through the engine API with host buffers driving the state: every
+    step uploads the fluid's x, y, u, v from pinned host memory -- the values
+    the previous step read back -- advances one PC step, and reads x, y, u,
+    v, rho, p back into pinned host memory.  The step depends on the last
+    read-back, so the copies cannot overlap the kernels."""
     import torch
     a = 0
     n = eng.user_n[a]
-    ins = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in ("x", "y", "u", "v")}
-    outs = {k: torch.empty(n, dtype=torch.float64).pin_memory()
-            for k in ("x", "y", "u", "v", "rho", "p")}
-    for k in ins:
-        ins[k].copy_(eng.get(a, k).cpu())
+    names_in = ("x", "y", "u", "v")
+    names_out = ("x", "y", "u", "v", "rho", "p")
+    host = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in names_out}
+    for k in names_out:
+        host[k].copy_(eng.get(a, k).cpu())
     f64 = dict(dtype=torch.float64, device=dev)
-    dev_in = [{k: torch.empty(n, **f64) for k in ins} for _ in range(2)]
-    dev_out = [{k: torch.empty(n, **f64) for k in outs} for _ in range(2)]
-    h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
-    ev = lambda: torch.cuda.Event()
-    in_ready, in_free = [ev(), ev()], [ev(), ev()]
-    out_ready, out_free = [ev(), ev()], [ev(), ev()]
-    k_steps = max(10, args.steps // 4)
+    dev_in = {k: torch.empty(n, **f64) for k in names_in}
+    dev_out = {k: torch.empty(n, **f64) for k in names_out}
 
-    def upload(b):
-        h2d.wait_event(in_free[b])
-        with torch.cuda.stream(h2d):
-            for k in ins:
-                dev_in[b][k].copy_(ins[k], non_blocking=True)
-        in_ready[b].record(h2d)
-
-    def device_step(b):
-        for k in ins:
-            eng.exchange_in(a, k, dev_in[b][k])
+    def device_step():
+        for k in names_in:
+            eng.exchange_in(a, k, dev_in[k])
         eng.invalidate_box()
         eng.pc_step()
-        for k in outs:
-            eng.exchange_out(a, k, out=dev_out[b][k])
+        for k in names_out:
+            eng.exchange_out(a, k, out=dev_out[k])
 
-    # one graph per buffer, captured after an eager warm-up of each (on the
-    # real state)
-    for b in range(2):
-        for k in ins:
-            dev_in[b][k].copy_(ins[k])
-    graphs = []
-    for b in range(2):
-        device_step(b)
-        torch.cuda.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            device_step(b)
-        graphs.append(g)
+    for k in names_in:
+        dev_in[k].copy_(host[k])
+    device_step()
     torch.cuda.synchronize()
-
-    for e in in_free + out_free:
-        e.record(stream)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        device_step()
     torch.cuda.synchronize()
+    k_steps = max(10, args.steps // 4)
     eng.reset_pair_counts()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    upload(0)
-    for i in range(k_steps):
-        b = i % 2
-        stream.wait_event(in_ready[b])
-        stream.wait_event(out_free[b])   # the read-back two steps ago is done
-        graphs[b].replay()
-        in_free[b].record(stream)
-        out_ready[b].record(stream)
-        if i + 1 < k_steps:
-            upload(1 - b)
-        d2h.wait_event(out_ready[b])
-        with torch.cuda.stream(d2h):
-            for k in outs:
-                outs[k].copy_(dev_out[b][k], non_blocking=True)
-        out_free[b].record(d2h)
-    stream.wait_stream(d2h)
+    for _ in range(k_steps):
+        for k in names_in:
+            dev_in[k].copy_(host[k], non_blocking=True)
+        g.replay()
+        for k in names_out:
+            host[k].copy_(dev_out[k], non_blocking=True)
     t1.record(stream)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     pd, pf = eng.pair_counts()
+    rebins = eng.device_rebins()
     eng.check_status()
-    del graphs
+    del g
     return {"value": (pd + pf) / (ms / 1e3), "unit": "pair-interactions/s",
-            "steps_per_s": k_steps / (ms / 1e3),
-            "h2d_bytes_per_step": 8 * n * len(ins),
-            "d2h_bytes_per_step": 8 * n * len(outs), "steps": k_steps,
-            "note": ("state uploaded and results read back every step, on copy streams "
-                     "overlapping the kernels")}
+            "steps_per_s": k_steps / (ms / 1e3), "steps": k_steps,
+            "rebins_per_stage": rebins / (2.0 * k_steps),
+            "h2d_bytes_per_step": 8 * n * len(names_in),
+            "d2h_bytes_per_step": 8 * n * len(names_out),
+            "note": "each step uploads the state the previous step read back (in stream "
+                    "order), one CUDA graph for the device part"}
+
+
+def e2e_facade(wl, args, shape, dev, stream):
+    """Through the reference-facing API with host (numpy) arrays: the dam
+    break's ParticleArrays, Particles, the Solver's operations (SPHRho,
+    TaitEquation, MomentumEquation, GravityForce, PositionStepping) and
+    PredictorCorrectorIntegrator.integrate with the device CFL rule.  Every
+    step sets the fluid's x, y, u, v from numpy arrays (the values the last
+    step read back), integrates, and reads x, y, u, v, rho, p back into
+    numpy arrays."""
+    import torch
+    from pysph_b200.base import api as base
+    from pysph_b200.solver import api as solver
+    from pysph_b200.sph import api as sph
+    from pysph_b200.base.particle_types import ParticleType
+    if args.workload != "dam_break":
+        return {"value": None, "note": "the facade run is the dam break's"}
+    arrays, p = wl["scenes"][0]
+    prec = "single" if args.precision == "fp32c" else "double"
+    f = base.get_particle_array(name="fluid", type=ParticleType.Fluid, cl_precision=prec,
+                                **{k: v for k, v in arrays[0].items()})
+    w = base.get_particle_array(name="wall", type=ParticleType.Solid, cl_precision=prec,
+                                **{k: v for k, v in arrays[1].items()})
+    particles = base.Particles([f, w])
+    particles.engine_options = {k: v for k, v in shape.items() if v is not None}
+    Fluid, Solid = ParticleType.Fluid, ParticleType.Solid
+    s = solver.Solver(dim=2, integrator_type=solver.PredictorCorrectorIntegrator)
+    s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid, Solid],
+                                        from_types=[Fluid, Solid], updates=["rho"], id="sd"))
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=p["c0"], ro=p["rho0"]),
+                                        on_types=[Fluid, Solid], updates=["p", "cs"],
+                                        id="eos"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=p["alpha"], beta=p["beta"]), on_types=[Fluid],
+        from_types=[Fluid, Solid], updates=["u", "v"], id="mom"))
+    s.add_operation(solver.SPHIntegration(sph.GravityForce.withargs(gy=p["gravity"][1]),
+                                          on_types=[Fluid], updates=["u", "v"], id="grav"))
+    s.add_operation_step([Fluid])
+    s.set_time_step(p["dt_initial"])
+    s.setup(particles)
+    integ = s.integrator
+    assert integ.plan is not None, "the dam break's scheme runs fused on the engine"
+    sess = integ._fused_session()
+    sess.engine.update_params(cfl=p["cfl"], c0=p["c0"], dt_initial=p["dt_initial"])
+    integ.plan.params = sess.engine.params[0]
+    names_out = ("x", "y", "u", "v", "rho", "p")
+    host = {k: f.get(k).cpu().numpy().copy() for k in names_out}
+
+    def step():
+        f.set(x=host["x"], y=host["y"], u=host["u"], v=host["v"])
+        integ.integrate(0.0, device_dt=True)
+        for k in names_out:
+            host[k] = f.get(k).cpu().numpy()
+
+    for _ in range(3):
+        step()
+    k_steps = max(10, args.steps // 4)
+    eng = particles.session().engine
+    eng.reset_pair_counts()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(k_steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    pd, pf = eng.pair_counts()
+    rebins = eng.device_rebins()
+    eng.check_status()
+    n = f.get_number_of_particles()
+    out = {"value": (pd + pf) / (ms / 1e3), "unit": "pair-interactions/s",
+           "steps_per_s": k_steps / (ms / 1e3), "steps": k_steps,
+           "rebins_per_stage": rebins / (2.0 * k_steps),
+           "h2d_bytes_per_step": 8 * n * 4, "d2h_bytes_per_step": 8 * n * len(names_out),
+           "api": "ParticleArray.set(numpy) -> PredictorCorrectorIntegrator.integrate "
+                  "(device CFL dt) -> ParticleArray.get -> numpy, every step",
+           "shape": particles.engine_options}
+    particles.session().detach()
+    del s, integ, particles, f, w
+    torch.cuda.empty_cache()
+    return out
 
 
 def oracle_systems(name, threads):
@@ -866,18 +1030,92 @@ def oracle_run(name, steps, warmup, threads, max_scenes=None):
             "steps_per_s": steps / dt, "particles": n, "desc": wl["desc"]}
 
 
-def cpu_baseline(args):
+def cpu_baseline(args, shape=None, dev=None):
     """The oracle port (C, 1 thread) on a bounded sample of the workload:
-    a few full steps (about 10-20 s of CPU work)."""
+    a few full steps (about 10-20 s of CPU work).  On the dam break the same
+    leg also checks the bench's FP32C engine and the FP64 GPU path against
+    the FP64 oracle (parity_vs_oracle)."""
     steps = {"dam_break": 16, "drop": 100, "lattice3d": 1, "batched": 2}[args.workload]
     scenes = 16 if args.workload == "batched" else None
     r = oracle_run(args.workload, steps, 1, threads=1, max_scenes=scenes)
     sample = f"{steps} PC steps of {r['desc']}"
     if scenes:
         sample += f" (first {scenes} scenes)"
-    return {"value": r["value"], "unit": "pair-interactions/s", "cores": 1,
-            "kind": "port", "sample": sample, "steps_per_s": r["steps_per_s"],
-            "cpu": cpu_model()}
+    out = {"value": r["value"], "unit": "pair-interactions/s", "cores": 1,
+           "kind": "port", "sample": sample, "steps_per_s": r["steps_per_s"],
+           "cpu": cpu_model()}
+    if args.workload == "dam_break" and shape is not None:
+        out["parity_vs_oracle"] = parity_vs_oracle(shape, dev)
+    return out
+
+
+def parity_vs_oracle(shape, dev):
+    """Per-quantity errors of the GPU engines against the FP64 oracle on the
+    2D dam break (332,018 particles): the first evaluation (rho, p of fluid
+    and walls; the fluid's accelerations, with gravity, and dt_fac) and two
+    predictor-corrector steps with the CFL time step (dt, positions in
+    particle spacings, velocities relative to the largest, densities).  The
+    FP32C engine runs the bench's launch shape."""
+    import torch
+    threads = os.cpu_count() or 1
+    out = {}
+    for prec in ("fp32c", "fp64"):
+        wl = workload("dam_break")
+        arrays, p = wl["scenes"][0]
+        sh = dict(shape) if prec == "fp32c" else dict(shape, pairs="lists")
+        eng = make_engine(wl, prec, sh, dev)
+        _, systems = oracle_systems("dam_break", threads)
+        osys = systems[0][0]
+        osys.update()
+        osys.eval()
+        eng.eval_stage()
+        eng.check_status()
+        B = p["c0"] ** 2 * p["rho0"] / p["gamma"]
+        r = {}
+        for a in range(2):
+            O = osys.arrays[a]
+            r[f"rho{a}_max_rel"] = float(np.max(np.abs(eng.get(a, "rho").cpu().numpy() - O.rho)
+                                                / np.abs(O.rho)))
+            r[f"p{a}_max_abs_over_B"] = float(np.max(np.abs(eng.get(a, "p").cpu().numpy() - O.p))
+                                              / B)
+        O = osys.arrays[0]
+        scale = max(np.max(np.abs(O.au)), np.max(np.abs(O.av)))
+        for n, ref in (("au", O.au), ("av", O.av)):
+            r[f"{n}_max_abs_over_max"] = float(np.max(np.abs(eng.get(0, n).cpu().numpy() - ref))
+                                               / scale)
+        # (at rest every dt_fac is 0: the absolute error then)
+        r["dt_fac_max_abs_over_max"] = float(
+            np.max(np.abs(eng.get(0, "dt_fac").cpu().numpy() - O.dt_fac))
+            / (np.max(O.dt_fac) or 1.0))
+        del eng
+        eng = make_engine(wl, prec, sh, dev)
+        _, systems = oracle_systems("dam_break", threads)
+        osys, po = systems[0]
+        dts = []
+        for _ in range(2):
+            dt = osys.cfl_time_step(po["cfl"], po["c0"], po["dt_initial"])
+            osys.pc_step(dt)
+            eng.pc_step()
+            dts.append(abs(eng.scene_state()[0].dt - dt) / dt)
+        eng.check_status()
+        O = osys.arrays[0]
+        r["step2_dt_max_rel"] = max(dts)
+        for n in ("x", "y"):
+            r[f"step2_{n}_max_abs_over_dx"] = float(
+                np.max(np.abs(eng.get(0, n).cpu().numpy() - getattr(O, n))) / 0.0025)
+        vs = max(np.max(np.abs(O.u)), np.max(np.abs(O.v)))
+        for n in ("u", "v"):
+            r[f"step2_{n}_max_abs_over_max"] = float(
+                np.max(np.abs(eng.get(0, n).cpu().numpy() - getattr(O, n))) / vs)
+        for a in range(2):
+            Oa = osys.arrays[a]
+            r[f"step2_rho{a}_max_rel"] = float(
+                np.max(np.abs(eng.get(a, "rho").cpu().numpy() - Oa.rho) / np.abs(Oa.rho)))
+        out[prec] = r
+        del eng
+        torch.cuda.empty_cache()
+    out["oracle"] = "oracle/sph_oracle.c (FP64), all host threads"
+    return out
 
 
 def cpu_model():

@@ -251,7 +251,9 @@ typedef struct {
     unsigned long long *pairs;  /* [4]  pairs evaluated: density, force;
                                    [2]: blocks of the tiled passes that read
                                    their records from global memory (their
-                                   ranges exceeded the shared memory); [3]: - */
+                                   ranges exceeded the shared memory); [3]:
+                                   rebins the device decisions ran
+                                   (SPHB_BIN_IF_NEEDED) */
 } sphb_work;
 
 /* Everything the kernels see.  Tables are device pointers. */

@@ -59,10 +59,11 @@ class Session:
                     d[name] = pa.properties[name]
             d["tag"] = pa.properties["tag"]
             specs.append(d)
+        opts = dict(lanes=lanes, pair_block=pair_block)
+        opts.update(particles.engine_options)
         self.engine = Engine([(specs, self.params)], scheme, dim=dim,
-                             precision=precision, lanes=lanes, pair_block=pair_block,
-                             device=arrays[0].device, variable_h=particles.variable_h,
-                             kernel=kernel)
+                             precision=precision, device=arrays[0].device,
+                             variable_h=particles.variable_h, kernel=kernel, **opts)
         self.valid = {}
         for a, pa in enumerate(arrays):
             for name in IMPORTABLE:
@@ -273,6 +274,11 @@ class Particles:
         self.max_radius_scale = max_radius_scale
         self.precision = precision or ("fp32c" if prec == "single" else "fp64")
         self.kernel = None
+        # launch shape of the engine behind these arrays (this build's own
+        # option, no reference counterpart): Engine keyword arguments such
+        # as pairs, stencil, lanes, pair_block, skin_margin, e.g. from
+        # pysph_b200.autotune.autotune
+        self.engine_options: dict = {}
         self.correction_manager = None
         self.misc_prop_update_functions = []
         self.nnps_manager = NNPSManager(self)

@@ -62,6 +62,7 @@ __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
         const bool keep = at_anchor || (lists && !s_far);
         e.work.meta[1] = keep ? 0 : 1;
         e.work.meta[2] = (keep && lists) ? 1 : 0;
+        if (!keep) e.work.pairs[3] += 1ull;   // rebins decided on the device
         // inside a captured graph: run the rebin's conditional body or not
         if (set_cond) cudaGraphSetConditional(cond, keep ? 0u : 1u);
     }

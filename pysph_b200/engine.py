@@ -829,6 +829,13 @@ class Engine:
         off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
         return int(self.work_buf[off + 16:off + 24].view(torch.int64).item())
 
+    def device_rebins(self) -> int:
+        """Rebins the device's decisions ran since the last
+        reset_pair_counts (each captured or eager SPHB_BIN_IF_NEEDED bin that
+        did not keep the cells)."""
+        off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
+        return int(self.work_buf[off + 24:off + 32].view(torch.int64).item())
+
     def reset_pair_counts(self):
         off = self.work_offsets[nat.WORK_NAMES.index("pairs")]
         self.work_buf[off:off + 32].zero_()

@@ -196,7 +196,7 @@ def test_dam_break_cfl(precision):
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
 def test_batched_scenes_match_single(precision):
     scenes = W.batched_drops(num_scenes=5, seed=1, n_lo=300, n_hi=1500)
-    specs = [(arrs, dict(p, dt=1e-5)) for arrs, _, p in scenes]
+    specs = [(arrs, p) for arrs, _, p in scenes]
     eng = Engine(specs, fluid_scheme(1), dim=2, precision=precision, lanes=4)
     for _ in range(4):
         eng.pc_step()
@@ -204,7 +204,7 @@ def test_batched_scenes_match_single(precision):
     for s, (arrs, p) in enumerate(specs):
         osys = oracle_from(arrs, p, fluid_scheme(1), 2)
         for _ in range(4):
-            osys.pc_step(1e-5)
+            osys.pc_step(p["dt"])
         x = eng.get(0, "x", scene=s).cpu().numpy()
         rho = eng.get(0, "rho", scene=s).cpu().numpy()
         assert traj_err(x, osys.arrays[0].x, arrs[0]["h"]) <= TRAJ_TOL[precision]

@@ -230,7 +230,7 @@ def test_batched_256_scenes_two_steps(precision):
     """All 256 drops (about 2.9 M particles) advanced together for two PC
     steps; every scene against its own oracle."""
     scenes = W.batched_drops(num_scenes=256, seed=0)
-    specs = [(arrs, dict(p, dt=1e-5)) for arrs, _, p in scenes]
+    specs = [(arrs, p) for arrs, _, p in scenes]
     eng = Engine(specs, fluid_scheme(1), dim=2, precision=precision, lanes=1,
                  pair_block=128, stencil=1)
     for _ in range(2):
@@ -244,7 +244,7 @@ def test_batched_256_scenes_two_steps(precision):
     for s, (arrs, p) in enumerate(specs):
         osys = oracle_from(arrs, p, fluid_scheme(1), 2)
         for _ in range(2):
-            osys.pc_step(1e-5)
+            osys.pc_step(p["dt"])
         O = osys.arrays[0]
         n = len(O.x)
         sl = slice(int(off[s]), int(off[s]) + n)

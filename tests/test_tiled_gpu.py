@@ -153,7 +153,7 @@ def test_tiled_graph_replay_matches_eager():
 def test_tiled_batched_scenes():
     """Many scenes of uneven size in one launch per pass."""
     scenes = W.batched_drops(num_scenes=12, seed=3, n_lo=300, n_hi=3000)
-    specs = [(arrs, dict(p, dt=1e-5)) for arrs, _, p in scenes]
+    specs = [(arrs, p) for arrs, _, p in scenes]
     eng = Engine(specs, fluid_scheme(1), dim=2, precision="fp32c", pairs="tiled")
     for _ in range(3):
         eng.pc_step()
@@ -161,7 +161,7 @@ def test_tiled_batched_scenes():
     for s, (arrs, p) in enumerate(specs):
         osys = oracle_from(arrs, p, fluid_scheme(1), 2)
         for _ in range(3):
-            osys.pc_step(1e-5)
+            osys.pc_step(p["dt"])
         O = osys.arrays[0]
         rho = eng.get(0, "rho", scene=s).cpu().numpy()
         x = eng.get(0, "x", scene=s).cpu().numpy()
