@@ -389,7 +389,12 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
  * then GravityForce when with_gravity; writes au/av/aw and dt_fac and the
  * per-scene max dt_fac and |a|^2.  S/sph/funcs/pressure_funcs.pyx:246-391,
  * .clt:69-157; S/sph/funcs/external_force.pyx:13-62.
- * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV).
+ * mode: 0 = MomentumEquation, 1 = SPHPressureGradient (:62-161, no AV),
+ * 2 = the split-form MonaghanArtificialViscosity alone
+ * (S/sph/funcs/viscosity_funcs.pyx:19-157): a += -m_b Pi_ab grad W when
+ * v_ab . r_ab < 0, with scene.eta as its eta (the reference's constructor
+ * never sets it, so its callers pass 0), and dt_fac with 0.01 h_ab^2 in the
+ * denominator whatever eta is.
  * mode | SPHB_FORCE_USE_LIST: iterate the lists of the last sphb_density
  * pass (same bin, same sources) instead of searching cells. */
 #define SPHB_FORCE_USE_LIST 16

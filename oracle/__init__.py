@@ -73,6 +73,8 @@ class _System(ctypes.Structure):
         ("xsph_eps", ctypes.c_double),
         ("variable_h", ctypes.c_int32), ("hks", ctypes.c_int32),
         ("kernel", ctypes.c_int32), ("pad2_", ctypes.c_int32),
+        ("split_av", ctypes.c_int32), ("pad3_", ctypes.c_int32),
+        ("av_eta", ctypes.c_double),
     ]
 
 # kernel type ids (KernelBase.get_type, S/base/kernels.pyx:31-40) and the
@@ -117,6 +119,9 @@ def lib():
         L.orc_momentum.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, dp, dp, dp, dp]
+        L.orc_monaghan_av.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, dp, dp, dp, dp]
         L.orc_pgrad.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
                                 ctypes.c_int, dp, dp, dp]
         L.orc_density_rate.argtypes = [P(_System), ctypes.c_void_p, ctypes.c_int,
@@ -183,13 +188,15 @@ class OracleSystem:
 
     rho_src / rate_src / mom_src / xsph_src map a dest array index to the
     list of its source array indices; tait_on / step_on list array
-    indices."""
+    indices.  split_av: the momentum is SPHPressureGradient then
+    MonaghanArtificialViscosity (eta = av_eta) on the mom_src pairs."""
 
     def __init__(self, arrays, dim=2, rho_src=None, tait_on=(), mom_src=None,
                  step_on=(), c0=1.0, rho0=1000.0, gamma=7.0, alpha=1.0,
                  beta=1.0, eta=0.1, gravity=(0.0, 0.0, 0.0), nthreads=0,
                  radius_scale=2.0, cell_scale=2.0, rate_src=None, xsph_src=None,
-                 xsph_eps=0.5, variable_h=False, hks=False, kernel=CUBIC_SPLINE):
+                 xsph_eps=0.5, variable_h=False, hks=False, kernel=CUBIC_SPLINE,
+                 split_av=False, av_eta=0.0):
         self.arrays = list(arrays)
         assert 1 <= len(self.arrays) <= MAX_ARRAYS
         self.dim = dim
@@ -211,6 +218,10 @@ class OracleSystem:
         s.xsph_eps = xsph_eps
         s.variable_h = int(bool(variable_h))
         s.hks = int(bool(hks))
+        # split momentum: SPHPressureGradient + MonaghanArtificialViscosity
+        # (its eta is 0 unless assigned, as in the reference)
+        s.split_av = int(bool(split_av))
+        s.av_eta = float(av_eta)
         if kernel not in KERNEL_RADIUS:
             raise ValueError("kernel must be 1 (cubic), 3 (quintic) or 4 (Wendland)")
         if kernel != CUBIC_SPLINE and dim != 2:
@@ -297,6 +308,13 @@ class OracleSystem:
         rc = lib().orc_momentum(ctypes.byref(self._s), self._c, d, s, alpha,
                                 beta, eta, _dptr(o1), _dptr(o2), _dptr(o3),
                                 _dptr(dt_fac))
+        assert rc == 0
+
+    def monaghan_av(self, d, s, alpha, beta, eta, o1, o2, o3, dt_fac):
+        """MonaghanArtificialViscosity (split form) of dest d from source s,
+        added into o1..o3; dt_fac takes the max."""
+        rc = lib().orc_monaghan_av(ctypes.byref(self._s), self._c, d, s, alpha, beta, eta,
+                                   _dptr(o1), _dptr(o2), _dptr(o3), _dptr(dt_fac))
         assert rc == 0
 
     def pgrad(self, d, s, o1, o2, o3):

@@ -31,6 +31,8 @@
  *   TaitEquation ................... S/sph/funcs/eos_funcs.pyx:88-129
  *   MomentumEquation ............... S/sph/funcs/pressure_funcs.pyx:246-391
  *   SPHPressureGradient ............ S/sph/funcs/pressure_funcs.pyx:62-161
+ *   MonaghanArtificialViscosity .... S/sph/funcs/viscosity_funcs.pyx:19-157
+ *                                    (the split form; its quirks kept)
  *   GravityForce, PositionStepping . S/sph/funcs/external_force.pyx:13-62,
  *                                    S/sph/funcs/position_funcs.pyx:10-56
  *   SPHFunction.eval (+= / tag) .... S/sph/sph_func.pyx:208-227
@@ -84,6 +86,13 @@ typedef struct {
     int32_t hks;               /* kernels averaged over h_a and h_b */
     int32_t kernel;            /* get_type(): 1 cubic, 3 quintic, 4 Wendland */
     int32_t pad2_;
+    /* split momentum: SPHPressureGradient then MonaghanArtificialViscosity
+     * (S/sph/funcs/viscosity_funcs.pyx:19-157) on the mom_src pairs, with
+     * the viscosity's own eta (av_eta; the reference never sets it: 0),
+     * instead of MomentumEquation */
+    int32_t split_av;
+    int32_t pad3_;
+    double av_eta;
 } orc_system;
 
 typedef struct {
@@ -819,6 +828,73 @@ int orc_momentum(const orc_system *s, const orc_nnps *c, int da, int sa,
     return 0;
 }
 
+/* MonaghanArtificialViscosity.eval_nbr (S/sph/funcs/viscosity_funcs.pyx:
+ * 75-157), the split form of the momentum equation's viscous term: per
+ * neighbour, dt_fac = max |h_ab dot / (r_ab^2 + 0.01 h_ab^2)| (the 0.01 is
+ * written into the reference, :103) and, when dot < 0, a += -m_b Pi_ab
+ * grad W(h_ab) with mu = h_ab dot / (r_ab^2 + eta^2 h_ab^2), where eta is
+ * the function's attribute, which its constructor never sets (:30-45), so
+ * 0 unless the caller assigns it. */
+int orc_monaghan_av(const orc_system *s, const orc_nnps *c, int da, int sa,
+                    double alpha, double beta, double eta, double *out1,
+                    double *out2, double *out3, double *dt_fac)
+{
+    const orc_array *D = &s->a[da];
+    const orc_array *S = &s->a[sa];
+    const int64_t *off = c->off[da][sa];
+    const int32_t *idx = c->idx[da][sa];
+    if (!off) return -1;
+    int dim = s->dim;
+    double kfac = kern_fac(s, dim);
+    set_threads(s);
+#pragma omp parallel for schedule(dynamic, 512)
+    for (int64_t i = 0; i < D->n; ++i) {
+        if (D->tag[i] != 0) { out1[i] = out2[i] = out3[i] = 0; continue; }
+        double nr0 = 0.0, nr1 = 0.0, nr2 = 0.0;
+        double ha = D->h[i];
+        double ca = D->cs[i];
+        double rhoa = D->rho[i];
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+            int32_t j = idx[k];
+            double hb = S->h[j];
+            double hab = 0.5 * (ha + hb);
+            double cb = S->cs[j];
+            double rx = D->x[i] - S->x[j];
+            double ry = D->y[i] - S->y[j];
+            double rz = D->z[i] - S->z[j];
+            double vx = D->u[i] - S->u[j];
+            double vy = D->v[i] - S->v[j];
+            double vz = D->w[i] - S->w[j];
+            double dot = vx * rx + vy * ry + vz * rz;
+            double rab2 = rx * rx + ry * ry + rz * rz;
+            double dtf = fabs(hab * dot / (rab2 + 0.01 * hab * hab));
+            dt_fac[i] = dt_fac[i] < dtf ? dtf : dt_fac[i];
+            double rhob = S->rho[j];
+            double mb = S->m[j];
+            double piab = 0;
+            if (dot < 0) {
+                double cab = 0.5 * (ca + cb);
+                double rhoab = 0.5 * (rhoa + rhob);
+                double mu = hab * dot;
+                mu /= (rab2 + eta * eta * hab * hab);
+                piab = -alpha * cab * mu + beta * mu * mu;
+                piab /= rhoab;
+            }
+            double tmp = piab;
+            tmp *= -mb;
+            double g[3];
+            pair_grad(s, D, i, S, j, hab, dim, kfac, g);
+            nr0 += tmp * g[0];
+            nr1 += tmp * g[1];
+            nr2 += tmp * g[2];
+        }
+        out1[i] += nr0;
+        out2[i] += nr1;
+        out3[i] += nr2;
+    }
+    return 0;
+}
+
 int orc_pgrad(const orc_system *s, const orc_nnps *c, int da, int sa,
               double *out1, double *out2, double *out3)
 {
@@ -990,8 +1066,35 @@ int orc_eval(orc_system *s, const orc_nnps *c)
                 s->pairs += c->off[d][a][D->n];
             }
     }
+    /* the split form: SPHPressureGradient's calc, then
+     * MonaghanArtificialViscosity's (its to_reset clears dt_fac), each
+     * adding into the accelerations source by source */
+    if (s->split_av) {
+        for (int d = 0; d < s->narrays; ++d) {
+            if (!s->mom_src[d]) continue;
+            const orc_array *D = &s->a[d];
+            for (int a = 0; a < s->narrays; ++a)
+                if (s->mom_src[d] & (1u << a)) {
+                    rc = orc_pgrad(s, c, d, a, D->au, D->av, D->aw);
+                    if (rc) return rc;
+                    s->pairs += c->off[d][a][D->n];
+                }
+        }
+        for (int d = 0; d < s->narrays; ++d) {
+            if (!s->mom_src[d]) continue;
+            const orc_array *D = &s->a[d];
+            for (int64_t i = 0; i < D->n; ++i) D->dt_fac[i] = 0.0;
+            for (int a = 0; a < s->narrays; ++a)
+                if (s->mom_src[d] & (1u << a)) {
+                    rc = orc_monaghan_av(s, c, d, a, s->alpha, s->beta, s->av_eta, D->au,
+                                         D->av, D->aw, D->dt_fac);
+                    if (rc) return rc;
+                    s->pairs += c->off[d][a][D->n];
+                }
+        }
+    }
     /* accelerations were reset by reset_accelerations; dt_fac by to_reset */
-    for (int d = 0; d < s->narrays; ++d) {
+    for (int d = 0; d < s->narrays && !s->split_av; ++d) {
         if (!s->mom_src[d]) continue;
         const orc_array *D = &s->a[d];
         for (int64_t i = 0; i < D->n; ++i) D->dt_fac[i] = 0.0;

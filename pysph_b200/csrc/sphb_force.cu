@@ -21,7 +21,7 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
     if (rc) return rc;
     if ((rc = check_pair_cfg(e))) return rc;
     const int fmode = mode & ~(SPHB_FORCE_USE_LIST | SPHB_FORCE_NO_MAXIMA | SPHB_FORCE_STAGE_MASK);
-    if (fmode != 0 && fmode != 1) return SPHB_ERR_ARG;
+    if (fmode != 0 && fmode != 1 && fmode != 2) return SPHB_ERR_ARG;
     const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
     if (kind > 3) return SPHB_ERR_ARG;
     if (kind >= 0) {
@@ -40,7 +40,7 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
         }
     }
     if (!e->f.au || !e->f.av || (e->cfg.dim == 3 && !e->f.aw)) return SPHB_ERR_ARG;
-    if ((mode & 15) == 0 && !e->f.dt_fac) return SPHB_ERR_ARG;
+    if ((fmode == 0 || fmode == 2) && !e->f.dt_fac) return SPHB_ERR_ARG;
     for (int a = 0; a < SPHB_MAX_ARRAYS; ++a) {
         if (e->cfg.rate_src[a] && !e->f.drho) return SPHB_ERR_ARG;
         if (e->cfg.xsph_src[a] && (!e->f.xu || !e->f.xv || (e->cfg.dim == 3 && !e->f.xw)))

@@ -32,7 +32,8 @@ namespace sphb {
 // dests get 0), gravity, dt_fac, the per-scene CFL maxima, the integrator
 // stage fused into the epilogue (FP32C) and the pair count.  Every thread
 // of the block calls it (block reductions inside); acc, dtf, drho and xs
-// are valid in lane 0 of each dest.
+// are valid in lane 0 of each dest; visc: the pass has a viscous term
+// and writes dt_fac.
 template <int DIM, bool F32, bool CONT>
 __device__ __forceinline__ void force_finish(const sphb_engine &e, int cur, int k, int s, int a,
                                              bool active, int lane, double *acc, double dtf,
@@ -169,6 +170,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
     const sphb_scene &sc = e.scene[s];
     const int *__restrict__ start = e.work.start;
     const bool visc = (mode & 15) == 0;
+    // split-form MonaghanArtificialViscosity alone (no pressure terms)
+    const bool avisc = (mode & 15) == 2;
     // reuse the density pass's lists (recorded over list_sources); without
     // the per-source filter they must hold the momentum sources exactly
     const bool use_list = (mode & SPHB_FORCE_USE_LIST) && e.f.list_cap > 0 && e.f.nbr &&
@@ -230,7 +233,7 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                 r.g = __ldg(geo + j);
                 r.t = __ldg(th + j);
                 r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
-                if (visc || CONT) {
+                if (visc || avisc || CONT) {
                     if (DIM == 2) {
                         const float2 vv = __ldg((const float2 *)e.f.vel + j);
                         r.vx = vv.x;
@@ -278,7 +281,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         hab = 0.5f * (hk + hj);
                         eh2 = eta2 * hab * hab;
                     }
-                    float tmp = tk.w + r.t.w;   // P_a/rho_a^2 + P_b/rho_b^2
+                    // P_a/rho_a^2 + P_b/rho_b^2 (none in the split viscosity)
+                    float tmp = avisc ? 0.f : tk.w + r.t.w;
                     const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
                     float dot = vx * rx + vy * ry;
                     if (DIM == 3) dot += vz * rz;
@@ -323,9 +327,13 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         }
                         if (!mom_on) return;
                     }
-                    if (visc) {
+                    if (visc || avisc) {
                         const float mu = __fdividef(hab * dot, r2 + eh2);
-                        dtmax = fmaxf(dtmax, fabsf(mu));
+                        // the split viscosity's dt_fac has 0.01 h_ab^2 written in
+                        // (viscosity_funcs.pyx:103) whatever its eta
+                        dtmax = fmaxf(dtmax, fabsf(avisc ? __fdividef(hab * dot,
+                                                                       r2 + 0.01f * hab * hab)
+                                                         : mu));
                         // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
                         // when v_ab . r_ab < 0, i.e. mu < 0; else 0: min(mu, 0)
                         const float mn = fminf(mu, 0.f);
@@ -460,15 +468,18 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
                         }
                         if (!(mm & bit)) return;
                     }
-                    double tmp = Pa * rhoa2 + Pb * (1.0 / (rhob * rhob));
-                    if (visc) {
+                    // P_a/rho_a^2 + P_b/rho_b^2; the split viscosity has none
+                    // (tmp = piab; tmp *= -mb, viscosity_funcs.pyx:125-126)
+                    double tmp = avisc ? 0.0 : Pa * rhoa2 + Pb * (1.0 / (rhob * rhob));
+                    if (visc || avisc) {
                         const double vx = uk - __ldg(B.u + j);
                         const double vy = vk - __ldg(B.v + j);
                         const double vz = DIM == 3 ? wk - __ldg(B.w + j) : 0.0;
                         double dot = vx * rx + vy * ry;
                         if (DIM == 3) dot += vz * rz;
                         const double den = rab2 + eta * eta * hab * hab;
-                        dtf = fmax(dtf, fabs(hab * dot / den));
+                        dtf = fmax(dtf, fabs(hab * dot /
+                                             (avisc ? rab2 + 0.01 * hab * hab : den)));
                         if (dot < 0) {
                             const double cab = 0.5 * (ca + __ldg(csnd + j));
                             const double rhoab = 0.5 * (rhoa + rhob);
@@ -498,8 +509,8 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         }
     }
 
-    force_finish<DIM, F32, CONT>(e, cur, k, s, a, active, lane, acc, dtf, drho, xs, visc, mm,
-                                 rm, xm, with_gravity, mode, np);
+    force_finish<DIM, F32, CONT>(e, cur, k, s, a, active, lane, acc, dtf, drho, xs,
+                                 visc || avisc, mm, rm, xm, with_gravity, mode, np);
 }
 
 template <int KT, int DIM, bool F32, int LV, int RV>

@@ -399,7 +399,8 @@ k_density_tiled(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_ma
     density_finish<true>(e, cur, k, s, a, active, 0, acc.value(), flags & SPHB_DENSITY_EOS, np);
 }
 
-// MomentumEquation (mode 0) / SPHPressureGradient (mode 1) + gravity, with
+// MomentumEquation (mode 0) / SPHPressureGradient (mode 1) / the split
+// MonaghanArtificialViscosity (mode 2) + gravity, with
 // the stage in the epilogue (2D FP32C, tiled).  Dynamic shared memory: cap
 // float4 geo and thermo records, cap float2 velocities, then TILE_LCAP x
 // blockDim.x list entries.  With SPHB_FORCE_USE_LIST and the density pass of
@@ -440,6 +441,7 @@ k_force_tiled(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
     const sphb_scene &sc = e.scene[s];
     const sphb_scene_state &st = e.sstate[s];
     const bool visc = (mode & 15) == 0;
+    const bool avisc = (mode & 15) == 2;   // split-form viscosity alone
     // the density pass's per-stage lists hold this array's SPHRho sources
     const bool use_list = (mode & SPHB_FORCE_USE_LIST) && e.f.list_cap > 0 && e.f.nbr &&
                           e.f.nbr_cnt && e.cfg.rho_src[a] == mm;
@@ -509,13 +511,16 @@ k_force_tiled(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
                         gw = Kern<KT>::gw_bf(r2 * ir * ih, ir, ih, kf * ih * ih * ih);
                     }
                     ++np;
-                    float tmp = tk.w + t.w;   // P_a/rho_a^2 + P_b/rho_b^2
-                    if (visc) {
+                    // P_a/rho_a^2 + P_b/rho_b^2 (none in the split viscosity)
+                    float tmp = avisc ? 0.f : tk.w + t.w;
+                    if (visc || avisc) {
                         const float2 vb = SH ? s_vel[en.j] : __ldg(vel + en.j);
                         const float vx = uk - vb.x, vy = vvk - vb.y;
                         const float dot = vx * rx + vy * ry;
                         const float mu = __fdividef(hab * dot, r2 + eh2);
-                        dtmax = fmaxf(dtmax, fabsf(mu));
+                        dtmax = fmaxf(dtmax, fabsf(avisc ? __fdividef(hab * dot,
+                                                                       r2 + 0.01f * hab * hab)
+                                                         : mu));
                         // Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab when mu < 0
                         const float mn = fminf(mu, 0.f);
                         const float cab = 0.5f * (tk.z + t.z);
@@ -560,8 +565,8 @@ k_force_tiled(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
     if (tr.fallback && threadIdx.x == 0) atomicAdd(&e.work.pairs[2], 1ull);
     double acc[3] = {ax.value(), ay.value(), 0.0};
     const double xs[3] = {0.0, 0.0, 0.0};
-    force_finish<2, true, false>(e, cur, k, s, a, active, 0, acc, (double)dtmax, 0.0, xs, visc,
-                                 mm, 0u, 0u, with_gravity, mode, np);
+    force_finish<2, true, false>(e, cur, k, s, a, active, 0, acc, (double)dtmax, 0.0, xs,
+                                 visc || avisc, mm, 0u, 0u, with_gravity, mode, np);
 }
 
 // Shared-memory slots of a tiled block: the (2R+1) rows of T dests plus

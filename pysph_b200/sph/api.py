@@ -3,10 +3,11 @@ path and SPHCalc."""
 from .sph_calc import SPHCalc
 from .sph_func import (Function, SPHFunction, SPHFunctionParticle,
                        CSPHFunctionParticle, SPHRho, TaitEquation,
-                       MomentumEquation, SPHPressureGradient, GravityForce,
+                       MomentumEquation, SPHPressureGradient,
+                       MonaghanArtificialViscosity, GravityForce,
                        PositionStepping, SPHDensityRate, XSPHCorrection)
 
 __all__ = ["SPHCalc", "Function", "SPHFunction", "SPHFunctionParticle",
            "CSPHFunctionParticle", "SPHRho", "TaitEquation", "MomentumEquation",
-           "SPHPressureGradient", "GravityForce", "PositionStepping",
+           "SPHPressureGradient", "MonaghanArtificialViscosity", "GravityForce", "PositionStepping",
            "SPHDensityRate", "XSPHCorrection"]

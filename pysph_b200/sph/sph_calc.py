@@ -146,9 +146,10 @@ def evaluate(calc: SPHCalc, outs):
     elif op == "tait":
         eng.tait(dest_mask=1 << a)
         fields = ["p", "cs"]
-    elif op in ("momentum", "pgrad"):
+    elif op in ("momentum", "pgrad", "avisc"):
         with eng.masks(mom_src={a: src_mask}):
-            eng.momentum(dest_mask=1 << a, gravity=False, mode=0 if op == "momentum" else 1)
+            eng.momentum(dest_mask=1 << a, gravity=False,
+                         mode={"momentum": 0, "pgrad": 1, "avisc": 2}[op])
         fields = ["_a_u_1", "_a_v_1", "_a_w_1"][:dim]
     elif op == "density_rate":
         # the force pass with only its SPHDensityRate term on
@@ -168,7 +169,7 @@ def evaluate(calc: SPHCalc, outs):
         _apply(dest, outs[k], res, tag)
         s.valid[(a, field)] = (outs[k] == field and not calc.integrates
                                and calc.reset_arrays)
-    if op == "momentum":
+    if op in ("momentum", "avisc"):
         res = eng.exchange_out(a, "dt_fac")
         if not dest.has_array("dt_fac"):
             dest.add_property({"name": "dt_fac"})

@@ -10,6 +10,7 @@ evaluates the pair sums.  Each class declares what the engine runs for it:
   TaitEquation         p, cs from rho               sphb_tait
   MomentumEquation     pressure gradient + Monaghan  sphb_momentum (mode 0)
   SPHPressureGradient  pressure gradient            sphb_momentum (mode 1)
+  MonaghanArtificialViscosity  split-form viscosity  sphb_momentum (mode 2)
   GravityForce         += g                         integrator / SPHCalc
   PositionStepping     dx/dt = v                    integrator / SPHCalc
 """
@@ -170,6 +171,39 @@ class MomentumEquation(SPHFunctionParticle):
 
     def params(self):
         return {"alpha": self.alpha, "beta": self.beta, "eta": self.eta}
+
+
+class MonaghanArtificialViscosity(SPHFunctionParticle):
+    """The split form of Monaghan's artificial viscosity, for schemes that
+    pair it with SPHPressureGradient: a_a += -m_b Pi_ab grad W_ab when
+    v_ab . r_ab < 0, and dt_fac (S/sph/funcs/viscosity_funcs.pyx:19-157).
+
+    Kept as the reference has it: the constructor takes eta but never
+    stores it, so the viscosity's eta is 0 until the attribute is assigned,
+    and its dt_fac uses 0.01 h_ab^2 whatever eta is.  gamma is accepted and
+    unused."""
+
+    engine_op = "avisc"
+
+    def __init__(self, source, dest, setup_arrays=True, alpha=1, beta=1, gamma=1.4,
+                 eta=0.1, **kwargs):
+        SPHFunctionParticle.__init__(self, source, dest, setup_arrays, **kwargs)
+        self.alpha = float(alpha)
+        self.beta = float(beta)
+        self.gamma = float(gamma)
+        self.eta = 0.0          # the eta argument is not stored (see above)
+        self.id = "momavisc"
+        self.tag = "velocity"
+        self.to_reset = ["dt_fac"]
+        if dest is not None and not dest.has_array("dt_fac"):
+            dest.add_property({"name": "dt_fac"})
+
+    def set_src_dst_reads(self):
+        self.src_reads = ["x", "y", "z", "h", "m", "rho", "u", "v", "w", "cs"]
+        self.dst_reads = ["x", "y", "z", "h", "p", "u", "v", "w", "cs", "rho", "tag"]
+
+    def params(self):
+        return {"alpha": self.alpha, "beta": self.beta, "eta": float(self.eta)}
 
 
 class SPHPressureGradient(SPHFunctionParticle):

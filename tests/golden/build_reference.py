@@ -1,7 +1,11 @@
 """Build the reference's own FP64 Cython particle path (PySPH 0.9beta) in a
 scratch directory, to generate the golden fixtures of tests/golden.
 
-    python tests/golden/build_reference.py [--ref /root/reference] [--out _work/refbuild]
+    python tests/golden/build_reference.py --ref <reference checkout> [--out oracle/_ref/refbuild]
+
+The reference location comes from --ref or the PYSPH_REFERENCE environment
+variable (there is no default); the build goes to oracle/_ref/refbuild,
+which git ignores.
 
 The snapshot is Python 2 / Cython 0.14-era and must be patched mechanically
 to build with Python 3.12 and Cython 3: Python-2 syntax and dict methods in
@@ -209,7 +213,10 @@ def build(ref, out):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--out", default=os.path.join(ROOT, "_work", "refbuild"))
+    ap.add_argument("--ref", default=os.environ.get("PYSPH_REFERENCE"),
+                    help="the reference checkout (default: $PYSPH_REFERENCE)")
+    ap.add_argument("--out", default=os.path.join(ROOT, "oracle", "_ref", "refbuild"))
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("name the reference checkout with --ref or PYSPH_REFERENCE")
     print(build(a.ref, a.out))

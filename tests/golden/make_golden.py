@@ -1,6 +1,7 @@
 """Write the golden fixtures of tests/golden from the reference itself.
 
-    python tests/golden/build_reference.py      # patched build in _work/refbuild
+    python tests/golden/build_reference.py --ref <reference checkout>
+                                                # patched build in oracle/_ref/refbuild
     python tests/golden/make_golden.py          # writes tests/golden/*.npz
 
 Every fixture is computed by the reference's own FP64 Cython path, through
@@ -21,6 +22,9 @@ ViscousAndForceBasedTimeStep, with the solver loop's order of calls
                   SPHRho and SPHPressureGradient
   dam.npz         dam break at dx = 0.05 with walls: 5 steps with the CFL
                   time step (the dt sequence and the final state)
+  avisc.npz       the split-form MonaghanArtificialViscosity: the unit square,
+                  and a drop scheme with SPHPressureGradient + the viscosity
+                  (first stage and 5 steps)
 """
 from __future__ import annotations
 
@@ -51,12 +55,13 @@ def ref_modules(build_dir):
     import pysph.sph.funcs.position_funcs as POS
     import pysph.sph.funcs.external_force as EF
     import pysph.sph.funcs.xsph_funcs as X
+    import pysph.sph.funcs.viscosity_funcs as V
     import pysph.solver.sph_equation as EQ
     import pysph.solver.integrator as I
     import pysph.solver.time_step_functions as T
     from pysph.base.point import Point
     return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T, X=X,
-                Point=Point)
+                V=V, Point=Point)
 
 
 def make_array(R, props, name, ptype):
@@ -424,9 +429,80 @@ def kernels(R):
     return out
 
 
+def avisc(R):
+    """The split-form MonaghanArtificialViscosity (S/sph/funcs/
+    viscosity_funcs.pyx:19-157): on the 4-particle unit square (alpha =
+    beta = 1, with the constructor's eta = 0.1 ignored and, once, the
+    attribute set to 0.1 by hand), and in a scheme of its own on the
+    elliptical drop at dx = 0.05 -- SPHRho, TaitEquation, then
+    SPHPressureGradient and MonaghanArtificialViscosity (alpha 0.1, beta 0)
+    both integrating u, v, and PositionStepping: the first stage's
+    accelerations and dt_fac, and 5 predictor-corrector steps of dt = 1e-5."""
+    out = {}
+    x = np.array([0, 0, 1, 1], np.float64)
+    y = np.array([0, 1, 1, 0], np.float64)
+    kernel = R["K"].CubicSplineKernel(dim=2)
+    for name, eta_attr in (("square", None), ("square_eta", 0.1)):
+        pa = R["PA"].get_particle_array(name="test", x=x.copy(), y=y.copy(), z=np.zeros(4),
+                                        m=np.ones(4), u=np.array([1, 0, 0, -1.0]),
+                                        v=np.array([0, 0.5, 0, 0.25]), h=np.ones(4),
+                                        p=np.array([0, 0, 1, 1.0]),
+                                        cs=np.array([1.0, 2.0, 0.5, 1.5]),
+                                        rho=np.array([1.0, 1.5, 0.98, 1.1]))
+        particles = R["P"].Particles([pa])
+        f = R["V"].MonaghanArtificialViscosity.withargs(alpha=1.0, beta=1.0, gamma=1.4,
+                                                        eta=0.1).get_func(pa, pa)
+        if eta_attr is not None:
+            f.eta = eta_attr
+        calc = R["C"].SPHCalc(particles, [pa], pa, kernel, [f], ["u", "v"], integrates=True)
+        for n in ("_tmpx", "_tmpy", "_tmpz"):
+            pa.get(n)[:] = 0
+        calc.sph("_tmpx", "_tmpy", "_tmpz")
+        for k, n in enumerate(("_tmpx", "_tmpy", "_tmpz")):
+            out[f"{name}_{k}"] = np.asarray(pa.get(n), np.float64).copy()
+        out[f"{name}_dt_fac"] = np.asarray(pa.get("dt_fac"), np.float64).copy()
+    arrays, types, params = W.elliptical_drop(dx=0.05)
+    EQ, D, E, PF, POS, V = R["EQ"], R["D"], R["E"], R["PF"], R["POS"], R["V"]
+
+    def sim():
+        pas = [make_array(R, arrays[0], "fluid", types[0])]
+        particles = R["P"].Particles(pas)
+        ops = [EQ.SPHOperation(D.SPHRho.withargs(), on_types=[0], from_types=[0],
+                               updates=["rho"], id="sd"),
+               EQ.SPHOperation(E.TaitEquation.withargs(co=params["c0"], ro=params["rho0"]),
+                               on_types=[0], updates=["p", "cs"], id="eos"),
+               EQ.SPHIntegration(PF.SPHPressureGradient.withargs(), on_types=[0],
+                                 from_types=[0], updates=["u", "v"], id="pgrad"),
+               EQ.SPHIntegration(V.MonaghanArtificialViscosity.withargs(
+                   alpha=params["alpha"], beta=params["beta"]), on_types=[0],
+                   from_types=[0], updates=["u", "v"], id="avisc"),
+               EQ.SPHIntegration(POS.PositionStepping.withargs(), on_types=[0],
+                                 updates=["x", "y"], id="step")]
+        calcs = []
+        for op in ops:
+            calcs.extend(op.get_calcs(particles, R["K"].CubicSplineKernel(dim=2)))
+        integ = R["I"].PredictorCorrectorIntegrator(particles, calcs)
+        integ.setup_integrator()
+        return pas, particles, integ
+
+    out.update({f"in_{k}": np.asarray(arrays[0][k]) for k in PROPS})
+    pas, particles, integ = sim()
+    integ.save_initial_arrays()
+    integ.reset_accelerations(step=1)
+    integ.eval()
+    out.update({f"stage0_{n}": np.asarray(pas[0].get(n), np.float64).copy()
+                for n in ("rho", "p", "cs", "_a_u_1", "_a_v_1", "dt_fac")})
+    pas, particles, integ = sim()
+    for _ in range(5):
+        particles.update()
+        integ.integrate(1e-5)
+    out.update({f"step5_{k}": v for k, v in state(pas).items()})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--build", default=os.path.join(ROOT, "_work", "refbuild"))
+    ap.add_argument("--build", default=os.path.join(ROOT, "oracle", "_ref", "refbuild"))
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--only", nargs="*", default=None, help="fixture names to write")
     a = ap.parse_args()
@@ -434,7 +510,7 @@ def main():
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
                      ("drop_cont", drop_cont), ("dam_cont", dam_cont),
                      ("integrators", integrators), ("varh", varh), ("kernels", kernels),
-                     ("varh3d", varh3d)):
+                     ("varh3d", varh3d), ("avisc", avisc)):
         if a.only and name not in a.only:
             continue
         data = fn(R)

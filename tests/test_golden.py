@@ -340,3 +340,49 @@ def test_varh3d_lists_stage_and_steps_bit_exact():
         o.pc_step(1e-4)
     for n in ("x", "y", "z", "u", "v", "w", "rho", "p"):
         np.testing.assert_array_equal(getattr(o.arrays[0], n), g[f"step3_{n}_0"], err_msg=n)
+
+
+# -- the split-form MonaghanArtificialViscosity ---------------------------------
+def test_monaghan_av_square_bit_exact():
+    """The viscosity alone on the unit square, with its eta left unset (0:
+    the constructor ignores its eta argument) and set by hand to 0.1; its
+    dt_fac always uses 0.01 h_ab^2."""
+    g = load("avisc")
+    base = dict(x=np.array([0, 0, 1, 1.0]), y=np.array([0, 1, 1, 0.0]), z=np.zeros(4),
+                m=np.ones(4), u=np.array([1, 0, 0, -1.0]), v=np.array([0, 0.5, 0, 0.25]),
+                h=np.ones(4), p=np.array([0, 0, 1, 1.0]), cs=np.array([1.0, 2.0, 0.5, 1.5]),
+                rho=np.array([1.0, 1.5, 0.98, 1.1]))
+    for name, eta in (("square", 0.0), ("square_eta", 0.1)):
+        o = OracleSystem([OracleArray("t", **base)], dim=2)
+        o.update_pairs([(0, 0)])
+        o3 = [np.zeros(4) for _ in range(3)]
+        dtf = np.zeros(4)
+        o.monaghan_av(0, 0, 1.0, 1.0, eta, *o3, dtf)
+        for k in range(3):
+            np.testing.assert_array_equal(o3[k], g[f"{name}_{k}"], err_msg=(name, k))
+        np.testing.assert_array_equal(dtf, g[f"{name}_dt_fac"], err_msg=name)
+
+
+def _split_drop(g):
+    pa = OracleArray("fluid", **{k: g[f"in_{k}"].copy() for k in PROPS})
+    return OracleSystem([pa], dim=2, rho_src={0: [0]}, tait_on=(0,), mom_src={0: [0]},
+                        step_on=(0,), split_av=True, av_eta=0.0, **DROP)
+
+
+def test_monaghan_av_split_scheme_bit_exact():
+    """SPHRho, Tait, SPHPressureGradient + MonaghanArtificialViscosity (both
+    into _a_u_1, _a_v_1) on the drop: the first stage, then 5 PC steps."""
+    g = load("avisc")
+    o = _split_drop(g)
+    o.update()
+    o.eval()
+    A = o.arrays[0]
+    for name, got in (("rho", A.rho), ("p", A.p), ("cs", A.cs), ("_a_u_1", A.au),
+                      ("_a_v_1", A.av), ("dt_fac", A.dt_fac)):
+        np.testing.assert_array_equal(got, g[f"stage0_{name}"], err_msg=name)
+    o = _split_drop(g)
+    for _ in range(5):
+        o.pc_step(1e-5)
+    A = o.arrays[0]
+    for n in ("x", "y", "u", "v", "rho", "p", "cs"):
+        np.testing.assert_array_equal(getattr(A, n), g[f"step5_{n}_0"], err_msg=n)
