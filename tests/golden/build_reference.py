@@ -9,7 +9,8 @@ which git ignores.
 
 The snapshot is Python 2 / Cython 0.14-era and must be patched mechanically
 to build with Python 3.12 and Cython 3: Python-2 syntax and dict methods in
-the pure-Python modules, numpy aliases, `cpdef inline`, `except -1`
+the pure-Python modules (and, in the output format's reader, numpy.load's
+allow_pickle for the pickled dicts), numpy aliases, `cpdef inline`, `except -1`
 mismatches between .pyx and .pxd, a Cython-3 name-mangling clash, and two
 bugs of the snapshot itself (nnps.pyx reads CellManager.coord_x/y/z, which no
 longer exist; Particles passes max_radius_scale= / periodic_domain= where
@@ -167,6 +168,13 @@ def patch_specific(pkg):
         "radius_scale=self.max_radius_scale")
     sub(os.path.join(B, "particles.py"), r"periodic_domain=self\.periodic_domain",
         "domain=self.periodic_domain")
+    # the output format's reader and writer (S/solver/utils.py): the unused
+    # Python-2 `commands` module, `basestring`, and numpy.load of the
+    # pickled dicts, which numpy >= 1.16.3 refuses without allow_pickle
+    U = os.path.join(pkg, "solver", "utils.py")
+    sub(U, r"^import commands$", "", flags=re.M)
+    sub(U, r"\bbasestring\b", "str")
+    sub(U, r"numpy\.load\(fname\)", "numpy.load(fname, allow_pickle=True)")
     # implicit relative imports of the pure-Python modules
     for f, mods in (("base/particles.py", ["cell", "nnps", "particle_array",
                                             "particle_types", "domain_manager", "locator"]),

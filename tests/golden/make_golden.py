@@ -22,6 +22,10 @@ ViscousAndForceBasedTimeStep, with the solver loop's order of calls
                   SPHRho and SPHPressureGradient
   dam.npz         dam break at dx = 0.05 with walls: 5 steps with the CFL
                   time step (the dt sequence and the final state)
+  npz_ref_read.npz  output format v1 across both implementations: what the
+                  reference's load reads from npz_repo_written.npz (written
+                  here by Solver.dump_output); npz_ref_written.npz is a file
+                  the reference's own savez wrote
   avisc.npz       the split-form MonaghanArtificialViscosity: the unit square,
                   and a drop scheme with SPHPressureGradient + the viscosity
                   (first stage and 5 steps)
@@ -500,6 +504,55 @@ def avisc(R):
     return out
 
 
+def npz_interop(R):
+    """The output format v1 (S/solver/utils.py:34-186, 294-340;
+    S/solver/solver.py:605-695) across the two implementations, on the
+    dam break at dx = 0.1 (fluid and wall arrays) with solver data dt =
+    1e-4, t = 0.25, count = 7:
+
+    * the reference writes npz_ref_written.npz with its own savez, from the
+      dicts its Solver.dump_output assembles (ParticleArray.
+      get_property_arrays);
+    * this build writes npz_repo_written.npz through its Solver.dump_output,
+      and the reference's own load reads it back: what it read is this
+      function's fixture (npz_ref_read.npz)."""
+    import shutil
+    import tempfile
+    sys.path.insert(0, ROOT)
+    import pysph.solver.utils as RU
+    from pysph_b200.base import api as base
+    from pysph_b200.solver.solver import Solver
+    arrays, types, params = W.dam_break(dx=0.1)
+    names = ("fluid", "wall")
+    pas = [make_array(R, a, n, t) for a, n, t in zip(arrays, names, types)]
+    props = {"arrays": {pa.name: pa.get_property_arrays(all=False) for pa in pas},
+             "solver_data": {"dt": 1e-4, "t": 0.25, "count": 7}}
+    RU.savez(os.path.join(HERE, "npz_ref_written.npz"), version=1, **props)
+    rpas = [base.get_particle_array(name=n, type=t, device="cpu",
+                                    **{k: np.asarray(a[k], np.float64) for k in PROPS
+                                       if k in a})
+            for a, n, t in zip(arrays, names, types)]
+    s = Solver(dim=2)
+    s.particles = base.Particles(rpas)
+    s.t, s.count = 0.25, 7
+    tmp = tempfile.mkdtemp()
+    try:
+        s.output_directory = tmp
+        s.fname = "npz_repo_written"
+        path = s.dump_output(1e-4)
+        shutil.copy(path, os.path.join(HERE, "npz_repo_written.npz"))
+    finally:
+        shutil.rmtree(tmp)
+    d = RU.load(os.path.join(HERE, "npz_repo_written.npz"))
+    out = {f"solver_{k}": np.float64(v) for k, v in d["solver_data"].items()}
+    for name, pa in d["arrays"].items():
+        pnames = sorted(pa.properties.keys())
+        out[f"{name}__names"] = np.array(pnames)
+        for p in pnames:
+            out[f"{name}_{p}"] = np.asarray(pa.get(p)).copy()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", default=os.path.join(ROOT, "oracle", "_ref", "refbuild"))
@@ -510,7 +563,7 @@ def main():
     for name, fn in (("square", square), ("drop", drop), ("lattice3d", lattice), ("dam", dam),
                      ("drop_cont", drop_cont), ("dam_cont", dam_cont),
                      ("integrators", integrators), ("varh", varh), ("kernels", kernels),
-                     ("varh3d", varh3d), ("avisc", avisc)):
+                     ("varh3d", varh3d), ("avisc", avisc), ("npz_ref_read", npz_interop)):
         if a.only and name not in a.only:
             continue
         data = fn(R)
