@@ -6,7 +6,9 @@ differentiable-rollout workload: elliptical drop with 50k particles
 (dx = 0.0079), 200 steps of dt = 2e-6, checkpoints every 20 steps, loss =
 mean squared distance of the final positions to those of a run with
 velocity scale 110.  Bars: 1e-6 relative to the autograd gradient (both
-FP64), 1e-4 median relative error against finite differences.
+FP64); 1e-4 relative error against finite differences on every direction
+whose FD is converged (test_adjoint_central_fd_full_rollout states the
+rule).
 """
 import math
 
@@ -142,40 +144,75 @@ def config4_gradient(precision):
 
 
 def test_adjoint_central_fd_full_rollout():
-    """FD in FP64 on 16 random unit directions (seed 0) of the initial
-    velocities, eps = 1e-4 (velocity units, |v| ~ 100).  Bars: median over
-    the directions of |FD - adjoint| / |FD| <= 1e-4, and every direction's
-    |FD - adjoint| <= 1e-5 |grad|.  The second form is the meaningful one
-    per direction: a random direction in 100k dimensions sees ~|grad| / 300
-    of the gradient, some far less, and there the FD's own noise (round-off
-    amplified over 200 stiff steps, pairs crossing the artificial-viscosity
-    switch v.r = 0 between the two evaluations) dominates |FD - adjoint| /
-    |FD|.  Measured on B200: median 8e-5, max 5e-7 |grad|; eps from 1e-3
-    to 1e-5 gives the same floor, 1e-6 and below is round-off bound."""
-    g, v0, xt, arrays, params, n = config4_gradient("fp64")
-    dev = v0.device
-    fd = Rollout(arrays, params, fluid_scheme(1), 2, CONFIG4["dt"], CONFIG4["steps"],
-                 checkpoint_every=CONFIG4["steps"], precision="fp64")
+    """Central FD in FP64 against the adjoint on 16 random unit directions
+    (seed 0) of the initial velocities, on the config-4 rollout.
+
+    The point: the workload's velocities plus a seeded perturbation of
+    1e-4 m/s per component (|v| ~ 100).  The unperturbed drop puts every
+    diagonal lattice pair exactly on the artificial-viscosity switch
+    (v_ab . r_ab = s (dy^2 - dx^2) = 0 for |dx| = |dy|), where the loss has a
+    kink: central differences there average the two one-sided slopes while
+    the adjoint follows the branch the forward takes, a systematic ~1e-4
+    disagreement that no eps removes (measured on B200: 8e-5 median for
+    eps 1e-4 .. 3e-3 at the unperturbed point, 1.2e-5 with the
+    perturbation).
+
+    The rule: a direction is smooth when its FD is converged -- the
+    estimates at eps = 1e-4 and 2e-4 agree to 5e-5 relative, half the bar
+    they are held to; otherwise the
+    stencil crossed a viscosity switch or a neighbour-set change between
+    its two runs (or the directional derivative is so small against
+    |grad| that round-off amplified over 200 stiff steps dominates), and
+    the FD measures that event, not the derivative.  Bars: at least 10 of
+    the 16 directions smooth; every smooth direction |FD - adjoint| <=
+    1e-4 |FD|; every direction |FD - adjoint| <= 1e-5 |grad|."""
+    dx, steps, dt = CONFIG4["dx"], CONFIG4["steps"], CONFIG4["dt"]
+    arrays, params = drop(dx)
+    a = arrays[0]
+    n = len(a["x"])
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(1)
+    v0 = torch.tensor(np.stack([a["u"], a["v"]]), dtype=torch.float64, device=dev)
+    v0 = v0 + 1e-4 * torch.tensor(rng.standard_normal((2, n)), dtype=torch.float64,
+                                  device=dev)
+    tarr, _ = drop(dx, scale=110.0)
+    xt = Rollout(tarr, params, fluid_scheme(1), 2, dt, steps, precision="fp64").forward(
+        {0: torch.tensor(np.stack([tarr[0]["u"], tarr[0]["v"]]), dtype=torch.float64,
+                         device=dev)})[0][0]
+    r = Rollout(arrays, params, fluid_scheme(1), 2, dt, steps, checkpoint_every=20,
+                precision="fp64")
+    v = v0.clone().requires_grad_(True)
+    loss = ((RolloutFunction.apply(v, r) - xt) ** 2).sum() / n
+    loss.backward()
+    g = v.grad
+    fd = Rollout(arrays, params, fluid_scheme(1), 2, dt, steps, checkpoint_every=steps,
+                 precision="fp64")
 
     def L(vv):
         xf = fd.forward({0: vv})[0][0]
         return float(((xf - xt) ** 2).sum() / n)
 
+    def central(d, eps):
+        return (L(v0 + eps * d) - L(v0 - eps * d)) / (2 * eps)
+
     rng = np.random.default_rng(0)
-    eps = 1e-4
     gnorm = float(torch.linalg.norm(g))
-    errs, errs_g = [], []
+    rows = []
     for _ in range(16):
         d = torch.tensor(rng.standard_normal((2, n)), dtype=torch.float64, device=dev)
         d /= torch.linalg.norm(d)
-        fdv = (L(v0 + eps * d) - L(v0 - eps * d)) / (2 * eps)
+        f1, f2 = central(d, 1e-4), central(d, 2e-4)
         adv = float((g * d).sum())
-        errs.append(abs(fdv - adv) / max(abs(fdv), 1e-30))
-        errs_g.append(abs(fdv - adv) / gnorm)
-    print("FD relative errors:", errs)
-    print("FD errors / |grad|:", errs_g)
-    assert np.median(errs) <= 1e-4, errs
-    assert np.max(errs_g) <= 1e-5, errs_g
+        conv = abs(f1 - f2) / max(abs(f1), 1e-300)
+        rows.append(dict(smooth=conv <= 5e-5, conv=conv,
+                         rel=abs(f1 - adv) / max(abs(f1), 1e-300),
+                         abs_g=abs(f1 - adv) / gnorm, proj=adv / gnorm))
+    for row in rows:
+        print("FD direction:", row)
+    smooth = [r_ for r_ in rows if r_["smooth"]]
+    assert len(smooth) >= 10, rows
+    assert max(r_["rel"] for r_ in smooth) <= 1e-4, rows
+    assert max(r_["abs_g"] for r_ in rows) <= 1e-5, rows
 
 
 def test_adjoint_fp32c_forward_gradient():
