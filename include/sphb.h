@@ -507,7 +507,9 @@ SPHB_API int sphb_density_vjp(const sphb_engine *e, int cur, uint32_t dest_mask,
 
 /* Neighbour count of every particle of one particle set: counts[i] = number
  * of j (self included) with |x_i - x_j|^2 < (radius_scale * h_i)^2, the FP64
- * predicate of sphb_neighbors; -1 for a particle with a non-finite position.
+ * predicate of sphb_neighbors; -1 for a particle with a non-finite position
+ * (which is then nobody's neighbour) or a non-finite smoothing length (the
+ * others still count it: the predicate takes each particle's own h).
  * x, y, z (z may be NULL when dim == 2), h and counts are device arrays of n
  * elements in the caller's order.
  *
@@ -521,11 +523,16 @@ SPHB_API int sphb_density_vjp(const sphb_engine *e, int cur, uint32_t dest_mask,
  * three int32 arrays of SPHB_STATIC_MAX_PARTICLES), which every GPU that
  * loads the library holds until the process exits.  n above
  * SPHB_STATIC_MAX_PARTICLES returns SPHB_ERR_WORKSPACE; the cell size grows
- * past radius_scale * max h when a grid would need more than 2^19 cells.
+ * past radius_scale * max h when a grid would need more than 2^19 cells or
+ * cell coordinates beyond 2^30 (particles far from the origin), which
+ * lengthens the cell walks but not the counts.  Cost: one pass over the
+ * particles per phase, and one block that scans the cell counts
+ * serially (up to 512 cells per thread at the 2^19-cell maximum).
  * The call allocates nothing (no cudaMalloc, cudaFree or allocating library
  * routine).  Its first call on a device looks up the scratch array's device
  * address with that device current; make that first call before any stream
- * capture.  All calls share the one array, which keeps the last call's
+ * capture.  A cudaDeviceReset leaves that address stale: do not call it on
+ * a device after resetting the device.  All calls share the one array, which keeps the last call's
  * contents, so calls that overlap on the GPU race: serialise them. */
 SPHB_API int sphb_neighbor_counts_static(int32_t n, int32_t dim, const double *x,
                                          const double *y, const double *z,

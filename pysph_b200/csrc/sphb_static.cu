@@ -14,7 +14,10 @@
 //
 // Set-up: the first call on a device looks up the array's device address
 // (cudaGetSymbolAddress, with that device current) and caches it; make that
-// first call on each device before any stream capture.  Every call shares the
+// first call on each device before any stream capture.  cudaDeviceReset
+// unloads the library's device code, so the cached address of that device
+// is then stale: the entry point must not be called on a device after it
+// was reset.  Every call shares the
 // one array and it keeps the last call's contents, so calls that overlap on
 // the GPU (different streams, or different host threads, same device) race:
 // serialise them.  The call allocates nothing.
@@ -131,6 +134,12 @@ __global__ void k_grid(unsigned char *base, Input in)
                 const double flo = floor(lo[d] / cs), fhi = floor(hi[d] / cs);
                 const double span = fhi - flo + 3.0;
                 if (!(span < (double)SPHB_STATIC_MAX_CELLS)) { fits = false; break; }
+                // global cell coordinates must fit an int: particles far
+                // from the origin against the cell size widen the cells
+                if (!(fabs(flo) < 1073741824.0 && fabs(fhi) < 1073741824.0)) {
+                    fits = false;
+                    break;
+                }
                 H.lo[d] = (int)flo - 1;
                 H.n[d] = (int)span;
             } else {
@@ -151,11 +160,14 @@ __global__ void k_grid(unsigned char *base, Input in)
     H.ncells = 0;  // unreachable for finite boxes; counts become -1
 }
 
+// Clears count[0 .. ncells) of the grid k_grid chose (grid-stride: the
+// launch does not know ncells).
 __global__ void __launch_bounds__(256) k_zero(unsigned char *base)
 {
     View v = carve(base);
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < v.hdr->ncells) v.count[c] = 0;
+    const int nc = v.hdr->ncells;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        v.count[c] = 0;
 }
 
 __device__ inline int cell_key(const Header &H, double x, double y, double z, int dim)
@@ -227,7 +239,8 @@ __global__ void __launch_bounds__(256) k_count(unsigned char *base, Input in, in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= in.n) return;
     const int key = v.key[i];
-    if (key < 0) {
+    // a non-finite position has no cell; a non-finite h no support radius
+    if (key < 0 || !isfinite(in.h[i])) {
         counts[i] = -1;
         return;
     }
@@ -304,7 +317,7 @@ extern "C" int sphb_neighbor_counts_static(int32_t n, int32_t dim, const double 
     k_reset<<<1, 32, 0, st>>>(base);
     k_bounds<<<nb, 256, 0, st>>>(base, in);
     k_grid<<<1, 1, 0, st>>>(base, in);
-    k_zero<<<(SPHB_STATIC_MAX_CELLS + 255) / 256, 256, 0, st>>>(base);
+    k_zero<<<148, 256, 0, st>>>(base);   // one block per SM, grid-stride
     k_hash<<<nb, 256, 0, st>>>(base, in);
     k_scan<<<1, 1024, 0, st>>>(base);
     k_scatter<<<nb, 256, 0, st>>>(base, n);
