@@ -245,9 +245,13 @@ def fma_peaks(dev):
     """Measured FP32 and FP64 FMA rates (TFLOP/s) of this GPU: sphb_fma_probe
     on 8 full blocks per SM, the compute denominators of the pair passes'
     roofline."""
+    import ctypes
     import torch
-    from pysph_b200 import _native as nat
-    L = nat.lib()
+    from pysph_b200 import build as B
+    L = ctypes.CDLL(B.PROBE_LIB)
+    L.sphb_fma_probe.restype = ctypes.c_int
+    L.sphb_fma_probe.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_void_p]
     props = torch.cuda.get_device_properties(dev)
     blocks = props.multi_processor_count * 8
     out = {}
@@ -255,8 +259,10 @@ def fma_peaks(dev):
         buf = torch.empty(blocks, dtype=dtype, device=dev)
         iters = 400 if fp64 else 1600
         stream = torch.cuda.current_stream(dev)
-        run = lambda: nat.check(L.sphb_fma_probe(fp64, buf.data_ptr(), blocks, iters,
-                                                 ctypes_stream(stream)), "sphb_fma_probe")
+        def run():
+            rc = L.sphb_fma_probe(fp64, buf.data_ptr(), blocks, iters, ctypes_stream(stream))
+            if rc:
+                raise RuntimeError(f"sphb_fma_probe failed ({rc})")
         run()
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)

@@ -539,12 +539,6 @@ SPHB_API int sphb_neighbor_counts_static(int32_t n, int32_t dim, const double *x
                                          const double *h, double radius_scale,
                                          int32_t *counts, void *stream);
 
-/* FMA issue-rate probe: `blocks` blocks of 256 threads, each running 8
- * independent FMA chains of 16 x iters steps (FP32 when fp64 == 0, else
- * FP64); flops = blocks * 256 * iters * 256.  `out` (blocks elements of the
- * probe's type) is written only to keep the work.  No counterpart in the
- * reference: the compute denominator of the pair passes' roofline. */
-SPHB_API int sphb_fma_probe(int fp64, void *out, int blocks, int iters, void *stream);
 
 #ifdef __cplusplus
 }

@@ -177,7 +177,6 @@ def lib():
         "sphb_eos_vjp": (i32, [E, i32, vp, vp, vp, vp]),
         "sphb_density_vjp": (i32, [E, i32, u32, vp, vp, vp]),
         "sphb_neighbor_counts_static": (i32, [i32, i32, vp, vp, vp, vp, f64, vp, vp]),
-        "sphb_fma_probe": (i32, [i32, vp, i32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -195,7 +194,7 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
             "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
             "sphb_set_dt", "sphb_refresh", "sphb_permute", "sphb_force_vjp", "sphb_eos_vjp",
-            "sphb_density_vjp", "sphb_neighbor_counts_static", "sphb_fma_probe")
+            "sphb_density_vjp", "sphb_neighbor_counts_static")
 
 STATIC_MAX_PARTICLES = 1 << 18
 

@@ -4,7 +4,9 @@
 
 Every .cu under csrc/ is compiled by nvcc for sm_100a only, in parallel, and
 linked into pysph_b200/_lib/libsphb.so with the CUDA runtime linked
-statically, so the library carries no dependency beyond the driver.
+statically, so the library carries no dependency beyond the driver.  The
+benchmark's FMA-rate probe (probe/) is built into its own
+_lib/libsphb_probe.so.
 """
 from __future__ import annotations
 
@@ -64,6 +66,23 @@ def _compile(src, extra):
     return obj, ""
 
 
+PROBE_SRC = os.path.join(HERE, "probe", "sphb_fma_probe.cu")
+PROBE_LIB = os.path.join(LIBDIR, "libsphb_probe.so")
+
+
+def build_probe(force: bool = False) -> str:
+    """The benchmark's FMA-rate probe, a library of its own (not part of
+    libsphb.so)."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    if force or _stale(PROBE_LIB, [PROBE_SRC, __file__]):
+        cmd = [nvcc(), "-shared", PROBE_SRC, "-o", PROBE_LIB + ".tmp"] + ARCH + [
+            "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+            "-cudart", "static"]
+        subprocess.check_call(cmd)
+        os.replace(PROBE_LIB + ".tmp", PROBE_LIB)
+    return PROBE_LIB
+
+
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -83,6 +102,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
             "-cudart", "static", "-Xcompiler", "-fPIC"]
         subprocess.check_call(cmd)
         os.replace(LIB + ".tmp", LIB)
+    build_probe(force)
     return LIB
 
 
