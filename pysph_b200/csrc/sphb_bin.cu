@@ -4,11 +4,17 @@
 // counting sort (histogram, two-level scan, scatter) -> gather of the
 // particle state into the other buffer in cell order, ranking the members of
 // each cell by particle index so the order is canonical, plus the FP32 pair
-// records and the anchors (binned positions).  With SPHB_BIN_IF_NEEDED a
-// one-block kernel first decides on the device whether the lists still
-// cover every pair (no particle has moved skin/2 from its anchor); when they
-// do, every later kernel of the rebin returns at once, and when they do not,
-// the gathered state is copied back so it stays in buf[cur].
+// records and the anchors (binned positions).  With SPHB_BIN_IF_NEEDED the
+// device first decides whether the lists (or, for tiled pair passes, the
+// cells) still cover every pair (no particle has moved skin/2 from its
+// anchor); when they do, the rebin ends there, and when they do not, the
+// gathered state is copied back so it stays in buf[cur].
+//
+// The whole rebin is one cooperative launch (every block resident, so a
+// grid-wide barrier between phases cannot deadlock): decision, boxes, grids,
+// hash, scan, scatter, gather, copy back, each a grid-stride loop over tiles
+// or scan chunks, separated by a bounded barrier.  A step that keeps its
+// cells costs one short launch, and a CUDA graph needs no conditional node.
 //
 // The reference bins with a Python dict of cells keyed by floor(x / cs)
 // (CellManager._insert_particles, S/base/cell.pyx:1229-1300); its OpenCL
@@ -25,24 +31,67 @@
 
 namespace sphb {
 
-// ---------------------------------------------------------------- boxes --
-// work.meta[1] == 0 after a decision to keep the lists: the rebin is off
-__device__ __forceinline__ bool skip_rebin(const sphb_engine &e, int gated)
+// ------------------------------------------------------- grid barrier --
+// polls of the barrier's generation word before giving up (each poll sleeps
+// ~100 ns; every block of a cooperative launch is resident, so the barrier
+// completes in microseconds)
+constexpr long BARRIER_POLLS = 1L << 24;
+
+// Grid-wide barrier of a cooperative launch, two-level so that no counter
+// takes more than a few dozen same-address atomics: block b arrives on
+// counter b % BARRIER_GROUPS (in the words after the scan's chunk totals,
+// bsum[nb + 1 ..]), the last of each group on the top counter, and the last
+// of those advances the generation work.meta[7] that every block polls.
+// Each counter is reset by its last arriver before the release.  The wait
+// is bounded: on the limit it sets SPHB_ST_STAGE_TIMEOUT and goes on.
+constexpr int BARRIER_GROUPS = 32;
+
+__device__ __forceinline__ void grid_barrier(const sphb_engine &e, int *cnt)
 {
-    return gated && *(volatile int *)&e.work.meta[1] == 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile int *gen = (volatile int *)&e.work.meta[7];
+        const int g = *gen;
+        const int nb = (int)gridDim.x;
+        const int grp = (int)blockIdx.x % BARRIER_GROUPS;
+        const int ngrp = nb < BARRIER_GROUPS ? nb : BARRIER_GROUPS;
+        const int members = nb / BARRIER_GROUPS + (grp < nb % BARRIER_GROUPS ? 1 : 0);
+        __threadfence();
+        bool release = false;
+        if (atomicAdd(&cnt[grp], 1) == members - 1) {
+            cnt[grp] = 0;
+            __threadfence();
+            if (atomicAdd(&cnt[BARRIER_GROUPS], 1) == ngrp - 1) {
+                cnt[BARRIER_GROUPS] = 0;
+                release = true;
+            }
+        }
+        if (release) {
+            __threadfence();
+            atomicAdd(&e.work.meta[7], 1);
+        } else {
+            long it = 0;
+            while (*gen == g) {
+                if (++it > BARRIER_POLLS) {
+                    flag(e, SPHB_ST_STAGE_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
 }
 
-// One block.  No rebin while the particles sit where the last rebin put
+// ---------------------------------------------------------------- boxes --
+// Block 0.  No rebin while the particles sit where the last rebin put
 // them (work.meta[3] == 2); otherwise rebin unless the lists were recorded
 // with the skin at those positions (work.meta[4]) and no particle of any
 // scene has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding
 // of the displacement) from its anchor.  max_disp2 restarts either way.
-__global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
-                             cudaGraphConditionalHandle cond, int set_cond, int step_begin)
+__device__ void decide_block(const sphb_engine &e, int step_begin)
 {
-    // launched as a programmatic dependent of the stage before: its
-    // displacements and meta must be complete
-    pdl_wait();
     __shared__ int s_far;
     if (threadIdx.x == 0) s_far = 0;
     __syncthreads();
@@ -63,27 +112,27 @@ __global__ void k_bin_decide(const __grid_constant__ sphb_engine e,
         e.work.meta[1] = keep ? 0 : 1;
         e.work.meta[2] = (keep && lists) ? 1 : 0;
         if (!keep) e.work.pairs[3] += 1ull;   // rebins decided on the device
-        // inside a captured graph: run the rebin's conditional body or not
-        if (set_cond) cudaGraphSetConditional(cond, keep ? 0u : 1u);
     }
 }
 
-__global__ void k_box_reset(const __grid_constant__ sphb_engine e, int gated)
+__device__ __forceinline__ void box_reset_scene(const sphb_engine &e, int s)
 {
-    if (skip_rebin(e, gated)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= e.cfg.num_scenes) return;
     for (int d = 0; d < 3; ++d) {
         e.sstate[s].box[d] = enc_double(INFINITY);
         e.sstate[s].box[3 + d] = enc_double(-INFINITY);
     }
 }
 
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_box_accum(const __grid_constant__ sphb_engine e, int cur, int gated)
+__global__ void k_box_reset(const __grid_constant__ sphb_engine e)
 {
-    if (skip_rebin(e, gated)) return;
-    const sphb_tile t = e.tiles[blockIdx.x];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < e.cfg.num_scenes) box_reset_scene(e, s);
+}
+
+// The bounding box of a tile's particles into its scene's box (every thread
+// of the block calls it).
+__device__ __forceinline__ void box_accum_tile(const sphb_engine &e, int cur, const sphb_tile &t)
+{
     const int s = t.seg / e.cfg.num_arrays;
     const int k = t.begin + threadIdx.x;
     const sphb_buffers &B = e.buf[cur];
@@ -104,6 +153,12 @@ k_box_accum(const __grid_constant__ sphb_engine e, int cur, int gated)
         if (threadIdx.x == 0 && hi > -INFINITY)
             atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi));
     }
+}
+
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_box_accum(const __grid_constant__ sphb_engine e, int cur)
+{
+    box_accum_tile(e, cur, e.tiles[blockIdx.x]);
 }
 
 // FP32 pair records from the FP64 state without reordering (FP32C):
@@ -175,12 +230,11 @@ k_refresh(const __grid_constant__ sphb_engine e, int cur)
 }
 
 // ----------------------------------------------------------- grid setup --
-// One block.  Grid of scene s: cells floor(lo/cs)-R .. floor(hi/cs)+R per
+// Block 0 (<= 1024 threads).  Grid of scene s: cells floor(lo/cs)-R .. floor(hi/cs)+R per
 // axis (R padding cells, so every stencil row of every particle exists);
 // exclusive prefix of A*ncells over scenes gives the scene key bases.
-__global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sphb_engine e, int gated)
+__device__ void grid_setup_block(const sphb_engine &e)
 {
-    if (skip_rebin(e, gated)) return;
     __shared__ long long sh[1024];
     __shared__ long long s_carry;
     const int S = e.cfg.num_scenes, A = e.cfg.num_arrays, R = e.cfg.stencil;
@@ -264,11 +318,8 @@ __global__ void __launch_bounds__(1024) k_grid_setup(const __grid_constant__ sph
 }
 
 // ----------------------------------------------------------------- hash --
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_hash(const __grid_constant__ sphb_engine e, int cur, int gated)
+__device__ __forceinline__ void hash_tile(const sphb_engine &e, int cur, const sphb_tile &t)
 {
-    if (skip_rebin(e, gated)) return;
-    const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
     const int A = e.cfg.num_arrays;
@@ -335,29 +386,22 @@ __device__ __forceinline__ int block_excl_scan_int(int v, int &total)
     return before + x - v;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
-k_scan_reduce(const __grid_constant__ sphb_engine e, int gated)
+// Chunk b of SPHB_SCAN_CHUNK cells: its count total into bsum[b].
+__device__ __forceinline__ void scan_reduce_chunk(const sphb_engine &e, int b)
 {
-    if (skip_rebin(e, gated)) return;
     const int T = e.work.meta[0];
-    const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
+    const long long base = (long long)b * SPHB_SCAN_CHUNK;
     int sum = 0;
-    if (base < T) {
-#pragma unroll
-        for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
-            const long long c = base + (long long)i * SPHB_SCAN_THREADS + threadIdx.x;
-            if (c < T) sum += e.work.count[c];
-        }
-    }
+    for (long long c = base + threadIdx.x; c < base + SPHB_SCAN_CHUNK && c < T; c += blockDim.x)
+        sum += e.work.count[c];
     int total;
     block_excl_scan_int(sum, total);
-    if (threadIdx.x == 0) e.work.bsum[blockIdx.x] = total;
+    if (threadIdx.x == 0) e.work.bsum[b] = total;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
-k_scan_top(const __grid_constant__ sphb_engine e, int nb, int gated)
+// One block: the exclusive scan of the nb chunk totals (bsum[nb] = all).
+__device__ void scan_top_block(const sphb_engine &e, int nb)
 {
-    if (skip_rebin(e, gated)) return;
     __shared__ int s_carry;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
@@ -375,29 +419,31 @@ k_scan_top(const __grid_constant__ sphb_engine e, int nb, int gated)
     if (threadIdx.x == 0) e.work.bsum[nb] = s_carry;
 }
 
-__global__ void __launch_bounds__(SPHB_SCAN_THREADS)
-k_scan_apply(const __grid_constant__ sphb_engine e, int gated)
+// Chunk b: start[c] for its cells (ITEMS consecutive cells per thread,
+// ITEMS x blockDim.x = SPHB_SCAN_CHUNK), and the counts cleared for the
+// next bin.
+template <int ITEMS>
+__device__ __forceinline__ void scan_apply_chunk(const sphb_engine &e, int b)
 {
-    if (skip_rebin(e, gated)) return;
     const int T = e.work.meta[0];
-    const long long base = (long long)blockIdx.x * SPHB_SCAN_CHUNK;
+    const long long base = (long long)b * SPHB_SCAN_CHUNK;
     if (T == 0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) e.work.start[0] = 0;
+        if (b == 0 && threadIdx.x == 0) e.work.start[0] = 0;
         return;
     }
-    if (base >= T) return;
-    const long long c0 = base + (long long)threadIdx.x * SPHB_SCAN_ITEMS;
-    int v[SPHB_SCAN_ITEMS];
+    if (base >= T) return;   // block-uniform
+    const long long c0 = base + (long long)threadIdx.x * ITEMS;
+    int v[ITEMS];
     int sum = 0;
 #pragma unroll
-    for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
+    for (int i = 0; i < ITEMS; ++i) {
         v[i] = (c0 + i < T) ? e.work.count[c0 + i] : 0;
         sum += v[i];
     }
     int total;
-    int run = block_excl_scan_int(sum, total) + e.work.bsum[blockIdx.x];
+    int run = block_excl_scan_int(sum, total) + e.work.bsum[b];
 #pragma unroll
-    for (int i = 0; i < SPHB_SCAN_ITEMS; ++i) {
+    for (int i = 0; i < ITEMS; ++i) {
         const long long c = c0 + i;
         if (c < T) {
             e.work.start[c] = run;
@@ -409,11 +455,8 @@ k_scan_apply(const __grid_constant__ sphb_engine e, int gated)
 }
 
 // -------------------------------------------------------------- scatter --
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_scatter(const __grid_constant__ sphb_engine e, int gated)
+__device__ __forceinline__ void scatter_tile(const sphb_engine &e, const sphb_tile &t)
 {
-    if (skip_rebin(e, gated)) return;
-    const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
     const int key = e.work.key[k];
@@ -433,11 +476,9 @@ k_scatter(const __grid_constant__ sphb_engine e, int gated)
 // is canonical whatever order the atomics handed out the slots, and it does
 // not depend on the order the particles had before.
 template <int DIM, bool F32>
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial, int gated)
+__device__ __forceinline__ void reorder_tile(const sphb_engine &e, int cur, int move_initial,
+                                             const sphb_tile &t)
 {
-    if (skip_rebin(e, gated)) return;
-    const sphb_tile t = e.tiles[blockIdx.x];
     const int kk = t.begin + threadIdx.x;
     if (kk >= t.end) return;
     const int A = e.cfg.num_arrays;
@@ -539,11 +580,9 @@ k_reorder(const __grid_constant__ sphb_engine e, int cur, int move_initial, int 
 // After a rebin decided on the device: the gathered state back into
 // buf[cur], same order (the records, anchors and cells already follow it).
 template <int DIM>
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_copy_back(const __grid_constant__ sphb_engine e, int cur, int move_initial, int gated)
+__device__ __forceinline__ void copy_back_tile(const sphb_engine &e, int cur, int move_initial,
+                                               const sphb_tile &t)
 {
-    if (skip_rebin(e, gated)) return;
-    const sphb_tile t = e.tiles[blockIdx.x];
     const int k = t.begin + threadIdx.x;
     if (k >= t.end) return;
     const sphb_buffers &S = e.buf[cur ^ 1];
@@ -572,6 +611,52 @@ k_copy_back(const __grid_constant__ sphb_engine e, int cur, int move_initial, in
             D.w0[k] = S.w0[k];
         }
     }
+}
+
+
+// ---------------------------------------------------------- the rebin --
+// One cooperative launch: [decision] -> boxes -> grids -> hash -> scan ->
+// scatter -> gather [-> copy back], the phases separated by grid_barrier.
+// With SPHB_BIN_IF_NEEDED block 0 decides first and every block returns
+// when the cells are kept; the gathered state then goes back to buf[cur].
+template <int DIM, bool F32>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_rebin(const __grid_constant__ sphb_engine e, int cur, int flags)
+{
+    const bool if_needed = (flags & SPHB_BIN_IF_NEEDED) != 0;
+    const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
+    const int nt = e.num_tiles;
+    const int nb = (int)((e.cfg.cell_capacity + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK);
+    int *const bar = e.work.bsum + nb + 1;   // the barrier's counters
+    if (blockIdx.x == 0) {
+        if (if_needed) decide_block(e, (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0);
+        // every rebin measures the scene boxes afresh (only a rebin reads them)
+        for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) box_reset_scene(e, s);
+    }
+    grid_barrier(e, bar);
+    if (if_needed && *(volatile int *)&e.work.meta[1] == 0) {   // kept (grid-uniform)
+        pdl_trigger();   // the density pass may launch
+        return;
+    }
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) box_accum_tile(e, cur, e.tiles[t]);
+    grid_barrier(e, bar);
+    if (blockIdx.x == 0) grid_setup_block(e);
+    grid_barrier(e, bar);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) hash_tile(e, cur, e.tiles[t]);
+    grid_barrier(e, bar);
+    for (int b = blockIdx.x; b < nb; b += gridDim.x) scan_reduce_chunk(e, b);
+    grid_barrier(e, bar);
+    if (blockIdx.x == 0) scan_top_block(e, nb);
+    grid_barrier(e, bar);
+    for (int b = blockIdx.x; b < nb; b += gridDim.x)
+        scan_apply_chunk<SPHB_SCAN_CHUNK / SPHB_ELEM_TILE>(e, b);
+    grid_barrier(e, bar);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) scatter_tile(e, e.tiles[t]);
+    grid_barrier(e, bar);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) reorder_tile<DIM, F32>(e, cur, mi, e.tiles[t]);
+    if (!if_needed) return;
+    grid_barrier(e, bar);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) copy_back_tile<DIM>(e, cur, mi, e.tiles[t]);
 }
 
 // --------------------------------------------------------- entry points --
@@ -606,9 +691,9 @@ extern "C" int sphb_box_init(const sphb_engine *e, int cur, void *stream)
     int rc = check_engine(e, cur);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    k_box_reset<<<(e->cfg.num_scenes + 127) / 128, 128, 0, st>>>(*e, 0);
+    k_box_reset<<<(e->cfg.num_scenes + 127) / 128, 128, 0, st>>>(*e);
     if (e->num_tiles > 0)
-        k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, 0);
+        k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur);
     return launch_status("sphb_box_init");
 }
 
@@ -631,110 +716,75 @@ extern "C" int sphb_refresh(const sphb_engine *e, int cur, void *stream)
     return launch_status("sphb_refresh");
 }
 
-// The kernels of one rebin, gated on work.meta[1] when gated.
-static void launch_rebin(const sphb_engine *e, int cur, int flags, int gated, cudaStream_t st)
-{
-    const sphb_config &c = e->cfg;
-    // every rebin measures the scene boxes afresh (only a rebin needs them)
-    k_box_reset<<<(c.num_scenes + 127) / 128, 128, 0, st>>>(*e, gated);
-    if (e->num_tiles > 0) k_box_accum<<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
-    k_grid_setup<<<1, 1024, 0, st>>>(*e, gated);
-    const int nt = e->num_tiles;
-    if (nt > 0) k_hash<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, gated);
-    const int nb = bin_scan_blocks(c);
-    k_scan_reduce<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e, gated);
-    k_scan_top<<<1, SPHB_SCAN_THREADS, 0, st>>>(*e, nb, gated);
-    k_scan_apply<<<nb, SPHB_SCAN_THREADS, 0, st>>>(*e, gated);
-    if (nt > 0) {
-        k_scatter<<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, gated);
-        const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
-        if (c.dim == 2 && c.precision == SPHB_FP32C)
-            k_reorder<2, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-        else if (c.dim == 2)
-            k_reorder<2, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-        else if (c.precision == SPHB_FP32C)
-            k_reorder<3, true><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-        else
-            k_reorder<3, false><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-        if (gated) {
-            if (c.dim == 2) k_copy_back<2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-            else k_copy_back<3><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, mi, gated);
-        }
-    }
-}
-
-// A stream of the library's own per device, to capture the body of the
-// conditional rebin node into (cudaStreamBeginCaptureToGraph needs a stream
-// that is not capturing already); one capture at a time.
-static std::mutex g_body_mu;
-static cudaStream_t g_body_stream[128];
-
-static int body_stream(cudaStream_t *out)
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return SPHB_ERR_CUDA;
-    if (!g_body_stream[dev] &&
-        cudaStreamCreateWithFlags(&g_body_stream[dev], cudaStreamNonBlocking) != cudaSuccess)
-        return SPHB_ERR_CUDA;
-    *out = g_body_stream[dev];
-    return SPHB_OK;
-}
-
 static int cuda_fail(const char *what, cudaError_t err)
 {
     record_cuda_error(what, err);
     return SPHB_ERR_CUDA;
 }
 
-// Captured form of a device-decided rebin: the decision kernel sets a graph
-// conditional handle, and the rebin kernels form the body of an IF node, so
-// a replay that keeps the lists launches none of them.
-static int bin_conditional(const sphb_engine *e, int cur, int flags, cudaStream_t st,
-                           cudaGraph_t graph)
+// Blocks of one cooperative rebin launch: every block resident at once
+// (occupancy x SMs), looked up once per device and instantiation.
+template <int DIM, bool F32>
+static int rebin_grid(int *out)
 {
-    cudaError_t err;
-    cudaGraphConditionalHandle cond;
-    if ((err = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault)))
-        return cuda_fail("sphb_bin: conditional handle", err);
-    if ((err = launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cond, 1,
-                          (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0)))
-        return cuda_fail("sphb_bin: decision", err);
-    cudaStreamCaptureStatus cs;
-    unsigned long long id;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    if ((err = cudaStreamGetCaptureInfo(st, &cs, &id, &graph, &deps, &ndeps)))
-        return cuda_fail("sphb_bin: capture info", err);
-    // (the union inside has no default constructor: zeroed storage)
-    alignas(cudaGraphNodeParams) unsigned char pbuf[sizeof(cudaGraphNodeParams)];
-    memset(pbuf, 0, sizeof(pbuf));
-    cudaGraphNodeParams &p = *reinterpret_cast<cudaGraphNodeParams *>(pbuf);
-    p.type = cudaGraphNodeTypeConditional;
-    p.conditional.handle = cond;
-    p.conditional.type = cudaGraphCondTypeIf;
-    p.conditional.size = 1;
-    cudaGraphNode_t node;
-    if ((err = cudaGraphAddNode(&node, graph, deps, ndeps, &p)))
-        return cuda_fail("sphb_bin: conditional node", err);
-    cudaGraph_t body = p.conditional.phGraph_out[0];
-    {
-        std::lock_guard<std::mutex> lock(g_body_mu);
-        cudaStream_t bs;
-        if (body_stream(&bs)) return cuda_fail("sphb_bin: body stream", cudaGetLastError());
-        if ((err = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
-                                                 cudaStreamCaptureModeRelaxed)))
-            return cuda_fail("sphb_bin: body capture", err);
-        launch_rebin(e, cur, flags, 1, bs);
-        const cudaError_t lerr = cudaGetLastError();
-        cudaGraph_t done;
-        err = cudaStreamEndCapture(bs, &done);
-        if (lerr) return cuda_fail("sphb_bin: body launch", lerr);
-        if (err) return cuda_fail("sphb_bin: body capture end", err);
+    static std::mutex mu;
+    static int cache[128];
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err || dev < 0 || dev >= 128) return cuda_fail("sphb_bin: device", err);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cache[dev]) {
+        int per_sm = 0, sms = 0;
+        if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebin<DIM, F32>,
+                                                                 SPHB_ELEM_TILE, 0)))
+            return cuda_fail("sphb_bin: occupancy", err);
+        if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)))
+            return cuda_fail("sphb_bin: SM count", err);
+        if (per_sm < 1 || sms < 1) return cuda_fail("sphb_bin: occupancy", cudaErrorInvalidValue);
+        cache[dev] = per_sm * sms;
     }
-    if ((err = cudaStreamUpdateCaptureDependencies(st, &node, 1,
-                                                   cudaStreamSetCaptureDependencies)))
-        return cuda_fail("sphb_bin: capture dependencies", err);
+    *out = cache[dev];
     return SPHB_OK;
+}
+
+// Blocks of a launch: about 4 tiles each, between 2 per SM (a kept-cells
+// launch costs little more than one small kernel) and every resident block
+// (measured on B200 with the 332k-particle dam break: 2 per SM keep the
+// cells in 2 us over a plain launch against 4 us at 3 per SM, while a full
+// rebin takes 88 us at 3 per SM and 94 us at 2)
+template <int DIM, bool F32>
+static int launch_rebin_t(const sphb_engine *e, int cur, int flags, cudaStream_t st)
+{
+    int resident = 0, sms = 0, dev = 0;
+    int rc = rebin_grid<DIM, F32>(&resident);
+    if (rc) return rc;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        sms = 1;
+    int blocks = (e->num_tiles + 3) / 4;
+    if (blocks < 2 * sms) blocks = 2 * sms;
+    if (blocks > resident) blocks = resident;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(SPHB_ELEM_TILE);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t err = cudaLaunchKernelEx(&cfg, k_rebin<DIM, F32>, *e, cur, flags);
+    if (err) return cuda_fail("sphb_bin: cooperative launch", err);
+    return SPHB_OK;
+}
+
+static int launch_rebin(const sphb_engine *e, int cur, int flags, cudaStream_t st)
+{
+    const sphb_config &c = e->cfg;
+    if (c.dim == 2 && c.precision == SPHB_FP32C) return launch_rebin_t<2, true>(e, cur, flags, st);
+    if (c.dim == 2) return launch_rebin_t<2, false>(e, cur, flags, st);
+    if (c.precision == SPHB_FP32C) return launch_rebin_t<3, true>(e, cur, flags, st);
+    return launch_rebin_t<3, false>(e, cur, flags, st);
 }
 
 extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
@@ -745,27 +795,9 @@ extern "C" int sphb_bin(const sphb_engine *e, int cur, int flags, void *stream)
                   SPHB_BIN_STEP_BEGIN))
         return SPHB_ERR_ARG;
     if ((flags & SPHB_BIN_STEP_BEGIN) && !(flags & SPHB_BIN_IF_NEEDED)) return SPHB_ERR_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
-    const int gated = (flags & SPHB_BIN_IF_NEEDED) ? 1 : 0;
-    if (!gated) {
-        launch_rebin(e, cur, flags, 0, st);
-        return launch_status("sphb_bin");
-    }
-    // the decision needs the displacements sphb_pc_stage measures from the
+    // the decision needs the displacements the stages measure from the
     // anchors
-    if (!e->f.anchor || !e->f.cell) return SPHB_ERR_ARG;
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaError_t err = cudaStreamIsCapturing(st, &cs);
-    if (err) return cuda_fail("sphb_bin: capture status", err);
-    if (cs == cudaStreamCaptureStatusActive) {
-        cudaGraph_t graph;
-        unsigned long long id;
-        if ((err = cudaStreamGetCaptureInfo(st, &cs, &id, &graph, nullptr, nullptr)))
-            return cuda_fail("sphb_bin: capture info", err);
-        return bin_conditional(e, cur, flags, st, graph);
-    }
-    launch_pdl(k_bin_decide, dim3(1), dim3(256), st, *e, cudaGraphConditionalHandle(), 0,
-               (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0);
-    launch_rebin(e, cur, flags, 1, st);
+    if ((flags & SPHB_BIN_IF_NEEDED) && (!e->f.anchor || !e->f.cell)) return SPHB_ERR_ARG;
+    if ((rc = launch_rebin(e, cur, flags, (cudaStream_t)stream))) return rc;
     return launch_status("sphb_bin");
 }

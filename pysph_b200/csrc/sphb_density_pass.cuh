@@ -82,7 +82,10 @@ template <int KT, int DIM, bool F32, int LANES, int R>
 __global__ void __launch_bounds__(256, F32 ? (DIM == 2 ? 5 : 4) : 3)
 k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags)
 {
-    // the force pass that follows may launch once every block has started
+    // launched as a programmatic dependent of the rebin before it: the cells,
+    // records and lists are read only after this; the force pass that
+    // follows may launch once every block has started
+    pdl_wait();
     pdl_trigger();
     const int with_eos = flags & SPHB_DENSITY_EOS;
     // list reuse: read the lists when the last rebin decision kept them
@@ -321,7 +324,7 @@ static void launch_density_p(const sphb_engine &e, int cur, uint32_t dm, int eos
                              cudaStream_t st)
 {
     const dim3 g(e.num_pair_tiles), b(e.cfg.pair_block);
-#define SPHB_L(LV, RV) k_density<KT, DIM, F32, LV, RV><<<g, b, 0, st>>>(e, cur, dm, eos)
+#define SPHB_L(LV, RV) launch_pdl(k_density<KT, DIM, F32, LV, RV>, g, b, st, e, cur, dm, eos)
     switch (e.cfg.lanes * 10 + e.cfg.stencil) {
     case 11: SPHB_L(1, 1); break;
     case 12: SPHB_L(1, 2); break;

@@ -264,8 +264,9 @@ extern "C" int sphb_workspace_layout(const sphb_config *cfg, size_t offsets[9],
     if (cfg->num_particles < 0 || cfg->cell_capacity < 1) return SPHB_ERR_ARG;
     const size_t N = (size_t)cfg->num_particles, C = (size_t)cfg->cell_capacity;
     const size_t nb = (C + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK;
+    // bsum: the scan's chunk totals, then the rebin barrier's counters
     const size_t sizes[9] = {C * 4, (C + 1) * 4, N * 4, N * 4, N * 4,
-                             (nb + 1) * 4, 8 * 4, 4, 4 * 8};
+                             (nb + 1 + 64) * 4, 8 * 4, 4, 4 * 8};
     size_t off = 0;
     for (int i = 0; i < 9; ++i) {
         offsets[i] = off;

@@ -293,6 +293,8 @@ __global__ void __launch_bounds__(256, 4)
 k_density_tiled(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, int flags,
                 int cap)
 {
+    // a programmatic dependent of the rebin before it (see k_density)
+    pdl_wait();
     pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileRanges tr;
@@ -602,13 +604,22 @@ void launch_density_tiled(const sphb_engine &e, int cur, uint32_t dm, int flags,
     const int cap = tile_cap(T, R);
     const size_t sm = tile_smem_density(T, cap);
     const dim3 g(e.num_pair_tiles), b(T);
-    if (R == 1) {
-        if (allow_smem(k_density_tiled<KT, 1>, sm) == cudaSuccess)
-            k_density_tiled<KT, 1><<<g, b, sm, st>>>(e, cur, dm, flags, cap);
-    } else {
-        if (allow_smem(k_density_tiled<KT, 2>, sm) == cudaSuccess)
-            k_density_tiled<KT, 2><<<g, b, sm, st>>>(e, cur, dm, flags, cap);
-    }
+    auto go = [&](auto kern) {
+        if (allow_smem(kern, sm) != cudaSuccess) return;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = g;
+        cfg.blockDim = b;
+        cfg.dynamicSmemBytes = sm;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kern, e, cur, dm, flags, cap);
+    };
+    if (R == 1) go(k_density_tiled<KT, 1>);
+    else go(k_density_tiled<KT, 2>);
 }
 
 template <int KT>
