@@ -950,13 +950,19 @@ def e2e_facade(wl, args, shape, dev, stream):
     sess.engine.update_params(cfl=p["cfl"], c0=p["c0"], dt_initial=p["dt_initial"])
     integ.plan.params = sess.engine.params[0]
     names_out = ("x", "y", "u", "v", "rho", "p")
-    host = {k: f.get(k).cpu().numpy().copy() for k in names_out}
+    # the caller's host arrays: numpy views of pinned host memory, allocated
+    # once, as a host driving the GPU every step would keep them
+    pinned = {k: torch.empty(f.get_number_of_particles(), dtype=torch.float64).pin_memory()
+              for k in names_out}
+    host = {k: pinned[k].numpy() for k in names_out}
+    for k in names_out:
+        pinned[k].copy_(f.get(k))
 
     def step():
         f.set(x=host["x"], y=host["y"], u=host["u"], v=host["v"])
         integ.integrate(0.0, device_dt=True)
         for k in names_out:
-            host[k] = f.get(k).cpu().numpy()
+            pinned[k].copy_(f.get(k))   # into the numpy arrays' memory
 
     for _ in range(3):
         step()
@@ -981,7 +987,10 @@ def e2e_facade(wl, args, shape, dev, stream):
            "rebins_per_stage": rebins / (2.0 * k_steps),
            "h2d_bytes_per_step": 8 * n * 4, "d2h_bytes_per_step": 8 * n * len(names_out),
            "api": "ParticleArray.set(numpy) -> PredictorCorrectorIntegrator.integrate "
-                  "(device CFL dt) -> ParticleArray.get -> numpy, every step",
+                  "(device CFL dt) -> ParticleArray.get -> numpy, every step; the numpy "
+                  "arrays live in pinned host memory allocated once",
+           "rebins": "device-decided after each host write of the positions (kept while "
+                     "every particle stays within half the list skin of its last rebin)",
            "shape": particles.engine_options}
     particles.session().detach()
     del s, integ, particles, f, w

@@ -160,7 +160,10 @@ class ParticleArray:
             t = self.properties[name]
             v = torch.as_tensor(np.asarray(value) if not isinstance(value, torch.Tensor)
                                 else value, dtype=t.dtype)
-            t.copy_(v.to(t.device).expand_as(t) if v.dim() == 0 else v.to(t.device))
+            if v.dim() == 0:
+                t.fill_(v.item())
+            else:
+                t.copy_(v)   # one copy, host memory straight into the property
             self._touch(name)
 
     def __getattr__(self, name):

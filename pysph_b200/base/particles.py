@@ -160,14 +160,23 @@ class Session:
             self.need_bin = True
 
     def bin(self):
-        """Rebin; derived fields the user has not read yet are copied out
-        first because the rebin reorders the particles under them."""
+        """Rebin after positions changed on the host; derived fields the
+        user has not read yet are copied out first because a rebin reorders
+        the particles under them.  With neighbour lists kept across steps the
+        device decides: it measures every particle's displacement from its
+        position at the last rebin and rebins only when some particle moved
+        half the list skin (or the lists were withdrawn, e.g. by new masses),
+        so host-driven steps that move the particles a little keep the lists
+        and cells, which still cover every pair."""
         for a, pa in enumerate(self.particles.arrays):
             for name in DERIVED:
                 if name in pa._engine_newer:
                     self.export_to_array(pa, name)
         self.engine.invalidate_box()
-        self.engine.bin(nat.BIN_MOVE_INITIAL)
+        if self.engine.step_lists:
+            self.engine.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
+        else:
+            self.engine.bin(nat.BIN_MOVE_INITIAL)
         for a in range(len(self.particles.arrays)):
             for name in DERIVED:
                 self.valid[(a, name)] = False
