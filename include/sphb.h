@@ -237,8 +237,9 @@ typedef struct {
     int32_t *slot;          /* [N] */
     int32_t *perm;          /* [N] */
     int32_t *bsum;          /* [scan blocks + 1 + 64]: the scan's chunk totals,
-                               then the rebin's grid-barrier counters (zero
-                               when the workspace is first used) */
+                               then the rebin's grid-barrier word (its low
+                               31 bits zero when the workspace is first
+                               used) */
     int32_t *meta;          /* [8]  meta[0] = cells in use (all scenes);
                                meta[1] = 1 when the last rebin decision
                                rebinned; meta[2] = 1 when it kept the lists
@@ -248,9 +249,7 @@ typedef struct {
                                were recorded with the skin at them;
                                meta[5] = 1 after the host wrote positions or
                                velocities, until sphb_refresh has rebuilt the
-                               records and measured the displacements;
-                               meta[7] = the rebin's grid-barrier
-                               generation (zero when first used) */
+                               records and measured the displacements */
     unsigned int *status;   /* [1]  SPHB_ST_* bits, cleared by the host */
     unsigned long long *pairs;  /* [4]  pairs evaluated: density, force;
                                    [2]: blocks of the tiled passes that read

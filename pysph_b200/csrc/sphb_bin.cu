@@ -32,52 +32,32 @@
 namespace sphb {
 
 // ------------------------------------------------------- grid barrier --
-// polls of the barrier's generation word before giving up (each poll sleeps
-// ~100 ns; every block of a cooperative launch is resident, so the barrier
-// completes in microseconds)
-constexpr long BARRIER_POLLS = 1L << 24;
+// polls of the barrier word before giving up (every block of a cooperative
+// launch is resident, so the barrier completes in microseconds)
+constexpr long BARRIER_POLLS = 1L << 22;
 
-// Grid-wide barrier of a cooperative launch, two-level so that no counter
-// takes more than a few dozen same-address atomics: block b arrives on
-// counter b % BARRIER_GROUPS (in the words after the scan's chunk totals,
-// bsum[nb + 1 ..]), the last of each group on the top counter, and the last
-// of those advances the generation work.meta[7] that every block polls.
-// Each counter is reset by its last arriver before the release.  The wait
-// is bounded: on the limit it sets SPHB_ST_STAGE_TIMEOUT and goes on.
-constexpr int BARRIER_GROUPS = 32;
-
-__device__ __forceinline__ void grid_barrier(const sphb_engine &e, int *cnt)
+// Grid-wide barrier of a cooperative launch on one word (the first word
+// after the scan's chunk totals, bsum[nb + 1]).  Each block adds 1 to it,
+// except block 0, which adds 2^31 - (blocks - 1): the word's top bit flips
+// exactly when the last block has arrived, and its low bits are back where
+// they were, so the word needs no reset between barriers or launches.  The
+// wait is bounded: on the limit it sets SPHB_ST_STAGE_TIMEOUT and goes on.
+__device__ __forceinline__ void grid_barrier(const sphb_engine &e, int *word_)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile int *gen = (volatile int *)&e.work.meta[7];
-        const int g = *gen;
-        const int nb = (int)gridDim.x;
-        const int grp = (int)blockIdx.x % BARRIER_GROUPS;
-        const int ngrp = nb < BARRIER_GROUPS ? nb : BARRIER_GROUPS;
-        const int members = nb / BARRIER_GROUPS + (grp < nb % BARRIER_GROUPS ? 1 : 0);
+        unsigned *word = (unsigned *)word_;
+        const unsigned nb = gridDim.x;
+        const unsigned add = blockIdx.x == 0 ? 0x80000000u - (nb - 1u) : 1u;
         __threadfence();
-        bool release = false;
-        if (atomicAdd(&cnt[grp], 1) == members - 1) {
-            cnt[grp] = 0;
-            __threadfence();
-            if (atomicAdd(&cnt[BARRIER_GROUPS], 1) == ngrp - 1) {
-                cnt[BARRIER_GROUPS] = 0;
-                release = true;
+        const unsigned old = atomicAdd(word, add);
+        long it = 0;
+        while (((old ^ *(volatile unsigned *)word) & 0x80000000u) == 0u) {
+            if (++it > BARRIER_POLLS) {
+                flag(e, SPHB_ST_STAGE_TIMEOUT);
+                break;
             }
-        }
-        if (release) {
-            __threadfence();
-            atomicAdd(&e.work.meta[7], 1);
-        } else {
-            long it = 0;
-            while (*gen == g) {
-                if (++it > BARRIER_POLLS) {
-                    flag(e, SPHB_ST_STAGE_TIMEOUT);
-                    break;
-                }
-                __nanosleep(64);
-            }
+            __nanosleep(32);
         }
         __threadfence();
     }
@@ -317,31 +297,154 @@ __device__ void grid_setup_block(const sphb_engine &e)
     }
 }
 
-// ----------------------------------------------------------------- hash --
-__device__ __forceinline__ void hash_tile(const sphb_engine &e, int cur, const sphb_tile &t)
+// ------------------------------------------------------- block work runs --
+// The rebin's per-particle phases give each block a contiguous run of tiles
+// and walk it RU tiles at a time, issuing every load of the RU particles a
+// thread owns before any of them is used.  The launch keeps only 2-3 blocks
+// per SM (a kept-cells launch must stay cheap), so with one particle per
+// thread in flight the phases waited one memory latency per tile; this way
+// they wait one per RU tiles.
+constexpr int RU = 4;
+// tiles at a time of the phases that carry little per particle (boxes,
+// keys, scatter)
+constexpr int RU8 = 8;
+
+__device__ __forceinline__ void block_tile_run(int nt, int &t0, int &t1)
 {
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
+    const long long G = gridDim.x, b = blockIdx.x;
+    t0 = (int)(b * nt / G);
+    t1 = (int)((b + 1) * nt / G);
+}
+
+// The particles of tiles [t, t + U) this thread owns (-1: none) and their
+// segments.
+template <int U>
+__device__ __forceinline__ void run_particles(const sphb_engine &e, int t, int t1, int *kk,
+                                              int *seg)
+{
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        kk[u] = -1;
+        seg[u] = -1;
+        if (t + u < t1) {
+            const sphb_tile tl = e.tiles[t + u];
+            seg[u] = tl.seg;
+            const int k = tl.begin + (int)threadIdx.x;
+            if (k < tl.end) kk[u] = k;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- boxes --
+// This block's minima / maxima into scene s's box (a block-uniform call),
+// then the partials restart.
+__device__ __forceinline__ void box_flush(const sphb_engine &e, int s, int dim, double *lo,
+                                          double *hi)
+{
+    __shared__ double sh[SPHB_ELEM_TILE / 32][6];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = warp_reduce(lo[d], OpMin());
+        hi[d] = warp_reduce(hi[d], OpMax());
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sh[w][d] = lo[d];
+            sh[w][3 + d] = hi[d];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fmin(lo[d], sh[i][d]);
+                hi[d] = fmax(hi[d], sh[i][3 + d]);
+            }
+        for (int d = 0; d < dim; ++d) {
+            if (lo[d] < INFINITY) atomic_min_enc(&e.sstate[s].box[d], enc_double(lo[d]));
+            if (hi[d] > -INFINITY) atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi[d]));
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+    }
+}
+
+// The scene boxes from the block's run of tiles: partials in registers,
+// published whenever the run passes into another scene and at its end.
+template <int DIM>
+__device__ void box_accum_run(const sphb_engine &e, int cur, int t0, int t1)
+{
+    if (t0 >= t1) return;   // block-uniform
     const int A = e.cfg.num_arrays;
-    const int s = t.seg / A, a = t.seg - s * A;
+    const sphb_buffers &B = e.buf[cur];
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int s_cur = e.tiles[t0].seg / A;
+    for (int t = t0; t < t1; t += RU8) {
+        int kk[RU8], seg[RU8];
+        run_particles<RU8>(e, t, t1, kk, seg);
+        double px[RU8], py[RU8], pz[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            px[u] = py[u] = pz[u] = 0.0;
+            if (kk[u] >= 0) {
+                px[u] = B.x[kk[u]];
+                py[u] = B.y[kk[u]];
+                if (DIM == 3) pz[u] = B.z[kk[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            if (seg[u] < 0) break;   // block-uniform
+            const int su = seg[u] / A;
+            if (su != s_cur) {
+                box_flush(e, s_cur, DIM, lo, hi);
+                s_cur = su;
+            }
+            if (kk[u] >= 0 && isfinite(px[u]) && isfinite(py[u]) && isfinite(pz[u])) {
+                lo[0] = fmin(lo[0], px[u]);
+                hi[0] = fmax(hi[0], px[u]);
+                lo[1] = fmin(lo[1], py[u]);
+                hi[1] = fmax(hi[1], py[u]);
+                if (DIM == 3) {
+                    lo[2] = fmin(lo[2], pz[u]);
+                    hi[2] = fmax(hi[2], pz[u]);
+                }
+            }
+        }
+    }
+    box_flush(e, s_cur, DIM, lo, hi);
+}
+
+// ----------------------------------------------------------------- hash --
+// Global cell key of a particle of segment seg at (x, y, z), or -1 (status
+// flagged) for a non-finite position or one outside its scene's grid.
+template <int DIM>
+__device__ __forceinline__ long long cell_key(const sphb_engine &e, int seg, double x, double y,
+                                              double z)
+{
+    const int A = e.cfg.num_arrays;
+    const int s = seg / A, a = seg - s * A;
     const sphb_scene_state &st = e.sstate[s];
     const double cs = e.scene[s].cell_size;
-    const sphb_buffers &B = e.buf[cur];
-    const int dim = e.cfg.dim;
-    double p[3] = {B.x[k], B.y[k], dim == 3 ? B.z[k] : 0.0};
+    const double p[3] = {x, y, z};
     int c[3] = {0, 0, 0};
-    for (int d = 0; d < dim; ++d) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
         if (!isfinite(p[d])) {
             flag(e, SPHB_ST_NONFINITE_POS);
-            e.work.key[k] = -1;
-            return;
+            return -1;
         }
         // floor(x / cs) exactly as find_cell_id (S/base/cell.pyx:44-84)
         const double f = floor(p[d] / cs) - (double)st.lo[d];
         if (!(f >= 0.0) || !(f < (double)st.n[d])) {
             flag(e, SPHB_ST_OUT_OF_GRID);
-            e.work.key[k] = -1;
-            return;
+            return -1;
         }
         c[d] = (int)f;
     }
@@ -349,11 +452,44 @@ __device__ __forceinline__ void hash_tile(const sphb_engine &e, int cur, const s
     const long long key = (long long)st.cell_base + (long long)a * st.ncells + local;
     if (local >= st.ncells || key >= (long long)e.work.meta[0]) {
         flag(e, SPHB_ST_OUT_OF_GRID);
-        e.work.key[k] = -1;
-        return;
+        return -1;
     }
-    e.work.slot[k] = atomicAdd(&e.work.count[key], 1);
-    e.work.key[k] = (int)key;
+    return key;
+}
+
+// Keys and the cell histogram: RU positions loaded, RU keys, RU atomics in
+// flight, then the stores.
+template <int DIM>
+__device__ void hash_run(const sphb_engine &e, int cur, int t0, int t1)
+{
+    const sphb_buffers &B = e.buf[cur];
+    for (int t = t0; t < t1; t += RU8) {
+        int kk[RU8], seg[RU8];
+        run_particles<RU8>(e, t, t1, kk, seg);
+        double px[RU8], py[RU8], pz[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            px[u] = py[u] = pz[u] = 0.0;
+            if (kk[u] >= 0) {
+                px[u] = B.x[kk[u]];
+                py[u] = B.y[kk[u]];
+                if (DIM == 3) pz[u] = B.z[kk[u]];
+            }
+        }
+        long long key[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u)
+            key[u] = kk[u] >= 0 ? cell_key<DIM>(e, seg[u], px[u], py[u], pz[u]) : -1;
+        int slot[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) slot[u] = key[u] >= 0 ? atomicAdd(&e.work.count[key[u]], 1) : 0;
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            if (kk[u] < 0) continue;
+            if (key[u] >= 0) e.work.slot[kk[u]] = slot[u];
+            e.work.key[kk[u]] = (int)key[u];
+        }
+    }
 }
 
 // ----------------------------------------------------------------- scan --
@@ -386,233 +522,328 @@ __device__ __forceinline__ int block_excl_scan_int(int v, int &total)
     return before + x - v;
 }
 
-// Chunk b of SPHB_SCAN_CHUNK cells: its count total into bsum[b].
-__device__ __forceinline__ void scan_reduce_chunk(const sphb_engine &e, int b)
+// Cells per thread in a scan chunk (256 threads x 16 = SPHB_SCAN_CHUNK).
+constexpr int SCAN_ITEMS = SPHB_SCAN_CHUNK / SPHB_ELEM_TILE;
+static_assert(SCAN_ITEMS % 4 == 0, "scan items come in int4 groups");
+
+// The counts of the thread's SCAN_ITEMS consecutive cells from c0 (zero past
+// T): int4 loads when the table is 16-byte aligned, all issued before use.
+__device__ __forceinline__ void scan_load(const int *count, long long c0, long long T, bool vec,
+                                          int *v)
 {
-    const int T = e.work.meta[0];
-    const long long base = (long long)b * SPHB_SCAN_CHUNK;
+    if (vec && c0 + SCAN_ITEMS <= T) {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS / 4; ++i) {
+            const int4 q = ((const int4 *)(count + c0))[i];
+            v[4 * i] = q.x;
+            v[4 * i + 1] = q.y;
+            v[4 * i + 2] = q.z;
+            v[4 * i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; ++i) v[i] = (c0 + i < T) ? count[c0 + i] : 0;
+    }
+}
+
+// Chunk b of the T used cells: its count total into bsum[b].
+__device__ __forceinline__ void scan_reduce_chunk(const sphb_engine &e, int b, long long T,
+                                                  bool vec)
+{
+    const long long c0 = (long long)b * SPHB_SCAN_CHUNK + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    scan_load(e.work.count, c0, T, vec, v);
     int sum = 0;
-    for (long long c = base + threadIdx.x; c < base + SPHB_SCAN_CHUNK && c < T; c += blockDim.x)
-        sum += e.work.count[c];
-    int total;
-    block_excl_scan_int(sum, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) sum += v[i];
+    const int total = block_reduce(sum, OpSumInt(), 0);
     if (threadIdx.x == 0) e.work.bsum[b] = total;
 }
 
-// One block: the exclusive scan of the nb chunk totals (bsum[nb] = all).
-__device__ void scan_top_block(const sphb_engine &e, int nb)
+// Chunk b: start[c] for its cells, start[T] after the last, and the counts
+// cleared for the next bin.  The chunk's offset is the sum of the totals
+// of the chunks before it, which every block adds up itself (a few
+// thousand L2-resident words at most), so no phase scans the totals.
+__device__ __forceinline__ void scan_apply_chunk(const sphb_engine &e, int b, long long T,
+                                                 bool vec)
 {
-    __shared__ int s_carry;
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    for (int base = 0; base < nb; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int v = i < nb ? e.work.bsum[i] : 0;
-        int total;
-        const int ex = block_excl_scan_int(v, total);
-        const int carry = s_carry;
-        if (i < nb) e.work.bsum[i] = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 0) s_carry = carry + total;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) e.work.bsum[nb] = s_carry;
-}
-
-// Chunk b: start[c] for its cells (ITEMS consecutive cells per thread,
-// ITEMS x blockDim.x = SPHB_SCAN_CHUNK), and the counts cleared for the
-// next bin.
-template <int ITEMS>
-__device__ __forceinline__ void scan_apply_chunk(const sphb_engine &e, int b)
-{
-    const int T = e.work.meta[0];
-    const long long base = (long long)b * SPHB_SCAN_CHUNK;
-    if (T == 0) {
-        if (b == 0 && threadIdx.x == 0) e.work.start[0] = 0;
-        return;
-    }
-    if (base >= T) return;   // block-uniform
-    const long long c0 = base + (long long)threadIdx.x * ITEMS;
-    int v[ITEMS];
+    int pre = 0;
+    for (int i = threadIdx.x; i < b; i += blockDim.x) pre += e.work.bsum[i];
+    __shared__ int s_pre;
+    pre = block_reduce(pre, OpSumInt(), 0);
+    if (threadIdx.x == 0) s_pre = pre;
+    const long long c0 = (long long)b * SPHB_SCAN_CHUNK + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    scan_load(e.work.count, c0, T, vec, v);
     int sum = 0;
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        v[i] = (c0 + i < T) ? e.work.count[c0 + i] : 0;
-        sum += v[i];
-    }
+    for (int i = 0; i < SCAN_ITEMS; ++i) sum += v[i];
     int total;
-    int run = block_excl_scan_int(sum, total) + e.work.bsum[b];
+    int run = block_excl_scan_int(sum, total);   // (its barriers publish s_pre)
+    run += s_pre;
+    int st[SCAN_ITEMS];
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const long long c = c0 + i;
-        if (c < T) {
-            e.work.start[c] = run;
-            e.work.count[c] = 0;  // ready for the next bin
-            run += v[i];
-            if (c == T - 1) e.work.start[T] = run;
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        st[i] = run;
+        run += v[i];
+    }
+    if (vec && c0 + SCAN_ITEMS <= T) {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS / 4; ++i) {
+            ((int4 *)(e.work.start + c0))[i] =
+                make_int4(st[4 * i], st[4 * i + 1], st[4 * i + 2], st[4 * i + 3]);
+            ((int4 *)(e.work.count + c0))[i] = make_int4(0, 0, 0, 0);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; ++i) {
+            if (c0 + i < T) {
+                e.work.start[c0 + i] = st[i];
+                e.work.count[c0 + i] = 0;
+            }
         }
     }
+    if (c0 <= T - 1 && T - 1 < c0 + SCAN_ITEMS) e.work.start[T] = run;
 }
 
 // -------------------------------------------------------------- scatter --
-__device__ __forceinline__ void scatter_tile(const sphb_engine &e, const sphb_tile &t)
+__device__ void scatter_run(const sphb_engine &e, int t0, int t1)
 {
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
-    const int key = e.work.key[k];
-    if (key < 0) return;
-    const int pos = e.work.start[key] + e.work.slot[k];
-    if (pos < 0 || pos >= e.cfg.num_particles) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        return;
+    const int N = e.cfg.num_particles;
+    for (int t = t0; t < t1; t += RU8) {
+        int kk[RU8], seg[RU8];
+        run_particles<RU8>(e, t, t1, kk, seg);
+        int key[RU8], sl[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            key[u] = -1;
+            sl[u] = 0;
+            if (kk[u] >= 0) {
+                key[u] = e.work.key[kk[u]];
+                sl[u] = e.work.slot[kk[u]];
+            }
+        }
+        int pos[RU8];
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) pos[u] = key[u] >= 0 ? e.work.start[key[u]] + sl[u] : -1;
+#pragma unroll
+        for (int u = 0; u < RU8; ++u) {
+            if (kk[u] < 0 || key[u] < 0) continue;
+            if (pos[u] < 0 || pos[u] >= N) flag(e, SPHB_ST_BAD_INDEX);
+            else e.work.perm[pos[u]] = kk[u];
+        }
     }
-    e.work.perm[pos] = k;
 }
 
 // -------------------------------------------------------------- reorder --
-// Thread k takes particle p = perm[k] (the scatter put it somewhere inside
-// its cell's range [b, e)), ranks it among the cell's members by their index
-// in the particle array, and writes it to b + rank: the order inside a cell
-// is canonical whatever order the atomics handed out the slots, and it does
-// not depend on the order the particles had before.
-template <int DIM, bool F32>
-__device__ __forceinline__ void reorder_tile(const sphb_engine &e, int cur, int move_initial,
-                                             const sphb_tile &t)
+// The state one particle carries through a rebin.
+template <int DIM>
+struct Carried {
+    double x, y, z, u, v, w, m, h, rho, rho0;
+    double x0, y0, z0, u0, v0, w0;
+    int idx, tag;
+};
+
+// Every load of particle p's state, issued together.
+template <int DIM>
+__device__ __forceinline__ Carried<DIM> carried_load(const sphb_buffers &S, int p, int mi)
 {
-    const int kk = t.begin + threadIdx.x;
-    if (kk >= t.end) return;
-    const int A = e.cfg.num_arrays;
-    const int s = t.seg / A, a = t.seg - s * A;
-    const int seg_lo = e.seg_offset[t.seg], seg_hi = e.seg_offset[t.seg + 1];
-    const int p = e.work.perm[kk];
-    if (p < seg_lo || p >= seg_hi) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        return;
+    Carried<DIM> c;
+    c.x = S.x[p];
+    c.y = S.y[p];
+    c.u = S.u[p];
+    c.v = S.v[p];
+    c.m = S.m[p];
+    c.h = S.h[p];
+    c.idx = S.idx[p];
+    c.tag = S.tag[p];
+    c.z = c.w = c.rho = c.rho0 = c.z0 = c.w0 = 0.0;
+    c.x0 = c.y0 = c.u0 = c.v0 = 0.0;
+    if (S.rho) c.rho = S.rho[p];
+    if (mi && S.rho0) c.rho0 = S.rho0[p];
+    if (DIM == 3) {
+        c.z = S.z[p];
+        c.w = S.w[p];
     }
-    int k = kk;
-    {
-        const int key = e.work.key[p];
-        const int b = key >= 0 ? e.work.start[key] : -1;
-        const int en = key >= 0 ? e.work.start[key + 1] : -1;
-        if (b < seg_lo || en > seg_hi || kk < b || kk >= en) {
-            flag(e, SPHB_ST_BAD_INDEX);
-            return;
+    if (mi) {
+        c.x0 = S.x0[p];
+        c.y0 = S.y0[p];
+        c.u0 = S.u0[p];
+        c.v0 = S.v0[p];
+        if (DIM == 3) {
+            c.z0 = S.z0[p];
+            c.w0 = S.w0[p];
         }
-        // canonical order inside a cell: by the particle's index in its
-        // array, so the order depends on the positions alone
-        const int *__restrict__ sidx = e.buf[cur].idx;
-        const int me = sidx[p];
-        int rank = 0;
-        for (int i = b; i < en; ++i) rank += (sidx[e.work.perm[i]] < me) ? 1 : 0;
-        k = b + rank;
     }
+    return c;
+}
+
+template <int DIM>
+__device__ __forceinline__ void carried_store(const sphb_buffers &S, const sphb_buffers &D, int k,
+                                              int mi, const Carried<DIM> &c)
+{
+    D.x[k] = c.x;
+    D.y[k] = c.y;
+    D.u[k] = c.u;
+    D.v[k] = c.v;
+    D.m[k] = c.m;
+    D.h[k] = c.h;
+    D.idx[k] = c.idx;
+    D.tag[k] = c.tag;
+    if (S.rho && D.rho) D.rho[k] = c.rho;   // integrated density (continuity)
+    if (mi && S.rho0 && D.rho0) D.rho0[k] = c.rho0;
+    if (DIM == 3) {
+        D.z[k] = c.z;
+        D.w[k] = c.w;
+    }
+    if (mi) {
+        D.x0[k] = c.x0;
+        D.y0[k] = c.y0;
+        D.u0[k] = c.u0;
+        D.v0[k] = c.v0;
+        if (DIM == 3) {
+            D.z0[k] = c.z0;
+            D.w0[k] = c.w0;
+        }
+    }
+}
+
+// Engine position kk takes particle p = perm[kk] (the scatter put it
+// somewhere inside its cell's range [b, e)), ranked among the cell's
+// members by their index in the particle array and written to b + rank: the
+// order inside a cell is canonical whatever order the atomics handed out the
+// slots, and it does not depend on the order the particles had before.  The
+// lookups run RU particles abreast (perm, then key and index, then the
+// cell's range, then the ranks), the state moves two particles at a time,
+// each with all its loads ahead of its stores.
+template <int DIM, bool F32>
+__device__ void reorder_run(const sphb_engine &e, int cur, int mi, int t0, int t1)
+{
+    const int A = e.cfg.num_arrays;
     const sphb_buffers &S = e.buf[cur];
     const sphb_buffers &D = e.buf[cur ^ 1];
-    const double x = S.x[p], y = S.y[p];
-    const double u = S.u[p], v = S.v[p];
-    const double m = S.m[p], h = S.h[p];
-    D.x[k] = x;
-    D.y[k] = y;
-    D.u[k] = u;
-    D.v[k] = v;
-    D.m[k] = m;
-    D.h[k] = h;
-    D.idx[k] = S.idx[p];
-    D.tag[k] = S.tag[p];
-    if (S.rho && D.rho) D.rho[k] = S.rho[p];   // integrated density (continuity)
-    if (move_initial && S.rho0 && D.rho0) D.rho0[k] = S.rho0[p];
-    double z = 0.0, w = 0.0;
-    if (DIM == 3) {
-        z = S.z[p];
-        w = S.w[p];
-        D.z[k] = z;
-        D.w[k] = w;
-    }
-    if (move_initial) {
-        D.x0[k] = S.x0[p];
-        D.y0[k] = S.y0[p];
-        D.u0[k] = S.u0[p];
-        D.v0[k] = S.v0[p];
-        if (DIM == 3) {
-            D.z0[k] = S.z0[p];
-            D.w0[k] = S.w0[p];
+    const int *__restrict__ sidx = S.idx;
+    const int *__restrict__ perm = e.work.perm;
+    for (int t = t0; t < t1; t += RU) {
+        int kk[RU], seg[RU];
+        run_particles<RU>(e, t, t1, kk, seg);
+        int p[RU], key[RU], me[RU], cb[RU], ce[RU], k[RU];
+#pragma unroll
+        for (int u = 0; u < RU; ++u) p[u] = kk[u] >= 0 ? perm[kk[u]] : -1;
+#pragma unroll
+        for (int u = 0; u < RU; ++u) {
+            key[u] = -1;
+            me[u] = 0;
+            if (kk[u] < 0) continue;
+            const int lo = e.seg_offset[seg[u]], hi = e.seg_offset[seg[u] + 1];
+            if (p[u] < lo || p[u] >= hi) {
+                flag(e, SPHB_ST_BAD_INDEX);
+                kk[u] = -1;
+                continue;
+            }
+            key[u] = e.work.key[p[u]];
+            me[u] = sidx[p[u]];
         }
-    }
-    const sphb_scene_state &st = e.sstate[s];
-    const int key = e.work.key[p];
-    int local = key - st.cell_base - a * st.ncells;
-    if (key < 0 || local < 0 || local >= st.ncells) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        local = 0;
-    }
-    e.f.cell[k] = local;
-    if (!F32 && !e.f.anchor) return;
-    const double cs = e.scene[s].cell_size;
-    int cx, cy, cz;
-    cell_coords(local, st.n, cx, cy, cz);
-    // position relative to the origin of the particle's own cell
-    const float xr = (float)(x - (double)(st.lo[0] + cx) * cs);
-    const float yr = (float)(y - (double)(st.lo[1] + cy) * cs);
-    const float zr = DIM == 3 ? (float)(z - (double)(st.lo[2] + cz) * cs) : 0.f;
-    if (F32) {
-        // both copies of the records when the force pass steps the state
-        const float4 g = DIM == 2 ? make_float4(xr, yr, (float)h, (float)m)
-                                  : make_float4(xr, yr, zr, (float)h);
-        ((float4 *)e.f.geo)[k] = g;
-        if (e.f.geo_next) ((float4 *)e.f.geo_next)[k] = g;
-        if (DIM == 2) {
-            const float2 vv = make_float2((float)u, (float)v);
-            ((float2 *)e.f.vel)[k] = vv;
-            if (e.f.vel_next) ((float2 *)e.f.vel_next)[k] = vv;
-        } else {
-            ((float *)e.f.mass)[k] = (float)m;
-            const float4 vv = make_float4((float)u, (float)v, (float)w, 0.f);
-            ((float4 *)e.f.vel)[k] = vv;
-            if (e.f.vel_next) ((float4 *)e.f.vel_next)[k] = vv;
+#pragma unroll
+        for (int u = 0; u < RU; ++u) {
+            cb[u] = ce[u] = -1;
+            if (kk[u] >= 0 && key[u] >= 0) {
+                cb[u] = e.work.start[key[u]];
+                ce[u] = e.work.start[key[u] + 1];
+            }
         }
-    }
-    if (e.f.anchor) {
-        if (DIM == 2) ((float2 *)e.f.anchor)[k] = make_float2(xr, yr);
-        else ((float4 *)e.f.anchor)[k] = make_float4(xr, yr, zr, 0.f);
+#pragma unroll
+        for (int u = 0; u < RU; ++u) {
+            k[u] = -1;
+            if (kk[u] < 0) continue;
+            const int lo = e.seg_offset[seg[u]], hi = e.seg_offset[seg[u] + 1];
+            if (key[u] < 0 || cb[u] < lo || ce[u] > hi || kk[u] < cb[u] || kk[u] >= ce[u]) {
+                flag(e, SPHB_ST_BAD_INDEX);
+                continue;
+            }
+            // canonical order inside a cell: by the particle's index in its
+            // array, so the order depends on the positions alone
+            int rank = 0;
+            for (int i = cb[u]; i < ce[u]; ++i) rank += (sidx[perm[i]] < me[u]) ? 1 : 0;
+            k[u] = cb[u] + rank;
+        }
+#pragma unroll
+        for (int u0 = 0; u0 < RU; u0 += 2) {
+            Carried<DIM> c[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (k[u0 + j] >= 0) c[j] = carried_load<DIM>(S, p[u0 + j], mi);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int u = u0 + j;
+                if (k[u] < 0) continue;
+                carried_store<DIM>(S, D, k[u], mi, c[j]);
+                const int s = seg[u] / A, a = seg[u] - s * A;
+                const sphb_scene_state &st = e.sstate[s];
+                int local = key[u] - st.cell_base - a * st.ncells;
+                if (local < 0 || local >= st.ncells) {
+                    flag(e, SPHB_ST_BAD_INDEX);
+                    local = 0;
+                }
+                e.f.cell[k[u]] = local;
+                if (!F32 && !e.f.anchor) continue;
+                const double cs = e.scene[s].cell_size;
+                int cx, cy, cz;
+                cell_coords(local, st.n, cx, cy, cz);
+                // position relative to the origin of the particle's own cell
+                const float xr = (float)(c[j].x - (double)(st.lo[0] + cx) * cs);
+                const float yr = (float)(c[j].y - (double)(st.lo[1] + cy) * cs);
+                const float zr = DIM == 3 ? (float)(c[j].z - (double)(st.lo[2] + cz) * cs) : 0.f;
+                if (F32) {
+                    // both copies of the records when the force pass steps the state
+                    const float4 g = DIM == 2 ? make_float4(xr, yr, (float)c[j].h, (float)c[j].m)
+                                              : make_float4(xr, yr, zr, (float)c[j].h);
+                    ((float4 *)e.f.geo)[k[u]] = g;
+                    if (e.f.geo_next) ((float4 *)e.f.geo_next)[k[u]] = g;
+                    if (DIM == 2) {
+                        const float2 vv = make_float2((float)c[j].u, (float)c[j].v);
+                        ((float2 *)e.f.vel)[k[u]] = vv;
+                        if (e.f.vel_next) ((float2 *)e.f.vel_next)[k[u]] = vv;
+                    } else {
+                        ((float *)e.f.mass)[k[u]] = (float)c[j].m;
+                        const float4 vv =
+                            make_float4((float)c[j].u, (float)c[j].v, (float)c[j].w, 0.f);
+                        ((float4 *)e.f.vel)[k[u]] = vv;
+                        if (e.f.vel_next) ((float4 *)e.f.vel_next)[k[u]] = vv;
+                    }
+                }
+                if (e.f.anchor) {
+                    if (DIM == 2) ((float2 *)e.f.anchor)[k[u]] = make_float2(xr, yr);
+                    else ((float4 *)e.f.anchor)[k[u]] = make_float4(xr, yr, zr, 0.f);
+                }
+            }
+        }
     }
 }
 
 // After a rebin decided on the device: the gathered state back into
-// buf[cur], same order (the records, anchors and cells already follow it).
+// buf[cur], same order (the records, anchors and cells already follow it),
+// two particles' loads ahead of their stores.
 template <int DIM>
-__device__ __forceinline__ void copy_back_tile(const sphb_engine &e, int cur, int move_initial,
-                                               const sphb_tile &t)
+__device__ void copy_back_run(const sphb_engine &e, int cur, int mi, int t0, int t1)
 {
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
     const sphb_buffers &S = e.buf[cur ^ 1];
     const sphb_buffers &D = e.buf[cur];
-    D.x[k] = S.x[k];
-    D.y[k] = S.y[k];
-    D.u[k] = S.u[k];
-    D.v[k] = S.v[k];
-    D.m[k] = S.m[k];
-    D.h[k] = S.h[k];
-    D.idx[k] = S.idx[k];
-    D.tag[k] = S.tag[k];
-    if (S.rho && D.rho) D.rho[k] = S.rho[k];
-    if (move_initial && S.rho0 && D.rho0) D.rho0[k] = S.rho0[k];
-    if (DIM == 3) {
-        D.z[k] = S.z[k];
-        D.w[k] = S.w[k];
-    }
-    if (move_initial) {
-        D.x0[k] = S.x0[k];
-        D.y0[k] = S.y0[k];
-        D.u0[k] = S.u0[k];
-        D.v0[k] = S.v0[k];
-        if (DIM == 3) {
-            D.z0[k] = S.z0[k];
-            D.w0[k] = S.w0[k];
+    for (int t = t0; t < t1; t += RU) {
+        int kk[RU], seg[RU];
+        run_particles<RU>(e, t, t1, kk, seg);
+#pragma unroll
+        for (int u0 = 0; u0 < RU; u0 += 2) {
+            Carried<DIM> c[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (kk[u0 + j] >= 0) c[j] = carried_load<DIM>(S, kk[u0 + j], mi);
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (kk[u0 + j] >= 0) carried_store<DIM>(S, D, kk[u0 + j], mi, c[j]);
         }
     }
 }
-
 
 // ---------------------------------------------------------- the rebin --
 // One cooperative launch: [decision] -> boxes -> grids -> hash -> scan ->
@@ -627,7 +858,7 @@ k_rebin(const __grid_constant__ sphb_engine e, int cur, int flags)
     const int mi = (flags & SPHB_BIN_MOVE_INITIAL) ? 1 : 0;
     const int nt = e.num_tiles;
     const int nb = (int)((e.cfg.cell_capacity + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK);
-    int *const bar = e.work.bsum + nb + 1;   // the barrier's counters
+    int *const bar = e.work.bsum + nb + 1;   // the barrier's word
     if (blockIdx.x == 0) {
         if (if_needed) decide_block(e, (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0);
         // every rebin measures the scene boxes afresh (only a rebin reads them)
@@ -638,25 +869,32 @@ k_rebin(const __grid_constant__ sphb_engine e, int cur, int flags)
         pdl_trigger();   // the density pass may launch
         return;
     }
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) box_accum_tile(e, cur, e.tiles[t]);
+    int t0, t1;
+    block_tile_run(nt, t0, t1);
+    box_accum_run<DIM>(e, cur, t0, t1);
     grid_barrier(e, bar);
     if (blockIdx.x == 0) grid_setup_block(e);
     grid_barrier(e, bar);
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) hash_tile(e, cur, e.tiles[t]);
+    hash_run<DIM>(e, cur, t0, t1);
     grid_barrier(e, bar);
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) scan_reduce_chunk(e, b);
+    // the scan covers the cells the grids use, not the whole capacity
+    const long long T = *(volatile int *)&e.work.meta[0];
+    const int nbu = (int)((T + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK);
+    const bool vec = ((reinterpret_cast<uintptr_t>(e.work.count) |
+                       reinterpret_cast<uintptr_t>(e.work.start)) & 15) == 0;
+    for (int b = blockIdx.x; b < nbu; b += gridDim.x) scan_reduce_chunk(e, b, T, vec);
     grid_barrier(e, bar);
-    if (blockIdx.x == 0) scan_top_block(e, nb);
+    if (T == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) e.work.start[0] = 0;
+    }
+    for (int b = blockIdx.x; b < nbu; b += gridDim.x) scan_apply_chunk(e, b, T, vec);
     grid_barrier(e, bar);
-    for (int b = blockIdx.x; b < nb; b += gridDim.x)
-        scan_apply_chunk<SPHB_SCAN_CHUNK / SPHB_ELEM_TILE>(e, b);
+    scatter_run(e, t0, t1);
     grid_barrier(e, bar);
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) scatter_tile(e, e.tiles[t]);
-    grid_barrier(e, bar);
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) reorder_tile<DIM, F32>(e, cur, mi, e.tiles[t]);
+    reorder_run<DIM, F32>(e, cur, mi, t0, t1);
     if (!if_needed) return;
     grid_barrier(e, bar);
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) copy_back_tile<DIM>(e, cur, mi, e.tiles[t]);
+    copy_back_run<DIM>(e, cur, mi, t0, t1);
 }
 
 // --------------------------------------------------------- entry points --
@@ -749,9 +987,11 @@ static int rebin_grid(int *out)
 
 // Blocks of a launch: about 4 tiles each, between 2 per SM (a kept-cells
 // launch costs little more than one small kernel) and every resident block
-// (measured on B200 with the 332k-particle dam break: 2 per SM keep the
-// cells in 2 us over a plain launch against 4 us at 3 per SM, while a full
-// rebin takes 88 us at 3 per SM and 94 us at 2)
+// (2 per SM at the rebin's 128 registers).  Measured on B200 with the
+// 332k-particle dam break: a kept-cells launch 4.6 us in a graph (a
+// one-block kernel 3.1 us), a full rebin 86-92 us; 256 drops (2.9M
+// particles) 375 us, of which the gather and the copy back, near the HBM
+// rate, are 260 us.
 template <int DIM, bool F32>
 static int launch_rebin_t(const sphb_engine *e, int cur, int flags, cudaStream_t st)
 {

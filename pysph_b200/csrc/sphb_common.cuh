@@ -161,6 +161,9 @@ struct OpMax {
         return fmax(a, b);
     }
 };
+struct OpSumInt {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a + b; }
+};
 struct OpAddU64 {
     __device__ __forceinline__ unsigned long long
     operator()(unsigned long long a, unsigned long long b) const
