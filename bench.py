@@ -73,7 +73,7 @@ def workload(name):
     from pysph_b200.engine import continuity_scheme, fluid_scheme
     if name == "dam_break":
         arrays, types, params = W.dam_break()
-        return dict(scenes=[(arrays, params)], scheme=fluid_scheme(2), dim=2,
+        return dict(scenes=[(arrays, params)], scheme=fluid_scheme(2), dim=2, types=types,
                     desc="2D dam break, dx=0.0025, 320,000 fluid + 12,018 wall, CFL dt")
     if name == "dam_break_continuity":
         arrays, types, params = W.dam_break()
@@ -83,7 +83,8 @@ def workload(name):
     if name == "drop":
         arrays, types, params = W.elliptical_drop(dx=0.025)
         return dict(scenes=[(arrays, dict(params, dt=1e-5))], scheme=fluid_scheme(1),
-                    dim=2, desc="2D elliptical drop, dx=0.025, 5,025 particles, dt=1e-5")
+                    dim=2, types=types,
+                    desc="2D elliptical drop, dx=0.025, 5,025 particles, dt=1e-5")
     if name == "lattice3d":
         arrays, types, params = W.lattice3d(n=128)
         return dict(scenes=[(arrays, dict(params, dt=1e-6))], scheme=fluid_scheme(1),
@@ -1046,20 +1047,54 @@ def oracle_run(name, steps, warmup, threads, max_scenes=None):
             "steps_per_s": steps / dt, "particles": n, "desc": wl["desc"]}
 
 
+# timed steps of the reference's own Cython path per sample (one host
+# thread: ~5 s per dam-break step on a current Xeon core)
+REF_STEPS = {"dam_break": 2, "drop": 20}
+REF_STEPS_MAX = {"dam_break": 8, "drop": 200}
+
+
+def reference_cython(name, steps, warmup):
+    """The reference's own FP64 Cython path (built from its sources into
+    oracle/_ref by oracle/build_reference.py) on one host thread, through its
+    own API, over `steps` steps after `warmup`; its pair count comes from the
+    oracle port over the same steps (the same states, bit for bit).  None
+    when the build is absent or the workload has no driver there."""
+    from oracle import reference as ref
+    if name not in REF_STEPS or not ref.available():
+        return None
+    wl = workload(name)
+    arrays, p = wl["scenes"][0]
+    r = ref.time_steps(arrays, wl["types"], p, wl["dim"], steps, warmup)
+    o = oracle_run(name, steps, warmup, threads=os.cpu_count() or 1)
+    pairs = o["value"] * o["ms_per_step"] * steps / 1e3
+    return {"value": pairs / r["seconds"], "ms_per_step": 1e3 * r["seconds"] / steps,
+            "steps_per_s": r["steps_per_s"], "steps": steps, "desc": wl["desc"]}
+
+
 def cpu_baseline(args, shape=None, dev=None):
-    """The oracle port (C, 1 thread) on a bounded sample of the workload:
-    a few full steps (about 10-20 s of CPU work).  On the dam break the same
-    leg also checks the bench's FP32C engine and the FP64 GPU path against
-    the FP64 oracle (parity_vs_oracle)."""
-    steps = {"dam_break": 16, "drop": 100, "lattice3d": 1, "batched": 2}[args.workload]
+    """The CPU path on a bounded sample of the workload (about 10-30 s of CPU
+    work): the reference's own Cython path when it is built (kind
+    "reference", one thread: it has no threads), with the oracle port (C,
+    1 thread) beside it; the port alone otherwise.  On the dam break the
+    same leg also checks the bench's FP32C engine and the FP64 GPU path
+    against the FP64 oracle (parity_vs_oracle)."""
+    steps = {"dam_break": 16, "drop": 100, "lattice3d": 1, "batched": 2,
+             "dam_break_continuity": 16}[args.workload]
     scenes = 16 if args.workload == "batched" else None
     r = oracle_run(args.workload, steps, 1, threads=1, max_scenes=scenes)
     sample = f"{steps} PC steps of {r['desc']}"
     if scenes:
         sample += f" (first {scenes} scenes)"
-    out = {"value": r["value"], "unit": "pair-interactions/s", "cores": 1,
-           "kind": "port", "sample": sample, "steps_per_s": r["steps_per_s"],
-           "cpu": cpu_model()}
+    port = {"value": r["value"], "unit": "pair-interactions/s", "cores": 1,
+            "kind": "port", "sample": sample, "steps_per_s": r["steps_per_s"]}
+    out = dict(port, cpu=cpu_model())
+    ref = reference_cython(args.workload, REF_STEPS.get(args.workload, 0), 1)
+    if ref is not None:
+        out = {"value": ref["value"], "unit": "pair-interactions/s", "cores": 1,
+               "kind": "reference",
+               "sample": f"{ref['steps']} PC steps (after 1) of {ref['desc']} through the "
+                         "reference's own Cython path",
+               "steps_per_s": ref["steps_per_s"], "cpu": cpu_model(), "port": port}
     if args.workload == "dam_break" and shape is not None:
         out["parity_vs_oracle"] = parity_vs_oracle(shape, dev)
     return out
@@ -1146,16 +1181,31 @@ def cpu_model():
 
 # ------------------------------------------------------------ reference arm
 def run_reference(args, rank, world):
+    """The reference's CPU implementation of the path on this host: its own
+    Cython build (oracle/_ref) where it is built and drives the workload,
+    on its one thread, over a bounded number of steps; else the oracle port
+    on every host core."""
     if rank != 0:
         return None
     ncores = os.cpu_count() or 1
-    scenes = 32 if args.workload == "batched" else None
-    r = oracle_run(args.workload, args.steps, args.warmup, threads=ncores,
-                   max_scenes=scenes)
-    sample = f"{args.steps} PC steps of {r['desc']}"
-    if scenes:
-        sample += f" (first {scenes} scenes)"
-    res = {"value": r["value"], "ms_per_step": r["ms_per_step"], "sample": sample}
+    ref = None
+    if args.workload in REF_STEPS:
+        steps = max(1, min(args.steps, REF_STEPS_MAX[args.workload]))
+        ref = reference_cython(args.workload, steps, min(args.warmup, 1))
+    if ref is not None:
+        cores, kind = 1, "reference"
+        sample = (f"{ref['steps']} PC steps (after {min(args.warmup, 1)}) of {ref['desc']} "
+                  "through the reference's own Cython path (one thread: it has no threads)")
+        res = {"value": ref["value"], "ms_per_step": ref["ms_per_step"], "sample": sample}
+    else:
+        scenes = 32 if args.workload == "batched" else None
+        r = oracle_run(args.workload, args.steps, args.warmup, threads=ncores,
+                       max_scenes=scenes)
+        sample = f"{args.steps} PC steps of {r['desc']} (the oracle port)"
+        if scenes:
+            sample += f" (first {scenes} scenes)"
+        cores, kind = ncores, "port"
+        res = {"value": r["value"], "ms_per_step": r["ms_per_step"], "sample": sample}
     out = {"metric": METRIC, "impl": "reference", "value": res["value"],
            "unit": "pair-interactions/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
@@ -1163,7 +1213,7 @@ def run_reference(args, rank, world):
            "dtype": "fp64", "data": "synthetic",
            "config": {"workload": args.workload, "sample": res["sample"]},
            "cpu_baseline": {"value": res["value"], "unit": "pair-interactions/s",
-                            "cores": ncores, "kind": "port", "sample": res["sample"]},
+                            "cores": cores, "kind": kind, "sample": res["sample"]},
            "e2e": {"value": res["value"], "unit": "pair-interactions/s",
                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return out

@@ -1,7 +1,8 @@
 """Build the reference's own FP64 Cython particle path (PySPH 0.9beta) in a
-scratch directory, to generate the golden fixtures of tests/golden.
+scratch directory: the checker behind the golden fixtures of tests/golden
+and the reference that bench.py times on the host.
 
-    python tests/golden/build_reference.py --ref <reference checkout> [--out oracle/_ref/refbuild]
+    python oracle/build_reference.py --ref <reference checkout> [--out oracle/_ref/refbuild]
 
 The reference location comes from --ref or the PYSPH_REFERENCE environment
 variable (there is no default); the build goes to oracle/_ref/refbuild,
@@ -19,7 +20,9 @@ imports (cl_utils, locator, domain_manager) are replaced by stubs: this build
 never takes the OpenCL path.  No arithmetic of the particle path is changed.
 
 Nothing here is imported by the product; the build output stays in the
-scratch directory (git-ignored) and is used only by make_golden.py.
+scratch directory (git-ignored) and is used only by the golden-fixture
+script and bench.py's CPU legs (through oracle/reference.py).  An existing
+build is kept unless --force is given.
 """
 from __future__ import annotations
 
@@ -31,7 +34,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ROOT = os.path.dirname(os.path.dirname(HERE))
+ROOT = os.path.dirname(HERE)
 
 MODULES = [
     "base/carray", "base/fast_utils", "base/point", "base/particle_array",
@@ -200,7 +203,13 @@ setup(name="pysph_ref", ext_modules=cythonize(exts, language_level=2, quiet=True
 '''
 
 
-def build(ref, out):
+def build(ref, out, force=False):
+    """Build the reference from the checkout `ref` into `out` (kept when
+    already built, unless force)."""
+    sys.path.insert(0, ROOT)
+    from oracle.reference import available
+    if not force and available(out):
+        return out
     src = os.path.join(ref, "source", "pysph")
     os.makedirs(out, exist_ok=True)
     pkg = os.path.join(out, "pysph")
@@ -224,7 +233,8 @@ if __name__ == "__main__":
     ap.add_argument("--ref", default=os.environ.get("PYSPH_REFERENCE"),
                     help="the reference checkout (default: $PYSPH_REFERENCE)")
     ap.add_argument("--out", default=os.path.join(ROOT, "oracle", "_ref", "refbuild"))
+    ap.add_argument("--force", action="store_true", help="rebuild an existing build")
     a = ap.parse_args()
     if not a.ref:
         ap.error("name the reference checkout with --ref or PYSPH_REFERENCE")
-    print(build(a.ref, a.out))
+    print(build(a.ref, a.out, a.force))

@@ -1,6 +1,6 @@
 """Write the golden fixtures of tests/golden from the reference itself.
 
-    python tests/golden/build_reference.py --ref <reference checkout>
+    python oracle/build_reference.py --ref <reference checkout>
                                                 # patched build in oracle/_ref/refbuild
     python tests/golden/make_golden.py          # writes tests/golden/*.npz
 
@@ -42,35 +42,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle.reference import (SolverView as _SolverView, build_sim,  # noqa: E402
+                              make_array, modules as ref_modules, scheme_ops)
 from pysph_b200 import workloads as W  # noqa: E402
 
 PROPS = ("x", "y", "z", "u", "v", "w", "m", "h", "rho", "p", "cs")
-
-
-def ref_modules(build_dir):
-    sys.path.insert(0, build_dir)
-    import pysph.base.particle_array as PA
-    import pysph.base.particles as P
-    import pysph.base.kernels as K
-    import pysph.sph.sph_calc as C
-    import pysph.sph.funcs.density_funcs as D
-    import pysph.sph.funcs.eos_funcs as E
-    import pysph.sph.funcs.pressure_funcs as PF
-    import pysph.sph.funcs.position_funcs as POS
-    import pysph.sph.funcs.external_force as EF
-    import pysph.sph.funcs.xsph_funcs as X
-    import pysph.sph.funcs.viscosity_funcs as V
-    import pysph.solver.sph_equation as EQ
-    import pysph.solver.integrator as I
-    import pysph.solver.time_step_functions as T
-    from pysph.base.point import Point
-    return dict(PA=PA, P=P, K=K, C=C, D=D, E=E, PF=PF, POS=POS, EF=EF, EQ=EQ, I=I, T=T, X=X,
-                V=V, Point=Point)
-
-
-def make_array(R, props, name, ptype):
-    d = {k: np.asarray(props[k], np.float64).copy() for k in PROPS if k in props}
-    return R["PA"].get_particle_array(name=name, type=ptype, **d)
 
 
 def lists_of(R, particles, src, dst, radius_scale=2.0):
@@ -81,54 +57,6 @@ def lists_of(R, particles, src, dst, radius_scale=2.0):
     off = np.zeros(n + 1, np.int64)
     off[1:] = np.cumsum([len(a) for a in out])
     return off, np.concatenate(out) if out else np.zeros(0, np.int32)
-
-
-def scheme_ops(R, ntypes, c0, rho0, alpha, beta, eta, gy, dim, xsph_eps=None, hks=False):
-    """The summation-density scheme, or with xsph_eps the continuity scheme
-    of the reference's dam-break example (examples/dam-break/dam_break.py:
-    184-241): Tait, SPHDensityRate (integrated rho on every array), momentum,
-    gravity, position stepping and XSPHCorrection on the fluid."""
-    EQ, D, E, PF, POS, EF = R["EQ"], R["D"], R["E"], R["PF"], R["POS"], R["EF"]
-    types = list(range(ntypes))
-    vel = ["u", "v", "w"][:dim]
-    pos = ["x", "y", "z"][:dim]
-    if xsph_eps is None:
-        ops = [EQ.SPHOperation(D.SPHRho.withargs(hks=hks), on_types=types, from_types=types,
-                               updates=["rho"], id="sd"),
-               EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
-                               updates=["p", "cs"], id="eos")]
-    else:
-        ops = [EQ.SPHOperation(E.TaitEquation.withargs(co=c0, ro=rho0), on_types=types,
-                               updates=["p", "cs"], id="eos"),
-               EQ.SPHIntegration(D.SPHDensityRate.withargs(hks=hks), on_types=types,
-                                 from_types=types, updates=["rho"], id="density")]
-    ops.append(EQ.SPHIntegration(PF.MomentumEquation.withargs(alpha=alpha, beta=beta, eta=eta,
-                                                              hks=hks),
-                                 on_types=[0], from_types=types, updates=vel, id="mom"))
-    if gy:
-        ops.append(EQ.SPHIntegration(EF.GravityForce.withargs(gy=gy), on_types=[0],
-                                     updates=vel, id="grav"))
-    ops.append(EQ.SPHIntegration(POS.PositionStepping.withargs(), on_types=[0],
-                                 updates=pos, id="step"))
-    if xsph_eps is not None:
-        ops.append(EQ.SPHIntegration(R["X"].XSPHCorrection.withargs(eps=xsph_eps, hks=hks),
-                                     on_types=[0], from_types=[0], updates=pos, id="xsph"))
-    return ops
-
-
-def build_sim(R, arrays, types, params, dim, xsph_eps=None, integrator=None,
-              variable_h=False, hks=False, kernel="CubicSplineKernel"):
-    pas = [make_array(R, a, f"a{i}", t) for i, (a, t) in enumerate(zip(arrays, types))]
-    particles = R["P"].Particles(pas, variable_h=variable_h)
-    kernel = getattr(R["K"], kernel)(dim=dim)
-    ops = scheme_ops(R, len(pas), params["c0"], params["rho0"], params["alpha"],
-                     params["beta"], params["eta"], params["gravity"][1], dim, xsph_eps, hks)
-    calcs = []
-    for op in ops:
-        calcs.extend(op.get_calcs(particles, kernel))
-    integ = (integrator or R["I"].PredictorCorrectorIntegrator)(particles, calcs)
-    integ.setup_integrator()
-    return pas, particles, integ
 
 
 def state(pas, names=("x", "y", "u", "v", "rho", "p", "cs")):
@@ -207,16 +135,6 @@ def lattice(R):
     for k, n in enumerate(("_tmpx", "_tmpy", "_tmpz")):
         out[f"pgrad_{k}"] = np.asarray(pa.get(n), np.float64).copy()
     return out
-
-
-class _SolverView:
-    """What the time-step functions read from a Solver."""
-
-    def __init__(self, integrator, dt, dim):
-        self.integrator = integrator
-        self.dt = dt
-        self.dim = dim
-        self.count = 0
 
 
 def dam(R):
