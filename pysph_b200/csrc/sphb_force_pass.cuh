@@ -135,12 +135,15 @@ __device__ __forceinline__ void force_finish(const sphb_engine &e, int cur, int 
 // (density_funcs.pyx:119-156) and XSPHCorrection (xsph_funcs.pyx:40-86),
 // each over its own sources, in the same traversal as the momentum.
 // The 2D FP32C momentum-only variants are held to 80 registers (three
-// 256-thread blocks per SM); left alone, the fused stage in the epilogue
-// would take them to 96 (two blocks).  Every other variant is held to 128
-// (two blocks): the FP64 continuity pass would otherwise take 132 and fit
-// one block per SM.
+// 256-thread blocks per SM) with list batches of 4, and to 64 (four blocks)
+// with batches of 2, which then need no spills: on the dam break the
+// latter's pass is 3% shorter (51.6 against 53.4 us), while batches of 4
+// at 64 registers spill 256 B and take 67.5 us.  Left alone, the fused
+// stage in the epilogue would take them to 96 (two blocks).  Every other
+// variant is held to 128 (two blocks): the FP64 continuity pass would
+// otherwise take 132 and fit one block per SM.
 template <int KT, int DIM, bool F32, int LANES, int R, int U, bool CONT>
-__global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? 3 : 2)
+__global__ void __launch_bounds__(256, (F32 && !CONT && DIM == 2) ? (U == 2 ? 4 : 3) : 2)
 k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
         int with_gravity, int mode)
 {
