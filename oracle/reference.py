@@ -119,11 +119,10 @@ class SolverView:
         self.count = 0
 
 
-def time_steps(arrays, types, params, dim, steps, warmup=1, build_dir=BUILD_DIR):
-    """Wall time of `steps` predictor-corrector steps of the summation-density
-    scheme, after `warmup` untimed ones, through the reference's own API on
-    one host thread (its particle path has no threads).  With params["cfl"]
-    > 0 each step is the solver loop's with the CFL rule (count,
+def stepper(arrays, types, params, dim, build_dir=BUILD_DIR):
+    """The reference's particle arrays and a function that advances them one
+    predictor-corrector step of the summation-density scheme.  With
+    params["cfl"] > 0 a step is the solver loop's with the CFL rule (count,
     Particles.update, ViscousAndForceBasedTimeStep.compute_time_step,
     integrate(dt)); otherwise Particles.update and integrate(params["dt"])."""
     R = modules(build_dir)
@@ -142,6 +141,13 @@ def time_steps(arrays, types, params, dim, steps, warmup=1, build_dir=BUILD_DIR)
         else:
             integ.integrate(params.get("dt", 1e-5))
 
+    return pas, step
+
+
+def time_steps(arrays, types, params, dim, steps, warmup=1, build_dir=BUILD_DIR):
+    """Wall time of `steps` steps of `stepper` after `warmup` untimed ones,
+    on one host thread (the reference's particle path has no threads)."""
+    pas, step = stepper(arrays, types, params, dim, build_dir)
     for _ in range(warmup):
         step()
     t0 = time.perf_counter()
