@@ -117,3 +117,40 @@ def test_pair_at_support_radius_excluded(precision):
         # the radius may round in; W and grad W vanish there, so only the
         # pair count can differ
         assert eng.pair_counts()[0] == 4 + 2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_list_overflow_falls_back_to_the_cell_search(precision, lanes):
+    """A 30 x 30 lattice (dx = 0.05, h = 1.3 dx) with a clump of 150 more
+    particles within one smoothing length of its centre: their neighbour
+    sets (~180) exceed the list capacity (88 slots, 44 a lane with 2 lanes),
+    so the density pass marks those lists overflowed (count -1) and every
+    pass searches their cells instead.  The first evaluation and two
+    predictor-corrector steps still match the oracle.  The EOS exponent is
+    1 so that the clump's pressure stays moderate."""
+    dx, n = 0.05, 30
+    gx, gy = np.meshgrid(np.arange(n) * dx, np.arange(n) * dx)
+    h = 1.3 * dx
+    rng = np.random.default_rng(3)
+    r = h * np.sqrt(rng.random(150))
+    t = 2 * np.pi * rng.random(150)
+    c = 0.5 * (n - 1) * dx
+    x = np.concatenate([gx.ravel(), c + r * np.cos(t)])
+    y = np.concatenate([gy.ravel(), c + r * np.sin(t)])
+    arr = _props(x, y, h=h, m=1000.0 * dx * dx, rho=1000.0)
+    params = dict(PARAMS, gamma=1.0)
+    scheme = fluid_scheme(1)
+    eng, osys = _check([arr], params, scheme, precision, lanes=lanes, pair_block=128)
+    cnt = eng.fields["nbr_cnt"][:lanes * eng.N].view(lanes, eng.N)
+    assert bool((cnt == -1).any()), "no list overflowed"
+    for _ in range(2):
+        eng.pc_step()
+        osys.pc_step(1e-5)
+    eng.check_status()
+    O = osys.arrays[0]
+    for nm in ("x", "y"):
+        err = float(np.max(np.abs(eng.get(0, nm).cpu().numpy() - getattr(O, nm)))) / dx
+        assert err <= (1e-10 if precision == "fp64" else 2e-6), nm
+    rho = eng.get(0, "rho").cpu().numpy()
+    assert float(np.max(np.abs(rho - O.rho) / O.rho)) <= RHO_TOL[precision]
