@@ -125,7 +125,8 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
     // meant for reuse
     const int N = e.cfg.num_particles;
     uint32_t *__restrict__ nbr = (e.f.list_cap > 0 && !from_list) ? e.f.nbr : nullptr;
-    const int cap_lane = e.f.list_cap / LANES;
+    // a lane's slots, whole pads of SPHB_LIST_PAD
+    const int cap_lane = (e.f.list_cap / LANES) & ~(SPHB_LIST_PAD - 1);
     const double skin = (nbr && reuse) ? sc.skin_max : 0.0;
     if (nbr && blockIdx.x == 0 && threadIdx.x == 0) {
         // reusable only when recorded with the skin at the anchors (the
@@ -170,9 +171,10 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
             };
             auto load = [&](const EntryF &en) {
                 Rec r;
-                r.ok = en.j < N;
-                const int j = r.ok ? en.j : k;
-                if (filt) r.ok = r.ok && ((rsrc >> seg.array_of(j)) & 1u);
+                // list entries index the set (pads the dest itself); the
+                // clamp only keeps a damaged list inside the arrays
+                const int j = min(en.j, N - 1);
+                r.ok = !filt || ((rsrc >> seg.array_of(j)) & 1u);
                 r.g = __ldg(geo + j);
                 r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
                 r.o = en.o;
@@ -315,7 +317,15 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
         rho = sum;
     }
 
-    if (active && nbr) e.f.nbr_cnt[(size_t)lane * N + k] = cnt <= cap_lane ? cnt : -1;
+    if (active && nbr) {
+        const int c_ok = cnt <= cap_lane ? cnt : -1;
+        if (c_ok >= 0) {
+            const int c_end = (c_ok + SPHB_LIST_PAD - 1) & ~(SPHB_LIST_PAD - 1);
+            for (int c = c_ok; c < c_end; ++c)
+                nbr[(size_t)(lane + LANES * c) * N + k] = nbr_pad<DIM>(k);
+        }
+        e.f.nbr_cnt[(size_t)lane * N + k] = c_ok;
+    }
     density_finish<F32>(e, cur, k, s, a, active && !lists_only, lane, rho, with_eos, np);
 }
 

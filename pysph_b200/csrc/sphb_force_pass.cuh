@@ -230,8 +230,10 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             };
             auto load = [&](const EntryF &en) {
                 Rec r;
-                r.ok = en.j < N;
-                const int j = r.ok ? en.j : k;
+                // list entries index the set (pads the dest itself); the
+                // clamp only keeps a damaged list inside the arrays
+                const int j = min(en.j, N - 1);
+                r.ok = true;
                 r.bit = filt ? 1u << seg.array_of(j) : ~0u;
                 r.g = __ldg(geo + j);
                 r.t = __ldg(th + j);

@@ -155,6 +155,21 @@ __device__ __forceinline__ uint32_t nbr_pack(int j, int o, int dy, int dz)
     return v;
 }
 
+// Each lane's list is padded with nbr_pad entries to a multiple of
+// SPHB_LIST_PAD slots, so the FP32 list loops load whole batches without a
+// per-entry bound.  A pad entry is the dest itself five cells away along x
+// (offset field 7): its squared distance exceeds every support radius
+// (cells are at least half the largest reach wide), so every pass rejects
+// it with the ordinary neighbour test.
+constexpr int SPHB_LIST_PAD = 4;
+
+template <int DIM>
+__device__ __forceinline__ uint32_t nbr_pad(int k)
+{
+    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
+    return (uint32_t)k | (7u << B);
+}
+
 template <int DIM>
 __device__ __forceinline__ void nbr_unpack(uint32_t v, int &j, int &o, int &dy, int &dz)
 {
@@ -234,24 +249,20 @@ __device__ __forceinline__ int list_count(const sphb_engine &e, bool use_list, i
 // U: a batch's U neighbour records are loaded before any is used, and the
 // next batch's list entries are fetched before this batch's records, so a
 // thread keeps U record gathers and U list loads in flight instead of one
-// dependent chain.  The last batch is padded with entries whose index is
-// out of range, which load() marks as not ok.
+// dependent chain.  The last batch reads the list's pad entries (U divides
+// SPHB_LIST_PAD), which the neighbour test rejects.
 template <int DIM, int LANES, int U, typename Load, typename Use>
 __device__ __forceinline__ void list_loop(const sphb_engine &e, int k, int lane, int cnt,
                                           Load &&load, Use &&use)
 {
-    constexpr int B = DIM == 2 ? SPHB_NBR_IDX_BITS_2D : SPHB_NBR_IDX_BITS_3D;
-    constexpr uint32_t PAD = (1u << B) - 1u;   // index >= num_particles
+    static_assert(SPHB_LIST_PAD % U == 0, "batches must end inside the padding");
     const int N = e.cfg.num_particles;
     const uint32_t *__restrict__ p = e.f.nbr + (size_t)lane * N + k;
     const size_t stride = (size_t)LANES * N;
     const int nb = (cnt + U - 1) / U;
     auto fetch = [&](int b, uint32_t *v) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int c = b * U + u;
-            v[u] = c < cnt ? __ldg(p + (size_t)c * stride) : PAD;
-        }
+        for (int u = 0; u < U; ++u) v[u] = __ldg(p + (size_t)(b * U + u) * stride);
     };
     uint32_t v[U];
     if (nb > 0) fetch(0, v);
