@@ -714,23 +714,28 @@ def adjoint_measure(dev, stream):
     r = Rollout(arrays, params, fluid_scheme(1), 2, 2e-6, 200, checkpoint_every=20,
                 precision="fp32c", device=dev)
     # warm: the first forward and backward run eagerly and capture the
-    # step and segment graphs that the timed pair replays
+    # step and segment graphs that the timed pairs replay
     xw = r.forward({0: v0})[0][0]
     r.backward({0: (2.0 * (xw - xt) / n, torch.zeros_like(xw))})
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    xf = r.forward({0: v0})[0][0]
-    ev[1].record(stream)
-    lam = {0: (2.0 * (xf - xt) / n, torch.zeros_like(xf))}
-    g = r.backward(lam)
-    ev[2].record(stream)
-    torch.cuda.synchronize()
-    fwd = ev[0].elapsed_time(ev[1])
-    bwd = ev[1].elapsed_time(ev[2])
+    fwds, bwds = [], []
+    for _ in range(3):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        xf = r.forward({0: v0})[0][0]
+        ev[1].record(stream)
+        lam = {0: (2.0 * (xf - xt) / n, torch.zeros_like(xf))}
+        g = r.backward(lam)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        fwds.append(ev[0].elapsed_time(ev[1]))
+        bwds.append(ev[1].elapsed_time(ev[2]))
+    fwd, bwd = statistics.median(fwds), statistics.median(bwds)
     return {"workload": "elliptical drop 50k (dx=0.0079), 200 steps dt=2e-6, "
                         "checkpoints every 20, FP32C forward, FP64 adjoint",
             "particles": n, "fwd_ms": fwd, "bwd_ms": bwd, "bwd_fwd_ratio": bwd / fwd,
+            "runs": "median of 3 forward + backward pairs",
+            "fwd_ms_runs": fwds, "bwd_ms_runs": bwds,
             "grad_norm": float(torch.linalg.norm(g[0][1]))}
 
 

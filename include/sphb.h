@@ -31,7 +31,7 @@ extern "C" {
 #endif
 
 #define SPHB_MAX_ARRAYS 4
-#define SPHB_ABI_VERSION 1
+#define SPHB_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define SPHB_API __attribute__((visibility("default")))
@@ -185,6 +185,11 @@ typedef struct {
     int32_t *tag;           /* 0 == LocalReal (S/base/particle_array.pxd:20) */
     double *rho, *rho0;     /* integrated density and its stage-initial copy
                                (continuity scheme; may be NULL otherwise) */
+    double *kx, *ky, *kz, *ku, *kv, *kw, *krho;
+                            /* RK4's running sum K1 + 2 K2 + 2 K3 of each
+                               integrated property (stage kinds 4-7; may be
+                               NULL otherwise), carried by rebins with
+                               SPHB_BIN_MOVE_INITIAL like x0 */
 } sphb_buffers;
 
 /* Fields recomputed every stage, in the current engine order.  Element type
@@ -405,14 +410,15 @@ SPHB_API int sphb_tait(const sphb_engine *e, int cur, uint32_t dest_mask, void *
  * alone (a predictor's pass, whose maxima the CFL rule does not read). */
 #define SPHB_FORCE_NO_MAXIMA 32
 /* mode | SPHB_FORCE_STAGE(kind), FP32C with f.geo_next / vel_next: the
- * sphb_pc_stage stage `kind` (0..3) of every dest particle in the pass's
+ * sphb_pc_stage stage `kind` (0..7) of every dest particle in the pass's
  * epilogue, on the accelerations, density rate and XSPH velocity it has
  * just computed.  The new records go to geo_next / vel_next; every stepped
  * array (cfg.step_on) and density-rate dest must be a dest of the pass.
  * Unlike sphb_pc_stage, stage 0 does not clear the CFL maxima: give the
- * predictor's pass SPHB_FORCE_NO_MAXIMA instead. */
+ * predictor's pass (and RK2's first, RK4's first three)
+ * SPHB_FORCE_NO_MAXIMA instead. */
 #define SPHB_FORCE_STAGE(kind) (((kind) + 1) << 8)
-#define SPHB_FORCE_STAGE_MASK 0x700
+#define SPHB_FORCE_STAGE_MASK 0xF00
 SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
                   int with_gravity, int mode, void *stream);
 
@@ -421,8 +427,13 @@ SPHB_API int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
  * RK2's first stage), stage 1 = correct and final (X = 2 (X0 + dt/2 F) -
  * X0), stage 2 = Euler (save X0, X = X0 + dt F;
  * EulerIntegrator.integrate, S/solver/integrator.py:420-447), stage 3 =
- * RK2's second stage (X = X0 + dt F; RK2Integrator, :452-499).  Stage 0 also clears the per-scene
- * dt_fac / |a| maxima, so sphb_step_begin sees the corrector's pass only.
+ * RK2's second stage (X = X0 + dt F; RK2Integrator, :452-499); stages 4-7
+ * are RK4Integrator's four (:504-609), with buf.kx .. krho holding the
+ * running sum S: 4 save X0, S = K1, X = X0 + dt/2 K1; 5 S = S + 2 K2,
+ * X = X0 + dt/2 K2; 6 S = S + 2 K3, X = X0 + dt K3; 7 X = X0 + (dt/6)
+ * (S + K4), in numpy's order of the reference's final_step.  Stages 0, 4,
+ * 5 and 6 also clear the per-scene dt_fac / |a| maxima, so sphb_step_begin
+ * sees the last stage's pass only.
  * Refreshes the FP32 pair records of the moved particles and, with
  * f.anchor, accumulates max_disp2 (cleared by the next SPHB_BIN_IF_NEEDED
  * decision).  PositionStepping

@@ -94,7 +94,11 @@ class Tile(ctypes.Structure):
 
 
 BUFFER_FIELDS = ("x", "y", "z", "u", "v", "w", "x0", "y0", "z0", "u0", "v0",
-                 "w0", "m", "h", "idx", "tag", "rho", "rho0")
+                 "w0", "m", "h", "idx", "tag", "rho", "rho0",
+                 "kx", "ky", "kz", "ku", "kv", "kw", "krho")
+
+
+ABI_VERSION = 2
 
 
 class Buffers(ctypes.Structure):
@@ -182,7 +186,7 @@ def lib():
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    if L.sphb_abi_version() != 1:
+    if L.sphb_abi_version() != ABI_VERSION:
         raise RuntimeError("libsphb.so ABI version mismatch")
     _lib = L
     return L

@@ -708,6 +708,34 @@ __device__ __forceinline__ void carried_store(const sphb_buffers &S, const sphb_
     }
 }
 
+// RK4's running sums of particle p to position k (engines that step RK4
+// have them; the pointers decide, uniformly over the launch).
+template <int DIM>
+__device__ __forceinline__ void carry_sums(const sphb_buffers &S, const sphb_buffers &D, int p,
+                                           int k)
+{
+    if (S.kx && D.kx) {
+        double q[6];
+        q[0] = S.kx[p];
+        q[1] = S.ky[p];
+        q[2] = S.ku[p];
+        q[3] = S.kv[p];
+        if (DIM == 3) {
+            q[4] = S.kz[p];
+            q[5] = S.kw[p];
+        }
+        D.kx[k] = q[0];
+        D.ky[k] = q[1];
+        D.ku[k] = q[2];
+        D.kv[k] = q[3];
+        if (DIM == 3) {
+            D.kz[k] = q[4];
+            D.kw[k] = q[5];
+        }
+    }
+    if (S.krho && D.krho) D.krho[k] = S.krho[p];
+}
+
 // Engine position kk takes particle p = perm[kk] (the scatter put it
 // somewhere inside its cell's range [b, e)), ranked among the cell's
 // members by their index in the particle array and written to b + rank: the
@@ -778,6 +806,7 @@ __device__ void reorder_run(const sphb_engine &e, int cur, int mi, int t0, int t
                 const int u = u0 + j;
                 if (k[u] < 0) continue;
                 carried_store<DIM>(S, D, k[u], mi, c[j]);
+                if (mi) carry_sums<DIM>(S, D, p[u], k[u]);
                 const int s = seg[u] / A, a = seg[u] - s * A;
                 const sphb_scene_state &st = e.sstate[s];
                 int local = key[u] - st.cell_base - a * st.ncells;
@@ -839,8 +868,11 @@ __device__ void copy_back_run(const sphb_engine &e, int cur, int mi, int t0, int
             for (int j = 0; j < 2; ++j)
                 if (kk[u0 + j] >= 0) c[j] = carried_load<DIM>(S, kk[u0 + j], mi);
 #pragma unroll
-            for (int j = 0; j < 2; ++j)
-                if (kk[u0 + j] >= 0) carried_store<DIM>(S, D, kk[u0 + j], mi, c[j]);
+            for (int j = 0; j < 2; ++j) {
+                if (kk[u0 + j] < 0) continue;
+                carried_store<DIM>(S, D, kk[u0 + j], mi, c[j]);
+                if (mi) carry_sums<DIM>(S, D, kk[u0 + j], kk[u0 + j]);
+            }
         }
     }
 }

@@ -9,6 +9,7 @@ namespace sphb {
 
 int check_engine_public(const sphb_engine *e, int cur);
 int check_pair_cfg(const sphb_engine *e);
+int check_stage_sums(const sphb_engine *e, int cur, int kind);
 
 }  // namespace sphb
 
@@ -23,7 +24,8 @@ extern "C" int sphb_momentum(const sphb_engine *e, int cur, uint32_t dest_mask,
     const int fmode = mode & ~(SPHB_FORCE_USE_LIST | SPHB_FORCE_NO_MAXIMA | SPHB_FORCE_STAGE_MASK);
     if (fmode != 0 && fmode != 1 && fmode != 2) return SPHB_ERR_ARG;
     const int kind = ((mode & SPHB_FORCE_STAGE_MASK) >> 8) - 1;
-    if (kind > 3) return SPHB_ERR_ARG;
+    if (kind > 7) return SPHB_ERR_ARG;
+    if ((rc = check_stage_sums(e, cur, kind))) return rc;
     if (kind >= 0) {
         // the fused stage: FP32C, both record copies, the stage buffers,
         // and every stepped / density-rate array a dest of this pass

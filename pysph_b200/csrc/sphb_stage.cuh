@@ -25,7 +25,8 @@ __device__ __forceinline__ double axpy_rn(double x0, double a, double dt)
 }
 
 // Stage kind `stage` (0 predict / RK2 first, 1 correct + final, 2 Euler,
-// 3 RK2 second) of particle k of array a in scene s, from its rates: f the
+// 3 RK2 second, 4-7 the four RK4 stages) of particle k of array a in scene
+// s, from its rates: f the
 // acceleration, xv the XSPH velocity (when xsph), dr the density rate (used
 // for density-rate dests).  Non-LocalReal particles get zero rates.  With
 // geo_out / vel_out (FP32C) the particle's new pair records are written
@@ -42,11 +43,23 @@ __device__ __forceinline__ float stage_particle(const sphb_engine &e, int cur, i
     const sphb_scene_state &st = e.sstate[s];
     const double dt2 = st.dt / 2;
     // the stage: 0 save X0, X = X0 + dt/2 F; 1 X = 2 (X0 + dt/2 F) - X0;
-    // 2 save X0, X = X0 + dt F; 3 X = X0 + dt F
-    const bool save = stage == 0 || stage == 2;
-    const double hstep = stage == 0 ? dt2 : st.dt;
-    auto advance = [&](double cur0, double init, double rate) {
-        if (stage == 1) return __dadd_rn(2 * axpy_rn(init, rate, dt2), -init);
+    // 2 save X0, X = X0 + dt F; 3 X = X0 + dt F.  RK4Integrator
+    // (S/solver/integrator.py:504-609), S the running sum in buf.k*: 4 save
+    // X0, S = F, X = X0 + dt/2 F; 5 S = S + 2 F, X = X0 + dt/2 F; 6 S = S +
+    // 2 F, X = X0 + dt F; 7 X = X0 + (1/6 dt) (S + F), numpy's order of
+    // final_step's X0 + fac dt (K1 + 2 K2 + 2 K3 + K4)
+    const bool save = stage == 0 || stage == 2 || stage == 4;
+    const double hstep = (stage == 0 || stage == 4 || stage == 5) ? dt2 : st.dt;
+    auto advance = [&](double cur0, double init, double rate, double *ks) {
+        switch (stage) {
+        case 1: return __dadd_rn(2 * axpy_rn(init, rate, dt2), -init);
+        case 4: ks[k] = rate; break;
+        case 5:
+        case 6: ks[k] = __dadd_rn(ks[k], 2 * rate); break;
+        case 7: return __dadd_rn(init, __dmul_rn(__dmul_rn(1.0 / 6.0, st.dt),
+                                                 __dadd_rn(ks[k], rate)));
+        default: break;
+        }
         return axpy_rn(save ? cur0 : init, rate, hstep);
     };
     // continuity scheme: the density of every SPHDensityRate dest is
@@ -55,7 +68,7 @@ __device__ __forceinline__ float stage_particle(const sphb_engine &e, int cur, i
         const double r = B.rho[k];
         const double r0 = save ? r : B.rho0[k];
         if (save) B.rho0[k] = r;
-        B.rho[k] = advance(r, r0, dr);
+        B.rho[k] = advance(r, r0, dr, B.krho);
     }
     if (!((e.cfg.step_on >> a) & 1u)) return 0.f;
     const bool disp = e.f.anchor != nullptr;   // displacement check
@@ -63,6 +76,8 @@ __device__ __forceinline__ float stage_particle(const sphb_engine &e, int cur, i
     double *V[3] = {B.u, B.v, B.w};
     double *X0[3] = {B.x0, B.y0, B.z0};
     double *V0[3] = {B.u0, B.v0, B.w0};
+    double *KX[3] = {B.kx, B.ky, B.kz};
+    double *KV[3] = {B.ku, B.kv, B.kw};
     const bool real = B.tag[k] == 0;
     // every load first, so a thread's loads are in flight together
     double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
@@ -100,8 +115,8 @@ __device__ __forceinline__ float stage_particle(const sphb_engine &e, int cur, i
             X0[d][k] = x[d];
             V0[d][k] = v[d];
         }
-        p[d] = advance(x[d], x0[d], fx);
-        vn[d] = advance(v[d], v0[d], fd);
+        p[d] = advance(x[d], x0[d], fx, KX[d]);
+        vn[d] = advance(v[d], v0[d], fd, KV[d]);
         X[d][k] = p[d];
         V[d][k] = vn[d];
     }

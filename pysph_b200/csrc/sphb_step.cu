@@ -43,10 +43,10 @@ k_pc_stage(const __grid_constant__ sphb_engine e, int cur, int stage)
         e.work.meta[2] = 0;
         e.work.meta[3] = 0;
     }
-    if (stage == 0 && blockIdx.x == 0) {
-        // the CFL rule reads the maxima of the corrector's force pass only
+    if ((stage == 0 || (stage >= 4 && stage <= 6)) && blockIdx.x == 0) {
+        // the CFL rule reads the maxima of the step's last force pass only
         // (dt_fac is reset per calc, S/sph/sph_calc.pyx:324): clear what the
-        // predictor's pass accumulated
+        // earlier stages' passes accumulated
         for (int q = threadIdx.x; q < e.cfg.num_scenes; q += blockDim.x) {
             e.sstate[q].max_dtfac = 0ull;
             e.sstate[q].max_acc2 = 0ull;
@@ -276,11 +276,29 @@ extern "C" int sphb_workspace_layout(const sphb_config *cfg, size_t offsets[9],
     return SPHB_OK;
 }
 
+// RK4's stages (kinds 4-7) need the running sums of every integrated
+// property: x, y(, z), u, v(, w) of the stepped arrays, rho of the density
+// rate dests.
+namespace sphb {
+int check_stage_sums(const sphb_engine *e, int cur, int kind)
+{
+    if (kind < 4) return SPHB_OK;
+    const sphb_config &c = e->cfg;
+    const sphb_buffers &B = e->buf[cur];
+    if (c.step_on && (!B.kx || !B.ky || !B.ku || !B.kv || (c.dim == 3 && (!B.kz || !B.kw))))
+        return SPHB_ERR_ARG;
+    for (int a = 0; a < c.num_arrays; ++a)
+        if (c.rate_src[a] && B.rho && !B.krho) return SPHB_ERR_ARG;
+    return SPHB_OK;
+}
+}  // namespace sphb
+
 extern "C" int sphb_pc_stage(const sphb_engine *e, int cur, int stage, void *stream)
 {
     int rc = check_engine_public(e, cur);
     if (rc) return rc;
-    if (stage < 0 || stage > 3) return SPHB_ERR_ARG;
+    if (stage < 0 || stage > 7) return SPHB_ERR_ARG;
+    if ((rc = check_stage_sums(e, cur, stage))) return rc;
     if (!e->f.au || !e->f.av) return SPHB_ERR_ARG;
     const sphb_buffers &B = e->buf[cur];
     if (!B.x0 || !B.y0 || !B.u0 || !B.v0) return SPHB_ERR_ARG;

@@ -336,6 +336,9 @@ class Engine:
             cont = self.scheme.continuity
             b["rho"] = torch.zeros(N, **f64) if cont else None
             b["rho0"] = torch.zeros(N, **f64) if cont else None
+            # RK4's running sums, allocated by the first RK4 step
+            for name in ("kx", "ky", "kz", "ku", "kv", "kw", "krho"):
+                b[name] = None
             self.bufs.append(b)
         f = {}
         if self.f32:
@@ -737,7 +740,10 @@ class Engine:
         if stage is not None:
             if not self.fuses_stage:
                 raise ValueError("this engine runs the integrator stage on its own")
-            mode |= nat.FORCE_STAGE(stage) | (nat.FORCE_NO_MAXIMA if stage == 0 else 0)
+            # the CFL rule reads the step's last force pass: the earlier
+            # stages' passes leave the maxima alone
+            mode |= nat.FORCE_STAGE(stage) | (nat.FORCE_NO_MAXIMA if stage in (0, 4, 5, 6)
+                                              else 0)
         if self.scheme.continuity:
             # TaitEquation on the integrated density, then one pair pass:
             # SPHDensityRate + MomentumEquation + XSPHCorrection; the density
@@ -781,13 +787,23 @@ class Engine:
 
     def step(self, integrator: str = "pc", on_half=None):
         """One step of the named integrator: "pc" (pc_step), "euler"
-        (EulerIntegrator: X = X0 + dt F) or "rk2" (RK2Integrator:
-        X_half = X0 + dt/2 F(X0), X = X0 + dt F(X_half))."""
+        (EulerIntegrator: X = X0 + dt F), "rk2" (RK2Integrator:
+        X_half = X0 + dt/2 F(X0), X = X0 + dt F(X_half)) or "rk4"
+        (RK4Integrator: K1 .. K4 at X0, X0 + dt/2 K1, X0 + dt/2 K2,
+        X0 + dt K3; X = X0 + dt/6 (K1 + 2 K2 + 2 K3 + K4))."""
         if integrator == "pc":
             return self.pc_step(on_half)
-        if integrator not in ("euler", "rk2"):
+        if integrator not in ("euler", "rk2", "rk4"):
             raise NotImplementedError(f"{integrator} is not fused on the engine")
         reuse = nat.BIN_IF_NEEDED if self.step_lists else 0
+        if integrator == "rk4":
+            self._rk4_sums()
+            self._begin_and_bin(reuse)
+            for kind in (4, 5, 6, 7):
+                if kind > 4:
+                    self.bin(nat.BIN_MOVE_INITIAL | reuse)
+                self._stage(kind)
+            return
         self._begin_and_bin(reuse)
         if integrator == "euler":
             self._stage(2)
@@ -797,6 +813,21 @@ class Engine:
             on_half()
         self.bin(nat.BIN_MOVE_INITIAL | reuse)
         self._stage(3)
+
+    def _rk4_sums(self):
+        """RK4's running sums (K1 + 2 K2 + 2 K3 of every integrated
+        property), in both state buffers so that rebins carry them; made
+        once, before the first RK4 step (and before any graph of one)."""
+        if self.bufs[0]["kx"] is not None:
+            return
+        f64 = dict(dtype=torch.float64, device=self.device)
+        names = ["kx", "ky", "ku", "kv"] + (["kz", "kw"] if self.dim == 3 else [])
+        if self.scheme.continuity:
+            names.append("krho")
+        for b in self.bufs:
+            for name in names:
+                b[name] = torch.zeros(self.N, **f64)
+        self._build_desc()
 
     def rebin_count(self) -> int:
         """1 when the last device-decided rebin happened (host sync)."""

@@ -259,15 +259,21 @@ class Integrator:
                 reads |= {(a, "p"), (a, "cs")}
         return reads
 
-    def _fused_outputs(self, s):
+    def _fused_outputs(self, s, last_stage=1):
+        """Mark what the fused step wrote as newer on the engine; the
+        rates of the step's last stage go to _a_<p>_<last_stage> (1 for the
+        predictor-corrector, Euler and RK2, whose stages all write k = 1;
+        4 for RK4, whose K1 .. K3 stay on the device as a running sum)."""
         sc = self.plan.scheme
         dim = self.plan.dim
+        acc = [f"_a_u_{last_stage}", f"_a_v_{last_stage}"] + (
+            [f"_a_w_{last_stage}"] if dim == 3 else [])
         for a in range(len(self.particles.arrays)):
             names = []
             if a in sc.rho_src:
                 names.append("rho")
             if a in sc.rate_src:
-                names += ["rho", "_rho0", "_a_rho_1"]
+                names += ["rho", "_rho0", f"_a_rho_{last_stage}"]
             if a in sc.tait_on:
                 names += ["p", "cs"]
             if a in sc.step_on:
@@ -275,7 +281,7 @@ class Integrator:
                           else ["x", "y", "z", "u", "v", "w"])
                 names += ["_x0", "_y0", "_u0", "_v0"] if dim == 2 else \
                     ["_x0", "_y0", "_z0", "_u0", "_v0", "_w0"]
-                names += ["_a_u_1", "_a_v_1"] + (["_a_w_1"] if dim == 3 else [])
+                names += acc
             if a in sc.mom_src and self.plan.mode == 0:
                 names.append("dt_fac")
             s.mark_engine_newer(a, names)
@@ -289,7 +295,7 @@ class Integrator:
         if not device_dt:
             eng.set_dt_async(dt)
         eng.step(kind)
-        self._fused_outputs(s)
+        self._fused_outputs(s, 4 if kind == "rk4" else 1)
         self.time += dt if not device_dt else 0.0
         self._steps = getattr(self, "_steps", 0) + 1
         if self.check_every and self._steps % self.check_every == 0:
@@ -372,17 +378,15 @@ class RK2Integrator(Integrator):
 
 class RK4Integrator(Integrator):
     """Classical RK4 with four evaluations and X(t+h) = X0 + h/6 (K1 + 2 K2
-    + 2 K3 + K4) (S/solver/integrator.py:504-609).  Its stages run calc by
-    calc on the engine (no fused plan): the four stage rates live in the
-    particle arrays as the reference keeps them."""
+    + 2 K3 + K4) (S/solver/integrator.py:504-609).  With a fused plan the
+    whole step runs on the engine (stage kinds 4-7, K1 + 2 K2 + 2 K3 kept as
+    a running sum on the device, K4 in _a_<p>_4); otherwise calc by calc,
+    the four stage rates in the particle arrays as the reference keeps
+    them."""
 
     def __init__(self, particles, calcs):
         Integrator.__init__(self, particles, calcs)
         self.nsteps = 4
-
-    def setup_integrator(self):
-        Integrator.setup_integrator(self)
-        self.plan = None
 
     def final_step(self, dt):
         fac = 1.0 / 6.0
@@ -394,6 +398,8 @@ class RK4Integrator(Integrator):
                 array.set(**{prop: init + fac * dt * (k1 + 2 * k2 + 2 * k3 + k4)})
 
     def integrate(self, dt, device_dt=False):
+        if self.plan is not None:
+            return self._fused_integrate(dt, device_dt, "rk4")
         self.save_initial_arrays()
         self.reset_accelerations(step=1)
         self.local_time = self.time

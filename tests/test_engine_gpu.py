@@ -14,7 +14,7 @@ import torch
 from helpers import (oracle_from, oracle_density_eos, oracle_momentum, rel_err,
                      pairs_from_oracle)
 from pysph_b200 import workloads as W
-from pysph_b200.engine import Engine, fluid_scheme, SceneParams
+from pysph_b200.engine import Engine, continuity_scheme, fluid_scheme, SceneParams
 from pysph_b200 import _native as nat
 
 pytestmark = pytest.mark.gpu
@@ -512,6 +512,64 @@ def test_euler_step_graph_replays_like_eager_steps():
     for n in ("x", "y", "u", "v", "rho"):
         assert torch.equal(a.get(0, n), b.get(0, n)), n
     del g
+
+
+def test_rk4_step_graph_replays_like_eager_steps():
+    """A captured RK4 step (four fused stages, the record copies swapped
+    four times) replays like eager steps, rebins and running sums
+    included."""
+    arrays, params, scheme, dim = drop(dx=0.05)
+    params = dict(params, dt=1e-5)
+    a = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    b = Engine([(arrays, params)], scheme, dim=2, precision="fp32c")
+    for e in (a, b):
+        e.step("rk4")
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        a.step("rk4")
+    for _ in range(5):
+        g.replay()
+        b.step("rk4")
+    torch.cuda.synchronize()
+    a.check_status()
+    b.check_status()
+    for n in ("x", "y", "u", "v", "rho"):
+        assert torch.equal(a.get(0, n), b.get(0, n)), n
+    del g
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("cont", [False, True])
+@pytest.mark.parametrize("lists", [True, False])
+def test_rk4_against_oracle_with_walls(precision, cont, lists):
+    """RK4 fused on the engine (stage kinds 4-7) on the dam break with walls,
+    summation density or the continuity scheme with XSPH, 3 steps of fixed
+    dt against the oracle's RK4Integrator.  Without list reuse every stage
+    rebins, so the running sums ride through a rebin between every two
+    stages."""
+    arrays, _, params = W.dam_break(dx=0.05)
+    params = dict(params, dt=1e-5, cfl=0.0)
+    scheme = continuity_scheme(2, 0.5) if cont else fluid_scheme(2)
+    eng = Engine([(arrays, params)], scheme, dim=2, precision=precision, step_lists=lists)
+    osys = oracle_from(arrays, params, scheme, 2)
+    for _ in range(3):
+        eng.step("rk4")
+        osys.step(1e-5, "rk4")
+    eng.check_status()
+    O = osys.arrays[0]
+    tol = 1e-10 if precision == "fp64" else 2e-6
+    for n in ("x", "y"):
+        err = float(np.max(np.abs(eng.get(0, n).cpu().numpy() - getattr(O, n)))) / 0.05
+        assert err <= tol, n
+    for n in ("u", "v"):
+        assert rel_err(eng.get(0, n).cpu().numpy(), getattr(O, n)) <= (
+            1e-10 if precision == "fp64" else 2e-5), n
+    for d in range(2):
+        rho = eng.get(d, "rho").cpu().numpy()
+        ref = osys.arrays[d].rho
+        assert float(np.max(np.abs(rho - ref) / ref)) <= (
+            1e-12 if precision == "fp64" else 1e-5), d
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])

@@ -201,10 +201,10 @@ def test_dam_break_continuity_cfl(precision):
         assert np.max(np.abs(rho - ref) / ref) <= rtol, i
 
 
-# -- Euler and RK2 fused on the engine; RK4 calc by calc (test_api_gpu) --------
+# -- Euler, RK2 and RK4 fused on the engine -----------------------------------
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
 @pytest.mark.parametrize("name,kind,cont", [("euler", "euler", False), ("rk2", "rk2", False),
-                                            ("rk2cont", "rk2", True)])
+                                            ("rk4", "rk4", False), ("rk2cont", "rk2", True)])
 def test_integrators_five_steps(precision, name, kind, cont):
     g = load("integrators")
     sch = continuity_scheme(1, 0.5) if cont else fluid_scheme(1)
