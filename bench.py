@@ -731,9 +731,43 @@ def adjoint_measure(dev, stream):
         fwds.append(ev[0].elapsed_time(ev[1]))
         bwds.append(ev[1].elapsed_time(ev[2]))
     fwd, bwd = statistics.median(fwds), statistics.median(bwds)
+    # the adjoint kernels, each timed alone per launch at the final state
+    # (CUDA events on the engine's stream, 20 launches each, L2 warm); the
+    # backward runs them twice per step (once per stage)
+    eng = r.adj
+    r.set_state(r.get_state(r.fwd), eng)
+    eng.density()
+    S = r._scratch
+    mom, rho = r.scheme.mom_dests, r.scheme.rho_dests
+
+    def per_launch(fn, reps=20):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        fn()
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    kernels = {
+        "force_vjp": per_launch(lambda: eng.call(
+            "sphb_force_vjp", eng.cur, mom, S["lam_a"].data_ptr(), S["lam_x"].data_ptr(),
+            S["lam_v"].data_ptr(), S["lam_rho"].data_ptr(), S["lam_p"].data_ptr(),
+            S["lam_c"].data_ptr())),
+        "eos_vjp": per_launch(lambda: eng.call(
+            "sphb_eos_vjp", eng.cur, S["lam_rho"].data_ptr(), S["lam_p"].data_ptr(),
+            S["lam_c"].data_ptr())),
+        "density_vjp": per_launch(lambda: eng.call(
+            "sphb_density_vjp", eng.cur, rho, S["lam_rho"].data_ptr(), S["lam_x"].data_ptr())),
+        "density_fp64": per_launch(eng.density),
+    }
+    eng.check_status()
     return {"workload": "elliptical drop 50k (dx=0.0079), 200 steps dt=2e-6, "
                         "checkpoints every 20, FP32C forward, FP64 adjoint",
             "particles": n, "fwd_ms": fwd, "bwd_ms": bwd, "bwd_fwd_ratio": bwd / fwd,
+            "adjoint_kernel_ms": kernels,
             "runs": "median of 3 forward + backward pairs",
             "fwd_ms_runs": fwds, "bwd_ms_runs": bwds,
             "grad_norm": float(torch.linalg.norm(g[0][1]))}
@@ -968,8 +1002,11 @@ def e2e_facade(wl, args, shape, dev, stream):
     def step():
         f.set(x=host["x"], y=host["y"], u=host["u"], v=host["v"])
         integ.integrate(0.0, device_dt=True)
+        # into the numpy arrays' memory: the six read-backs queued on the
+        # stream, then one wait before the host touches them
         for k in names_out:
-            pinned[k].copy_(f.get(k))   # into the numpy arrays' memory
+            pinned[k].copy_(f.get(k), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
 
     for _ in range(3):
         step()
@@ -995,7 +1032,8 @@ def e2e_facade(wl, args, shape, dev, stream):
            "h2d_bytes_per_step": 8 * n * 4, "d2h_bytes_per_step": 8 * n * len(names_out),
            "api": "ParticleArray.set(numpy) -> PredictorCorrectorIntegrator.integrate "
                   "(device CFL dt) -> ParticleArray.get -> numpy, every step; the numpy "
-                  "arrays live in pinned host memory allocated once",
+                  "arrays live in pinned host memory allocated once, the read-backs "
+                  "queued together and waited for once per step",
            "rebins": "device-decided after each host write of the positions (kept while "
                      "every particle stays within half the list skin of its last rebin)",
            "shape": particles.engine_options}

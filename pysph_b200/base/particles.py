@@ -124,9 +124,13 @@ class Session:
             self.valid[(a, n)] = True
             pa._engine_newer.add(n)
 
-    def ensure(self, reads):
+    def ensure(self, reads, step_decides=False):
         """Import every (array, property) in reads the engine does not hold,
-        then rebin if any position changed."""
+        then rebin if any position changed.  step_decides: an engine step
+        with its own rebin decision follows at once (the fused integrators),
+        so with list reuse and nothing else to import after a rebin the
+        decision is left to that step, which measures the host-written
+        positions first."""
         eng = self.engine
         if self._pos_versions() != self.positions_version:
             self.need_bin = True
@@ -141,6 +145,14 @@ class Session:
         derived = [(a, n) for a, n in reads if n not in MASTER]
         for a, name in masters:
             self._import(a, name)
+        if self.need_bin and step_decides and eng.step_lists and not derived:
+            # the step's first bin refreshes the records and decides; every
+            # derived field the step reads it computes itself
+            eng.invalidate_box()
+            self.need_bin = False
+            self.positions_version = self._pos_versions()
+            for pa in self.particles.arrays:
+                pa.is_dirty = False
         if self.need_bin:
             self.bin()
         for a, name in derived:

@@ -290,7 +290,7 @@ class Integrator:
     def _fused_integrate(self, dt, device_dt, kind):
         """The whole step on the engine (fused plan)."""
         s = self._fused_session()
-        s.ensure(self._fused_reads(s))
+        s.ensure(self._fused_reads(s), step_decides=True)
         eng = s.engine
         if not device_dt:
             eng.set_dt_async(dt)
