@@ -85,9 +85,12 @@ __device__ __forceinline__ bool for_each_candidate(
     int num_particles, unsigned *status, const CellTrim &trim, F &&f)
 {
     // one loop over the whole row range in 3D (cells of ~2.6 particles: the
-    // per-cell loops of a warp diverge), one per cell in 2D (measured: 3D
-    // density search 2.53 -> 2.33 ms, 2D 83 -> 88 us the other way)
-    constexpr bool SPAN = LANES > 1 || DIM == 3;
+    // per-cell loops of a warp diverge) and with cells of half the reach
+    // (R = 2, ~2.3 particles a cell in 2D), one per cell in 2D with cells of
+    // the whole reach (measured: 3D density search 2.53 -> 2.33 ms; the
+    // dam break's recording pass 86.4 -> 83.1 us at R = 2, 83 -> 88 us the
+    // other way at R = 1)
+    constexpr bool SPAN = LANES > 1 || DIM == 3 || R == 2;
     constexpr float RC2 = (R + 1e-3f) * (R + 1e-3f);
     if (!dest_cell_ok<DIM, R>(cx, cy, cz, n)) {
         atomicOr(status, (unsigned)SPHB_ST_BAD_INDEX);
