@@ -761,7 +761,7 @@ def adjoint_measure(dev, stream):
             S["lam_c"].data_ptr())),
         "density_vjp": per_launch(lambda: eng.call(
             "sphb_density_vjp", eng.cur, rho, S["lam_rho"].data_ptr(), S["lam_x"].data_ptr())),
-        "density_fp64": per_launch(eng.density),
+        "density_fp64": per_launch(lambda: eng.density(reuse=True)),
     }
     eng.check_status()
     return {"workload": "elliptical drop 50k (dx=0.0079), 200 steps dt=2e-6, "

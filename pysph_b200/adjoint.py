@@ -79,10 +79,12 @@ class Rollout:
         return {a: (torch.stack([eng.get(a, c) for c in px]),
                     torch.stack([eng.get(a, c) for c in pv])) for a in self.moving}
 
-    def set_state(self, state, eng=None):
+    def set_state(self, state, eng=None, rebin=True):
         """The state into an engine, rebinned there: every restart from the
-        same state (the forward's checkpoints, the backward's recomputes, the
-        VJPs) then starts from the same order and lists."""
+        same state (the forward's checkpoints, the backward's recomputes)
+        then starts from the same order and lists.  rebin=False leaves the
+        rebin to the engine's next decision (the VJPs' stage states, which
+        lie within the list skin of each other)."""
         eng = eng or self.fwd
         px, pv = self._comps()
         for a, (X, V) in state.items():
@@ -91,7 +93,8 @@ class Rollout:
             for d, c in enumerate(pv):
                 eng.exchange_in(a, c, V[d])
         eng.invalidate_box()
-        eng.rebin_now()
+        if rebin:
+            eng.rebin_now()
 
     # -------------------------------------------------------------- forward
     def forward(self, velocities):
@@ -144,18 +147,23 @@ class Rollout:
     def vjp_F(self, state, lam_F):
         """(d F / d(X, V))^T lam_F at state: {array: (lX, lV)}."""
         eng = self.adj
-        self.set_state(state, eng)
-        eng.density()
+        # the stage states of a segment lie close together: the lists of the
+        # last rebin (with their skin) hold every pair while the decision
+        # keeps them, and the VJP kernels test each pair themselves
+        self.set_state(state, eng, rebin=False)
+        eng.density(reuse=True)
         N = eng.N
         dim = self.dim
         dev = self.device
         if self._scratch is None:
-            z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)
-            self._scratch = dict(lam_a=z(dim, N), lam_x=z(dim, N), lam_v=z(dim, N),
-                                 lam_rho=z(N), lam_p=z(N), lam_c=z(N))
+            # one buffer, cleared by one launch per VJP
+            self._scratch_buf = torch.zeros((3 * dim + 3) * N, dtype=torch.float64, device=dev)
+            parts = self._scratch_buf.split([dim * N] * 3 + [N] * 3)
+            self._scratch = dict(lam_a=parts[0].view(dim, N), lam_x=parts[1].view(dim, N),
+                                 lam_v=parts[2].view(dim, N), lam_rho=parts[3],
+                                 lam_p=parts[4], lam_c=parts[5])
         S = self._scratch
-        for t in S.values():
-            t.zero_()
+        self._scratch_buf.zero_()
         for a, L in lam_F.items():
             for d in range(dim):
                 eng.call("sphb_permute", eng.cur, a, 0, L[d].contiguous().data_ptr(),

@@ -666,11 +666,18 @@ class Engine:
         if self.step_lists:
             self.bin(nat.BIN_IF_NEEDED | nat.BIN_MOVE_INITIAL)
 
-    def density(self, dest_mask=None, eos=True):
+    def density(self, dest_mask=None, eos=True, reuse=False):
+        """SPHRho (+ Tait) on the dest arrays.  reuse: with list reuse, read
+        the neighbour lists when the rebin decision that just ran kept them
+        (else record them with the skin), as an integrator stage does; the
+        lists then hold every pair within the support plus the skin."""
         if dest_mask is None:
             dest_mask = self.scheme.rho_dests
         self._sync_cells()
-        self.call("sphb_density", self.cur, dest_mask, 1 if eos else 0)
+        flags = nat.DENSITY_EOS if eos else 0
+        if reuse and self.step_lists:
+            flags |= nat.DENSITY_LIST_IF_VALID
+        self.call("sphb_density", self.cur, dest_mask, flags)
 
     def tait(self, dest_mask=None):
         if dest_mask is None:
