@@ -222,25 +222,24 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 
 
 # DRAM bytes (read + write) per launch from `ncu --set full` on the bench's
-# own workload and launch shape (the dam break, FP32C, lists, 1 lane,
-# 256-thread blocks, cells of half the reach; the force pass with the
-# integrator stage fused into it): the mean of the two captured launches
-# of each kernel (profiles/k_force_dam_break_fp32c.md,
+# own workload (the dam break, FP32C, lists, 1 lane, 256-thread blocks,
+# cells of half the reach, force list batches of 2; the force pass with the
+# integrator stage fused into it): the mean of the two captured launches of
+# each kernel (profiles/k_force_dam_break_fp32c.md,
 # profiles/k_density_dam_break_fp32c.md)
-NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((72.00e6 + 2.66e6) +
-                                                                (61.76e6 + 3.24e6)),
-               ("dam_break", "fp32c", "lists", "density"): 40.98e6 + 0.007e6,
+NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((73.26e6 + 2.63e6) +
+                                                                (63.02e6 + 2.79e6)),
+               ("dam_break", "fp32c", "lists", "density"): 44.89e6 + 0.03e6,
                ("dam_break", "fp32c", "lists", "pc_stage"): 17.951e6 + 0.000256e6}
 
 
-# FP32 work of one launch: flops = 2 FFMA + FADD + FMUL + 4 FFMA2 + 2 FADD2 +
-# 2 FMUL2 (sm__sass_thread_inst_executed_op_*, from a capture with those
-# metrics; the list entries, hence the flops, do not depend on the cell
-# size), and the fraction of cycles the schedulers issued
-# (smsp__issue_active.avg.pct_of_peak_sustained_active, the capture above)
-NCU_FP32 = {("dam_break", "fp32c", "lists", "force"): {"flops": 398.5e6, "issue_active": 0.564},
+# FP32 work of one launch from the same capture: flops = 2 FFMA + FADD +
+# FMUL + 4 FFMA2 + 2 FADD2 + 2 FMUL2 (sm__sass_thread_inst_executed_op_*;
+# no paired instructions were issued), and the fraction of cycles the
+# schedulers issued (smsp__issue_active.avg.pct_of_peak_sustained_active)
+NCU_FP32 = {("dam_break", "fp32c", "lists", "force"): {"flops": 402.0e6, "issue_active": 0.584},
             ("dam_break", "fp32c", "lists", "density"): {"flops": 228.9e6,
-                                                         "issue_active": 0.738}}
+                                                         "issue_active": 0.728}}
 
 
 def fma_peaks(dev):
