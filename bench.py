@@ -774,9 +774,9 @@ def adjoint_measure(dev, stream):
 
 def launches_per_step(eng):
     """Kernels launched per PC step (every launch counts, including the
-    rebin kernels that return at once when the device keeps the lists)."""
-    # per rebin: [decide] + grid, hash, 3 scan, scatter, reorder [+ copy back]
-    rebin = 7 + (2 if eng.step_lists else 0)
+    rebin launches that return at once when the device keeps the lists)."""
+    # per bin: one cooperative k_rebin (decision, and every phase of a rebin)
+    rebin = 1
     # per stage: density, force, and pc_stage unless the force pass runs it
     stage = 2 if eng.fuses_stage else 3
     # the step prologue: its own launch, or inside the first decision
