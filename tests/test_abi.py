@@ -105,3 +105,30 @@ def test_host_helpers(lib):
     assert lib.sphb_bin(None, 0, 0, None) == -1
     assert lib.sphb_density(None, 0, 1, 1, None) == -1
     assert lib.sphb_make_tiles(None, 1, 256, None, ctypes.byref(n)) == -1
+
+
+def test_stage_kinds_checked_on_the_host(lib):
+    """sphb_pc_stage and sphb_momentum refuse stage kinds outside 0..7, and
+    RK4's kinds 4-7 without the running-sum buffers, before any launch.
+    The descriptor's pointers are placeholders: the host checks never
+    dereference them, and every call here returns before a launch."""
+    d = nat.EngineDesc()
+    c = d.cfg
+    c.dim, c.precision, c.num_scenes, c.num_arrays = 2, nat.FP64, 1, 1
+    c.stencil, c.lanes, c.pair_block = 1, 1, 128
+    c.num_particles, c.cell_capacity, c.step_on = 10, 100, 1
+    c.mom_src[0] = 1
+    p = 0x1000
+    d.tiles = d.pair_tiles = d.seg_offset = d.scene = d.sstate = p
+    d.num_tiles = d.num_pair_tiles = 1
+    for name in ("x", "y", "u", "v", "x0", "y0", "u0", "v0", "m", "h", "idx", "tag"):
+        setattr(d.buf[0], name, p)
+    d.f.au = d.f.av = d.f.dt_fac = p
+    e = ctypes.byref(d)
+    for kind in (-1, 8):
+        assert lib.sphb_pc_stage(e, 0, kind, None) == -1, kind
+    assert lib.sphb_pc_stage(e, 0, 4, None) == -1   # RK4 without its sums
+    assert lib.sphb_pc_stage(e, 0, 7, None) == -1
+    # the fused stage's kind travels in the mode's bits 8-11
+    assert lib.sphb_momentum(e, 0, 1, 1, (8 + 1) << 8, None) == -1
+    assert lib.sphb_momentum(e, 0, 1, 1, (4 + 1) << 8, None) == -1
