@@ -230,7 +230,11 @@ def replica_result(ms_per_rank, pairs_per_rank, steps, world, device="cuda"):
 NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((73.26e6 + 2.63e6) +
                                                                 (63.02e6 + 2.79e6)),
                ("dam_break", "fp32c", "lists", "density"): 44.89e6 + 0.03e6,
-               ("dam_break", "fp32c", "lists", "pc_stage"): 17.951e6 + 0.000256e6}
+               ("dam_break", "fp32c", "lists", "pc_stage"): 17.951e6 + 0.000256e6,
+               # the 256 drops (block 128, the rest as above;
+               # profiles/k_pairs_batched_fp32c.md)
+               ("batched", "fp32c", "lists", "force"): 584.14e6 + 257.38e6,
+               ("batched", "fp32c", "lists", "density"): 389.21e6 + 40.19e6}
 
 
 # FP32 work of one launch from the same capture: flops = 2 FFMA + FADD +
@@ -239,7 +243,10 @@ NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((73.26e6 + 2.63e
 # schedulers issued (smsp__issue_active.avg.pct_of_peak_sustained_active)
 NCU_FP32 = {("dam_break", "fp32c", "lists", "force"): {"flops": 402.0e6, "issue_active": 0.584},
             ("dam_break", "fp32c", "lists", "density"): {"flops": 228.9e6,
-                                                         "issue_active": 0.728}}
+                                                         "issue_active": 0.728},
+            ("batched", "fp32c", "lists", "force"): {"flops": 3566.3e6, "issue_active": 0.618},
+            ("batched", "fp32c", "lists", "density"): {"flops": 1962.6e6,
+                                                       "issue_active": 0.865}}
 
 
 def fma_peaks(dev):
