@@ -230,6 +230,30 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 };
                 const int lc = list_count<LANES>(e, from_list, k, lane);
                 if (lc >= 0) {
+                    if (UH && !filt && !lists_only) {
+                        // the common case, with the tests that cannot fail
+                        // there out of the loop: the same arithmetic as use()
+                        auto load_all = [&](const EntryF &en) {
+                            Rec r;
+                            const int j = min(en.j, N - 1);
+                            r.ok = true;
+                            r.g = __ldg(geo + j);
+                            r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
+                            r.o = en.o;
+                            r.dy = en.dy;
+                            r.dz = en.dz;
+                            return r;
+                        };
+                        list_loop<DIM, LANES, 4>(e, k, lane, lc, load_all, [&](const Rec &r) {
+                            const float r2 = dist2(r);
+                            if (r2 < rad2) {
+                                const float ir = rsqrtf(fmaxf(r2, 1e-30f));   // q = 0 at r = 0
+                                acc.add(r.m * Kern<KT>::w_bf(r2 * ir * ihk, fack));
+                                ++np;
+                            }
+                        });
+                        return;
+                    }
                     list_loop<DIM, LANES, 4>(e, k, lane, lc, load,
                                              [&](const Rec &r) { use(r, dist2(r)); });
                     return;

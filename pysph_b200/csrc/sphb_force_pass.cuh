@@ -260,102 +260,125 @@ k_force(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
             };
             auto pass = [&](auto uniform) {
                 constexpr bool UH = decltype(uniform)::value;
-                auto use = [&](const Rec &r) {
-                    const float rx = (xk - r.g.x) - r.o * csf;
-                    const float ry = (yk - r.g.y) - r.dy * csf;
-                    float rz = 0.f;
-                    float r2 = rx * rx + ry * ry;
-                    if (DIM == 3) {
-                        rz = (zk - r.g.z) - r.dz * csf;
-                        r2 += rz * rz;
-                    }
-                    if (!r.ok) return;
-                    const float hj = DIM == 3 ? r.g.w : r.g.z;
-                    if (UH || !vh) {
-                        if (!(r2 < rad2)) return;
-                    } else {
-                        const float rj = hj * rsf;   // r < radius_scale max(h_a, h_b)
-                        if (!(r2 < rad2 || r2 < rj * rj)) return;
-                    }
-                    ++np;
-                    const bool mom_on = !CONT || (mm & r.bit);
-                    const bool rate_on = CONT && (rm & r.bit);
-                    const bool xs_on = CONT && (xm & r.bit);
-                    float hab = hk, eh2 = eh2k;
-                    if (!UH) {
-                        hab = 0.5f * (hk + hj);
-                        eh2 = eta2 * hab * hab;
-                    }
-                    // P_a/rho_a^2 + P_b/rho_b^2 (none in the split viscosity)
-                    float tmp = avisc ? 0.f : tk.w + r.t.w;
-                    const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
-                    float dot = vx * rx + vy * ry;
-                    if (DIM == 3) dot += vz * rz;
-                    // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
-                    const float ir = rsqrtf(fmaxf(r2, 1e-30f));
-                    // grad W / r (and W for XSPH) at h_ab, or with hks the means
-                    // of the values at h_a and h_b: one evaluation in a loop
-                    // keeps the register count of the uniform-h path
-                    float gw, w = 0.f;
-                    if (UH) {
-                        const float q = r2 * ir * ihk;
-                        gw = Kern<KT>::gw_bf(q, ir, ihk, fihk);
-                        if (CONT && xs_on) w = Kern<KT>::w_bf(q, fihk * hk);
-                    } else {
-                        const float rr = r2 * ir;
-                        float hs = hks ? hk : hab;
-                        gw = 0.f;
-#pragma unroll 1
-                        for (int t = 0;; ++t) {
-                            const float ih = __fdividef(1.0f, hs);
-                            const float fih = DIM == 2 ? kf * ih * ih * ih : kf * ih * ih * ih * ih;
-                            const float q = rr * ih;
-                            gw += Kern<KT>::gw_bf(q, ir, ih, fih);
-                            if (CONT && xs_on) w += Kern<KT>::w_bf(q, fih * hs);
-                            if (!hks || t == 1) break;
-                            hs = hj;
+                // the pair body; with the force mode known at compile time
+                // (KM = 0 MomentumEquation, 1 SPHPressureGradient, 2 the
+                // split viscosity; -1 read at run time) the list loop
+                // carries no test of it
+                auto make_use = [&](auto known) {
+                    constexpr int KM = decltype(known)::value;
+                    const bool visc_k = KM < 0 ? visc : KM == 0;
+                    const bool avisc_k = KM < 0 ? avisc : KM == 2;
+                    return [&, visc_k, avisc_k](const Rec &r) {
+                        const float rx = (xk - r.g.x) - r.o * csf;
+                        const float ry = (yk - r.g.y) - r.dy * csf;
+                        float rz = 0.f;
+                        float r2 = rx * rx + ry * ry;
+                        if (DIM == 3) {
+                            rz = (zk - r.g.z) - r.dz * csf;
+                            r2 += rz * rz;
                         }
-                        if (hks) {
-                            gw *= 0.5f;
-                            w *= 0.5f;
+                        if (!r.ok) return;
+                        const float hj = DIM == 3 ? r.g.w : r.g.z;
+                        if (UH || !vh) {
+                            if (!(r2 < rad2)) return;
+                        } else {
+                            const float rj = hj * rsf;   // r < radius_scale max(h_a, h_b)
+                            if (!(r2 < rad2 || r2 < rj * rj)) return;
                         }
-                    }
-                    if (CONT) {
-                        // drho_a += m_b (v_a - v_b) . grad_a W
-                        if (rate_on) kr.add(r.m * (dot * gw));
-                        // XSPH: eps m_b W_ab (v_b - v_a) / rho_ab (eps at the end)
-                        if (xs_on) {
-                            const float temp = __fdividef(r.m * w, 0.5f * (tk.x + r.t.x));
-                            kxx.add(-temp * vx);
-                            kxy.add(-temp * vy);
-                            if (DIM == 3) kxz.add(-temp * vz);
+                        ++np;
+                        const bool mom_on = !CONT || (mm & r.bit);
+                        const bool rate_on = CONT && (rm & r.bit);
+                        const bool xs_on = CONT && (xm & r.bit);
+                        float hab = hk, eh2 = eh2k;
+                        if (!UH) {
+                            hab = 0.5f * (hk + hj);
+                            eh2 = eta2 * hab * hab;
                         }
-                        if (!mom_on) return;
-                    }
-                    if (visc || avisc) {
-                        const float mu = __fdividef(hab * dot, r2 + eh2);
-                        // the split viscosity's dt_fac has 0.01 h_ab^2 written in
-                        // (viscosity_funcs.pyx:103) whatever its eta
-                        dtmax = fmaxf(dtmax, fabsf(avisc ? __fdividef(hab * dot,
-                                                                       r2 + 0.01f * hab * hab)
-                                                         : mu));
-                        // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
-                        // when v_ab . r_ab < 0, i.e. mu < 0; else 0: min(mu, 0)
-                        const float mn = fminf(mu, 0.f);
-                        const float cab = 0.5f * (tk.z + r.t.z);
-                        const float rhoab = 0.5f * (tk.x + r.t.x);
-                        tmp += __fdividef(-alpha * cab * mn + beta * mn * mn, rhoab);
-                    }
-                    const float f = -r.m * tmp * gw;
-                    ax.add(f * rx);
-                    ay.add(f * ry);
-                    if (DIM == 3) az.add(f * rz);
+                        // P_a/rho_a^2 + P_b/rho_b^2 (none in the split viscosity)
+                        float tmp = avisc_k ? 0.f : tk.w + r.t.w;
+                        const float vx = uk - r.vx, vy = vk - r.vy, vz = wk - r.vz;
+                        float dot = vx * rx + vy * ry;
+                        if (DIM == 3) dot += vz * rz;
+                        // r = 0 (self) gives q = 0 and a finite gradient times r_ab = 0
+                        const float ir = rsqrtf(fmaxf(r2, 1e-30f));
+                        // grad W / r (and W for XSPH) at h_ab, or with hks the means
+                        // of the values at h_a and h_b: one evaluation in a loop
+                        // keeps the register count of the uniform-h path
+                        float gw, w = 0.f;
+                        if (UH) {
+                            const float q = r2 * ir * ihk;
+                            gw = Kern<KT>::gw_bf(q, ir, ihk, fihk);
+                            if (CONT && xs_on) w = Kern<KT>::w_bf(q, fihk * hk);
+                        } else {
+                            const float rr = r2 * ir;
+                            float hs = hks ? hk : hab;
+                            gw = 0.f;
+    #pragma unroll 1
+                            for (int t = 0;; ++t) {
+                                const float ih = __fdividef(1.0f, hs);
+                                const float fih = DIM == 2 ? kf * ih * ih * ih : kf * ih * ih * ih * ih;
+                                const float q = rr * ih;
+                                gw += Kern<KT>::gw_bf(q, ir, ih, fih);
+                                if (CONT && xs_on) w += Kern<KT>::w_bf(q, fih * hs);
+                                if (!hks || t == 1) break;
+                                hs = hj;
+                            }
+                            if (hks) {
+                                gw *= 0.5f;
+                                w *= 0.5f;
+                            }
+                        }
+                        if (CONT) {
+                            // drho_a += m_b (v_a - v_b) . grad_a W
+                            if (rate_on) kr.add(r.m * (dot * gw));
+                            // XSPH: eps m_b W_ab (v_b - v_a) / rho_ab (eps at the end)
+                            if (xs_on) {
+                                const float temp = __fdividef(r.m * w, 0.5f * (tk.x + r.t.x));
+                                kxx.add(-temp * vx);
+                                kxy.add(-temp * vy);
+                                if (DIM == 3) kxz.add(-temp * vz);
+                            }
+                            if (!mom_on) return;
+                        }
+                        if (visc_k || avisc_k) {
+                            const float mu = __fdividef(hab * dot, r2 + eh2);
+                            // the split viscosity's dt_fac has 0.01 h_ab^2 written in
+                            // (viscosity_funcs.pyx:103) whatever its eta
+                            dtmax = fmaxf(dtmax, fabsf(avisc_k ? __fdividef(hab * dot,
+                                                                           r2 + 0.01f * hab * hab)
+                                                             : mu));
+                            // Monaghan Pi_ab = (-alpha c_ab mu + beta mu^2) / rho_ab
+                            // when v_ab . r_ab < 0, i.e. mu < 0; else 0: min(mu, 0)
+                            const float mn = fminf(mu, 0.f);
+                            const float cab = 0.5f * (tk.z + r.t.z);
+                            const float rhoab = 0.5f * (tk.x + r.t.x);
+                            tmp += __fdividef(-alpha * cab * mn + beta * mn * mn, rhoab);
+                        }
+                        const float f = -r.m * tmp * gw;
+                        ax.add(f * rx);
+                        ay.add(f * ry);
+                        if (DIM == 3) az.add(f * rz);
+                    };
                 };
                 const int lc = list_count<LANES>(e, use_list, k, lane);
                 if (lc >= 0) {
-                    list_loop<DIM, LANES, U>(e, k, lane, lc, load, use);
+                    switch (mode & 15) {   // block-uniform
+                    case 0:
+                        list_loop<DIM, LANES, U>(e, k, lane, lc, load,
+                                                 make_use(std::integral_constant<int, 0>{}));
+                        break;
+                    case 1:
+                        list_loop<DIM, LANES, U>(e, k, lane, lc, load,
+                                                 make_use(std::integral_constant<int, 1>{}));
+                        break;
+                    default:
+                        list_loop<DIM, LANES, U>(e, k, lane, lc, load,
+                                                 make_use(std::integral_constant<int, 2>{}));
+                        break;
+                    }
                     return;
                 }
+                auto use = make_use(std::integral_constant<int, -1>{});
                 int cx, cy, cz;
                 cell_coords(e.f.cell[k], n, cx, cy, cz);
                 for_each_candidate<DIM, R, LANES>(
