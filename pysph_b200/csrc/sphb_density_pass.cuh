@@ -228,30 +228,33 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                     acc.add(r.m * w);
                     ++np;
                 };
+                // the common case (one h, every source summed, densities
+                // wanted) with the tests that cannot fail there out of the
+                // loops: the same arithmetic as load() and use()
+                const bool plain = UH && !filt && !lists_only;
+                auto load_all = [&](const EntryF &en) {
+                    Rec r;
+                    const int j = min(en.j, N - 1);
+                    r.ok = true;
+                    r.g = __ldg(geo + j);
+                    r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
+                    r.o = en.o;
+                    r.dy = en.dy;
+                    r.dz = en.dz;
+                    return r;
+                };
+                auto sum_plain = [&](const Rec &r, float r2) {
+                    if (r2 < rad2) {
+                        const float ir = rsqrtf(fmaxf(r2, 1e-30f));   // q = 0 at r = 0
+                        acc.add(r.m * Kern<KT>::w_bf(r2 * ir * ihk, fack));
+                        ++np;
+                    }
+                };
                 const int lc = list_count<LANES>(e, from_list, k, lane);
                 if (lc >= 0) {
-                    if (UH && !filt && !lists_only) {
-                        // the common case, with the tests that cannot fail
-                        // there out of the loop: the same arithmetic as use()
-                        auto load_all = [&](const EntryF &en) {
-                            Rec r;
-                            const int j = min(en.j, N - 1);
-                            r.ok = true;
-                            r.g = __ldg(geo + j);
-                            r.m = DIM == 3 ? __ldg(mass + j) : r.g.w;
-                            r.o = en.o;
-                            r.dy = en.dy;
-                            r.dz = en.dz;
-                            return r;
-                        };
-                        list_loop<DIM, LANES, 4>(e, k, lane, lc, load_all, [&](const Rec &r) {
-                            const float r2 = dist2(r);
-                            if (r2 < rad2) {
-                                const float ir = rsqrtf(fmaxf(r2, 1e-30f));   // q = 0 at r = 0
-                                acc.add(r.m * Kern<KT>::w_bf(r2 * ir * ihk, fack));
-                                ++np;
-                            }
-                        });
+                    if (plain) {
+                        list_loop<DIM, LANES, 4>(e, k, lane, lc, load_all,
+                                                 [&](const Rec &r) { sum_plain(r, dist2(r)); });
                         return;
                     }
                     list_loop<DIM, LANES, 4>(e, k, lane, lc, load,
@@ -260,6 +263,23 @@ k_density(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, in
                 }
                 int cx, cy, cz;
                 cell_coords(e.f.cell[k], n, cx, cy, cz);
+                if (plain && nbr) {
+                    // the recording pass of the common case
+                    for_each_candidate<DIM, R, LANES>(
+                        start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
+                        cell_trim_rel(e, xk, yk, zk, csf), [&](int j, int o, int dy, int dz) {
+                            const Rec r = load_all(EntryF{j, (float)o, (float)dy, (float)dz});
+                            const float r2 = dist2(r);
+                            if (r2 < radl2) {
+                                if (cnt < cap_lane)
+                                    nbr[(size_t)(lane + LANES * cnt) * N + k] =
+                                        nbr_pack<DIM>(j, o, dy, dz);
+                                ++cnt;
+                            }
+                            sum_plain(r, r2);
+                        });
+                    return;
+                }
                 for_each_candidate<DIM, R, LANES>(
                     start, A, src, cell_base, ncells, n, cx, cy, cz, lane, N, e.work.status,
                     cell_trim_rel(e, xk, yk, zk, csf), [&](int j, int o, int dy, int dz) {
