@@ -233,8 +233,8 @@ NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((73.27e6 + 3.05e
                ("dam_break", "fp32c", "lists", "pc_stage"): 17.951e6 + 0.000256e6,
                # the 256 drops (block 128, the rest as above;
                # profiles/k_pairs_batched_fp32c.md)
-               ("batched", "fp32c", "lists", "force"): 584.14e6 + 257.38e6,
-               ("batched", "fp32c", "lists", "density"): 389.21e6 + 40.19e6}
+               ("batched", "fp32c", "lists", "force"): 583.87e6 + 257.02e6,
+               ("batched", "fp32c", "lists", "density"): 389.22e6 + 43.41e6}
 
 
 # FP32 work of one launch from the same capture: flops = 2 FFMA + FADD +
@@ -244,9 +244,9 @@ NCU_TRAFFIC = {("dam_break", "fp32c", "lists", "force"): 0.5 * ((73.27e6 + 3.05e
 NCU_FP32 = {("dam_break", "fp32c", "lists", "force"): {"flops": 396.3e6, "issue_active": 0.587},
             ("dam_break", "fp32c", "lists", "density"): {"flops": 225.6e6,
                                                          "issue_active": 0.663},
-            ("batched", "fp32c", "lists", "force"): {"flops": 3566.3e6, "issue_active": 0.618},
-            ("batched", "fp32c", "lists", "density"): {"flops": 1962.6e6,
-                                                       "issue_active": 0.865}}
+            ("batched", "fp32c", "lists", "force"): {"flops": 3507.2e6, "issue_active": 0.585},
+            ("batched", "fp32c", "lists", "density"): {"flops": 1934.9e6,
+                                                       "issue_active": 0.801}}
 
 
 def fma_peaks(dev):
