@@ -242,9 +242,11 @@ typedef struct {
     int32_t *slot;          /* [N] */
     int32_t *perm;          /* [N] */
     int32_t *bsum;          /* [scan blocks + 1 + 64]: the scan's chunk totals,
-                               then the rebin's grid-barrier word (its low
-                               31 bits zero when the workspace is first
-                               used) */
+                               then the rebin's grid-barrier word and the
+                               arrival count of a launch that keeps the
+                               cells (both zero when the workspace is first
+                               used; the barrier word's low 31 bits and the
+                               count return to zero after every launch) */
     int32_t *meta;          /* [8]  meta[0] = cells in use (all scenes);
                                meta[1] = 1 when the last rebin decision
                                rebinned; meta[2] = 1 when it kept the lists

@@ -64,37 +64,49 @@ __device__ __forceinline__ void grid_barrier(const sphb_engine &e, int *word_)
     __syncthreads();
 }
 
-// ---------------------------------------------------------------- boxes --
-// Block 0.  No rebin while the particles sit where the last rebin put
-// them (work.meta[3] == 2); otherwise rebin unless the lists were recorded
-// with the skin at those positions (work.meta[4]) and no particle of any
-// scene has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding
-// of the displacement) from its anchor.  max_disp2 restarts either way.
-__device__ void decide_block(const sphb_engine &e, int step_begin)
+// ------------------------------------------------------------ decision --
+// No rebin while the particles sit where the last rebin put them
+// (work.meta[3] == 2); otherwise rebin unless the lists were recorded with
+// the skin at those positions (work.meta[4]) and no particle of any scene
+// has moved skin_max / 2 (less a relative 1e-4 for the FP32 rounding of the
+// displacement) from its anchor.  Every block reads the same words, written
+// by earlier launches, and reaches the same decision (block-uniform), so a
+// launch that keeps the cells needs no grid barrier; *lists tells whether
+// the kept lists hold every pair.
+__device__ bool decide_keep(const sphb_engine &e, bool *lists)
 {
     __shared__ int s_far;
     if (threadIdx.x == 0) s_far = 0;
     __syncthreads();
     for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) {
-        if (step_begin) step_begin_scene(e, s);
-        sphb_scene_state &st = e.sstate[s];
-        const double d2 = __longlong_as_double((long long)st.max_disp2);
+        const double d2 = __longlong_as_double((long long)e.sstate[s].max_disp2);
         const double lim = 0.5 * e.scene[s].skin_max * (1.0 - 1e-4);
         if (!(d2 < lim * lim)) s_far = 1;
-        st.max_disp2 = 0ull;
     }
     __syncthreads();
+    const bool at_anchor = e.work.meta[3] == 2;
+    // host-written state nobody has measured: no trusting the lists
+    *lists = e.work.meta[4] == 1 && e.work.meta[5] == 0;
+    return at_anchor || (*lists && !s_far);
+}
+
+// One block, once every block has read the decision's inputs: the step
+// prologue when asked, max_disp2 restarting, and the decision published
+// (meta[1] = 1 when it rebins, meta[2] = 1 when it kept the lists).
+__device__ void decide_commit(const sphb_engine &e, int step_begin, bool keep, bool lists)
+{
+    for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) {
+        if (step_begin) step_begin_scene(e, s);
+        e.sstate[s].max_disp2 = 0ull;
+    }
     if (threadIdx.x == 0) {
-        const bool at_anchor = e.work.meta[3] == 2;
-        // host-written state nobody has measured: no trusting the lists
-        const bool lists = e.work.meta[4] == 1 && e.work.meta[5] == 0;
-        const bool keep = at_anchor || (lists && !s_far);
         e.work.meta[1] = keep ? 0 : 1;
         e.work.meta[2] = (keep && lists) ? 1 : 0;
         if (!keep) e.work.pairs[3] += 1ull;   // rebins decided on the device
     }
 }
 
+// ---------------------------------------------------------------- boxes --
 __device__ __forceinline__ void box_reset_scene(const sphb_engine &e, int s)
 {
     for (int d = 0; d < 3; ++d) {
@@ -356,16 +368,17 @@ __device__ __forceinline__ void box_flush(const sphb_engine &e, int s, int dim, 
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    // one thread per bound: its value over the warps, then one fire-and-
+    // forget atomic (the encoded doubles order like the doubles)
+    const int t = threadIdx.x;
+    if (t < 2 * dim) {
+        const bool is_lo = t < dim;
+        const int c = is_lo ? t : 3 + (t - dim);
+        double v = sh[0][c];
         for (int i = 1; i < (int)(blockDim.x >> 5); ++i)
-            for (int d = 0; d < 3; ++d) {
-                lo[d] = fmin(lo[d], sh[i][d]);
-                hi[d] = fmax(hi[d], sh[i][3 + d]);
-            }
-        for (int d = 0; d < dim; ++d) {
-            if (lo[d] < INFINITY) atomic_min_enc(&e.sstate[s].box[d], enc_double(lo[d]));
-            if (hi[d] > -INFINITY) atomic_max_enc(&e.sstate[s].box[3 + d], enc_double(hi[d]));
-        }
+            v = is_lo ? fmin(v, sh[i][c]) : fmax(v, sh[i][c]);
+        if (is_lo && v < INFINITY) atomicMin(&e.sstate[s].box[c], enc_double(v));
+        if (!is_lo && v > -INFINITY) atomicMax(&e.sstate[s].box[c], enc_double(v));
     }
     __syncthreads();
 #pragma unroll
@@ -891,16 +904,31 @@ k_rebin(const __grid_constant__ sphb_engine e, int cur, int flags)
     const int nt = e.num_tiles;
     const int nb = (int)((e.cfg.cell_capacity + SPHB_SCAN_CHUNK - 1) / SPHB_SCAN_CHUNK);
     int *const bar = e.work.bsum + nb + 1;   // the barrier's word
-    if (blockIdx.x == 0) {
-        if (if_needed) decide_block(e, (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0);
-        // every rebin measures the scene boxes afresh (only a rebin reads them)
+    const int step_begin = (flags & SPHB_BIN_STEP_BEGIN) ? 1 : 0;
+    if (if_needed) {
+        bool lists;
+        if (decide_keep(e, &lists)) {   // block-uniform, the same in every block
+            // kept: the last block to arrive (every block has read the
+            // inputs by then) commits; nobody waits
+            __shared__ int s_last;
+            if (threadIdx.x == 0) {
+                __threadfence();
+                int *arrive = bar + 1;
+                s_last = atomicAdd(arrive, 1) == (int)gridDim.x - 1;
+                if (s_last) *arrive = 0;
+            }
+            __syncthreads();
+            if (s_last) decide_commit(e, step_begin, true, lists);
+            pdl_trigger();   // the density pass may launch
+            return;
+        }
+        grid_barrier(e, bar);   // every block has read the inputs
+        if (blockIdx.x == 0) decide_commit(e, step_begin, false, lists);
+    }
+    // every rebin measures the scene boxes afresh (only a rebin reads them)
+    if (blockIdx.x == 0)
         for (int s = threadIdx.x; s < e.cfg.num_scenes; s += blockDim.x) box_reset_scene(e, s);
-    }
     grid_barrier(e, bar);
-    if (if_needed && *(volatile int *)&e.work.meta[1] == 0) {   // kept (grid-uniform)
-        pdl_trigger();   // the density pass may launch
-        return;
-    }
     int t0, t1;
     block_tile_run(nt, t0, t1);
     box_accum_run<DIM>(e, cur, t0, t1);
