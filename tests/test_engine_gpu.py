@@ -603,3 +603,28 @@ def test_host_written_state_within_the_skin_keeps_the_lists(precision):
     x[:5] += 3.0 * skin
     a.exchange_in(0, "x", x)
     assert _decisions(a, 1)[0][0] == 1
+
+
+@pytest.mark.parametrize("case", ["dam", "lattice3d"])
+@pytest.mark.parametrize("lists", [True, False])
+def test_common_case_loops_match_the_general_loops(case, lists):
+    """The pair passes compile the common case (one h in the scene, every
+    source summed; the force pass per mode) apart from the general loops.
+    Writing the same h back from the host marks the scene as having several
+    h, which sends every pass through the general loops with arithmetic that
+    is the same for equal h: three FP32C steps (lists kept, or the cells
+    searched every stage) must agree bit for bit."""
+    a, arrays, params, scheme, dim = engine_for(case, "fp32c", step_lists=lists)
+    b, _, _, _, _ = engine_for(case, "fp32c", step_lists=lists)
+    for arr in range(b.A):
+        b.exchange_in(arr, "h", torch.as_tensor(arrays[arr]["h"], dtype=torch.float64))
+    assert not any(t.uniform_h for t in b._scene_host)
+    for e in (a, b):
+        e.rebin_now()
+        for _ in range(3):
+            e.pc_step()
+        e.check_status()
+    for arr in range(a.A):
+        for n in ("x", "y", "u", "v", "rho", "p"):
+            assert torch.equal(a.get(arr, n), b.get(arr, n)), (arr, n)
+    assert a.pair_counts() == b.pair_counts()
