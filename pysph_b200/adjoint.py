@@ -42,7 +42,8 @@ from .engine import Engine, Scheme, SceneParams
 class Rollout:
     def __init__(self, arrays, params, scheme: Scheme, dim: int = 2, dt: float = 1e-5,
                  steps: int = 200, checkpoint_every: int = 20, precision: str = "fp32c",
-                 device=None, lanes: int = 1, pair_block: int = 128, graphs: bool = True):
+                 device=None, lanes: int = 1, pair_block: int = 128, graphs: bool = True,
+                 adj_lanes: int = 2, adj_pair_block: int = 128):
         if scheme.continuity:
             raise NotImplementedError("the adjoint covers the summation-density scheme")
         if scheme.hks:
@@ -60,8 +61,12 @@ class Rollout:
         self.k = checkpoint_every
         self.fwd = Engine([(arrays, self.params)], scheme, dim=dim, precision=precision,
                           device=device, lanes=lanes, pair_block=pair_block)
+        # the FP64 adjoint engine: two lanes per particle (the VJP kernels
+        # carry far more work per pair than the forward passes; on the 50k
+        # drop the backward took 92.8 ms with one lane, 80.9 with two, 89.3
+        # with four and 101.8 with eight)
         self.adj = Engine([(arrays, self.params)], scheme, dim=dim, precision="fp64",
-                          device=device)
+                          device=device, lanes=adj_lanes, pair_block=adj_pair_block)
         self.device = self.fwd.device
         self.moving = list(scheme.step_on)
         self.checkpoints = []

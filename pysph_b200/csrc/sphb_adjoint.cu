@@ -65,17 +65,32 @@ struct AdjPtrs {
     double *lam_c;         // [N] written (=)
 };
 
+// The sum of v over the LANES lanes of a particle (every lane of the warp
+// calls it); valid in every lane.
+template <int LANES>
+__device__ __forceinline__ double lane_sum(double v)
+{
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Force VJP.  Inputs: positions, velocities, h, m (buf[cur]) and rho, p, cs
-// (FP64 fields) of the current stage, cell tables of the current bin.
-template <int DIM, int R>
+// (FP64 fields) of the current stage, cell tables of the current bin.  One
+// pair tile per block, LANES threads per particle (the engine's pair-pass
+// shape): each lane takes its share of the neighbours and the lanes' sums
+// meet with shuffles.
+template <int DIM, int R, int LANES>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, AdjPtrs P)
 {
-    const sphb_tile t = e.tiles[blockIdx.x];
+    const sphb_tile t = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int k_raw = t.begin + (int)(threadIdx.x / LANES);
+    const bool active = k_raw < t.end;
+    const int k = active ? k_raw : t.begin;   // inactive lanes read a valid particle
     const int N = e.cfg.num_particles;
     const sphb_buffers &B = e.buf[cur];
     const sphb_scene &sc = e.scene[s];
@@ -108,11 +123,11 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
     // the lists of the density pass (recorded one lane per particle) hold
     // every pair of both roles when h is uniform (the predicate is then
     // symmetric)
-    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
+    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == LANES &&
                           e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
-    traverse<DIM, R, 1>(
-        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, CellTrim{},
-        [&](int j, int, int, int) {
+    if (active) traverse<DIM, R, LANES>(
+        e, use_list, k, lane, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
+        CellTrim{}, [&](int j, int, int, int) {
             if (j == k) return;
             double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};
             const double r2 = dist2_ref<DIM>(r[0], r[1], r[2]);
@@ -208,6 +223,14 @@ k_force_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask, 
             }
         });
     for (int d = 0; d < DIM; ++d) {
+        gx[d] = lane_sum<LANES>(gx[d]);
+        gv[d] = lane_sum<LANES>(gv[d]);
+    }
+    grho = lane_sum<LANES>(grho);
+    gp = lane_sum<LANES>(gp);
+    gc = lane_sum<LANES>(gc);
+    if (!active || lane != 0) return;
+    for (int d = 0; d < DIM; ++d) {
         P.lam_x[(size_t)d * N + k] += gx[d];
         P.lam_v[(size_t)d * N + k] += gv[d];
     }
@@ -237,17 +260,19 @@ k_eos_vjp(const __grid_constant__ sphb_engine e, int cur, double *lam_rho,
 }
 
 // Density VJP: lam_x_k += sum_j (lam_rho_k m_j [k dest] + lam_rho_j m_k
-// [j dest]) G(x_k - x_j).
-template <int DIM, int R>
+// [j dest]) G(x_k - x_j).  The force VJP's launch shape.
+template <int DIM, int R, int LANES>
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
 k_density_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask,
               const double *lam_rho, double *lam_x)
 {
-    const sphb_tile t = e.tiles[blockIdx.x];
+    const sphb_tile t = e.pair_tiles[blockIdx.x];
     const int A = e.cfg.num_arrays;
     const int s = t.seg / A, a = t.seg - s * A;
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int k_raw = t.begin + (int)(threadIdx.x / LANES);
+    const bool active = k_raw < t.end;
+    const int k = active ? k_raw : t.begin;   // inactive lanes read a valid particle
     const int N = e.cfg.num_particles;
     const sphb_buffers &B = e.buf[cur];
     const sphb_scene &sc = e.scene[s];
@@ -266,11 +291,11 @@ k_density_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
     // the lists of the density pass (recorded one lane per particle) hold
     // every pair of both roles when h is uniform (the predicate is then
     // symmetric)
-    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == 1 &&
+    const bool use_list = sc.uniform_h && e.cfg.rho_src[a] != 0u && e.cfg.lanes == LANES &&
                           e.f.list_cap > 0 && e.f.nbr && e.f.nbr_cnt;
-    traverse<DIM, R, 1>(
-        e, use_list, k, 0, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz, CellTrim{},
-        [&](int j, int, int, int) {
+    if (active) traverse<DIM, R, LANES>(
+        e, use_list, k, lane, e.work.start, A, all, st.cell_base, st.ncells, n, cx, cy, cz,
+        CellTrim{}, [&](int j, int, int, int) {
             if (j == k) return;
             const double r[3] = {xk[0] - B.x[j], xk[1] - B.y[j], DIM == 3 ? xk[2] - B.z[j] : 0.0};
             const double r2 = dist2_ref<DIM>(r[0], r[1], r[2]);
@@ -289,6 +314,8 @@ k_density_vjp(const __grid_constant__ sphb_engine e, int cur, uint32_t dest_mask
             const double g = kernel_g<DIM>(sqrt(r2), 0.5 * (hk + hj), dgs);
             for (int d = 0; d < DIM; ++d) gx[d] += w * g * r[d];
         });
+    for (int d = 0; d < DIM; ++d) gx[d] = lane_sum<LANES>(gx[d]);
+    if (!active || lane != 0) return;
     for (int d = 0; d < DIM; ++d) lam_x[(size_t)d * N + k] += gx[d];
 }
 
@@ -318,6 +345,18 @@ k_permute(const __grid_constant__ sphb_engine e, int cur, int array, int dir,
 
 using namespace sphb;
 
+// The pair kernels' launch shape: pair tiles of pair_block / lanes
+// particles, lanes a power of two up to 8, blocks of at most 256 threads.
+static int adj_shape(const sphb_engine *e)
+{
+    const sphb_config &c = e->cfg;
+    if (c.lanes != 1 && c.lanes != 2 && c.lanes != 4 && c.lanes != 8) return SPHB_ERR_ARG;
+    if (c.pair_block < 32 || c.pair_block > SPHB_ELEM_TILE || (c.pair_block & 31))
+        return SPHB_ERR_ARG;
+    if (e->num_pair_tiles < 0 || (e->num_pair_tiles > 0 && !e->pair_tiles)) return SPHB_ERR_ARG;
+    return SPHB_OK;
+}
+
 static int adj_check(const sphb_engine *e, int cur)
 {
     int rc = check_engine_public(e, cur);
@@ -334,15 +373,21 @@ extern "C" int sphb_force_vjp(const sphb_engine *e, int cur, uint32_t dest_mask,
     int rc = adj_check(e, cur);
     if (rc) return rc;
     if (!lam_a || !lam_x || !lam_v || !lam_rho || !lam_p || !lam_c) return SPHB_ERR_ARG;
-    if (e->num_tiles == 0) return SPHB_OK;
+    if ((rc = adj_shape(e))) return rc;
+    if (e->num_pair_tiles == 0) return SPHB_OK;
     AdjPtrs P{lam_a, lam_x, lam_v, lam_rho, lam_p, lam_c};
     cudaStream_t st = (cudaStream_t)stream;
-    const int nt = e->num_tiles;
-    switch (e->cfg.dim * 10 + e->cfg.stencil) {
-    case 21: k_force_vjp<2, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, P); break;
-    case 22: k_force_vjp<2, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, P); break;
-    case 31: k_force_vjp<3, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, P); break;
-    case 32: k_force_vjp<3, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, P); break;
+    const dim3 g(e->num_pair_tiles), b(e->cfg.pair_block);
+    switch (e->cfg.dim * 100 + e->cfg.stencil * 10 + e->cfg.lanes) {
+#define SPHB_FV(D, RR, L)                                                         \
+    case D * 100 + RR * 10 + L:                                                  \
+        k_force_vjp<D, RR, L><<<g, b, 0, st>>>(*e, cur, dest_mask, P);           \
+        break;
+    SPHB_FV(2, 1, 1) SPHB_FV(2, 1, 2) SPHB_FV(2, 1, 4) SPHB_FV(2, 1, 8)
+    SPHB_FV(2, 2, 1) SPHB_FV(2, 2, 2) SPHB_FV(2, 2, 4) SPHB_FV(2, 2, 8)
+    SPHB_FV(3, 1, 1) SPHB_FV(3, 1, 2) SPHB_FV(3, 1, 4) SPHB_FV(3, 1, 8)
+    SPHB_FV(3, 2, 1) SPHB_FV(3, 2, 2) SPHB_FV(3, 2, 4) SPHB_FV(3, 2, 8)
+#undef SPHB_FV
     default: return SPHB_ERR_UNSUPPORTED;
     }
     return launch_status("sphb_force_vjp");
@@ -365,14 +410,20 @@ extern "C" int sphb_density_vjp(const sphb_engine *e, int cur, uint32_t dest_mas
     int rc = adj_check(e, cur);
     if (rc) return rc;
     if (!lam_rho || !lam_x) return SPHB_ERR_ARG;
-    if (e->num_tiles == 0) return SPHB_OK;
+    if ((rc = adj_shape(e))) return rc;
+    if (e->num_pair_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    const int nt = e->num_tiles;
-    switch (e->cfg.dim * 10 + e->cfg.stencil) {
-    case 21: k_density_vjp<2, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, lam_rho, lam_x); break;
-    case 22: k_density_vjp<2, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, lam_rho, lam_x); break;
-    case 31: k_density_vjp<3, 1><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, lam_rho, lam_x); break;
-    case 32: k_density_vjp<3, 2><<<nt, SPHB_ELEM_TILE, 0, st>>>(*e, cur, dest_mask, lam_rho, lam_x); break;
+    const dim3 g(e->num_pair_tiles), b(e->cfg.pair_block);
+    switch (e->cfg.dim * 100 + e->cfg.stencil * 10 + e->cfg.lanes) {
+#define SPHB_DV(D, RR, L)                                                                 \
+    case D * 100 + RR * 10 + L:                                                          \
+        k_density_vjp<D, RR, L><<<g, b, 0, st>>>(*e, cur, dest_mask, lam_rho, lam_x);    \
+        break;
+    SPHB_DV(2, 1, 1) SPHB_DV(2, 1, 2) SPHB_DV(2, 1, 4) SPHB_DV(2, 1, 8)
+    SPHB_DV(2, 2, 1) SPHB_DV(2, 2, 2) SPHB_DV(2, 2, 4) SPHB_DV(2, 2, 8)
+    SPHB_DV(3, 1, 1) SPHB_DV(3, 1, 2) SPHB_DV(3, 1, 4) SPHB_DV(3, 1, 8)
+    SPHB_DV(3, 2, 1) SPHB_DV(3, 2, 2) SPHB_DV(3, 2, 4) SPHB_DV(3, 2, 8)
+#undef SPHB_DV
     default: return SPHB_ERR_UNSUPPORTED;
     }
     return launch_status("sphb_density_vjp");

@@ -223,3 +223,25 @@ def test_adjoint_fp32c_forward_gradient():
     err = float(torch.linalg.norm(g32 - g64) / torch.linalg.norm(g64))
     print("fp32c vs fp64 gradient:", err)
     assert err <= 1e-2, err
+
+
+@pytest.mark.parametrize("lanes,block", [(2, 64), (4, 128), (8, 256)])
+def test_adjoint_lanes_agree(lanes, block):
+    """The VJP kernels run on the adjoint engine's pair-pass shape, several
+    lanes per particle whose sums meet with shuffles: every shape gives the
+    one-lane gradient to FP64 round-off (the sums run in another order)."""
+    dx = 0.05
+    arrays, params = drop(dx)
+    a = arrays[0]
+    n = len(a["x"])
+    dev = torch.device("cuda")
+    v0 = torch.tensor(np.stack([a["u"], a["v"]]), dtype=torch.float64, device=dev)
+    grads = []
+    for L, B in ((1, 128), (lanes, block)):
+        r = Rollout(arrays, params, fluid_scheme(1), dim=2, dt=1e-5, steps=10,
+                    checkpoint_every=5, precision="fp64", adj_lanes=L, adj_pair_block=B)
+        x = r.forward({0: v0})[0][0]
+        g = r.backward({0: (2.0 * x / n, torch.zeros_like(x))})
+        grads.append(torch.cat([g[0][0].flatten(), g[0][1].flatten()]))
+    scale = float(torch.max(torch.abs(grads[0])))
+    assert float(torch.max(torch.abs(grads[1] - grads[0]))) <= 1e-12 * scale
