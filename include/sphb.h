@@ -499,7 +499,10 @@ SPHB_API int sphb_permute(const sphb_engine *e, int cur, int array, int dir, dou
  * velocities, rho, p, cs from sphb_density) and its bin.  In a scene of
  * uniform h, the pair kernels walk the neighbour lists that sphb_density
  * recorded for that bin (every array with SPHRho sources, f.list_cap > 0);
- * otherwise they search the cells. */
+ * otherwise they search the cells.  The pair kernels launch on the engine's
+ * pair-pass shape (its pair tiles, pair_block threads, `lanes` lanes per
+ * dest particle merged by warp shuffles), so an engine made for the
+ * adjoint picks its own lanes (2 suits these kernels' FP64 pair work). */
 
 /* Given lam_a, the adjoint of the MomentumEquation acceleration of the dest
  * arrays in dest_mask: lam_x += (da/dx)^T lam_a, lam_v += (da/dv)^T lam_a;
