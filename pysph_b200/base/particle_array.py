@@ -154,7 +154,10 @@ class ParticleArray:
         return self.get(name)
 
     def set(self, **props):
-        """Copy values into properties (ParticleArray.set)."""
+        """Copy values into properties (ParticleArray.set).  The values are
+        copied when it returns: host-to-device copies of several properties
+        are queued together and waited for once."""
+        held = []   # host sources of queued copies, alive until the wait
         for name, value in props.items():
             self._check_property(name)
             t = self.properties[name]
@@ -162,9 +165,15 @@ class ParticleArray:
                                 else value, dtype=t.dtype)
             if v.dim() == 0:
                 t.fill_(v.item())
+            elif v.device.type == "cpu" and t.device.type == "cuda":
+                # one copy, host memory straight into the property
+                t.copy_(v, non_blocking=True)
+                held.append(v)
             else:
-                t.copy_(v)   # one copy, host memory straight into the property
+                t.copy_(v)
             self._touch(name)
+        if held:
+            torch.cuda.current_stream(self.device).synchronize()
 
     def __getattr__(self, name):
         props = self.__dict__.get("properties")

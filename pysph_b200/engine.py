@@ -158,6 +158,11 @@ class Engine:
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the engine runs on CUDA devices only")
+        if self.device.index is None:
+            # an explicit index: every launch looks up the device's current
+            # stream, which for a bare "cuda" device costs a query of the
+            # current device each time
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.L = nat.lib()
         self.dim = dim
         self.precision = precision
@@ -230,6 +235,10 @@ class Engine:
         self.fuse_stage = bool(fuse_stage)
         self.force_mode = 0       # 0 MomentumEquation, 1 SPHPressureGradient
         self.tait_only_mask = 0    # Tait dests that are not SPHRho dests
+        # step_graphed: on/off, launch states seen once, their captured steps
+        self.graphs = True
+        self._graph_seen: set = set()
+        self._graphs: dict = {}
         self._host_scene_tables(scenes)
         if cell_capacity is None:
             cell_capacity = self._estimate_capacity(grid_growth)
@@ -820,6 +829,52 @@ class Engine:
             on_half()
         self.bin(nat.BIN_MOVE_INITIAL | reuse)
         self._stage(3)
+
+    def _launch_state(self):
+        """Everything a step's launches depend on besides device memory:
+        the descriptor the kernels receive by value, and the host-side flags
+        and masks that choose the calls and their arguments."""
+        sc = self.scheme
+        return (ctypes.string_at(ctypes.addressof(self.desc), ctypes.sizeof(self.desc)),
+                self.cur, bool(getattr(self, "_host_state", False)), self._box_valid,
+                self.step_lists, self.fuses_stage, self.force_mode, self.list_cap,
+                self.tait_only_mask, sc.continuity, sc.rho_dests, sc.mom_dests,
+                sc.pair_dests)
+
+    def step_graphed(self, integrator: str = "pc"):
+        """step(integrator) through a CUDA graph: the first step from a given
+        launch state runs as it is (loading every kernel), the second is
+        captured, and later ones replay it -- one launch instead of one per
+        pass, so the host no longer paces the device.  Steps whose launches
+        would differ (another descriptor, flags or masks) get their own
+        graph.  With graphs off, off CUDA, or inside another capture, it is
+        step()."""
+        if (not self.graphs or self.device.type != "cuda"
+                or torch.cuda.is_current_stream_capturing()):
+            return self.step(integrator)
+        if integrator == "rk4":
+            self._rk4_sums()   # buffers made outside any capture
+        key = (integrator, self._launch_state())
+        hit = self._graphs.get(key)
+        if hit is None:
+            if key not in self._graph_seen:
+                self._graph_seen.add(key)
+                return self.step(integrator)
+            if len(self._graphs) >= 8:
+                self._graphs.clear()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.step(integrator)
+            hit = (g, (self.cur, self._host_state, self._box_valid))
+            # kept for replays only when the step leaves the descriptor as
+            # it found it (an even number of record swaps, as every fused
+            # integrator's step has); replayed this once either way
+            if self._launch_state()[0] == key[1][0]:
+                self._graphs[key] = hit
+            self._graph_last = hit
+        g, after = hit
+        g.replay()
+        self.cur, self._host_state, self._box_valid = after
 
     def _rk4_sums(self):
         """RK4's running sums (K1 + 2 K2 + 2 K3 of every integrated

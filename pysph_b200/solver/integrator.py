@@ -294,7 +294,8 @@ class Integrator:
         eng = s.engine
         if not device_dt:
             eng.set_dt_async(dt)
-        eng.step(kind)
+        # one CUDA graph per step once the step repeats (Engine.step_graphed)
+        eng.step_graphed(kind)
         self._fused_outputs(s, 4 if kind == "rk4" else 1)
         self.time += dt if not device_dt else 0.0
         self._steps = getattr(self, "_steps", 0) + 1

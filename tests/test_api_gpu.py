@@ -498,3 +498,50 @@ def test_solver_other_kernels_match_oracle(kname, cont):
         a = pa.get(n).cpu().numpy()
         b = pa2.get(n).cpu().numpy()
         assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, np.max(np.abs(a))), n
+
+
+def _drop_for(cls, precision):
+    arrays, _, _ = W.elliptical_drop(dx=0.05)
+    pa = base.get_particle_array(name="fluid", cl_precision=precision, **arrays[0])
+    particles = base.Particles([pa])
+    s = solver.Solver(dim=2, integrator_type=cls)
+    s.add_operation(solver.SPHOperation(sph.SPHRho.withargs(), on_types=[Fluid],
+                                        from_types=[Fluid], updates=["rho"], id="sd"))
+    s.add_operation(solver.SPHOperation(sph.TaitEquation.withargs(co=1400.0, ro=1.0),
+                                        on_types=[Fluid], updates=["p", "cs"], id="eos"))
+    s.add_operation(solver.SPHIntegration(
+        sph.MomentumEquation.withargs(alpha=0.1, beta=0.0, eta=0.1),
+        on_types=[Fluid], from_types=[Fluid], updates=["u", "v"], id="mom"))
+    s.add_operation_step([Fluid])
+    s.set_time_step(1e-5)
+    s.setup(particles)
+    assert s.integrator.plan is not None
+    return s, pa
+
+
+@pytest.mark.parametrize("precision", ["single", "double"])
+@pytest.mark.parametrize("integ", ["pc", "euler", "rk2", "rk4"])
+def test_graphed_steps_match_eager_steps(integ, precision):
+    """The fused integrators replay one captured CUDA graph per step once
+    the step repeats (Engine.step_graphed): bit for bit the eager launches,
+    over steps that run alone, steps after host writes of the state (which
+    refresh the records and re-measure the displacements), and a change of
+    dt, for every integrator (Euler's one stage runs unfused in a graph)."""
+    cls = {"pc": solver.PredictorCorrectorIntegrator, "euler": solver.EulerIntegrator,
+           "rk2": solver.RK2Integrator, "rk4": solver.RK4Integrator}[integ]
+    runs = []
+    for graphs in (True, False):
+        s, pa = _drop_for(cls, precision)
+        eng = s.integrator._fused_session().engine
+        eng.graphs = graphs
+        for i in range(12):
+            if 4 <= i < 8:
+                # the host rewrites the state it has just read
+                pa.set(x=pa.get("x").cpu().numpy(), u=pa.get("u").cpu().numpy() * 1.001)
+            s.integrator.integrate(1e-5 if i < 10 else 2e-5)
+        if graphs:
+            assert eng._graphs, "no step was replayed from a graph"
+        runs.append({n: pa.get(n).cpu().numpy().copy() for n in ("x", "y", "u", "v", "rho", "p")})
+        eng.check_status()
+    for n in runs[0]:
+        assert np.array_equal(runs[0][n], runs[1][n]), n
