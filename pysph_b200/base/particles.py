@@ -124,13 +124,16 @@ class Session:
             self.valid[(a, n)] = True
             pa._engine_newer.add(n)
 
-    def ensure(self, reads, step_decides=False):
+    def ensure(self, reads, step_decides=False, defer=None):
         """Import every (array, property) in reads the engine does not hold,
         then rebin if any position changed.  step_decides: an engine step
         with its own rebin decision follows at once (the fused integrators),
         so with list reuse and nothing else to import after a rebin the
         decision is left to that step, which measures the host-written
-        positions first."""
+        positions first.  defer: a list that receives the (array, name,
+        tensor) imports of positions and velocities that the step is to
+        launch itself (Engine.step_graphed), when nothing here needs them
+        first; the rest are imported at once."""
         eng = self.engine
         if self._pos_versions() != self.positions_version:
             self.need_bin = True
@@ -143,8 +146,10 @@ class Session:
                 self.valid[(a, "tag")] = True
         masters = [(a, n) for a, n in reads if n in MASTER]
         derived = [(a, n) for a, n in reads if n not in MASTER]
+        if derived:
+            defer = None
         for a, name in masters:
-            self._import(a, name)
+            self._import(a, name, defer)
         if self.need_bin and step_decides and eng.step_lists and not derived:
             # the step's first bin refreshes the records and decides; every
             # derived field the step reads it computes itself
@@ -154,11 +159,16 @@ class Session:
             for pa in self.particles.arrays:
                 pa.is_dirty = False
         if self.need_bin:
+            if defer:
+                # the rebin reads them
+                for a, name, t in defer:
+                    eng.exchange_in(a, name, t)
+                defer.clear()
             self.bin()
         for a, name in derived:
             self._import(a, name)
 
-    def _import(self, a, name):
+    def _import(self, a, name, defer=None):
         if self.dim == 2 and name in ("z", "w", "_z0", "_w0"):
             return
         if self.valid.get((a, name), False):
@@ -166,7 +176,10 @@ class Session:
         pa = self.particles.arrays[a]
         if not pa.has_array(name):
             pa.add_property({"name": name})
-        self.engine.exchange_in(a, name, pa.properties[name])
+        if defer is not None and name in ("x", "y", "z", "u", "v", "w"):
+            defer.append((a, name, pa.properties[name]))
+        else:
+            self.engine.exchange_in(a, name, pa.properties[name])
         self.valid[(a, name)] = True
         if name in ("x", "y", "z"):
             self.need_bin = True

@@ -841,35 +841,60 @@ class Engine:
                 self.tait_only_mask, sc.continuity, sc.rho_dests, sc.mom_dests,
                 sc.pair_dests)
 
-    def step_graphed(self, integrator: str = "pc"):
+    def _import_inline(self, imports):
+        for a, name, t in imports:
+            if t.numel():
+                self.call("sphb_exchange", self.cur, a, self._field_id(a, name), 0,
+                          t.data_ptr(), self.user_offset[a].data_ptr())
+
+    def step_graphed(self, integrator: str = "pc", imports=()):
         """step(integrator) through a CUDA graph: the first step from a given
         launch state runs as it is (loading every kernel), the second is
         captured, and later ones replay it -- one launch instead of one per
         pass, so the host no longer paces the device.  Steps whose launches
         would differ (another descriptor, flags or masks) get their own
-        graph.  With graphs off, off CUDA, or inside another capture, it is
-        step()."""
+        graph.  imports: (array, name, tensor) positions or velocities that
+        the host wrote, imported as the step's first launches (the graph
+        reads the tensors' memory, so a replay imports their values of the
+        moment).  With graphs off, off CUDA, or inside another capture, it
+        is the imports and step()."""
+        inline = []
+        for a, name, t in imports:
+            if (name in ("x", "y", "z", "u", "v", "w") and t.dtype == torch.float64
+                    and t.device == self.device and t.is_contiguous()
+                    and t.numel() == self.user_n[a]):
+                inline.append((a, name, t))
+            else:
+                self.exchange_in(a, name, t)
+        if inline:
+            # the host flags such an import sets (_exchange_in)
+            self._box_valid = False
+            self._host_state = True
         if (not self.graphs or self.device.type != "cuda"
                 or torch.cuda.is_current_stream_capturing()):
+            self._import_inline(inline)
             return self.step(integrator)
         if integrator == "rk4":
             self._rk4_sums()   # buffers made outside any capture
-        key = (integrator, self._launch_state())
+        key = (integrator, tuple((a, n, t.data_ptr()) for a, n, t in inline),
+               self._launch_state())
         hit = self._graphs.get(key)
         if hit is None:
             if key not in self._graph_seen:
                 self._graph_seen.add(key)
+                self._import_inline(inline)
                 return self.step(integrator)
             if len(self._graphs) >= 8:
                 self._graphs.clear()
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
+                self._import_inline(inline)
                 self.step(integrator)
             hit = (g, (self.cur, self._host_state, self._box_valid))
             # kept for replays only when the step leaves the descriptor as
             # it found it (an even number of record swaps, as every fused
             # integrator's step has); replayed this once either way
-            if self._launch_state()[0] == key[1][0]:
+            if self._launch_state()[0] == key[2][0]:
                 self._graphs[key] = hit
             self._graph_last = hit
         g, after = hit

@@ -290,12 +290,13 @@ class Integrator:
     def _fused_integrate(self, dt, device_dt, kind):
         """The whole step on the engine (fused plan)."""
         s = self._fused_session()
-        s.ensure(self._fused_reads(s), step_decides=True)
+        imports = []   # host-written positions / velocities, imported by the step
+        s.ensure(self._fused_reads(s), step_decides=True, defer=imports)
         eng = s.engine
         if not device_dt:
             eng.set_dt_async(dt)
         # one CUDA graph per step once the step repeats (Engine.step_graphed)
-        eng.step_graphed(kind)
+        eng.step_graphed(kind, imports)
         self._fused_outputs(s, 4 if kind == "rk4" else 1)
         self.time += dt if not device_dt else 0.0
         self._steps = getattr(self, "_steps", 0) + 1
