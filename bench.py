@@ -1012,10 +1012,11 @@ def e2e_facade(wl, args, shape, dev, stream):
     def step():
         f.set(x=host["x"], y=host["y"], u=host["u"], v=host["v"])
         integ.integrate(0.0, device_dt=True)
-        # into the numpy arrays' memory: the six read-backs queued on the
-        # stream, then one wait before the host touches them
-        for k in names_out:
-            pinned[k].copy_(f.get(k), non_blocking=True)
+        # into the numpy arrays' memory: the six properties read in one get,
+        # the six read-backs queued on the stream, then one wait before the
+        # host touches them
+        for k, t in zip(names_out, f.get(*names_out)):
+            pinned[k].copy_(t, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
     for _ in range(3):
@@ -1041,7 +1042,8 @@ def e2e_facade(wl, args, shape, dev, stream):
            "rebins_per_stage": rebins / (2.0 * k_steps),
            "h2d_bytes_per_step": 8 * n * 4, "d2h_bytes_per_step": 8 * n * len(names_out),
            "api": "ParticleArray.set(numpy) -> PredictorCorrectorIntegrator.integrate "
-                  "(device CFL dt) -> ParticleArray.get -> numpy, every step; the numpy "
+                  "(device CFL dt) -> ParticleArray.get(x, y, u, v, rho, p) -> numpy, every "
+                  "step; the numpy "
                   "arrays live in pinned host memory allocated once, the read-backs "
                   "queued together and waited for once per step",
            "rebins": "device-decided after each host write of the positions (kept while "

@@ -473,6 +473,18 @@ SPHB_API int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
                   int dir, double *user, const int32_t *user_offset,
                   void *stream);
 
+/* sphb_exchange of count (1..SPHB_EXCHANGE_MAX) fields of one array in one
+ * launch: fields[i] <-> users[i], fields and users being host arrays read
+ * during the call; each thread finds its particle's user position once for
+ * all of them.  The same import marks as the single calls.  Used by the
+ * integrators' imports of host-written x, y, u, v and by
+ * ParticleArray.get of several properties (S/base/particle_array.pyx:
+ * get(*args) returns each of them). */
+#define SPHB_EXCHANGE_MAX 8
+SPHB_API int sphb_exchange_many(const sphb_engine *e, int cur, int array, int dir,
+                                int32_t count, const int32_t *fields, double *const *users,
+                                const int32_t *user_offset, void *stream);
+
 /* Same for the int32 tag field. */
 SPHB_API int sphb_exchange_tag(const sphb_engine *e, int cur, int array, int dir,
                       int32_t *user, const int32_t *user_offset, void *stream);

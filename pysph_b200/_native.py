@@ -172,6 +172,7 @@ def lib():
         "sphb_pc_stage": (i32, [E, i32, i32, vp]),
         "sphb_step_begin": (i32, [E, vp]),
         "sphb_exchange": (i32, [E, i32, i32, i32, i32, vp, vp, vp]),
+        "sphb_exchange_many": (i32, [E, i32, i32, i32, i32, vp, vp, vp, vp]),
         "sphb_exchange_tag": (i32, [E, i32, i32, i32, vp, vp, vp]),
         "sphb_init_index": (i32, [E, i32, vp]),
         "sphb_set_dt": (i32, [E, f64, vp]),
@@ -196,11 +197,12 @@ EXPORTED = ("sphb_abi_version", "sphb_last_cuda_error", "sphb_make_tiles",
             "sphb_workspace_layout", "sphb_box_init", "sphb_bin",
             "sphb_neighbors", "sphb_cell_coords", "sphb_density", "sphb_tait",
             "sphb_momentum", "sphb_pc_stage", "sphb_step_begin",
-            "sphb_exchange", "sphb_exchange_tag", "sphb_init_index",
+            "sphb_exchange", "sphb_exchange_many", "sphb_exchange_tag", "sphb_init_index",
             "sphb_set_dt", "sphb_refresh", "sphb_permute", "sphb_force_vjp", "sphb_eos_vjp",
             "sphb_density_vjp", "sphb_neighbor_counts_static")
 
 STATIC_MAX_PARTICLES = 1 << 18
+EXCHANGE_MAX = 8
 
 
 def check(rc: int, what: str):

@@ -143,9 +143,14 @@ class ParticleArray:
         """The tensor(s) of the named properties (one tensor for one name)."""
         if not names:
             return None
-        out = []
         for name in names:
             self._check_property(name)
+        stale = [n for n in dict.fromkeys(names) if n in self._engine_newer]
+        if len(stale) > 1 and self._session is not None:
+            # the engine's newer values of several properties: one launch
+            self._session.export_many(self, stale)
+        out = []
+        for name in names:
             self._sync(name)
             out.append(self.properties[name])
         return out[0] if len(out) == 1 else out

@@ -116,6 +116,23 @@ class Session:
         self.engine.exchange_out(a, name, out=pa.properties[name])
         pa._engine_newer.discard(name)
 
+    def export_many(self, pa, names):
+        """export_to_array of several properties in one launch (FP64,
+        contiguous properties; the others one by one)."""
+        a = self.index(pa)
+        batch = []
+        for name in names:
+            if name not in pa.properties:
+                pa.add_property({"name": name})
+            t = pa.properties[name]
+            if t.dtype == torch.float64 and t.is_contiguous():
+                batch.append(name)
+            else:
+                self.export_to_array(pa, name)
+        self.engine.exchange_out_many(a, batch, [pa.properties[n] for n in batch])
+        for name in batch:
+            pa._engine_newer.discard(name)
+
     def mark_engine_newer(self, a, names):
         pa = self.particles.arrays[a]
         for n in names:

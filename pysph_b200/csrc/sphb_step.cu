@@ -134,35 +134,25 @@ __device__ __forceinline__ double *field_ptr(const sphb_engine &e, int cur, int 
     return nullptr;
 }
 
-template <bool F32>
-__global__ void __launch_bounds__(SPHB_ELEM_TILE)
-k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
-           int dir, double *user, const int *user_offset)
+// Import marks of a gather (dir 0): new masses or smoothing lengths mean
+// the lists must be recorded again; new positions or velocities mean the
+// records are stale and the particles may have left their anchors, so the
+// next decision rebins unless sphb_refresh measures them first (meta[5]).
+__device__ __forceinline__ void exchange_marks(const sphb_engine &e, int field, int dir)
 {
-    // new masses or smoothing lengths: the lists must be recorded again;
-    // new positions or velocities: the records are stale and the particles
-    // may have left their anchors, so the next decision rebins unless
-    // sphb_refresh measures them first (meta[5])
-    if (dir == 0 && (field <= 5 || field == 12 || field == 13) && blockIdx.x == 0 &&
-        threadIdx.x == 0) {
+    if (dir == 0 && (field <= 5 || field == 12 || field == 13)) {
         e.work.meta[2] = 0;
         e.work.meta[3] = 0;
         if (field <= 5) e.work.meta[5] = 1;
         else e.work.meta[4] = 0;
     }
-    const sphb_tile t = e.tiles[blockIdx.x];
-    const int A = e.cfg.num_arrays;
-    const int s = t.seg / A, a = t.seg - s * A;
-    if (a != array) return;
-    const int k = t.begin + threadIdx.x;
-    if (k >= t.end) return;
-    const int n_seg = e.seg_offset[t.seg + 1] - e.seg_offset[t.seg];
-    const int li = e.buf[cur].idx[k];
-    if (li < 0 || li >= n_seg) {
-        flag(e, SPHB_ST_BAD_INDEX);
-        return;
-    }
-    const long long ui = (long long)user_offset[s] + li;
+}
+
+// Engine position k <-> user position ui of one field.
+template <bool F32>
+__device__ __forceinline__ void exchange_field(const sphb_engine &e, int cur, int field, int dir,
+                                               double *user, long long ui, int k)
+{
     if (field <= 13 || field == 21 || field == 22) {
         double *f = field_ptr<F32>(e, cur, field);
         if (dir == 0) f[k] = user[ui];
@@ -203,6 +193,59 @@ k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
         if (dir == 0) f[k] = user[ui];
         else user[ui] = f[k];
     }
+}
+
+// Engine position of this thread, and its user position in the array
+// `array` (false when the thread has no particle of that array).
+__device__ __forceinline__ bool exchange_slot(const sphb_engine &e, int cur, int array,
+                                              const int *user_offset, int &k, long long &ui)
+{
+    const sphb_tile t = e.tiles[blockIdx.x];
+    const int A = e.cfg.num_arrays;
+    const int s = t.seg / A, a = t.seg - s * A;
+    if (a != array) return false;
+    k = t.begin + threadIdx.x;
+    if (k >= t.end) return false;
+    const int n_seg = e.seg_offset[t.seg + 1] - e.seg_offset[t.seg];
+    const int li = e.buf[cur].idx[k];
+    if (li < 0 || li >= n_seg) {
+        flag(e, SPHB_ST_BAD_INDEX);
+        return false;
+    }
+    ui = (long long)user_offset[s] + li;
+    return true;
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_exchange(const __grid_constant__ sphb_engine e, int cur, int array, int field,
+           int dir, double *user, const int *user_offset)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) exchange_marks(e, field, dir);
+    int k;
+    long long ui;
+    if (exchange_slot(e, cur, array, user_offset, k, ui))
+        exchange_field<F32>(e, cur, field, dir, user, ui, k);
+}
+
+// Several fields of one array: the tile, index and offset loads once.
+struct ExchangeList {
+    int count;
+    int field[SPHB_EXCHANGE_MAX];
+    double *user[SPHB_EXCHANGE_MAX];
+};
+
+template <bool F32>
+__global__ void __launch_bounds__(SPHB_ELEM_TILE)
+k_exchange_many(const __grid_constant__ sphb_engine e, int cur, int array, int dir,
+                const __grid_constant__ ExchangeList l, const int *user_offset)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int i = 0; i < l.count; ++i) exchange_marks(e, l.field[i], dir);
+    int k;
+    long long ui;
+    if (!exchange_slot(e, cur, array, user_offset, k, ui)) return;
+    for (int i = 0; i < l.count; ++i) exchange_field<F32>(e, cur, l.field[i], dir, l.user[i], ui, k);
 }
 
 __global__ void __launch_bounds__(SPHB_ELEM_TILE)
@@ -344,13 +387,9 @@ extern "C" int sphb_init_index(const sphb_engine *e, int cur, void *stream)
     return launch_status("sphb_init_index");
 }
 
-extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
-                             int dir, double *user, const int32_t *user_offset,
-                             void *stream)
+// SPHB_OK when `field` can be exchanged in direction `dir` on this engine.
+static int exchange_field_ok(const sphb_engine *e, int cur, int field, int dir)
 {
-    int rc = check_engine_public(e, cur);
-    if (rc) return rc;
-    if (!user || !user_offset || array < 0 || array >= e->cfg.num_arrays) return SPHB_ERR_ARG;
     if (field < 0 || field > 26 || (dir != 0 && dir != 1)) return SPHB_ERR_ARG;
     if (dir == 0 && ((field >= 17 && field <= 20) || field >= 23)) return SPHB_ERR_ARG;
     const bool f32 = e->cfg.precision == SPHB_FP32C;
@@ -362,6 +401,19 @@ extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field
                             e->f.dt_fac, B.rho, B.rho0, e->f.drho,
                             e->f.xu, e->f.xv, e->f.xw};
     if (!ptrs[field] || !B.idx) return SPHB_ERR_ARG;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field,
+                             int dir, double *user, const int32_t *user_offset,
+                             void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if (!user || !user_offset || array < 0 || array >= e->cfg.num_arrays) return SPHB_ERR_ARG;
+    rc = exchange_field_ok(e, cur, field, dir);
+    if (rc) return rc;
+    const bool f32 = e->cfg.precision == SPHB_FP32C;
     if (e->num_tiles == 0) return SPHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
     if (f32)
@@ -369,6 +421,37 @@ extern "C" int sphb_exchange(const sphb_engine *e, int cur, int array, int field
     else
         k_exchange<false><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, array, field, dir, user, user_offset);
     return launch_status("sphb_exchange");
+}
+
+extern "C" int sphb_exchange_many(const sphb_engine *e, int cur, int array, int dir,
+                                  int32_t count, const int32_t *fields, double *const *users,
+                                  const int32_t *user_offset, void *stream)
+{
+    int rc = check_engine_public(e, cur);
+    if (rc) return rc;
+    if (!fields || !users || !user_offset || array < 0 || array >= e->cfg.num_arrays ||
+        count < 1 || count > SPHB_EXCHANGE_MAX)
+        return SPHB_ERR_ARG;
+    ExchangeList l;
+    l.count = count;
+    for (int i = 0; i < count; ++i) {
+        rc = exchange_field_ok(e, cur, fields[i], dir);
+        if (rc) return rc;
+        if (!users[i]) return SPHB_ERR_ARG;
+        l.field[i] = fields[i];
+        l.user[i] = users[i];
+    }
+    for (int i = count; i < SPHB_EXCHANGE_MAX; ++i) {
+        l.field[i] = 0;
+        l.user[i] = nullptr;
+    }
+    if (e->num_tiles == 0) return SPHB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (e->cfg.precision == SPHB_FP32C)
+        k_exchange_many<true><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, array, dir, l, user_offset);
+    else
+        k_exchange_many<false><<<e->num_tiles, SPHB_ELEM_TILE, 0, st>>>(*e, cur, array, dir, l, user_offset);
+    return launch_status("sphb_exchange_many");
 }
 
 extern "C" int sphb_exchange_tag(const sphb_engine *e, int cur, int array, int dir,

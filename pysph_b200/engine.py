@@ -842,10 +842,28 @@ class Engine:
                 sc.pair_dests)
 
     def _import_inline(self, imports):
+        by_array: dict = {}
         for a, name, t in imports:
             if t.numel():
-                self.call("sphb_exchange", self.cur, a, self._field_id(a, name), 0,
-                          t.data_ptr(), self.user_offset[a].data_ptr())
+                by_array.setdefault(a, []).append((name, t))
+        for a, items in by_array.items():
+            self._exchange_many(a, 0, items)
+
+    def _exchange_many(self, array: int, direction: int, items):
+        """sphb_exchange of several (name, FP64 user-order tensor) of one
+        array, SPHB_EXCHANGE_MAX per launch."""
+        for i in range(0, len(items), nat.EXCHANGE_MAX):
+            part = items[i:i + nat.EXCHANGE_MAX]
+            fields = (ctypes.c_int32 * len(part))(*[self._field_id(array, n) for n, _ in part])
+            users = (ctypes.c_void_p * len(part))(*[t.data_ptr() for _, t in part])
+            self.call("sphb_exchange_many", self.cur, array, direction, len(part), fields,
+                      users, self.user_offset[array].data_ptr())
+
+    def exchange_out_many(self, array: int, names, outs):
+        """exchange_out of several properties into the given FP64 tensors in
+        one launch."""
+        if self.user_n[array] and names:
+            self._exchange_many(array, 1, list(zip(names, outs)))
 
     def step_graphed(self, integrator: str = "pc", imports=()):
         """step(integrator) through a CUDA graph: the first step from a given

@@ -628,3 +628,37 @@ def test_common_case_loops_match_the_general_loops(case, lists):
         for n in ("x", "y", "u", "v", "rho", "p"):
             assert torch.equal(a.get(arr, n), b.get(arr, n)), (arr, n)
     assert a.pair_counts() == b.pair_counts()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_exchange_many_matches_single_exchanges(precision):
+    """sphb_exchange_many (several properties of one array in one launch)
+    moves the same values as one sphb_exchange per property, both ways, and
+    leaves the engine in the same state: the imports of positions,
+    velocities, rho and p followed by a PC step agree bit for bit."""
+    engs = [engine_for("dam", precision)[0] for _ in range(2)]
+    assert engs[0].user_n[0] > 0
+    for eng in engs:
+        for _ in range(3):
+            eng.pc_step()
+    names = ["x", "y", "u", "v", "rho", "p"]
+    a = 0
+    n = engs[0].user_n[a]
+    outs1 = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in names]
+    engs[0].exchange_out_many(a, names, outs1)
+    outs2 = [engs[1].exchange_out(a, k) for k in names]
+    for k, t1, t2 in zip(names, outs1, outs2):
+        assert torch.equal(t1, t2), k
+    # host-style edits imported back: all at once into one engine, one by
+    # one into the other
+    new = [t * (1.0 + 1e-4) if k in ("u", "v") else t.clone() for k, t in zip(names, outs1)]
+    engs[0]._exchange_many(a, 0, list(zip(names, new)))
+    for k, t in zip(names, new):
+        engs[1].exchange_in(a, k, t)
+    for eng in engs:
+        eng.invalidate_box()
+        eng._host_state = True
+        eng.pc_step()
+        eng.check_status()
+    for k in names:
+        assert torch.equal(engs[0].exchange_out(a, k), engs[1].exchange_out(a, k)), k
