@@ -467,6 +467,8 @@ def run_ours(args, rank, world, local):
             out["fp64_gpu"]["fp32c_speedup_steps"] = steps_per_s / out["fp64_gpu"]["steps_per_s"]
         out["e2e"] = e2e_facade(wl, args, shape, dev, stream)
         out["e2e"]["engine_api"] = e2e_engine(eng, stream, dev, args)
+        if args.precision == "fp32c":
+            out["calc_by_calc"] = calc_by_calc(wl, args, shape, dev, stream)
         del eng
         torch.cuda.empty_cache()
         if args.workload == "dam_break":
@@ -957,21 +959,16 @@ def e2e_engine(eng, stream, dev, args):
                     "order), one CUDA graph for the device part"}
 
 
-def e2e_facade(wl, args, shape, dev, stream):
-    """Through the reference-facing API with host (numpy) arrays: the dam
-    break's ParticleArrays, Particles, the Solver's operations (SPHRho,
-    TaitEquation, MomentumEquation, GravityForce, PositionStepping) and
-    PredictorCorrectorIntegrator.integrate with the device CFL rule.  Every
-    step sets the fluid's x, y, u, v from numpy arrays (the values the last
-    step read back), integrates, and reads x, y, u, v, rho, p back into
-    numpy arrays."""
-    import torch
+def dam_break_solver(wl, args, shape):
+    """The dam break through the reference-facing API: its ParticleArrays,
+    Particles, the Solver's operations (SPHRho, TaitEquation,
+    MomentumEquation, GravityForce, PositionStepping) and a
+    PredictorCorrectorIntegrator, set up; returns (solver, fluid array,
+    particles, params)."""
     from pysph_b200.base import api as base
     from pysph_b200.solver import api as solver
     from pysph_b200.sph import api as sph
     from pysph_b200.base.particle_types import ParticleType
-    if args.workload != "dam_break":
-        return {"value": None, "note": "the facade run is the dam break's"}
     arrays, p = wl["scenes"][0]
     prec = "single" if args.precision == "fp32c" else "double"
     f = base.get_particle_array(name="fluid", type=ParticleType.Fluid, cl_precision=prec,
@@ -995,6 +992,55 @@ def e2e_facade(wl, args, shape, dev, stream):
     s.add_operation_step([Fluid])
     s.set_time_step(p["dt_initial"])
     s.setup(particles)
+    return s, f, particles, p
+
+
+def calc_by_calc(wl, args, shape, dev, stream):
+    """The integrator's general path on the dam break, for a calc list it
+    does not fuse: every SPHCalc one engine pass (the same kernels, one
+    operation at a time, each density and force pass searching the cells),
+    the stage arithmetic in torch elementwise ops, at a fixed dt of 1e-5
+    (below the CFL step, ~1.5e-5; the workload's dt_initial of 1e-4 is only
+    the CFL rule's first guess).  Device-resident, CUDA events around 10
+    steps after 3."""
+    import torch
+    if args.workload != "dam_break":
+        return None
+    s, f, particles, p = dam_break_solver(wl, args, shape)
+    integ = s.integrator
+    integ.plan = None
+    for _ in range(3):
+        integ.integrate(1e-5)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    k = 10
+    t0.record(stream)
+    for _ in range(k):
+        integ.integrate(1e-5)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / k
+    particles.session().engine.check_status()
+    particles.session().detach()
+    del s, integ, particles, f
+    torch.cuda.empty_cache()
+    return {"ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps": k,
+            "note": "Integrator.eval / step calc by calc (plan None): one engine pass per "
+                    "SPHCalc, torch elementwise stepping; fixed dt 1e-5"}
+
+
+def e2e_facade(wl, args, shape, dev, stream):
+    """Through the reference-facing API with host (numpy) arrays: the dam
+    break's Solver (dam_break_solver) and
+    PredictorCorrectorIntegrator.integrate with the device CFL rule.  Every
+    step sets the fluid's x, y, u, v from numpy arrays (the values the last
+    step read back), integrates, and reads x, y, u, v, rho, p back into
+    numpy arrays."""
+    import torch
+    if args.workload != "dam_break":
+        return {"value": None, "note": "the facade run is the dam break's"}
+    s, f, particles, p = dam_break_solver(wl, args, shape)
     integ = s.integrator
     assert integ.plan is not None, "the dam break's scheme runs fused on the engine"
     sess = integ._fused_session()
@@ -1050,7 +1096,7 @@ def e2e_facade(wl, args, shape, dev, stream):
                      "every particle stays within half the list skin of its last rebin)",
            "shape": particles.engine_options}
     particles.session().detach()
-    del s, integ, particles, f, w
+    del s, integ, particles, f
     torch.cuda.empty_cache()
     return out
 
