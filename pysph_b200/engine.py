@@ -899,6 +899,10 @@ class Engine:
         hit = self._graphs.get(key)
         if hit is None:
             if key not in self._graph_seen:
+                if len(self._graph_seen) >= 64:
+                    # states that never repeat (e.g. new tensors every step)
+                    # must not grow the record without bound
+                    self._graph_seen.clear()
                 self._graph_seen.add(key)
                 self._import_inline(inline)
                 return self.step(integrator)
