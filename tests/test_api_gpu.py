@@ -545,3 +545,19 @@ def test_graphed_steps_match_eager_steps(integ, precision):
         eng.check_status()
     for n in runs[0]:
         assert np.array_equal(runs[0][n], runs[1][n]), n
+
+
+def test_get_of_several_properties_matches_single_gets():
+    """ParticleArray.get of several properties the engine has newer values
+    of copies them back in one launch (sphb_exchange_many): the same values
+    as one get per property."""
+    vals = []
+    for batched in (True, False):
+        s, pa = _drop_for(solver.PredictorCorrectorIntegrator, "single")
+        for _ in range(3):
+            s.integrator.integrate(1e-5)
+        names = ("x", "y", "u", "v", "rho", "p", "_a_u_1", "dt_fac")
+        got = pa.get(*names) if batched else [pa.get(n) for n in names]
+        vals.append([t.cpu().numpy().copy() for t in got])
+    for n, a, b in zip(("x", "y", "u", "v", "rho", "p", "_a_u_1", "dt_fac"), *vals):
+        assert np.array_equal(a, b), n
